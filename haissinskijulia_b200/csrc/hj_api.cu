@@ -1,0 +1,971 @@
+// hj_api.cu -- C ABI of the tracking library (include/haissinski_gpu.h).
+//
+// Host orchestration of the device kernels.  A run is a "bunch": its state
+// z/dE stays on the device; per turn the host only enqueues three kernels
+// (particle pass, histogram reduction, bins step) whose turn-to-turn state
+// (E0, pending kick, turn counter) lives in device memory, so turns never
+// wait for the host.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hj_host.h"
+#include "hj_internal.h"
+
+using namespace hj;
+
+struct hj_ctx {
+  int device = 0;
+  int num_sms = 148;
+  int max_smem_optin = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+};
+
+struct hj_bunch {
+  hj_ctx* ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  double* z = nullptr;
+  double* dE = nullptr;
+  int64_t n = 0;
+  hj_params p{};
+  hj_wake w{};
+  int use_wake = 0;
+  int B = 0, P = 0, M = 0, H = 0, logH = 0;
+  double e0 = 0, eN = 0, estep = 0, inv_e = 0, c1 = 0, cB = 0, inv_c = 0;
+  std::vector<double> centers;
+  double sigma_E0_initial = 0, sigma_z0_initial = 0;
+  uint64_t seed = 0;
+  int qe_mode = QE_OFF;
+  const double* draws = nullptr;
+  int64_t draws_first = 0, draws_turns = 0;
+  int nblk = 1, nblk_m = 1;
+  int64_t turns_done = 0;
+  // device buffers
+  TurnState* ts = nullptr;
+  double* pot = nullptr;
+  unsigned long long* cnt = nullptr;
+  unsigned long long* cic = nullptr;
+  double* lam = nullptr;
+  double* W = nullptr;
+  double2* Wf = nullptr;
+  double2* twP = nullptr;
+  double2* Xg = nullptr;
+  double2* zE = nullptr;
+  uint32_t* part_cnt = nullptr;
+  unsigned long long* part_cic = nullptr;
+  double* part_sum = nullptr;
+  double* part_mom = nullptr;
+  double* h_mom = nullptr;    // pinned
+  TurnState* h_ts = nullptr;  // pinned
+  // profiling: three events per profiled turn (before pass, after pass, after bins)
+  bool profiling = false;
+  std::vector<cudaEvent_t> events;
+  size_t events_used = 0;
+  int64_t profiled_turns = 0;
+  int64_t profiled_launches = 0;
+};
+
+namespace {
+
+const char* kVersion = "haissinski-b200 0.1.0 (sm_100a)";
+
+hj_status set_err(hj_ctx* ctx, hj_status code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return code;
+}
+
+#define HJ_CUDA(ctx, call)                                                            \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return set_err((ctx), e_ == cudaErrorMemoryAllocation ? HJ_ERR_NOMEM : HJ_ERR_CUDA, \
+                     "%s failed: %s", #call, cudaGetErrorString(e_));                 \
+  } while (0)
+
+#define HJ_TRY(expr)             \
+  do {                           \
+    hj_status s_ = (expr);       \
+    if (s_ != HJ_OK) return s_;  \
+  } while (0)
+
+template <typename T>
+hj_status dalloc(hj_ctx* ctx, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_err(ctx, HJ_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T),
+                   cudaGetErrorString(e));
+  }
+  return HJ_OK;
+}
+
+int64_t next_pow2(int64_t n) {
+  if (n <= 0) return 1;
+  int64_t p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+int ilog2(int64_t v) {
+  int l = 0;
+  while ((int64_t(1) << l) < v) ++l;
+  return l;
+}
+
+// compute_global_std from sums (src/utils.jl:593-605).
+double global_std(double s, double s2, int64_t n) {
+  if (n <= 1) return 0.0;
+  const double nd = (double)n;
+  const double mean = s / nd;
+  const double var = (s2 / nd) - (mean * mean);
+  double sv = var * nd / (double)(n - 1);
+  if (!(sv > 0.0)) sv = (sv != sv) ? sv : 0.0;
+  return std::sqrt(sv);
+}
+
+hj_status ctx_ok(hj_ctx* ctx) {
+  if (!ctx) return HJ_ERR_ARG;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess)
+    return set_err(ctx, HJ_ERR_CUDA, "cudaSetDevice(%d): %s", ctx->device, cudaGetErrorString(e));
+  ctx->err.clear();
+  return HJ_OK;
+}
+
+hj_status scratch(hj_ctx* ctx, size_t bytes, void** out) {
+  if (bytes > ctx->scratch_bytes) {
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
+    if (e != cudaSuccess)
+      return set_err(ctx, HJ_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes,
+                     cudaGetErrorString(e));
+    ctx->scratch_bytes = bytes;
+  }
+  *out = ctx->scratch;
+  return HJ_OK;
+}
+
+size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
+
+hj_status check_params(hj_ctx* ctx, const hj_params* p) {
+  if (!p) return set_err(ctx, HJ_ERR_ARG, "params is NULL");
+  if (p->n_turns < 0) return set_err(ctx, HJ_ERR_ARG, "n_turns must be >= 0");
+  if (!(p->mass > 0)) return set_err(ctx, HJ_ERR_ARG, "mass must be > 0");
+  return HJ_OK;
+}
+
+hj_status check_grid(hj_ctx* ctx, const hj_grid* g) {
+  if (!g) return set_err(ctx, HJ_ERR_ARG, "grid is NULL");
+  if (g->nbins <= 0) return set_err(ctx, HJ_ERR_NBINS, "nbins must be > 0 (got %lld)",
+                                    (long long)g->nbins);
+  if (!g->centers) return set_err(ctx, HJ_ERR_ARG, "grid.centers is NULL");
+  if (!(g->edge_step != 0.0))
+    return set_err(ctx, HJ_ERR_ARG, "Bin edges have zero step size.");
+  return HJ_OK;
+}
+
+// Device sums of the moments kernel, reduced on the host in block order.
+hj_status read_moments(hj_bunch* b, double m[4]) {
+  HJ_CUDA(b->ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 4 * b->nblk_m,
+                                  cudaMemcpyDeviceToHost, b->stream));
+  HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
+  m[0] = m[1] = m[2] = m[3] = 0.0;
+  for (int i = 0; i < b->nblk_m; ++i)
+    for (int k = 0; k < 4; ++k) m[k] += b->h_mom[4 * i + k];
+  return HJ_OK;
+}
+
+hj_status launch_moments(hj_bunch* b, int apply, double* z_out, double* dE_out) {
+  FlushArgs f{};
+  f.z = b->z;
+  f.dE = b->dE;
+  f.n = b->n;
+  f.ts = b->ts;
+  f.pot = b->pot;
+  f.B = b->B;
+  f.use_wake = b->use_wake;
+  f.update_E0 = b->p.update_E0;
+  f.c1 = b->c1;
+  f.cB = b->cB;
+  f.inv_cstep = b->inv_c;
+  f.apply = apply;
+  f.z_out = z_out;
+  f.dE_out = dE_out;
+  f.part = b->part_mom;
+  HJ_CUDA(b->ctx, launch_flush(f, b->nblk_m, b->stream));
+  return HJ_OK;
+}
+
+hj_status read_state(hj_bunch* b) {
+  HJ_CUDA(b->ctx, cudaMemcpyAsync(b->h_ts, b->ts, sizeof(TurnState), cudaMemcpyDeviceToHost,
+                                  b->stream));
+  HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
+  int st = b->h_ts->status;
+  if (st & (1 << HJ_ERR_NONFINITE))
+    return set_err(b->ctx, HJ_ERR_NONFINITE,
+                   "non-finite bunch moments detected on the device (turn %lld)",
+                   (long long)b->h_ts->turn - 1);
+  if (st & (1 << HJ_ERR_ARG))
+    return set_err(b->ctx, HJ_ERR_ARG, "host-fed draws do not cover turn %lld",
+                   (long long)b->h_ts->turn - 1);
+  return HJ_OK;
+}
+
+void fill_result(hj_bunch* b, const double m[4], hj_result* res) {
+  if (!res) return;
+  res->sigma_z = global_std(m[0], m[1], b->n);
+  res->sigma_E = global_std(m[2], m[3], b->n);
+  res->E0 = b->h_ts->cur.E0;
+  res->sigma_E0_initial = b->sigma_E0_initial;
+  res->sigma_z0_initial = b->sigma_z0_initial;
+  res->mean_z = b->n > 0 ? m[0] / (double)b->n : 0.0;
+  res->mean_dE = b->n > 0 ? m[2] / (double)b->n : 0.0;
+  res->turns = b->turns_done;
+}
+
+void set_kernel_attributes(hj_ctx* ctx) {
+  prepare_track_kernels(ctx->max_smem_optin);
+  prepare_wake_kernels(ctx->max_smem_optin);
+}
+
+}  // namespace
+
+// ====================================================================== context
+
+extern "C" const char* hj_version(void) { return kVersion; }
+
+extern "C" const char* hj_status_string(hj_status s) {
+  switch (s) {
+    case HJ_OK: return "HJ_OK";
+    case HJ_ERR_ARG: return "HJ_ERR_ARG";
+    case HJ_ERR_NBINS: return "HJ_ERR_NBINS";
+    case HJ_ERR_WAKE_PARAM: return "HJ_ERR_WAKE_PARAM";
+    case HJ_ERR_CUDA: return "HJ_ERR_CUDA";
+    case HJ_ERR_NOMEM: return "HJ_ERR_NOMEM";
+    case HJ_ERR_TOO_LARGE: return "HJ_ERR_TOO_LARGE";
+    case HJ_ERR_EMPTY: return "HJ_ERR_EMPTY";
+    case HJ_ERR_NONFINITE: return "HJ_ERR_NONFINITE";
+    case HJ_ERR_TIMEOUT: return "HJ_ERR_TIMEOUT";
+    case HJ_ERR_NO_DEVICE: return "HJ_ERR_NO_DEVICE";
+    case HJ_ERR_STATE: return "HJ_ERR_STATE";
+    default: return "HJ_ERR_UNKNOWN";
+  }
+}
+
+extern "C" hj_status hj_create(int32_t device, hj_ctx** out) {
+  if (!out) return HJ_ERR_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return HJ_ERR_NO_DEVICE;
+  if (device < 0 || device >= count) return HJ_ERR_NO_DEVICE;
+  if (cudaSetDevice(device) != cudaSuccess) return HJ_ERR_CUDA;
+  hj_ctx* ctx = new hj_ctx();
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  set_kernel_attributes(ctx);
+  *out = ctx;
+  return HJ_OK;
+}
+
+extern "C" void hj_destroy(hj_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->scratch) cudaFree(ctx->scratch);
+  delete ctx;
+}
+
+extern "C" const char* hj_last_error(const hj_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+// ====================================================================== bunch
+
+extern "C" void hj_bunch_destroy(hj_bunch* b) {
+  if (!b) return;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->stream);
+  void* dev[] = {b->ts,  b->pot, b->cnt, b->cic,      b->lam,      b->W,        b->Wf,
+                 b->twP, b->Xg,  b->zE,  b->part_cnt, b->part_cic, b->part_sum, b->part_mom};
+  for (void* p : dev)
+    if (p) cudaFree(p);
+  if (b->h_mom) cudaFreeHost(b->h_mom);
+  if (b->h_ts) cudaFreeHost(b->h_ts);
+  for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+  delete b;
+}
+
+static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                   const hj_params* params, const hj_wake* wake,
+                                   int64_t nbins, const hj_grid* grid, uint64_t seed,
+                                   void* stream, hj_bunch* b) {
+  b->ctx = ctx;
+  b->stream = (cudaStream_t)stream;
+  b->z = d_z;
+  b->dE = d_dE;
+  b->n = n;
+  b->p = *params;
+  b->seed = seed;
+  b->use_wake = params->use_wakefield ? 1 : 0;
+  if (wake) b->w = *wake;
+  else hj_wake_reference(params, &b->w);
+  b->qe_mode = params->use_excitation ? QE_PHILOX : QE_OFF;
+
+  if (b->use_wake) {
+    const int64_t B = grid ? grid->nbins : nbins;
+    if (B <= 0) return set_err(ctx, HJ_ERR_NBINS, "Buffer nbins invalid (must be > 0).");
+    if (B > kMaxBins)
+      return set_err(ctx, HJ_ERR_TOO_LARGE, "nbins = %lld exceeds the supported %lld",
+                     (long long)B, (long long)kMaxBins);
+    if (b->w.ctau <= 0) return set_err(ctx, HJ_ERR_WAKE_PARAM, "Wake parameter cτ must be positive.");
+    if (params->pipe_radius <= 0)
+      return set_err(ctx, HJ_ERR_WAKE_PARAM, "Wake parameter pipe_radius must be positive.");
+    if (n == 0)
+      return set_err(ctx, HJ_ERR_EMPTY, "wakefield with zero particles: log10(0) in the particle factor");
+    if (grid) HJ_TRY(check_grid(ctx, grid));
+    b->B = (int)B;
+  }
+
+  // Initial spreads, src/evolution.jl:247-249.
+  b->nblk_m = (int)std::min<int64_t>(std::max<int64_t>((n + 4095) / 4096, 1),
+                                     (int64_t)ctx->num_sms * 4);
+  HJ_TRY(dalloc(ctx, &b->part_mom, (size_t)4 * b->nblk_m));
+  HJ_TRY(dalloc(ctx, &b->ts, 1));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&b->h_mom, sizeof(double) * 4 * b->nblk_m));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&b->h_ts, sizeof(TurnState)));
+  double m[4];
+  HJ_TRY(launch_moments(b, 0, nullptr, nullptr));
+  HJ_TRY(read_moments(b, m));
+  b->sigma_z0_initial = global_std(m[0], m[1], n);
+  b->sigma_E0_initial = global_std(m[2], m[3], n);
+
+  if (b->use_wake) {
+    const int B = b->B;
+    b->centers.resize(B);
+    hj_grid g{};
+    if (grid) {
+      std::memcpy(b->centers.data(), grid->centers, sizeof(double) * B);
+      g = *grid;
+    } else {
+      HJ_TRY(hj_make_grid(b->sigma_z0_initial, b->w.half_width_sigmas, B, b->centers.data(), &g));
+    }
+    b->e0 = g.edge_first;
+    b->eN = g.edge_last;
+    b->estep = g.edge_step;
+    b->inv_e = 1.0 / g.edge_step;                        // src/utils.jl:378
+    b->c1 = b->centers[0];
+    b->cB = b->centers[B - 1];
+    if (B >= 2) {
+      const double step = (b->cB - b->c1) / (double)(B - 1);  // src/wakefield.jl:41-42
+      b->inv_c = 1.0 / step;
+    }
+    b->P = (int)next_pow2(2 * (int64_t)B);               // src/evolution.jl:265
+    b->M = b->P / 2;
+    b->H = b->M / 2;
+    b->logH = b->H >= 1 ? ilog2(b->H) : 0;
+    std::vector<double> W(B), lam(B), tw(2 * (size_t)b->P);
+    host_wake_tables(b->centers.data(), B, b->w, W.data(), lam.data());
+    host_twiddles(b->P, tw.data());
+    HJ_TRY(dalloc(ctx, &b->W, B));
+    HJ_TRY(dalloc(ctx, &b->lam, B));
+    HJ_TRY(dalloc(ctx, &b->twP, b->P));
+    HJ_TRY(dalloc(ctx, &b->Wf, (size_t)b->M + 1));
+    HJ_TRY(dalloc(ctx, &b->Xg, b->M));
+    HJ_TRY(dalloc(ctx, &b->zE, std::max(b->H, 1)));
+    HJ_TRY(dalloc(ctx, &b->pot, B));
+    HJ_TRY(dalloc(ctx, &b->cnt, B));
+    HJ_TRY(dalloc(ctx, &b->cic, B));
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->W, W.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, lam.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->twP, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice, b->stream));
+    HJ_CUDA(ctx, cudaMemsetAsync(b->pot, 0, sizeof(double) * B, b->stream));
+    HJ_CUDA(ctx, cudaMemsetAsync(b->cnt, 0, sizeof(unsigned long long) * B, b->stream));
+    if (b->H >= 4)
+      HJ_CUDA(ctx, launch_wake_spectrum(b->W, B, b->P, b->M, b->H, b->logH, b->twP, b->Xg,
+                                        b->Wf, b->stream));
+    HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));     // host vectors go out of scope
+  }
+
+  const int bps = track_blocks_per_sm(b->B, b->qe_mode, b->use_wake);
+  b->nblk = track_grid_size(n, b->B, ctx->num_sms, bps);
+  HJ_TRY(dalloc(ctx, &b->part_sum, (size_t)kNumSums * b->nblk));
+  if (b->use_wake) {
+    HJ_TRY(dalloc(ctx, &b->part_cnt, (size_t)b->nblk * b->B));
+    HJ_TRY(dalloc(ctx, &b->part_cic, (size_t)b->nblk * b->B));
+  }
+
+  TurnState t{};
+  t.cur = make_turn_scalars(params->E0, *params, b->sigma_E0_initial);
+  t.pending = 0;
+  t.pending_mean = 0.0;
+  t.turn = 1;
+  t.status = 0;
+  *b->h_ts = t;
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice, b->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_create(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                     const hj_params* params, const hj_wake* wake,
+                                     int64_t nbins, const hj_grid* grid, uint64_t seed,
+                                     void* stream, hj_bunch** out) {
+  HJ_TRY(ctx_ok(ctx));
+  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  HJ_TRY(check_params(ctx, params));
+  if (n < 0) return set_err(ctx, HJ_ERR_ARG, "Number of particles must be non-negative. Got %lld.", (long long)n);
+  if (n > 0 && (!d_z || !d_dE)) return set_err(ctx, HJ_ERR_ARG, "particle arrays are NULL");
+  if ((((uintptr_t)d_z) | ((uintptr_t)d_dE)) & 31)
+    return set_err(ctx, HJ_ERR_ARG, "device particle arrays must be 32-byte aligned");
+  if (n == 0 && !params->use_wakefield)
+    return set_err(ctx, HJ_ERR_ARG, "a resident bunch needs at least one particle");
+  hj_bunch* b = new hj_bunch();
+  hj_status s = bunch_create_impl(ctx, d_z, d_dE, n, params, wake, nbins, grid, seed, stream, b);
+  if (s != HJ_OK) {
+    hj_bunch_destroy(b);
+    return s;
+  }
+  *out = b;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_set_draws(hj_bunch* b, const double* d_draws, int64_t first_turn,
+                                        int64_t turns) {
+  if (!b) return HJ_ERR_ARG;
+  if (d_draws && turns <= 0) return set_err(b->ctx, HJ_ERR_ARG, "turns must be > 0");
+  b->draws = d_draws;
+  b->draws_first = first_turn;
+  b->draws_turns = turns;
+  if (!b->p.use_excitation) b->qe_mode = QE_OFF;
+  else b->qe_mode = d_draws ? QE_DRAWS : QE_PHILOX;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
+  if (!b) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
+  PassArgs a{};
+  a.z = b->z;
+  a.dE = b->dE;
+  a.n = b->n;
+  a.ts = b->ts;
+  a.pot = b->pot;
+  a.B = b->B;
+  a.use_wake = b->use_wake;
+  a.e0 = b->e0;
+  a.eN = b->eN;
+  a.inv_estep = b->inv_e;
+  a.c1 = b->c1;
+  a.cB = b->cB;
+  a.inv_cstep = b->inv_c;
+  a.V = b->p.voltage;
+  a.phi_s = b->p.phi_s;
+  a.inv_mass = 1.0 / b->p.mass;
+  a.alpha_c = b->p.alpha_c;
+  a.two_pi_h = kTwoPi * (double)b->p.harmonic;
+  a.update_eta = b->p.update_eta;
+  a.update_E0 = b->p.update_E0;
+  a.sr = b->p.SR_damping;
+  a.qe_mode = b->qe_mode;
+  a.seed = b->seed;
+  a.draws = b->draws;
+  a.draws_first_turn = b->draws_first;
+  a.draws_turns = b->draws_turns;
+  a.part_cnt = b->part_cnt;
+  a.part_cic = b->part_cic;
+  a.part_sum = b->part_sum;
+
+  BinsArgs g{};
+  g.ts = b->ts;
+  g.part_sum = b->part_sum;
+  g.nblk = b->nblk;
+  g.n = b->n;
+  g.params = b->p;
+  g.sigma_E0_initial = b->sigma_E0_initial;
+  g.population = b->w.population;
+  g.use_wake = b->use_wake;
+  g.B = b->B;
+  g.P = b->P;
+  g.M = b->M;
+  g.H = b->H;
+  g.logH = b->logH;
+  g.cnt = b->cnt;
+  g.cic = b->cic;
+  g.lam = b->lam;
+  g.Wf = b->Wf;
+  g.twP = b->twP;
+  g.Xg = b->Xg;
+  g.zE = b->zE;
+  g.pot = b->pot;
+  g.W = b->W;
+  g.conv_only = 0;
+
+  for (int64_t t = 0; t < turns; ++t) {
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    if (b->profiling) {
+      while (b->events.size() < b->events_used + 3) {
+        cudaEvent_t e;
+        HJ_CUDA(ctx, cudaEventCreate(&e));
+        b->events.push_back(e);
+      }
+      for (int k = 0; k < 3; ++k) ev[k] = b->events[b->events_used + k];
+      b->events_used += 3;
+      HJ_CUDA(ctx, cudaEventRecord(ev[0], b->stream));
+    }
+    HJ_CUDA(ctx, launch_track_pass(a, b->nblk, b->stream));
+    if (b->profiling) HJ_CUDA(ctx, cudaEventRecord(ev[1], b->stream));
+    if (b->use_wake)
+      HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->cnt, b->cic,
+                                      b->stream));
+    HJ_CUDA(ctx, launch_bins(g, b->stream));
+    if (b->profiling) {
+      HJ_CUDA(ctx, cudaEventRecord(ev[2], b->stream));
+      b->profiled_turns += 1;
+      b->profiled_launches += b->use_wake ? 3 : 2;
+    }
+  }
+  b->turns_done += turns;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_set_profiling(hj_bunch* b, int32_t enable) {
+  if (!b) return HJ_ERR_ARG;
+  HJ_TRY(ctx_ok(b->ctx));
+  b->profiling = enable != 0;
+  b->events_used = 0;
+  b->profiled_turns = 0;
+  b->profiled_launches = 0;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_read_profile(hj_bunch* b, double* out4) {
+  if (!b || !out4) return HJ_ERR_ARG;
+  HJ_TRY(ctx_ok(b->ctx));
+  HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
+  double pass = 0.0, bins = 0.0;
+  for (size_t i = 0; i + 3 <= b->events_used; i += 3) {
+    float a = 0.f, c = 0.f;
+    HJ_CUDA(b->ctx, cudaEventElapsedTime(&a, b->events[i], b->events[i + 1]));
+    HJ_CUDA(b->ctx, cudaEventElapsedTime(&c, b->events[i + 1], b->events[i + 2]));
+    pass += a;
+    bins += c;
+  }
+  out4[0] = pass;
+  out4[1] = bins;
+  out4[2] = (double)b->profiled_turns;
+  out4[3] = (double)b->profiled_launches;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_observe(hj_bunch* b, double* d_z_out, double* d_dE_out,
+                                      hj_result* res) {
+  if (!b) return HJ_ERR_ARG;
+  HJ_TRY(ctx_ok(b->ctx));
+  HJ_TRY(launch_moments(b, 1, d_z_out, d_dE_out));
+  double m[4];
+  HJ_TRY(read_moments(b, m));
+  HJ_TRY(read_state(b));
+  fill_result(b, m, res);
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_finish(hj_bunch* b, hj_result* res) {
+  if (!b) return HJ_ERR_ARG;
+  HJ_TRY(ctx_ok(b->ctx));
+  HJ_TRY(launch_moments(b, 1, b->z, b->dE));
+  const int32_t zero = 0;
+  HJ_CUDA(b->ctx, cudaMemcpyAsync(&b->ts->pending, &zero, sizeof(int32_t),
+                                  cudaMemcpyHostToDevice, b->stream));
+  double m[4];
+  HJ_TRY(read_moments(b, m));
+  HJ_TRY(read_state(b));
+  fill_result(b, m, res);
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_histogram(hj_bunch* b, int64_t* counts_host) {
+  if (!b || !counts_host) return HJ_ERR_ARG;
+  HJ_TRY(ctx_ok(b->ctx));
+  if (!b->use_wake) return set_err(b->ctx, HJ_ERR_STATE, "bunch has no wakefield histogram");
+  HJ_CUDA(b->ctx, cudaMemcpyAsync(counts_host, b->cnt, sizeof(int64_t) * b->B,
+                                  cudaMemcpyDeviceToHost, b->stream));
+  HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_potential(hj_bunch* b, double* pot_host) {
+  if (!b || !pot_host) return HJ_ERR_ARG;
+  HJ_TRY(ctx_ok(b->ctx));
+  if (!b->use_wake) return set_err(b->ctx, HJ_ERR_STATE, "bunch has no wake potential");
+  HJ_CUDA(b->ctx, cudaMemcpyAsync(pot_host, b->pot, sizeof(double) * b->B,
+                                  cudaMemcpyDeviceToHost, b->stream));
+  HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
+  return HJ_OK;
+}
+
+// ====================================================================== whole loop
+
+static hj_status evolve_empty(hj_ctx* ctx, const hj_params* p, hj_result* out) {
+  if (p->use_wakefield)
+    return set_err(ctx, HJ_ERR_EMPTY, "wakefield with zero particles: log10(0) in the particle factor");
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->E0 = p->E0;
+    // MPI branch: mean = 0/0 per turn (src/evolution.jl:426)
+    if (p->update_E0 && p->n_turns > 0) out->E0 = p->E0 + 0.0 / 0.0;
+    out->turns = p->n_turns;
+  }
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_evolve_device(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                      const hj_params* params, const hj_wake* wake,
+                                      int64_t nbins, const hj_grid* grid,
+                                      const double* d_qe_draws, uint64_t seed, void* stream,
+                                      hj_result* out) {
+  HJ_TRY(ctx_ok(ctx));
+  HJ_TRY(check_params(ctx, params));
+  if (n < 0) return set_err(ctx, HJ_ERR_ARG, "Number of particles must be non-negative. Got %lld.", (long long)n);
+  if (n == 0) return evolve_empty(ctx, params, out);
+  hj_bunch* b = nullptr;
+  HJ_TRY(hj_bunch_create(ctx, d_z, d_dE, n, params, wake, nbins, grid, seed, stream, &b));
+  hj_status s = HJ_OK;
+  if (d_qe_draws) s = hj_bunch_set_draws(b, d_qe_draws, 1, params->n_turns);
+  if (s == HJ_OK) s = hj_bunch_advance(b, params->n_turns);
+  if (s == HJ_OK) s = hj_bunch_finish(b, out);
+  hj_bunch_destroy(b);
+  return s;
+}
+
+extern "C" hj_status hj_evolve(hj_ctx* ctx, double* z, double* dE, int64_t n,
+                               const hj_params* params, const hj_wake* wake, int64_t nbins,
+                               const hj_grid* grid, const double* qe_draws, uint64_t seed,
+                               hj_result* out) {
+  HJ_TRY(ctx_ok(ctx));
+  HJ_TRY(check_params(ctx, params));
+  if (n < 0) return set_err(ctx, HJ_ERR_ARG, "Number of particles must be non-negative. Got %lld.", (long long)n);
+  if (n == 0) return evolve_empty(ctx, params, out);
+  if (!z || !dE) return set_err(ctx, HJ_ERR_ARG, "particle arrays are NULL");
+  double *d_z = nullptr, *d_dE = nullptr, *d_draws = nullptr;
+  hj_status s = dalloc(ctx, &d_z, (size_t)n);
+  if (s == HJ_OK) s = dalloc(ctx, &d_dE, (size_t)n);
+  const bool draws = qe_draws && params->use_excitation && params->n_turns > 0;
+  if (s == HJ_OK && draws) s = dalloc(ctx, &d_draws, (size_t)n * (size_t)params->n_turns);
+  cudaStream_t st = ctx->stream;
+  if (s == HJ_OK) {
+    cudaError_t e = cudaMemcpyAsync(d_z, z, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_dE, dE, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && draws)
+      e = cudaMemcpyAsync(d_draws, qe_draws, sizeof(double) * n * params->n_turns,
+                          cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) s = set_err(ctx, HJ_ERR_CUDA, "host->device copy failed: %s", cudaGetErrorString(e));
+  }
+  if (s == HJ_OK)
+    s = hj_evolve_device(ctx, d_z, d_dE, n, params, wake, nbins, grid, d_draws, seed, st, out);
+  if (s == HJ_OK) {
+    cudaError_t e = cudaMemcpyAsync(z, d_z, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dE, d_dE, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) s = set_err(ctx, HJ_ERR_CUDA, "device->host copy failed: %s", cudaGetErrorString(e));
+  }
+  if (d_z) cudaFree(d_z);
+  if (d_dE) cudaFree(d_dE);
+  if (d_draws) cudaFree(d_draws);
+  return s;
+}
+
+// ====================================================================== single steps
+
+namespace {
+// Copy n doubles of host arrays into the context scratch; returns device pointers.
+hj_status stage(hj_ctx* ctx, int64_t n, int k, double** dev, const double* const* host) {
+  void* base = nullptr;
+  const size_t one = align_up(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  HJ_TRY(scratch(ctx, one * k, &base));
+  for (int i = 0; i < k; ++i) {
+    dev[i] = (double*)((char*)base + one * i);
+    if (host[i] && n > 0)
+      HJ_CUDA(ctx, cudaMemcpyAsync(dev[i], host[i], sizeof(double) * n, cudaMemcpyHostToDevice,
+                                   ctx->stream));
+  }
+  return HJ_OK;
+}
+
+hj_status unstage(hj_ctx* ctx, int64_t n, double* host, const double* dev) {
+  if (n > 0)
+    HJ_CUDA(ctx, cudaMemcpyAsync(host, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return HJ_OK;
+}
+}  // namespace
+
+extern "C" hj_status hj_rf_kick(hj_ctx* ctx, double voltage, double sin_phis, double rf_factor,
+                                double phi_s, const double* z, double* dE, int64_t n) {
+  HJ_TRY(ctx_ok(ctx));
+  if (n < 0 || (n > 0 && (!z || !dE))) return set_err(ctx, HJ_ERR_ARG, "bad particle arrays");
+  if (n == 0) return HJ_OK;
+  double* d[2];
+  const double* h[2] = {z, dE};
+  HJ_TRY(stage(ctx, n, 2, d, h));
+  HJ_CUDA(ctx, launch_rf_kick(voltage, sin_phis, rf_factor, phi_s, d[0], d[1], n, ctx->stream));
+  return unstage(ctx, n, dE, d[1]);
+}
+
+extern "C" hj_status hj_quantum_excitation(hj_ctx* ctx, double E0, double radius,
+                                           double sigma_E0, const double* draws, uint64_t seed,
+                                           int64_t turn, double* dE, int64_t n) {
+  HJ_TRY(ctx_ok(ctx));
+  if (n < 0 || (n > 0 && !dE)) return set_err(ctx, HJ_ERR_ARG, "bad particle arrays");
+  if (n == 0) return HJ_OK;
+  const double t = E0 / 1e9;
+  const double dU = 4 * 8.85e-5 * (t * t * t) / radius;   // src/quantum_excitation.jl:58
+  const double om = 1 - dU;
+  const double excitation = std::sqrt(1 - om * om) * sigma_E0;  // :59
+  double* d[2];
+  const double* h[2] = {dE, draws};
+  HJ_TRY(stage(ctx, n, 2, d, h));
+  HJ_CUDA(ctx, launch_qe(excitation, draws ? d[1] : nullptr, seed, turn, d[0], n, ctx->stream));
+  return unstage(ctx, n, dE, d[0]);
+}
+
+extern "C" hj_status hj_synchrotron_radiation(hj_ctx* ctx, double E0, double radius, double* dE,
+                                              int64_t n) {
+  HJ_TRY(ctx_ok(ctx));
+  if (n < 0 || (n > 0 && !dE)) return set_err(ctx, HJ_ERR_ARG, "bad particle arrays");
+  if (n == 0) return HJ_OK;
+  const double t = E0 / 1e9;
+  const double dU = 4 * 8.85e-5 * (t * t * t) / radius;  // src/synchrotron_radiation.jl:44
+  const double damping = 1 - dU;                         // :45
+  double* d[1];
+  const double* h[1] = {dE};
+  HJ_TRY(stage(ctx, n, 1, d, h));
+  HJ_CUDA(ctx, launch_sr(damping, d[0], n, ctx->stream));
+  return unstage(ctx, n, dE, d[0]);
+}
+
+extern "C" hj_status hj_phase_advance(hj_ctx* ctx, int32_t update_eta, double E0, double mass,
+                                      double alpha_c, int64_t harmonic, double phi_s,
+                                      double freq_rf, const double* dE, double* z, int64_t n) {
+  HJ_TRY(ctx_ok(ctx));
+  if (n < 0 || (n > 0 && (!z || !dE))) return set_err(ctx, HJ_ERR_ARG, "bad particle arrays");
+  if (n == 0) return HJ_OK;
+  hj_params p{};
+  p.mass = mass;
+  p.alpha_c = alpha_c;
+  p.harmonic = harmonic;
+  p.phi_s = phi_s;
+  p.freq_rf = freq_rf;
+  p.radius = 1.0;
+  const TurnScalars s = make_turn_scalars(E0, p, 0.0);
+  double* d[2];
+  const double* h[2] = {z, dE};
+  HJ_TRY(stage(ctx, n, 2, d, h));
+  HJ_CUDA(ctx, launch_phase_advance(update_eta, s, 1.0 / mass, alpha_c,
+                                    kTwoPi * (double)harmonic, phi_s, d[1], d[0], n,
+                                    ctx->stream));
+  return unstage(ctx, n, z, d[0]);
+}
+
+extern "C" hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64_t n,
+                                 double* out) {
+  HJ_TRY(ctx_ok(ctx));
+  if (n < 0 || (n > 0 && !out)) return set_err(ctx, HJ_ERR_ARG, "bad output array");
+  if (n == 0) return HJ_OK;
+  double* d[1];
+  const double* h[1] = {nullptr};
+  HJ_TRY(stage(ctx, n, 1, d, h));
+  HJ_CUDA(ctx, launch_gaussian(seed, turn, n, d[0], ctx->stream));
+  return unstage(ctx, n, out, d[0]);
+}
+
+namespace {
+// Device histogram of z on `grid` into dcnt (u64 counts), using scratch after `off` bytes.
+hj_status device_histogram(hj_ctx* ctx, const double* d_z, int64_t n, const hj_grid* grid,
+                           unsigned long long* dcnt, uint32_t* part, int nblk) {
+  const int B = (int)grid->nbins;
+  HJ_CUDA(ctx, launch_histogram_only(d_z, n, B, grid->edge_first, grid->edge_last,
+                                     1.0 / grid->edge_step, part, nblk, ctx->stream));
+  HJ_CUDA(ctx, launch_hist_reduce(part, nullptr, nblk, B, dcnt, nullptr, ctx->stream));
+  return HJ_OK;
+}
+
+int hist_blocks(hj_ctx* ctx, int64_t n) {
+  int64_t g = (n + 8191) / 8192;
+  if (g < 1) g = 1;
+  if (g > ctx->num_sms * 2) g = ctx->num_sms * 2;
+  return (int)g;
+}
+
+struct ConvBuffers {
+  double* W;
+  double* lam;
+  double2* twP;
+  double2* Wf;
+  double2* Xg;
+  double2* zE;
+  double* pot;
+  unsigned long long* cnt;
+};
+
+// Potential at the centers from device counts (conv_only bins kernel).
+hj_status device_conv(hj_ctx* ctx, const hj_grid* grid, const hj_wake* wake, double current,
+                      ConvBuffers& cb) {
+  const int B = (int)grid->nbins;
+  const int P = (int)next_pow2(2 * (int64_t)B), M = P / 2, H = M / 2;
+  const int logH = H >= 1 ? ilog2(H) : 0;
+  std::vector<double> W(B), lam(B), tw(2 * (size_t)P);
+  host_wake_tables(grid->centers, B, *wake, W.data(), lam.data());
+  host_twiddles(P, tw.data());
+  HJ_CUDA(ctx, cudaMemcpyAsync(cb.W, W.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->stream));
+  HJ_CUDA(ctx, cudaMemcpyAsync(cb.lam, lam.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->stream));
+  HJ_CUDA(ctx, cudaMemcpyAsync(cb.twP, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if (H >= 4)
+    HJ_CUDA(ctx, launch_wake_spectrum(cb.W, B, P, M, H, logH, cb.twP, cb.Xg, cb.Wf, ctx->stream));
+  BinsArgs g{};
+  g.use_wake = 1;
+  g.B = B;
+  g.P = P;
+  g.M = M;
+  g.H = H;
+  g.logH = logH;
+  g.cnt = cb.cnt;
+  g.cic = nullptr;
+  g.lam = cb.lam;
+  g.Wf = cb.Wf;
+  g.twP = cb.twP;
+  g.Xg = cb.Xg;
+  g.zE = cb.zE;
+  g.pot = cb.pot;
+  g.W = cb.W;
+  g.conv_only = 1;
+  g.conv_current = current;
+  HJ_CUDA(ctx, launch_bins(g, ctx->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // host tables go out of scope
+  return HJ_OK;
+}
+
+// Carve the conv buffers (and extra doubles) out of the context scratch.
+hj_status conv_scratch(hj_ctx* ctx, int B, size_t extra_doubles, int extra_arrays,
+                       int64_t part_words, ConvBuffers& cb, double** extra,
+                       uint32_t** part) {
+  const int P = (int)next_pow2(2 * (int64_t)B), M = P / 2, H = std::max(M / 2, 1);
+  size_t sizes[] = {align_up(sizeof(double) * B),     align_up(sizeof(double) * B),
+                    align_up(sizeof(double2) * P),    align_up(sizeof(double2) * (M + 1)),
+                    align_up(sizeof(double2) * M),    align_up(sizeof(double2) * H),
+                    align_up(sizeof(double) * B),     align_up(sizeof(uint64_t) * B),
+                    align_up(sizeof(uint32_t) * (size_t)std::max<int64_t>(part_words, 1))};
+  size_t total = 0;
+  for (size_t s : sizes) total += s;
+  const size_t ex = align_up(sizeof(double) * std::max<size_t>(extra_doubles, 1));
+  total += ex * extra_arrays;
+  void* base = nullptr;
+  HJ_TRY(scratch(ctx, total, &base));
+  char* p = (char*)base;
+  cb.W = (double*)p; p += sizes[0];
+  cb.lam = (double*)p; p += sizes[1];
+  cb.twP = (double2*)p; p += sizes[2];
+  cb.Wf = (double2*)p; p += sizes[3];
+  cb.Xg = (double2*)p; p += sizes[4];
+  cb.zE = (double2*)p; p += sizes[5];
+  cb.pot = (double*)p; p += sizes[6];
+  cb.cnt = (unsigned long long*)p; p += sizes[7];
+  *part = (uint32_t*)p; p += sizes[8];
+  for (int i = 0; i < extra_arrays; ++i) {
+    extra[i] = (double*)p;
+    p += ex;
+  }
+  return HJ_OK;
+}
+}  // namespace
+
+extern "C" hj_status hj_histogram(hj_ctx* ctx, const double* z, int64_t n, const hj_grid* grid,
+                                  int64_t* counts) {
+  HJ_TRY(ctx_ok(ctx));
+  HJ_TRY(check_grid(ctx, grid));
+  if (n < 0 || (n > 0 && !z) || !counts) return set_err(ctx, HJ_ERR_ARG, "bad arrays");
+  if (grid->nbins * (int64_t)sizeof(uint32_t) > (int64_t)ctx->max_smem_optin)
+    return set_err(ctx, HJ_ERR_TOO_LARGE, "nbins = %lld too large for the shared-memory histogram",
+                   (long long)grid->nbins);
+  const int B = (int)grid->nbins;
+  const int nblk = hist_blocks(ctx, n);
+  ConvBuffers cb{};
+  double* ex[1];
+  uint32_t* part = nullptr;
+  HJ_TRY(conv_scratch(ctx, B, (size_t)n, 1, (int64_t)nblk * B, cb, ex, &part));
+  if (n > 0)
+    HJ_CUDA(ctx, cudaMemcpyAsync(ex[0], z, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  HJ_TRY(device_histogram(ctx, ex[0], n, grid, cb.cnt, part, nblk));
+  HJ_CUDA(ctx, cudaMemcpyAsync(counts, cb.cnt, sizeof(int64_t) * B, cudaMemcpyDeviceToHost, ctx->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_wake_potential(hj_ctx* ctx, const int64_t* counts, const hj_grid* grid,
+                                       const hj_wake* wake, double current, double* pot) {
+  HJ_TRY(ctx_ok(ctx));
+  HJ_TRY(check_grid(ctx, grid));
+  if (!counts || !wake || !pot) return set_err(ctx, HJ_ERR_ARG, "bad arrays");
+  if (grid->nbins > kMaxBins)
+    return set_err(ctx, HJ_ERR_TOO_LARGE, "nbins = %lld exceeds the supported %lld",
+                   (long long)grid->nbins, (long long)kMaxBins);
+  if (wake->ctau <= 0) return set_err(ctx, HJ_ERR_WAKE_PARAM, "Wake parameter cτ must be positive.");
+  const int B = (int)grid->nbins;
+  for (int i = 0; i < B; ++i)
+    if (counts[i] < 0) return set_err(ctx, HJ_ERR_ARG, "negative bin count");
+  ConvBuffers cb{};
+  uint32_t* part = nullptr;
+  HJ_TRY(conv_scratch(ctx, B, 0, 0, 0, cb, nullptr, &part));
+  HJ_CUDA(ctx, cudaMemcpyAsync(cb.cnt, counts, sizeof(int64_t) * B, cudaMemcpyHostToDevice, ctx->stream));
+  HJ_TRY(device_conv(ctx, grid, wake, current, cb));
+  HJ_CUDA(ctx, cudaMemcpyAsync(pot, cb.pot, sizeof(double) * B, cudaMemcpyDeviceToHost, ctx->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE, int64_t n,
+                                        const hj_wake* wake, double current, double sigma_z,
+                                        const hj_grid* grid) {
+  (void)sigma_z;  // unused by the reference's MPI branch as well
+  HJ_TRY(ctx_ok(ctx));
+  HJ_TRY(check_grid(ctx, grid));
+  if (n < 0 || (n > 0 && (!z || !dE)) || !wake) return set_err(ctx, HJ_ERR_ARG, "bad arrays");
+  if (grid->nbins > kMaxBins)
+    return set_err(ctx, HJ_ERR_TOO_LARGE, "nbins = %lld exceeds the supported %lld",
+                   (long long)grid->nbins, (long long)kMaxBins);
+  if (wake->ctau <= 0) return set_err(ctx, HJ_ERR_WAKE_PARAM, "Wake parameter cτ must be positive.");
+  const int B = (int)grid->nbins;
+  const int nblk = hist_blocks(ctx, n);
+  ConvBuffers cb{};
+  double* ex[2];
+  uint32_t* part = nullptr;
+  HJ_TRY(conv_scratch(ctx, B, (size_t)n, 2, (int64_t)nblk * B, cb, ex, &part));
+  if (n > 0) {
+    HJ_CUDA(ctx, cudaMemcpyAsync(ex[0], z, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    HJ_CUDA(ctx, cudaMemcpyAsync(ex[1], dE, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  HJ_TRY(device_histogram(ctx, ex[0], n, grid, cb.cnt, part, nblk));
+  HJ_TRY(device_conv(ctx, grid, wake, current, cb));
+  if (n > 0) {
+    const double c1 = grid->centers[0], cB = grid->centers[B - 1];
+    const double inv_c = B >= 2 ? 1.0 / ((cB - c1) / (double)(B - 1)) : 0.0;
+    HJ_CUDA(ctx, launch_interp_kick(ex[0], ex[1], n, cb.pot, B, c1, cB, inv_c, ctx->stream));
+  }
+  return unstage(ctx, n, dE, ex[1]);
+}

@@ -1,0 +1,110 @@
+// hj_host.cpp -- host-side set-up of a run: bin grid, wake and smoothing
+// tables, FFT twiddles.  Compiled by the host C++ compiler with
+// -ffp-contract=off so every rounding happens where the reference source
+// puts it (these tables are constant over a run and computed once).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#include "../../include/haissinski_gpu.h"
+#include "hj_host.h"
+
+namespace {
+const double kTwoPi = 6.283185307179586;    // Float64(2π)
+const double kPi = 3.141592653589793;       // Float64(π)
+const double kSpeedLight = 299792458.0;     // src/constants.jl:5
+}  // namespace
+
+extern "C" hj_status hj_wake_reference(const hj_params* p, hj_wake* out) {
+  if (!p || !out) return HJ_ERR_ARG;
+  const double kp = 3e1, Z0 = 120 * kPi, ctau = 4e-3;        // src/evolution.jl:276
+  out->wake_factor = Z0 * kSpeedLight / (kPi * p->pipe_radius);  // :279
+  const double a = 2 * kp / p->pipe_radius;
+  out->wake_sqrt = std::sqrt(a > 0 ? a : 0.0);              // :280
+  out->ctau = ctau;
+  out->sin_coef = 0.0;
+  out->population = 0.0;
+  out->half_width_sigmas = 7.5;                              // :270
+  out->delta_std = 0.15;                                     // src/wakefield.jl:204
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_wake_resonator(double Rs, double Q, double fr, double population,
+                                       double half_width_sigmas, hj_wake* out) {
+  if (!out || !(Rs > 0) || !(Q > 0.5) || !(fr > 0) || !(half_width_sigmas > 0))
+    return HJ_ERR_ARG;
+  // Broadband resonator wake W(τ) = 2αRs e^{-ατ}(cos ω̄τ - (α/ω̄) sin ω̄τ),
+  // α = ω_r/2Q, ω̄ = sqrt(ω_r² - α²), written in the reference's variable
+  // c = -cτ (c <= 0 behind the source).
+  const double wr = kTwoPi * fr;
+  const double alpha = wr / (2.0 * Q);
+  const double wbar = std::sqrt(wr * wr - alpha * alpha);
+  out->wake_factor = 2.0 * alpha * Rs;
+  out->wake_sqrt = wbar / kSpeedLight;
+  out->ctau = kSpeedLight / alpha;
+  // cos(s c) with c = -cτ is even; sin(ω̄τ) = -sin(s c), so the -(α/ω̄) sin
+  // term becomes +(α/ω̄) sin(s c).
+  out->sin_coef = alpha / wbar;
+  out->population = population;
+  out->half_width_sigmas = half_width_sigmas;
+  out->delta_std = 0.15;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_make_grid(double sigma_z0, double half_width_sigmas, int64_t nbins,
+                                  double* centers, hj_grid* out) {
+  if (!centers || !out) return HJ_ERR_ARG;
+  if (nbins <= 0) return HJ_ERR_NBINS;
+  double w = half_width_sigmas * sigma_z0;                   // src/evolution.jl:270
+  if (w < 1e-9) w = 1e-6;                                    // :272
+  // Julia's range(-w, w, length=B+1) and its midpoints hold the correctly
+  // rounded values of w(2k-B)/B and w(2k+1-B)/B; with B a power of two the
+  // quad-precision product below is exact before the single rounding.
+  const __float128 W = (__float128)w, Bq = (__float128)nbins;
+  for (int64_t k = 0; k < nbins; ++k)
+    centers[k] = (double)(W * (__float128)(2 * k + 1 - nbins) / Bq);
+  out->nbins = nbins;
+  out->edge_first = -w;
+  out->edge_last = w;
+  out->edge_step = (double)((W * 2) / Bq);
+  out->centers = centers;
+  return HJ_OK;
+}
+
+namespace hj {
+
+// calculate_wake_function, src/wakefield.jl:115-118.
+double host_wake_function(double c, const hj_wake& w) {
+  if (c > 0.0) return 0.0;
+  const double inv_ctau = 1.0 / w.ctau;
+  double osc = std::cos(w.wake_sqrt * c);
+  if (w.sin_coef != 0.0) osc = osc + w.sin_coef * std::sin(w.wake_sqrt * c);
+  return w.wake_factor * std::exp(c * inv_ctau) * osc;
+}
+
+// delta, src/utils.jl:58-66.
+double host_delta(double x, double sigma) {
+  const double inv = 1.0 / (std::sqrt(kTwoPi) * sigma);
+  const double f = -0.5 / (sigma * sigma);
+  return inv * std::exp(x * x * f);
+}
+
+void host_wake_tables(const double* centers, int64_t B, const hj_wake& w, double* W,
+                      double* lam) {
+  for (int64_t i = 0; i < B; ++i) {
+    W[i] = host_wake_function(centers[i], w);
+    lam[i] = host_delta(centers[i], w.delta_std);
+  }
+}
+
+// tw[k] = exp(-2πi k/P) in long double, rounded once.
+void host_twiddles(int64_t P, double* tw_interleaved) {
+  const long double kPiL = 3.141592653589793238462643383279502884L;
+  for (int64_t k = 0; k < P; ++k) {
+    const long double a = -2.0L * kPiL * (long double)k / (long double)P;
+    tw_interleaved[2 * k] = (double)cosl(a);
+    tw_interleaved[2 * k + 1] = (double)sinl(a);
+  }
+}
+
+}  // namespace hj

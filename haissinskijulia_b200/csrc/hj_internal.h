@@ -1,0 +1,122 @@
+// hj_internal.h -- launch interface between the C-ABI layer (hj_api.cu) and
+// the kernels (hj_track.cu, hj_wake.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hj_device.cuh"
+
+namespace hj {
+
+constexpr int kNumSums = 4;         // per-block partial sums of the particle pass
+constexpr int kTrackThreads = 512;  // threads per block of the particle kernels
+constexpr int kBinsThreads = 1024;  // threads of the single-CTA bins kernel
+constexpr int64_t kMaxBins = 16384; // largest grid the shared-memory FFT holds (P = 32768)
+
+// Quantum-excitation source of the particle pass.
+enum QeMode { QE_OFF = 0, QE_PHILOX = 1, QE_DRAWS = 2 };
+
+// Arguments of the fused per-turn particle pass (one launch per turn).
+struct PassArgs {
+  double* z;
+  double* dE;
+  int64_t n;
+  TurnState* ts;
+  const double* pot;       // potential of the previous turn at the bin centers
+  // bin grid
+  int32_t B;
+  int32_t use_wake;
+  double e0, eN, inv_estep;       // histogram (edges)
+  double c1, cB, inv_cstep;       // interpolation (centers)
+  // physics constants of the run
+  double V, phi_s, inv_mass, alpha_c, two_pi_h;
+  int32_t update_eta, update_E0, sr, qe_mode;
+  uint64_t seed;
+  const double* draws;     // QE_DRAWS: turns x n, row = turn - draws_first_turn
+  int64_t draws_first_turn;
+  int64_t draws_turns;
+  // per-block outputs
+  uint32_t* part_cnt;              // [grid][B]
+  unsigned long long* part_cic;    // [grid][B]
+  double* part_sum;                // [grid][kNumSums]
+};
+
+// Arguments of the per-turn bins step (single CTA).
+struct BinsArgs {
+  TurnState* ts;
+  const double* part_sum;
+  int32_t nblk;
+  int64_t n;
+  hj_params params;
+  double sigma_E0_initial;
+  double population;
+  int32_t use_wake;
+  int32_t B, P, M, H, logH;
+  const unsigned long long* cnt;   // [B]
+  const unsigned long long* cic;   // [B]
+  const double* lam;               // [B]
+  const double2* Wf;               // [M+1]
+  const double2* twP;              // [P]
+  double2* Xg;                     // [M]
+  double2* zE;                     // [H]
+  double* pot;                     // [B]
+  const double* W;                 // [B] wake table (direct path for tiny grids)
+  // standalone convolution (hj_wake_potential): no turn-state update
+  int32_t conv_only;
+  double conv_current;
+};
+
+// Moments of (z, dE) per block: [Σz, Σz², ΣdE, ΣdE²], optionally after
+// applying a pending kick/re-centring (flush) and writing the result.
+struct FlushArgs {
+  double* z;          // state
+  double* dE;
+  int64_t n;
+  const TurnState* ts;
+  const double* pot;
+  int32_t B;
+  int32_t use_wake, update_E0;
+  double c1, cB, inv_cstep;
+  int32_t apply;      // 1: apply pending ops
+  double* z_out;      // destination (may alias z/dE); NULL -> not written
+  double* dE_out;
+  double* part;       // [grid][4]
+};
+
+// ---- launchers (hj_track.cu) ----
+void prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
+int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm);
+int track_blocks_per_sm(int B, int qe_mode, int use_wake);
+size_t track_smem_bytes(int B, int use_wake);
+cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
+cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
+                               int nblk, int B, unsigned long long* cnt,
+                               unsigned long long* cic, cudaStream_t st);
+cudaError_t launch_flush(const FlushArgs& a, int grid, cudaStream_t st);
+cudaError_t launch_histogram_only(const double* z, int64_t n, int B, double e0, double eN,
+                                  double inv_estep, uint32_t* part_cnt, int grid,
+                                  cudaStream_t st);
+cudaError_t launch_interp_kick(const double* z, double* dE, int64_t n, const double* pot,
+                               int B, double c1, double cB, double inv_cstep,
+                               cudaStream_t st);
+cudaError_t launch_rf_kick(double V, double sin_phis, double k, double phi_s,
+                           const double* z, double* dE, int64_t n, cudaStream_t st);
+cudaError_t launch_qe(double excitation, const double* draws, uint64_t seed, int64_t turn,
+                      double* dE, int64_t n, cudaStream_t st);
+cudaError_t launch_sr(double damping, double* dE, int64_t n, cudaStream_t st);
+cudaError_t launch_phase_advance(int update_eta, TurnScalars s, double inv_mass,
+                                 double alpha_c, double two_pi_h, double phi_s,
+                                 const double* dE, double* z, int64_t n, cudaStream_t st);
+cudaError_t launch_gaussian(uint64_t seed, int64_t turn, int64_t n, double* out,
+                            cudaStream_t st);
+
+// ---- launchers (hj_wake.cu) ----
+void prepare_wake_kernels(int max_smem);    // once per device: dynamic smem limits
+cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, int logH,
+                                 const double2* twP, double2* Xg, double2* Wf,
+                                 cudaStream_t st);
+cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st);
+size_t bins_smem_bytes(int H);
+
+}  // namespace hj

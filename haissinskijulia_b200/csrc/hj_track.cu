@@ -1,0 +1,549 @@
+// hj_track.cu -- particle-side kernels of the tracking loop (sm_100a, FP64).
+//
+// One fused pass per turn replaces the reference's chain of per-particle
+// loops in longitudinal_evolve! (src/evolution.jl:307-451):
+//   [previous turn]  wake kick  dE -= lerp(pot, z)      src/wakefield.jl:22-105, :342-344
+//                    E0 re-centring  dE -= mean         src/evolution.jl:434
+//   [this turn]      RF kick                            src/rf_kick.jl:84-87
+//                    quantum excitation                 src/quantum_excitation.jl:58-71
+//                    SR damping                         src/synchrotron_radiation.jl:44-56
+//                    drift (phase advance)              src/evolution.jl:331-344 / :143-167
+//                    histogram of z                     src/utils.jl:384-398
+//                    Σz, Σz² (σ_z, src/utils.jl:576-580), Σ(ΔE - ΔE_start) (src/evolution.jl:408-411)
+//                    CIC deposit of the interpolation weights, so that the bins step
+//                    can form Σ_i lerp(pot, z_i) = Σ_k H[k] pot[k] for the E0 update
+//                    without another pass over the particles.
+// z is unchanged between the drift of turn t and the wake kick of turn t, so
+// the kick is applied at the start of the next pass from the same z.
+//
+// Each thread owns four consecutive particles and moves them with one
+// 32-byte load/store per array (ld.global.v4.f64), so a warp touches 1 KB of
+// contiguous HBM per array per iteration.  Histograms are privatised in
+// shared memory per block and written out as per-block partials; the
+// reduction over blocks is a separate, deterministic kernel.
+#include "hj_internal.h"
+
+namespace hj {
+namespace {
+
+struct PassConst {
+  double V, phi_s, sin_phis, k, inv_k, excitation, damping, gamma0, inv_mass, alpha_c,
+      two_pi_h, inv_b2E0, coeff0;
+  int drift_ok, update_eta, sr;
+};
+
+struct GridConst {
+  int B;
+  double e0, eN, inv_e, c1, cB, inv_c;
+};
+
+__device__ __forceinline__ void ld4(const double* p, double v[4]) {
+  asm("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+               : "l"(p));
+}
+
+__device__ __forceinline__ void st4(double* p, const double v[4]) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
+               "d"(v[2]), "d"(v[3])
+               : "memory");
+}
+
+// Interpolation cell of z on the bin centers (src/wakefield.jl:64-78), 0-based:
+// idx = clamp(floor(u), 0, B-2), w = u - floor(u), u = (clamp(z,c1,cB)-c1)/Δc.
+__device__ __forceinline__ void cic_cell(double z, const GridConst& g, int& idx, double& w) {
+  double cl = z > g.cB ? g.cB : (z < g.c1 ? g.c1 : z);
+  double u = __dmul_rn(__dsub_rn(cl, g.c1), g.inv_c);
+  double fl = floor(u);
+  double fi = (fl >= 0.0) ? (fl > (double)(g.B - 2) ? (double)(g.B - 2) : fl) : 0.0;
+  idx = (int)fi;
+  w = __dsub_rn(u, fl);
+}
+
+// lerp of the potential table (src/wakefield.jl:94-102).
+__device__ __forceinline__ double wake_kick(double z, const GridConst& g,
+                                            const double* __restrict__ pot) {
+  if (g.B < 2) return __ldg(pot);
+  int idx;
+  double w;
+  cic_cell(z, g, idx, w);
+  return __dadd_rn(__dmul_rn(__ldg(pot + idx), __dsub_rn(1.0, w)),
+                   __dmul_rn(__ldg(pot + idx + 1), w));
+}
+
+// Histogram bin of z (src/utils.jl:387-397), 0-based: clamp(floor((z-e0)/Δe), 0, B-1).
+__device__ __forceinline__ int ngp_bin(double z, const GridConst& g, bool& in) {
+  in = (z >= g.e0) & (z <= g.eN);
+  double u = floor(__dmul_rn(__dsub_rn(z, g.e0), g.inv_e));
+  return (u >= 0.0) ? (u < (double)g.B ? (int)u : g.B - 1) : 0;
+}
+
+// RF kick, QE, SR and drift of one particle for one turn.
+__device__ __forceinline__ void turn_particle(double& z, double& e, double r, bool qe,
+                                              const PassConst& c) {
+  double phi = __dadd_rn(__dmul_rn(-z, c.k), c.phi_s);
+  e = __dadd_rn(e, __dmul_rn(c.V, __dsub_rn(sin(phi), c.sin_phis)));
+  if (qe) e = __dadd_rn(e, __dmul_rn(c.excitation, r));
+  if (c.sr) e = __dmul_rn(e, c.damping);
+  if (c.update_eta) {
+    double dg = __dmul_rn(e, c.inv_mass);
+    double gp = __dadd_rn(c.gamma0, dg);
+    double eta = __dsub_rn(c.alpha_c, 1.0 / __dmul_rn(gp, gp));
+    double coeff = __dmul_rn(__dmul_rn(c.two_pi_h, eta), c.inv_b2E0);
+    double ph = -__dsub_rn(__dmul_rn(z, c.k), c.phi_s);
+    ph = __dadd_rn(ph, __dmul_rn(coeff, e));
+    z = __dmul_rn(__dadd_rn(-ph, c.phi_s), c.inv_k);
+  } else if (c.drift_ok) {
+    double ph = -__dsub_rn(__dmul_rn(z, c.k), c.phi_s);
+    ph = __dadd_rn(ph, __dmul_rn(c.coeff0, e));
+    z = __dmul_rn(__dadd_rn(-ph, c.phi_s), c.inv_k);
+  }
+}
+
+template <bool WAKE>
+__device__ __forceinline__ void pass_particle(double& z, double& e, double r, bool qe,
+                                              const PassConst& c, const GridConst& g,
+                                              bool pending, bool upd_E0, double pmean,
+                                              const double* __restrict__ pot, double& acc_z,
+                                              double& acc_z2, double& acc_d, uint32_t& n_in,
+                                              uint32_t* s_cnt, unsigned long long* s_cic) {
+  if (pending) {
+    if (WAKE) e = __dsub_rn(e, wake_kick(z, g, pot));
+    if (upd_E0) e = __dsub_rn(e, pmean);
+  }
+  const double e_start = e;
+  turn_particle(z, e, r, qe, c);
+  if (upd_E0) acc_d += __dsub_rn(e, e_start);
+  if (WAKE) {
+    acc_z += z;
+    acc_z2 = fma(z, z, acc_z2);
+    bool in;
+    int j = ngp_bin(z, g, in);
+    if (in) {
+      atomicAdd(&s_cnt[j], 1u);
+      ++n_in;
+    }
+    if (g.B >= 2) {
+      int idx;
+      double w;
+      cic_cell(z, g, idx, w);
+      unsigned long long q = __double2ull_rn(w * 4294967296.0);
+      if (!(w >= 0.0)) q = 0ull;  // NaN z: deposit in the first cell, flagged by the moments
+      atomicAdd(&s_cic[idx], (1ull << 32) - q);
+      atomicAdd(&s_cic[idx + 1], q);
+    } else {
+      atomicAdd(&s_cic[0], 1ull << 32);
+    }
+  }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Fixed-order block reduction of four accumulators into out[0..3] (thread 0).
+__device__ __forceinline__ void block_sum4(double a0, double a1, double a2, double a3,
+                                           double* out) {
+  __shared__ double red[kTrackThreads / 32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  a0 = warp_sum(a0);
+  a1 = warp_sum(a1);
+  a2 = warp_sum(a2);
+  a3 = warp_sum(a3);
+  if (lane == 0) {
+    red[warp][0] = a0;
+    red[warp][1] = a1;
+    red[warp][2] = a2;
+    red[warp][3] = a3;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+template <bool WAKE, int QE>
+__global__ void __launch_bounds__(kTrackThreads) k_track_pass(PassArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned long long* s_cic = reinterpret_cast<unsigned long long*>(smem_raw);
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_cic + (WAKE ? a.B : 0));
+
+  TurnState* ts = a.ts;
+  const TurnScalars sc = ts->cur;
+  const bool pending = ts->pending != 0;
+  const double pmean = ts->pending_mean;
+  const int64_t turn = ts->turn;
+  const bool upd_E0 = a.update_E0 != 0;
+
+  PassConst c;
+  c.V = a.V;
+  c.phi_s = a.phi_s;
+  c.sin_phis = sc.sin_phis;
+  c.k = sc.k;
+  c.inv_k = sc.inv_k;
+  c.excitation = sc.excitation;
+  c.damping = sc.damping;
+  c.gamma0 = sc.gamma0;
+  c.inv_mass = a.inv_mass;
+  c.alpha_c = a.alpha_c;
+  c.two_pi_h = a.two_pi_h;
+  c.inv_b2E0 = sc.inv_b2E0;
+  c.coeff0 = sc.coeff0;
+  c.drift_ok = sc.drift_ok;
+  c.update_eta = a.update_eta;
+  c.sr = a.sr;
+  GridConst g{a.B, a.e0, a.eN, a.inv_estep, a.c1, a.cB, a.inv_cstep};
+
+  const double* drow = nullptr;
+  if (QE == QE_DRAWS) {
+    int64_t row = turn - a.draws_first_turn;
+    if (row >= 0 && row < a.draws_turns) {
+      drow = a.draws + row * a.n;
+    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+      atomicOr(&ts->status, 1 << HJ_ERR_ARG);
+    }
+  }
+
+  if (WAKE) {
+    for (int i = threadIdx.x; i < a.B; i += blockDim.x) {
+      s_cic[i] = 0ull;
+      s_cnt[i] = 0u;
+    }
+    __syncthreads();
+  }
+
+  double acc_z = 0.0, acc_z2 = 0.0, acc_d = 0.0;
+  uint32_t n_in = 0;
+  const double* __restrict__ pot = a.pot;
+  const int64_t nq = a.n >> 2;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+    double zz[4], ee[4], rr[4] = {0.0, 0.0, 0.0, 0.0};
+    ld4(a.z + 4 * q, zz);
+    ld4(a.dE + 4 * q, ee);
+    if (QE == QE_PHILOX) {
+      philox_normals4(a.seed, turn, q, rr);
+    } else if (QE == QE_DRAWS) {
+      if (drow) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) rr[j] = __ldg(drow + 4 * q + j);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      pass_particle<WAKE>(zz[j], ee[j], rr[j], QE != QE_OFF, c, g, pending, upd_E0, pmean,
+                          pot, acc_z, acc_z2, acc_d, n_in, s_cnt, s_cic);
+    st4(a.z + 4 * q, zz);
+    st4(a.dE + 4 * q, ee);
+  }
+  // Tail of n % 4 particles: threads 0..2 of block 0, scalar.
+  if (blockIdx.x == 0 && threadIdx.x < (int)(a.n & 3)) {
+    const int64_t i = nq * 4 + threadIdx.x;
+    double rr[4] = {0.0, 0.0, 0.0, 0.0};
+    if (QE == QE_PHILOX) philox_normals4(a.seed, turn, nq, rr);
+    double r = rr[threadIdx.x];
+    if (QE == QE_DRAWS && drow) r = __ldg(drow + i);
+    double z = a.z[i], e = a.dE[i];
+    pass_particle<WAKE>(z, e, r, QE != QE_OFF, c, g, pending, upd_E0, pmean, pot, acc_z,
+                        acc_z2, acc_d, n_in, s_cnt, s_cic);
+    a.z[i] = z;
+    a.dE[i] = e;
+  }
+
+  block_sum4(acc_z, acc_z2, acc_d, (double)n_in, a.part_sum + (size_t)blockIdx.x * kNumSums);
+
+  if (WAKE) {
+    __syncthreads();
+    uint32_t* pc = a.part_cnt + (size_t)blockIdx.x * a.B;
+    unsigned long long* pq = a.part_cic + (size_t)blockIdx.x * a.B;
+    for (int i = threadIdx.x; i < a.B; i += blockDim.x) {
+      pc[i] = s_cnt[i];
+      pq[i] = s_cic[i];
+    }
+  }
+}
+
+// Deterministic reduction of the per-block histograms (fixed block order).
+__global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
+                              const unsigned long long* __restrict__ part_cic, int nblk, int B,
+                              unsigned long long* __restrict__ cnt,
+                              unsigned long long* __restrict__ cic) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  unsigned long long sc = 0ull, sq = 0ull;
+  for (int k = 0; k < nblk; ++k) {
+    sc += __ldg(part_cnt + (size_t)k * B + b);
+    if (part_cic) sq += __ldg(part_cic + (size_t)k * B + b);
+  }
+  cnt[b] = sc;
+  if (cic) cic[b] = sq;
+}
+
+// Pending kick + re-centring (optional), copy-out (optional) and the moments
+// [Σz, Σz², ΣdE, ΣdE²] per block.
+__global__ void __launch_bounds__(kTrackThreads) k_flush(FlushArgs a) {
+  const bool apply = a.apply && a.ts && a.ts->pending;
+  const double pmean = apply ? a.ts->pending_mean : 0.0;
+  GridConst g{a.B, 0.0, 0.0, 0.0, a.c1, a.cB, a.inv_cstep};
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    double z = a.z[i], e = a.dE[i];
+    if (apply) {
+      if (a.use_wake) e = __dsub_rn(e, wake_kick(z, g, a.pot));
+      if (a.update_E0) e = __dsub_rn(e, pmean);
+    }
+    if (a.z_out) a.z_out[i] = z;
+    if (a.dE_out) a.dE_out[i] = e;
+    s0 += z;
+    s1 = fma(z, z, s1);
+    s2 += e;
+    s3 = fma(e, e, s3);
+  }
+  block_sum4(s0, s1, s2, s3, a.part + (size_t)blockIdx.x * 4);
+}
+
+// NGP histogram only (hj_histogram, hj_apply_wakefield).
+__global__ void __launch_bounds__(kTrackThreads) k_histogram(const double* __restrict__ z,
+                                                            int64_t n, GridConst g,
+                                                            uint32_t* __restrict__ part_cnt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem_raw);
+  for (int i = threadIdx.x; i < g.B; i += blockDim.x) s_cnt[i] = 0u;
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    bool in;
+    int j = ngp_bin(__ldg(z + i), g, in);
+    if (in) atomicAdd(&s_cnt[j], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < g.B; i += blockDim.x)
+    part_cnt[(size_t)blockIdx.x * g.B + i] = s_cnt[i];
+}
+
+__global__ void k_interp_kick(const double* __restrict__ z, double* __restrict__ dE, int64_t n,
+                              const double* __restrict__ pot, GridConst g) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    dE[i] = __dsub_rn(dE[i], wake_kick(__ldg(z + i), g, pot));
+}
+
+__global__ void k_rf_kick(double V, double sin_phis, double k, double phi_s,
+                          const double* __restrict__ z, double* __restrict__ dE, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double phi = __dadd_rn(__dmul_rn(-__ldg(z + i), k), phi_s);
+    dE[i] = __dadd_rn(dE[i], __dmul_rn(V, __dsub_rn(sin(phi), sin_phis)));
+  }
+}
+
+__global__ void k_qe(double excitation, const double* __restrict__ draws, uint64_t seed,
+                     int64_t turn, double* __restrict__ dE, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nq = (n + 3) >> 2;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+    double rr[4];
+    if (!draws) philox_normals4(seed, turn, q, rr);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int64_t i = 4 * q + j;
+      if (i < n) {
+        double r = draws ? __ldg(draws + i) : rr[j];
+        dE[i] = __dadd_rn(dE[i], __dmul_rn(excitation, r));
+      }
+    }
+  }
+}
+
+__global__ void k_sr(double damping, double* __restrict__ dE, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    dE[i] = __dmul_rn(dE[i], damping);
+}
+
+__global__ void k_phase_advance(PassConst c, const double* __restrict__ dE,
+                                double* __restrict__ z, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double zi = z[i], e = __ldg(dE + i);
+    // Drift only: RF/QE/SR disabled by zero voltage/flags in `c`.
+    if (c.update_eta) {
+      double dg = __dmul_rn(e, c.inv_mass);
+      double gp = __dadd_rn(c.gamma0, dg);
+      double eta = __dsub_rn(c.alpha_c, 1.0 / __dmul_rn(gp, gp));
+      double coeff = __dmul_rn(__dmul_rn(c.two_pi_h, eta), c.inv_b2E0);
+      double ph = -__dsub_rn(__dmul_rn(zi, c.k), c.phi_s);
+      ph = __dadd_rn(ph, __dmul_rn(coeff, e));
+      zi = __dmul_rn(__dadd_rn(-ph, c.phi_s), c.inv_k);
+    } else if (c.drift_ok) {
+      double ph = -__dsub_rn(__dmul_rn(zi, c.k), c.phi_s);
+      ph = __dadd_rn(ph, __dmul_rn(c.coeff0, e));
+      zi = __dmul_rn(__dadd_rn(-ph, c.phi_s), c.inv_k);
+    }
+    z[i] = zi;
+  }
+}
+
+__global__ void k_gaussian(uint64_t seed, int64_t turn, int64_t n, double* __restrict__ out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nq = (n + 3) >> 2;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+    double rr[4];
+    philox_normals4(seed, turn, q, rr);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (4 * q + j < n) out[4 * q + j] = rr[j];
+  }
+}
+
+int elementwise_grid(int64_t n) {
+  int64_t g = (n + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)g;
+}
+
+}  // namespace
+
+void prepare_track_kernels(int max_smem) {
+  const void* fns[] = {(const void*)k_track_pass<true, QE_OFF>,
+                       (const void*)k_track_pass<true, QE_PHILOX>,
+                       (const void*)k_track_pass<true, QE_DRAWS>,
+                       (const void*)k_track_pass<false, QE_OFF>,
+                       (const void*)k_track_pass<false, QE_PHILOX>,
+                       (const void*)k_track_pass<false, QE_DRAWS>,
+                       (const void*)k_histogram};
+  for (const void* f : fns)
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+}
+
+size_t track_smem_bytes(int B, int use_wake) {
+  return use_wake ? (size_t)B * (sizeof(unsigned long long) + sizeof(uint32_t)) : 0;
+}
+
+int track_blocks_per_sm(int B, int qe_mode, int use_wake) {
+  size_t smem = track_smem_bytes(B, use_wake);
+  int bps = 0;
+  const void* fn = nullptr;
+  if (use_wake) {
+    fn = qe_mode == QE_PHILOX ? (const void*)k_track_pass<true, QE_PHILOX>
+         : qe_mode == QE_DRAWS ? (const void*)k_track_pass<true, QE_DRAWS>
+                               : (const void*)k_track_pass<true, QE_OFF>;
+  } else {
+    fn = qe_mode == QE_PHILOX ? (const void*)k_track_pass<false, QE_PHILOX>
+         : qe_mode == QE_DRAWS ? (const void*)k_track_pass<false, QE_DRAWS>
+                               : (const void*)k_track_pass<false, QE_OFF>;
+  }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kTrackThreads, smem) !=
+      cudaSuccess)
+    bps = 1;
+  return bps < 1 ? 1 : bps;
+}
+
+// Blocks of the particle pass: enough to fill the GPU, but each block should
+// own at least ~2 bins' worth of histogram traffic per particle it moves.
+int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm) {
+  int64_t per_block = 4 * (int64_t)kTrackThreads;
+  if (per_block < 2 * (int64_t)B) per_block = 2 * (int64_t)B;
+  int64_t g = (n + per_block - 1) / per_block;
+  int64_t cap = (int64_t)num_sms * blocks_per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
+  size_t smem = track_smem_bytes(a.B, a.use_wake);
+  if (a.use_wake) {
+    switch (a.qe_mode) {
+      case QE_PHILOX: k_track_pass<true, QE_PHILOX><<<grid, kTrackThreads, smem, st>>>(a); break;
+      case QE_DRAWS: k_track_pass<true, QE_DRAWS><<<grid, kTrackThreads, smem, st>>>(a); break;
+      default: k_track_pass<true, QE_OFF><<<grid, kTrackThreads, smem, st>>>(a); break;
+    }
+  } else {
+    switch (a.qe_mode) {
+      case QE_PHILOX: k_track_pass<false, QE_PHILOX><<<grid, kTrackThreads, 0, st>>>(a); break;
+      case QE_DRAWS: k_track_pass<false, QE_DRAWS><<<grid, kTrackThreads, 0, st>>>(a); break;
+      default: k_track_pass<false, QE_OFF><<<grid, kTrackThreads, 0, st>>>(a); break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
+                               int nblk, int B, unsigned long long* cnt,
+                               unsigned long long* cic, cudaStream_t st) {
+  k_hist_reduce<<<(B + 255) / 256, 256, 0, st>>>(part_cnt, part_cic, nblk, B, cnt, cic);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flush(const FlushArgs& a, int grid, cudaStream_t st) {
+  k_flush<<<grid, kTrackThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_histogram_only(const double* z, int64_t n, int B, double e0, double eN,
+                                  double inv_estep, uint32_t* part_cnt, int grid,
+                                  cudaStream_t st) {
+  GridConst g{B, e0, eN, inv_estep, 0.0, 0.0, 0.0};
+  size_t smem = (size_t)B * sizeof(uint32_t);
+  k_histogram<<<grid, kTrackThreads, smem, st>>>(z, n, g, part_cnt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_interp_kick(const double* z, double* dE, int64_t n, const double* pot,
+                               int B, double c1, double cB, double inv_cstep,
+                               cudaStream_t st) {
+  GridConst g{B, 0.0, 0.0, 0.0, c1, cB, inv_cstep};
+  k_interp_kick<<<elementwise_grid(n), 256, 0, st>>>(z, dE, n, pot, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rf_kick(double V, double sin_phis, double k, double phi_s,
+                           const double* z, double* dE, int64_t n, cudaStream_t st) {
+  k_rf_kick<<<elementwise_grid(n), 256, 0, st>>>(V, sin_phis, k, phi_s, z, dE, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_qe(double excitation, const double* draws, uint64_t seed, int64_t turn,
+                      double* dE, int64_t n, cudaStream_t st) {
+  k_qe<<<elementwise_grid((n + 3) / 4), 256, 0, st>>>(excitation, draws, seed, turn, dE, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sr(double damping, double* dE, int64_t n, cudaStream_t st) {
+  k_sr<<<elementwise_grid(n), 256, 0, st>>>(damping, dE, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_phase_advance(int update_eta, TurnScalars s, double inv_mass,
+                                 double alpha_c, double two_pi_h, double phi_s,
+                                 const double* dE, double* z, int64_t n, cudaStream_t st) {
+  PassConst c{};
+  c.phi_s = phi_s;
+  c.k = s.k;
+  c.inv_k = s.inv_k;
+  c.gamma0 = s.gamma0;
+  c.inv_mass = inv_mass;
+  c.alpha_c = alpha_c;
+  c.two_pi_h = two_pi_h;
+  c.inv_b2E0 = s.inv_b2E0;
+  c.coeff0 = s.coeff0;
+  c.drift_ok = s.drift_ok;
+  c.update_eta = update_eta;
+  k_phase_advance<<<elementwise_grid(n), 256, 0, st>>>(c, dE, z, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gaussian(uint64_t seed, int64_t turn, int64_t n, double* out,
+                            cudaStream_t st) {
+  k_gaussian<<<elementwise_grid((n + 3) / 4), 256, 0, st>>>(seed, turn, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace hj

@@ -1,0 +1,292 @@
+/*
+ * haissinski_gpu.h -- C ABI of the B200 (sm_100a) longitudinal tracking library.
+ *
+ * The reference (HaissinskiJulia, module StochasticHaissinski) exposes its
+ * per-turn tracking loop as Julia methods; it has no FFI of its own.  This
+ * header is the drop-in boundary a Julia `ccall` (or Python ctypes) binds:
+ * plain pointers, sizes and POD structs, no CUDA or torch types.
+ *
+ * Every entry point below names the reference interface it replaces.
+ * Conventions shared by all calls:
+ *   - particle state is structure-of-arrays Float64: z[n] in metres and dE[n]
+ *     in eV, exactly `particles.coordinates.z` / `particles.coordinates.ΔE`
+ *     of the reference's StructArray{Particle{Float64}}
+ *     (src/data_structures.jl:26-42);
+ *   - functions without `_device` in their name take HOST pointers, copy to
+ *     the GPU, run, and copy results back (in-place semantics like the
+ *     reference's mutating `!` methods);
+ *   - every call returns an hj_status; HJ_OK is 0.  The message of the last
+ *     failure on a context is available from hj_last_error().
+ *   - a context is bound to one device and is not re-entrant: use one
+ *     context per host thread.  Several contexts may share a GPU.
+ */
+#ifndef HAISSINSKI_GPU_H
+#define HAISSINSKI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t hj_status;
+
+enum {
+  HJ_OK = 0,
+  HJ_ERR_ARG = 1,          /* invalid argument (null pointer, negative size, ...) */
+  HJ_ERR_NBINS = 2,        /* nbins <= 0: src/evolution.jl:264, src/utils.jl:155-157 */
+  HJ_ERR_WAKE_PARAM = 3,   /* ctau <= 0 or pipe_radius <= 0: src/evolution.jl:277-278 */
+  HJ_ERR_CUDA = 4,         /* a CUDA runtime call failed (message has the CUDA error) */
+  HJ_ERR_NOMEM = 5,        /* device allocation failed */
+  HJ_ERR_TOO_LARGE = 6,    /* a size exceeds what the library supports */
+  HJ_ERR_EMPTY = 7,        /* zero particles with the wakefield on: the reference's
+                              log10(0) particle-factor path raises (src/evolution.jl:377-379) */
+  HJ_ERR_NONFINITE = 8,    /* a NaN/Inf appeared in the bunch moments */
+  HJ_ERR_TIMEOUT = 9,      /* a bounded device-side wait gave up */
+  HJ_ERR_NO_DEVICE = 10,   /* no CUDA device, or device index out of range */
+  HJ_ERR_STATE = 11        /* call out of order (e.g. advance after finish) */
+};
+
+/*
+ * Simulation parameters: field for field the reference's
+ * SimulationParameters (src/data_structures.jl:81-97), Float64 instantiation.
+ */
+typedef struct hj_params {
+  double E0;            /* reference energy [eV] */
+  double mass;          /* particle mass [eV/c^2] */
+  double voltage;       /* RF voltage [V] */
+  int64_t harmonic;     /* RF harmonic number */
+  double radius;        /* bending radius used by SR damping / quantum excitation [m] */
+  double pipe_radius;   /* beam pipe radius [m] (enters the reference wake constants) */
+  double alpha_c;       /* momentum compaction */
+  double phi_s;         /* synchronous phase [rad] */
+  double freq_rf;       /* RF frequency [Hz] */
+  int64_t n_turns;      /* turns to track */
+  uint8_t use_wakefield;
+  uint8_t update_eta;
+  uint8_t update_E0;
+  uint8_t SR_damping;
+  uint8_t use_excitation;
+  uint8_t _pad[3];
+} hj_params;
+
+/*
+ * Wake model and intensity.  The reference hard-codes these inside
+ * longitudinal_evolve! (src/evolution.jl:270-280 and :377-386);
+ * hj_wake_reference() fills exactly those values.  The extra fields let a
+ * caller describe a broadband resonator and a bunch population.
+ *
+ *   W(c) = 0                                          for c > 0
+ *   W(c) = F * exp(c/ctau) * (cos(s c) + sin_coef * sin(s c))   for c <= 0
+ * (src/wakefield.jl:115-118 with sin_coef = 0).
+ */
+typedef struct hj_wake {
+  double wake_factor;        /* F */
+  double wake_sqrt;          /* s [1/m] */
+  double ctau;               /* c*tau [m] */
+  double sin_coef;           /* 0 in reference mode */
+  double population;         /* > 0: replaces the reference's particle_factor; 0: reference formula */
+  double half_width_sigmas;  /* bins span +-half_width_sigmas * sigma_z0_initial; reference 7.5 */
+  double delta_std;          /* width of the pointwise Gaussian weight delta(); reference 0.15 */
+} hj_wake;
+
+/*
+ * Uniform bin grid.  In the reference, edges = range(-w, w, length=nbins+1)
+ * and centers = (edges[1:end-1] + edges[2:end]) ./ 2 (src/evolution.jl:270-274).
+ * The histogram uses edge_first, edge_last and step(edges)
+ * (src/utils.jl:367-380); the wake table and the interpolation use the
+ * centers (src/wakefield.jl:39-42, :194-196).  A Julia caller passes the
+ * values of its own ranges so that bins agree bit for bit.
+ */
+typedef struct hj_grid {
+  int64_t nbins;
+  double edge_first;
+  double edge_last;
+  double edge_step;
+  const double* centers;     /* nbins values, host memory */
+} hj_grid;
+
+/* Return tuple of longitudinal_evolve! (src/evolution.jl:470) plus diagnostics. */
+typedef struct hj_result {
+  double sigma_E;            /* final sample std of dE */
+  double sigma_z;            /* final sample std of z */
+  double E0;                 /* final reference energy */
+  double sigma_E0_initial;   /* src/evolution.jl:248 */
+  double sigma_z0_initial;   /* src/evolution.jl:249 */
+  double mean_z;             /* final centroid of z */
+  double mean_dE;            /* final centroid of dE */
+  int64_t turns;             /* turns tracked so far */
+} hj_result;
+
+typedef struct hj_ctx hj_ctx;
+typedef struct hj_bunch hj_bunch;
+
+/* ---------------------------------------------------------------- context */
+
+/* Library version string. */
+const char* hj_version(void);
+/* Human-readable name of a status code. */
+const char* hj_status_string(hj_status s);
+/* Create a context on CUDA device `device`.  No reference counterpart (the
+ * reference allocates per call in create_simulation_buffers, src/utils.jl:147). */
+hj_status hj_create(int32_t device, hj_ctx** out);
+void hj_destroy(hj_ctx* ctx);
+/* Message of the last failure on this context ("" if none). */
+const char* hj_last_error(const hj_ctx* ctx);
+
+/* ---------------------------------------------------------------- set-up helpers */
+
+/* Fill the reference's hard-coded wake: kp = 30, Z0 = 120*pi, ctau = 4e-3,
+ * F = Z0*c/(pi*pipe_radius), s = sqrt(2 kp / pipe_radius)
+ * (src/evolution.jl:276-280), particle_factor intensity, +-7.5 sigma bins,
+ * delta_std = 0.15 (src/wakefield.jl:204). */
+hj_status hj_wake_reference(const hj_params* p, hj_wake* out);
+
+/* Broadband resonator (shunt impedance Rs [Ohm], quality factor Q, resonant
+ * frequency fr [Hz]) expressed in the reference's wake form:
+ * ctau = c/alpha, s = omega_bar/c, F = 2 alpha Rs, sin_coef = +alpha/omega_bar
+ * (the -(alpha/omega_bar) sin(omega_bar tau) term of the resonator wake with
+ * c = -c tau), alpha = omega_r/(2Q), omega_bar = sqrt(omega_r^2 - alpha^2).  No reference counterpart (the reference has only
+ * the hard-coded form above). */
+hj_status hj_wake_resonator(double Rs, double Q, double fr, double population,
+                            double half_width_sigmas, hj_wake* out);
+
+/* Build the uniform grid for nbins bins over +-half_width_sigmas*sigma_z0
+ * (width floor 1e-6 m when 7.5 sigma < 1e-9, src/evolution.jl:270-272).
+ * Each edge and center is the correctly rounded value of its exact rational
+ * position.  `centers` (nbins doubles) is caller storage and is referenced by
+ * the returned grid. */
+hj_status hj_make_grid(double sigma_z0, double half_width_sigmas, int64_t nbins,
+                       double* centers, hj_grid* out);
+
+/* ---------------------------------------------------------------- whole loop */
+
+/*
+ * Drop-in for
+ *   longitudinal_evolve!(particles, params, buffers, comm, use_mpi) -> (σ_E, σ_z, E0)
+ * (src/evolution.jl:206-212, returns at :470), MPI-branch semantics at any
+ * rank count (the only branch that runs with the wakefield on).
+ *   z, dE      host arrays of n Float64, updated in place;
+ *   wake       NULL -> hj_wake_reference(params);
+ *   nbins      bin count (length(buffers.λ) in the reference);
+ *   grid       NULL -> grid built on the device's sigma_z0_initial with
+ *              hj_make_grid; non-NULL -> used as given (nbins must match);
+ *   qe_draws   NULL -> on-device Philox-4x32-10 Gaussians keyed by
+ *              (seed, particle, turn); non-NULL -> host array of
+ *              n_turns*n standard normals, turn-major, used in place of
+ *              randn! (src/quantum_excitation.jl:36);
+ *   out        receives (sigma_E, sigma_z, E0) and diagnostics.
+ */
+hj_status hj_evolve(hj_ctx* ctx, double* z, double* dE, int64_t n,
+                    const hj_params* params, const hj_wake* wake, int64_t nbins,
+                    const hj_grid* grid, const double* qe_draws, uint64_t seed,
+                    hj_result* out);
+
+/* Same as hj_evolve on DEVICE arrays, enqueued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream); returns after the final moments are read. */
+hj_status hj_evolve_device(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                           const hj_params* params, const hj_wake* wake, int64_t nbins,
+                           const hj_grid* grid, const double* d_qe_draws, uint64_t seed,
+                           void* stream, hj_result* out);
+
+/* ---------------------------------------------------------------- resident bunch */
+
+/*
+ * A bunch whose state stays on the device between calls (the reference
+ * keeps the state in the caller's StructArray across the turn loop,
+ * src/evolution.jl:295-456).  create() computes the initial spreads
+ * (src/evolution.jl:245-253) and the wake set-up (:261-281); advance()
+ * enqueues turns without host synchronisation; observe() writes the
+ * turn-boundary state to caller DEVICE buffers without disturbing the
+ * bunch; finish() completes the last turn and returns the final tuple.
+ * d_z/d_dE are caller-owned device arrays that must outlive the bunch.
+ */
+hj_status hj_bunch_create(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                          const hj_params* params, const hj_wake* wake, int64_t nbins,
+                          const hj_grid* grid, uint64_t seed, void* stream,
+                          hj_bunch** out);
+/* Host-fed draws for the following turns: device array of turns*n normals,
+ * turn-major; turn t of the bunch reads row (t - first_turn).  NULL switches
+ * back to on-device Philox. */
+hj_status hj_bunch_set_draws(hj_bunch* b, const double* d_draws, int64_t first_turn,
+                             int64_t turns);
+/* Enqueue `turns` more turns on the bunch's stream. */
+hj_status hj_bunch_advance(hj_bunch* b, int64_t turns);
+/* Turn-boundary state (all pending kicks applied) into d_z_out/d_dE_out
+ * (device, n each; either may be NULL), plus moments and E0 in *res. */
+hj_status hj_bunch_observe(hj_bunch* b, double* d_z_out, double* d_dE_out, hj_result* res);
+/* Apply the pending wake kick and E0 re-centring of the last turn in place
+ * and return the final tuple (src/evolution.jl:458-470). */
+hj_status hj_bunch_finish(hj_bunch* b, hj_result* res);
+/* Device-time profiling of the turns enqueued while enabled: CUDA events are
+ * recorded on the bunch's stream around each particle pass and each bins
+ * step (histogram reduction + convolution + E0 update).  enable = 0 stops
+ * and clears.  No reference counterpart (the reference times whole calls
+ * with BenchmarkTools, tests/benchmark_total.jl:343-369). */
+hj_status hj_bunch_set_profiling(hj_bunch* b, int32_t enable);
+/* out[0] = particle-pass milliseconds, out[1] = bins-step milliseconds,
+ * out[2] = turns profiled, out[3] = kernel launches profiled.
+ * Synchronises the bunch's stream. */
+hj_status hj_bunch_read_profile(hj_bunch* b, double* out4);
+/* Line density of the last completed turn: integer bin counts (nbins). */
+hj_status hj_bunch_histogram(hj_bunch* b, int64_t* counts_host);
+/* Potential at the bin centers from the last completed turn (nbins). */
+hj_status hj_bunch_potential(hj_bunch* b, double* pot_host);
+void hj_bunch_destroy(hj_bunch* b);
+
+/* ---------------------------------------------------------------- single steps (host buffers) */
+
+/* rf_kick!(voltage, sin_ϕs, rf_factor, ϕs, particles, buffers)
+ * (src/rf_kick.jl:18-25, body :84-87): dE += V (sin(-z k + ϕs) - sin ϕs). */
+hj_status hj_rf_kick(hj_ctx* ctx, double voltage, double sin_phis, double rf_factor,
+                     double phi_s, const double* z, double* dE, int64_t n);
+
+/* quantum_excitation!(E0, radius, σ_E0, buffers, particles)
+ * (src/quantum_excitation.jl:24-30, :58-71).  draws: host array of n normals
+ * or NULL for Philox(seed, particle, turn). */
+hj_status hj_quantum_excitation(hj_ctx* ctx, double E0, double radius, double sigma_E0,
+                                const double* draws, uint64_t seed, int64_t turn,
+                                double* dE, int64_t n);
+
+/* synchrotron_radiation!(E0, radius, particles, buffers)
+ * (src/synchrotron_radiation.jl:12-17, :44-56): dE *= 1 - 4*8.85e-5*(E0/1e9)^3/radius. */
+hj_status hj_synchrotron_radiation(hj_ctx* ctx, double E0, double radius, double* dE,
+                                   int64_t n);
+
+/* Phase advance of longitudinal_evolve!: update_eta != 0 is the inline loop
+ * at src/evolution.jl:331-344; update_eta == 0 is apply_phase_advance!
+ * (src/evolution.jl:143-167, skipped for non-physical beta0/E0/rf_factor). */
+hj_status hj_phase_advance(hj_ctx* ctx, int32_t update_eta, double E0, double mass,
+                           double alpha_c, int64_t harmonic, double phi_s,
+                           double freq_rf, const double* dE, double* z, int64_t n);
+
+/* calculate_local_histogram! (src/utils.jl:351-401): counts[nbins] of z. */
+hj_status hj_histogram(hj_ctx* ctx, const double* z, int64_t n, const hj_grid* grid,
+                       int64_t* counts);
+
+/* The convolution of apply_wakefield_inplace! (MPI branch,
+ * src/wakefield.jl:186-327): potential at the bin centers from integer
+ * counts, pot = Re(IFFT(FFT(W) FFT(delta*counts/sum(counts)) * current)). */
+hj_status hj_wake_potential(hj_ctx* ctx, const int64_t* counts, const hj_grid* grid,
+                            const hj_wake* wake, double current, double* pot);
+
+/* apply_wakefield_inplace!(particles, buffers, wake_factor, wake_sqrt, cτ,
+ * current, sigma_z, bin_edges, bin_centers, comm, use_mpi=true)
+ * (src/wakefield.jl:137-345): histogram, convolution, interpolation
+ * (src/wakefield.jl:22-105) and dE -= potential.  sigma_z is accepted for
+ * signature parity and, as in the reference's MPI branch, unused. */
+hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE, int64_t n,
+                             const hj_wake* wake, double current, double sigma_z,
+                             const hj_grid* grid);
+
+/* The Philox-4x32-10 standard normals used for quantum excitation:
+ * out[i] = N(0,1) draw of particle i at `turn` under `seed`.  No reference
+ * counterpart (the reference calls randn!, src/quantum_excitation.jl:36). */
+hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64_t n, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HAISSINSKI_GPU_H */
