@@ -239,9 +239,10 @@ void fill_result(hj_bunch* b, const double m[4], hj_result* res) {
   res->turns = b->turns_done;
 }
 
-void set_kernel_attributes(hj_ctx* ctx) {
-  prepare_track_kernels(ctx->max_smem_optin);
-  prepare_wake_kernels(ctx->max_smem_optin);
+cudaError_t set_kernel_attributes(hj_ctx* ctx) {
+  cudaError_t e = prepare_track_kernels(ctx->max_smem_optin);
+  if (e == cudaSuccess) e = prepare_wake_kernels(ctx->max_smem_optin);
+  return e;
 }
 
 }  // namespace
@@ -279,7 +280,10 @@ extern "C" hj_status hj_create(int32_t device, hj_ctx** out) {
   ctx->device = device;
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-  set_kernel_attributes(ctx);
+  if (set_kernel_attributes(ctx) != cudaSuccess) {
+    delete ctx;
+    return HJ_ERR_CUDA;
+  }
   *out = ctx;
   return HJ_OK;
 }

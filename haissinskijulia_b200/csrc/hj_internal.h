@@ -85,7 +85,8 @@ struct FlushArgs {
 };
 
 // ---- launchers (hj_track.cu) ----
-void prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
+cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin);
+cudaError_t prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
 int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm);
 int track_blocks_per_sm(int B, int qe_mode, int use_wake);
 size_t track_smem_bytes(int B, int use_wake);
@@ -112,7 +113,7 @@ cudaError_t launch_gaussian(uint64_t seed, int64_t turn, int64_t n, double* out,
                             cudaStream_t st);
 
 // ---- launchers (hj_wake.cu) ----
-void prepare_wake_kernels(int max_smem);    // once per device: dynamic smem limits
+cudaError_t prepare_wake_kernels(int max_smem);    // once per device: dynamic smem limits
 cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, int logH,
                                  const double2* twP, double2* Xg, double2* Wf,
                                  cudaStream_t st);

@@ -410,7 +410,17 @@ int elementwise_grid(int64_t n) {
 
 }  // namespace
 
-void prepare_track_kernels(int max_smem) {
+// Raise a kernel's dynamic shared-memory limit to what the device allows
+// beside the kernel's own static shared memory.
+cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin) {
+  cudaFuncAttributes attr{};
+  cudaError_t e = cudaFuncGetAttributes(&attr, fn);
+  if (e != cudaSuccess) return e;
+  const int dyn = max_smem_optin - (int)attr.sharedSizeBytes;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn > 0 ? dyn : 0);
+}
+
+cudaError_t prepare_track_kernels(int max_smem) {
   const void* fns[] = {(const void*)k_track_pass<true, QE_OFF>,
                        (const void*)k_track_pass<true, QE_PHILOX>,
                        (const void*)k_track_pass<true, QE_DRAWS>,
@@ -418,8 +428,11 @@ void prepare_track_kernels(int max_smem) {
                        (const void*)k_track_pass<false, QE_PHILOX>,
                        (const void*)k_track_pass<false, QE_DRAWS>,
                        (const void*)k_histogram};
-  for (const void* f : fns)
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  for (const void* f : fns) {
+    cudaError_t e = allow_dynamic_smem(f, max_smem);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 size_t track_smem_bytes(int B, int use_wake) {

@@ -307,16 +307,19 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
     ts->last_n_in = sh[3];
     ts->turn = ts->turn + 1;
     ts->cur = make_turn_scalars(E0n, a.params, a.sigma_E0_initial);
-    if (!isfinite(mean) || !isfinite(sh[5]) || !isfinite(current))
+    // Flag what the turn actually used: a NaN current with no particle in
+    // range never reaches the bunch (src/wakefield.jl:305-311).
+    if (!isfinite(mean) || (a.use_wake && !isfinite(sh[5])) || (do_conv && !isfinite(current)))
       ts->status |= (1 << HJ_ERR_NONFINITE);
   }
 }
 
 }  // namespace
 
-void prepare_wake_kernels(int max_smem) {
-  cudaFuncSetAttribute(k_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-  cudaFuncSetAttribute(k_wake_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+cudaError_t prepare_wake_kernels(int max_smem) {
+  cudaError_t e = allow_dynamic_smem((const void*)k_bins, max_smem);
+  if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_wake_spectrum, max_smem);
+  return e;
 }
 
 size_t bins_smem_bytes(int H) { return (size_t)(H < 4 ? 4 : H) * sizeof(double2); }
