@@ -204,9 +204,11 @@ def test_single_particle_with_wake(gpu_ctx, oracle):
     assert r.E0 == pytest.approx(ro.E0, rel=1e-12)
     assert p.coordinates.dE[0] == pytest.approx(eo[0], rel=1e-12)
 
-    zo, eo = np.array([0.0]), np.array([1e5])
-    rc, ro = oracle.evolve(zo, eo, cfg.params.to_c(), cfg.wake.to_c(), 16)
+    # at rest on the synchronous particle (no QE): z stays 0, inside the bins
+    quiet = cfg.params.replace(use_excitation=False)
+    zo, eo = np.array([0.0]), np.array([0.0])
+    rc, ro = oracle.evolve(zo, eo, quiet.to_c(), cfg.wake.to_c(), 16)
     assert rc == 0 and math.isnan(ro.E0)
-    p = Particles(np.array([0.0]), np.array([1e5]))
+    p = Particles(np.array([0.0]), np.array([0.0]))
     with pytest.raises(HaissinskiError, match="HJ_ERR_NONFINITE"):
-        longitudinal_evolve(p, cfg.params, buf, wake=cfg.wake)
+        longitudinal_evolve(p, quiet, buf, wake=cfg.wake)
