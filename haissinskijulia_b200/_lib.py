@@ -126,6 +126,8 @@ SIGNATURES = {
     "hj_histogram": (c_int32, [_CTX, _DP, c_int64, POINTER(HjGrid), _IP]),
     "hj_wake_potential": (c_int32, [_CTX, _IP, POINTER(HjGrid), POINTER(HjWake), c_double,
                                     _DP]),
+    "hj_wake_potential_noalloc": (c_int32, [_CTX, c_void_p, POINTER(HjGrid), POINTER(HjWake),
+                                            c_double, c_void_p, c_void_p]),
     "hj_apply_wakefield": (c_int32, [_CTX, _DP, _DP, c_int64, POINTER(HjWake), c_double,
                                      c_double, POINTER(HjGrid)]),
     "hj_gaussian": (c_int32, [_CTX, c_uint64, c_int64, c_int64, _DP]),

@@ -22,7 +22,7 @@ INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libhaissinski_gpu.so"
 
-CU_SOURCES = ["hj_track.cu", "hj_wake.cu", "hj_api.cu"]
+CU_SOURCES = ["hj_track.cu", "hj_wake.cu", "hj_api.cu", "hj_noalloc.cu"]
 CPP_SOURCES = ["hj_host.cpp"]
 HEADERS = ["hj_device.cuh", "hj_internal.h", "hj_host.h"]
 

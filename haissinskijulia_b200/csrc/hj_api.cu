@@ -249,6 +249,13 @@ cudaError_t set_kernel_attributes(hj_ctx* ctx) {
 
 // ====================================================================== context
 
+int hj::ctx_device(const hj_ctx* ctx) { return ctx->device; }
+
+hj_status hj::ctx_set_error(hj_ctx* ctx, hj_status code, const char* msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
 extern "C" const char* hj_version(void) { return kVersion; }
 
 extern "C" const char* hj_status_string(hj_status s) {

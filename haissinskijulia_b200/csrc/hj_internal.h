@@ -120,4 +120,8 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st);
 size_t bins_smem_bytes(int H);
 
+// ---- context access for entry points outside hj_api.cu ----
+int ctx_device(const hj_ctx* ctx);
+hj_status ctx_set_error(hj_ctx* ctx, hj_status code, const char* msg);
+
 }  // namespace hj

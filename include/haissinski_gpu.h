@@ -271,6 +271,26 @@ hj_status hj_histogram(hj_ctx* ctx, const double* z, int64_t n, const hj_grid* g
 hj_status hj_wake_potential(hj_ctx* ctx, const int64_t* counts, const hj_grid* grid,
                             const hj_wake* wake, double current, double* pot);
 
+/* Same potential as hj_wake_potential, on DEVICE buffers, with no allocation.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * those whose device memory is all owned by another allocator (a framework's
+ * pool, a fixed arena sized at start-up), and latency-critical loops, since
+ * cudaMalloc/cudaFree can synchronise the device.  It calls no
+ * cudaMalloc/cudaFree and keeps its FFT tables and work space in one static
+ * device array of about 1.4 MB that every GPU loading the library holds
+ * until exit.  Limit: nbins <= 16384 (HJ_ERR_TOO_LARGE beyond).
+ *   d_counts  device array of nbins non-negative bin counts;
+ *   grid      host struct and host centres (copied into the static array);
+ *   d_pot     device array of nbins doubles, written on `stream`.
+ * The work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) and is complete when that stream is.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the array: calls
+ * whose work overlaps on the GPU race, so serialise them. */
+hj_status hj_wake_potential_noalloc(hj_ctx* ctx, const int64_t* d_counts, const hj_grid* grid,
+                                    const hj_wake* wake, double current, double* d_pot,
+                                    void* stream);
+
 /* apply_wakefield_inplace!(particles, buffers, wake_factor, wake_sqrt, cτ,
  * current, sigma_z, bin_edges, bin_centers, comm, use_mpi=true)
  * (src/wakefield.jl:137-345): histogram, convolution, interpolation
