@@ -48,8 +48,7 @@ struct hj_bunch {
   // device buffers
   TurnState* ts = nullptr;
   double* pot = nullptr;
-  unsigned long long* cnt = nullptr;
-  unsigned long long* cic = nullptr;
+  unsigned long long* hist = nullptr;   // counts[B] | CIC counts[B] | CIC Σw·2^24 [B]
   double* lam = nullptr;
   double* W = nullptr;
   double2* Wf = nullptr;
@@ -310,8 +309,8 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   if (!b) return;
   cudaSetDevice(b->ctx->device);
   cudaStreamSynchronize(b->stream);
-  void* dev[] = {b->ts,  b->pot, b->cnt, b->cic,      b->lam,      b->W,        b->Wf,
-                 b->twP, b->Xg,  b->zE,  b->part_cnt, b->part_cic, b->part_sum, b->part_mom};
+  void* dev[] = {b->ts,  b->pot, b->hist, b->lam,      b->W,        b->Wf,
+                 b->twP, b->Xg,  b->zE,   b->part_cnt, b->part_cic, b->part_sum, b->part_mom};
   for (void* p : dev)
     if (p) cudaFree(p);
   if (b->h_mom) cudaFreeHost(b->h_mom);
@@ -398,13 +397,12 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     HJ_TRY(dalloc(ctx, &b->Xg, b->M));
     HJ_TRY(dalloc(ctx, &b->zE, std::max(b->H, 1)));
     HJ_TRY(dalloc(ctx, &b->pot, B));
-    HJ_TRY(dalloc(ctx, &b->cnt, B));
-    HJ_TRY(dalloc(ctx, &b->cic, B));
+    HJ_TRY(dalloc(ctx, &b->hist, 3 * (size_t)B));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->W, W.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, lam.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->twP, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->pot, 0, sizeof(double) * B, b->stream));
-    HJ_CUDA(ctx, cudaMemsetAsync(b->cnt, 0, sizeof(unsigned long long) * B, b->stream));
+    HJ_CUDA(ctx, cudaMemsetAsync(b->hist, 0, sizeof(unsigned long long) * 3 * B, b->stream));
     if (b->H >= 4)
       HJ_CUDA(ctx, launch_wake_spectrum(b->W, B, b->P, b->M, b->H, b->logH, b->twP, b->Xg,
                                         b->Wf, b->stream));
@@ -502,6 +500,7 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   a.part_cnt = b->part_cnt;
   a.part_cic = b->part_cic;
   a.part_sum = b->part_sum;
+  a.hist_out = b->hist;
 
   BinsArgs g{};
   g.ts = b->ts;
@@ -517,8 +516,8 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   g.M = b->M;
   g.H = b->H;
   g.logH = b->logH;
-  g.cnt = b->cnt;
-  g.cic = b->cic;
+  g.cnt = b->hist;
+  g.cic = b->hist ? b->hist + b->B : nullptr;
   g.lam = b->lam;
   g.Wf = b->Wf;
   g.twP = b->twP;
@@ -543,7 +542,7 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
     HJ_CUDA(ctx, launch_track_pass(a, b->nblk, b->stream));
     if (b->profiling) HJ_CUDA(ctx, cudaEventRecord(ev[1], b->stream));
     if (b->use_wake)
-      HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->cnt, b->cic,
+      HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->hist, false,
                                       b->stream));
     HJ_CUDA(ctx, launch_bins(g, b->stream));
     if (b->profiling) {
@@ -615,7 +614,7 @@ extern "C" hj_status hj_bunch_histogram(hj_bunch* b, int64_t* counts_host) {
   if (!b || !counts_host) return HJ_ERR_ARG;
   HJ_TRY(ctx_ok(b->ctx));
   if (!b->use_wake) return set_err(b->ctx, HJ_ERR_STATE, "bunch has no wakefield histogram");
-  HJ_CUDA(b->ctx, cudaMemcpyAsync(counts_host, b->cnt, sizeof(int64_t) * b->B,
+  HJ_CUDA(b->ctx, cudaMemcpyAsync(counts_host, b->hist, sizeof(int64_t) * b->B,
                                   cudaMemcpyDeviceToHost, b->stream));
   HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
   return HJ_OK;
@@ -813,7 +812,7 @@ hj_status device_histogram(hj_ctx* ctx, const double* d_z, int64_t n, const hj_g
   const int B = (int)grid->nbins;
   HJ_CUDA(ctx, launch_histogram_only(d_z, n, B, grid->edge_first, grid->edge_last,
                                      1.0 / grid->edge_step, part, nblk, ctx->stream));
-  HJ_CUDA(ctx, launch_hist_reduce(part, nullptr, nblk, B, dcnt, nullptr, ctx->stream));
+  HJ_CUDA(ctx, launch_hist_reduce(part, nullptr, nblk, B, dcnt, true, ctx->stream));
   return HJ_OK;
 }
 

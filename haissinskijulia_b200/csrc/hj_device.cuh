@@ -27,6 +27,7 @@ struct TurnScalars {
   double beta0;
   double eta0;
   double sin_phis;
+  double cos_phis;
   double k;           // rf_factor = 2π f_rf / (β0 c)
   double inv_k;
   double excitation;  // sqrt(1-(1-∂U/∂E)^2) σ_E0_initial
@@ -62,6 +63,7 @@ __host__ __device__ inline TurnScalars make_turn_scalars(double E0, const hj_par
   s.beta0 = sqrt(b2 > 0.0 ? b2 : 0.0);
   s.eta0 = p.alpha_c - (1.0 / (s.gamma0 * s.gamma0));
   s.sin_phis = sin(p.phi_s);
+  s.cos_phis = cos(p.phi_s);
   s.k = (s.beta0 <= 0.0) ? (1.0 / 0.0) : p.freq_rf * kTwoPi / (s.beta0 * kSpeedLight);
   s.inv_k = 1.0 / s.k;
   double t = E0 / 1e9;
@@ -110,24 +112,28 @@ __host__ __device__ inline U32x4 philox4x32_10(U32x4 c, uint32_t k0, uint32_t k1
 
 // Four standard normals for particles 4q..4q+3 at `turn`: counter
 // (q_lo, q_hi, turn_lo, turn_hi), key (seed_lo, seed_hi); Box-Muller on
-// (x,y) and (z,w) with uniforms in (0,1).  The transform runs in single
-// precision (accurate logf/sincospif, not the fast intrinsics); the normals
-// are widened to double before they scale the Float64 kick.
+// (x,y) and (z,w) with uniforms u in (0,1): r = sqrt(-2 ln u1),
+// θ = 2π (u2 - 1/2) in (-π, π).  The transform runs in single precision on the
+// special-function unit (__logf, __sincosf: absolute error below 2^-21 on
+// these ranges), and the normals are widened to double before they scale the
+// Float64 kick; the statistical quality of the variates is unaffected at the
+// 1e-6 level.
 __device__ __forceinline__ void philox_normals4(uint64_t seed, int64_t turn, int64_t q,
                                                 double out[4]) {
   U32x4 c{(uint32_t)q, (uint32_t)((uint64_t)q >> 32), (uint32_t)turn,
           (uint32_t)((uint64_t)turn >> 32)};
   U32x4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
   const float kScale = 2.3283064365386963e-10f;  // 2^-32
-  float u1 = fmaf((float)r.x, kScale, 0.5f * kScale);
-  float u2 = fmaf((float)r.y, kScale, 0.5f * kScale);
-  float u3 = fmaf((float)r.z, kScale, 0.5f * kScale);
-  float u4 = fmaf((float)r.w, kScale, 0.5f * kScale);
-  float ra = sqrtf(-2.0f * logf(u1));
-  float rb = sqrtf(-2.0f * logf(u3));
+  const float kTwoPiF = 6.2831853071795865f;
+  const float u1 = fmaf((float)r.x, kScale, 0.5f * kScale);
+  const float u3 = fmaf((float)r.z, kScale, 0.5f * kScale);
+  const float ta = kTwoPiF * fmaf((float)r.y, kScale, -0.5f);
+  const float tb = kTwoPiF * fmaf((float)r.w, kScale, -0.5f);
+  const float ra = sqrtf(-2.0f * __logf(u1));
+  const float rb = sqrtf(-2.0f * __logf(u3));
   float sa, ca, sb, cb;
-  sincospif(2.0f * u2, &sa, &ca);
-  sincospif(2.0f * u4, &sb, &cb);
+  __sincosf(ta, &sa, &ca);
+  __sincosf(tb, &sb, &cb);
   out[0] = (double)(ra * ca);
   out[1] = (double)(ra * sa);
   out[2] = (double)(rb * cb);

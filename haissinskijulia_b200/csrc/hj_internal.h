@@ -13,6 +13,9 @@ constexpr int kNumSums = 4;         // per-block partial sums of the particle pa
 constexpr int kTrackThreads = 512;  // threads per block of the particle kernels
 constexpr int kBinsThreads = 1024;  // threads of the single-CTA bins kernel
 constexpr int64_t kMaxBins = 16384; // largest grid the shared-memory FFT holds (P = 32768)
+// Particles one block of the fused pass may deposit per turn (the packed CIC
+// counter keeps a 20-bit count per cell).
+constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 
 // Quantum-excitation source of the particle pass.
 enum QeMode { QE_OFF = 0, QE_PHILOX = 1, QE_DRAWS = 2 };
@@ -38,8 +41,9 @@ struct PassArgs {
   int64_t draws_turns;
   // per-block outputs
   uint32_t* part_cnt;              // [grid][B]
-  unsigned long long* part_cic;    // [grid][B]
+  unsigned long long* part_cic;    // [grid][B] packed CIC (count << 44 | Σw·2^24)
   double* part_sum;                // [grid][kNumSums]
+  unsigned long long* hist_out;    // [3B] merged histograms, zeroed by the pass
 };
 
 // Arguments of the per-turn bins step (single CTA).
@@ -53,8 +57,8 @@ struct BinsArgs {
   double population;
   int32_t use_wake;
   int32_t B, P, M, H, logH;
-  const unsigned long long* cnt;   // [B]
-  const unsigned long long* cic;   // [B]
+  const unsigned long long* cnt;   // [B] bin counts
+  const unsigned long long* cic;   // [2B] CIC counts | CIC Σw·2^24 (NULL: not needed)
   const double* lam;               // [B]
   const double2* Wf;               // [M+1]
   const double2* twP;              // [P]
@@ -91,9 +95,11 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm);
 int track_blocks_per_sm(int B, int qe_mode, int use_wake);
 size_t track_smem_bytes(int B, int use_wake);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
+// out: counts[B] (| CIC counts[B] | CIC Σw·2^24 [B] when part_cic != NULL);
+// zero_first clears out before the merge (the fused pass clears it itself).
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
-                               int nblk, int B, unsigned long long* cnt,
-                               unsigned long long* cic, cudaStream_t st);
+                               int nblk, int B, unsigned long long* out, bool zero_first,
+                               cudaStream_t st);
 cudaError_t launch_flush(const FlushArgs& a, int grid, cudaStream_t st);
 cudaError_t launch_histogram_only(const double* z, int64_t n, int B, double e0, double eN,
                                   double inv_estep, uint32_t* part_cnt, int grid,

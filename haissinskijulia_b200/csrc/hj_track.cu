@@ -18,18 +18,39 @@
 //
 // Each thread owns four consecutive particles and moves them with one
 // 32-byte load/store per array (ld.global.v4.f64), so a warp touches 1 KB of
-// contiguous HBM per array per iteration.  Histograms are privatised in
-// shared memory per block and written out as per-block partials; the
-// reduction over blocks is a separate, deterministic kernel.
+// contiguous HBM per array per iteration; the next quad is loaded while the
+// current one is computed.  Histograms are privatised in shared memory per
+// block and written out as per-block partials, merged by k_hist_reduce.
+//
+// Per-particle arithmetic of the fused pass (the single-step kernels further
+// down keep the reference's exact operation order instead):
+//   * RF kick: V(sin(ϕs - x) - sin ϕs) = V sin ϕs (cos x - 1) - V cos ϕs sin x with
+//     x = z k, sin x and cos x - 1 from their Taylor series through x^15 and
+//     x^16 when |x| <= 0.5 (truncation error < 3e-20); the general sin() path
+//     otherwise.  This avoids the cancellation of sin(ϕ) - sin ϕs.
+//   * 1/γ² of the drift: rcp.approx.ftz.f64 refined by two Newton steps
+//     (relative error at double rounding level).
+//   * reciprocals of k, mass and β0²E0 are precomputed per turn.
 #include "hj_internal.h"
 
 namespace hj {
 namespace {
 
-struct PassConst {
-  double V, phi_s, sin_phis, k, inv_k, excitation, damping, gamma0, inv_mass, alpha_c,
-      two_pi_h, inv_b2E0, coeff0;
+// Run- and turn-constants of the fused pass.
+struct FusedConst {
+  double Vs, Vc;            // V sin ϕs, V cos ϕs
+  double V, phi_s, sin_phis;
+  double k, inv_k;
+  double excitation, damping;
+  double gamma0, inv_mass, alpha_c, K;   // K = 2π h / (β0² E0)
+  double coeff0;            // K η0 (constant-η drift)
   int drift_ok, update_eta, sr;
+};
+
+// Constants of the single-step phase-advance kernel (reference operation order).
+struct StepConst {
+  double phi_s, k, inv_k, gamma0, inv_mass, alpha_c, two_pi_h, inv_b2E0, coeff0;
+  int drift_ok, update_eta;
 };
 
 struct GridConst {
@@ -37,10 +58,17 @@ struct GridConst {
   double e0, eN, inv_e, c1, cB, inv_c;
 };
 
+// Packed CIC accumulator: particle count in the top 20 bits, Σ w·2^24 in the
+// low 44 bits.  A block deposits at most kMaxBlockParticles particles per
+// turn, so neither field can overflow.
+constexpr int kCicWeightBits = 24;
+constexpr int kCicSumBits = 44;
+constexpr unsigned long long kCicSumMask = (1ull << kCicSumBits) - 1ull;
+
 __device__ __forceinline__ void ld4(const double* p, double v[4]) {
   asm("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
-               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
-               : "l"(p));
+      : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+      : "l"(p));
 }
 
 __device__ __forceinline__ void st4(double* p, const double v[4]) {
@@ -49,8 +77,16 @@ __device__ __forceinline__ void st4(double* p, const double v[4]) {
                : "memory");
 }
 
+__device__ __forceinline__ double rcp_approx(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  return r;
+}
+
 // Interpolation cell of z on the bin centers (src/wakefield.jl:64-78), 0-based:
 // idx = clamp(floor(u), 0, B-2), w = u - floor(u), u = (clamp(z,c1,cB)-c1)/Δc.
+// The deposit of turn t and the kick applied in turn t+1 call this with the
+// same z, so they agree exactly.
 __device__ __forceinline__ void cic_cell(double z, const GridConst& g, int& idx, double& w) {
   double cl = z > g.cB ? g.cB : (z < g.c1 ? g.c1 : z);
   double u = __dmul_rn(__dsub_rn(cl, g.c1), g.inv_c);
@@ -78,47 +114,81 @@ __device__ __forceinline__ int ngp_bin(double z, const GridConst& g, bool& in) {
   return (u >= 0.0) ? (u < (double)g.B ? (int)u : g.B - 1) : 0;
 }
 
-// RF kick, QE, SR and drift of one particle for one turn.
+// V(sin(ϕs - x) - sin ϕs) for |x| > 0.5, as the reference forms it.
+__device__ __noinline__ double rf_kick_general(double z, double k, double phi_s,
+                                               double sin_phis, double V) {
+  return V * (sin(fma(-z, k, phi_s)) - sin_phis);
+}
+
+// V(sin(ϕs - x) - sin ϕs), x = z k, by angle addition and Taylor series.
+__device__ __forceinline__ double rf_kick_term(double z, const FusedConst& c) {
+  const double x = z * c.k;
+  if (!(fabs(x) <= 0.5)) return rf_kick_general(z, c.k, c.phi_s, c.sin_phis, c.V);
+  const double t = x * x;
+  // sin x = x + x^3 P(t): coefficients (-1)^n / (2n+1)!, n = 1..7
+  double p = -7.647163731819816e-13;          // -1/15!
+  p = fma(t, p, 1.6059043836821613e-10);      // +1/13!
+  p = fma(t, p, -2.505210838544172e-08);      // -1/11!
+  p = fma(t, p, 2.7557319223985893e-06);      // +1/9!
+  p = fma(t, p, -1.984126984126984e-04);      // -1/7!
+  p = fma(t, p, 8.333333333333333e-03);       // +1/5!
+  p = fma(t, p, -1.6666666666666666e-01);     // -1/3!
+  const double sn = fma(t * x, p, x);
+  // cos x - 1 = t Q(t): coefficients (-1)^n / (2n)!, n = 1..8
+  double q = 4.779477332387385e-14;           // +1/16!
+  q = fma(t, q, -1.1470745597729725e-11);     // -1/14!
+  q = fma(t, q, 2.08767569878681e-09);        // +1/12!
+  q = fma(t, q, -2.755731922398589e-07);      // -1/10!
+  q = fma(t, q, 2.48015873015873e-05);        // +1/8!
+  q = fma(t, q, -1.388888888888889e-03);      // -1/6!
+  q = fma(t, q, 4.1666666666666664e-02);      // +1/4!
+  q = fma(t, q, -0.5);                        // -1/2!
+  const double cm1 = t * q;
+  return fma(c.Vs, cm1, -c.Vc * sn);
+}
+
+// RF kick, QE, SR and drift of one particle for one turn (fused-pass arithmetic).
 __device__ __forceinline__ void turn_particle(double& z, double& e, double r, bool qe,
-                                              const PassConst& c) {
-  double phi = __dadd_rn(__dmul_rn(-z, c.k), c.phi_s);
-  e = __dadd_rn(e, __dmul_rn(c.V, __dsub_rn(sin(phi), c.sin_phis)));
-  if (qe) e = __dadd_rn(e, __dmul_rn(c.excitation, r));
-  if (c.sr) e = __dmul_rn(e, c.damping);
+                                              const FusedConst& c) {
+  e = e + rf_kick_term(z, c);
+  if (qe) e = fma(c.excitation, r, e);
+  if (c.sr) e = e * c.damping;
+  double coeff;
   if (c.update_eta) {
-    double dg = __dmul_rn(e, c.inv_mass);
-    double gp = __dadd_rn(c.gamma0, dg);
-    double eta = __dsub_rn(c.alpha_c, 1.0 / __dmul_rn(gp, gp));
-    double coeff = __dmul_rn(__dmul_rn(c.two_pi_h, eta), c.inv_b2E0);
-    double ph = -__dsub_rn(__dmul_rn(z, c.k), c.phi_s);
-    ph = __dadd_rn(ph, __dmul_rn(coeff, e));
-    z = __dmul_rn(__dadd_rn(-ph, c.phi_s), c.inv_k);
-  } else if (c.drift_ok) {
-    double ph = -__dsub_rn(__dmul_rn(z, c.k), c.phi_s);
-    ph = __dadd_rn(ph, __dmul_rn(c.coeff0, e));
-    z = __dmul_rn(__dadd_rn(-ph, c.phi_s), c.inv_k);
+    const double gp = fma(e, c.inv_mass, c.gamma0);   // γ0 + ΔE/m
+    const double g2 = gp * gp;
+    double ri = rcp_approx(g2);
+    ri = fma(ri, fma(-g2, ri, 1.0), ri);
+    ri = fma(ri, fma(-g2, ri, 1.0), ri);
+    coeff = c.K * (c.alpha_c - ri);                    // 2π h η_i / (β0² E0)
+  } else {
+    if (!c.drift_ok) return;                           // apply_phase_advance! skip
+    coeff = c.coeff0;
   }
+  double ph = fma(-z, c.k, c.phi_s);                   // ϕ = -(z k - ϕs)
+  ph = fma(coeff, e, ph);
+  z = (c.phi_s - ph) * c.inv_k;                        // z = (-ϕ + ϕs)/k
 }
 
 template <bool WAKE>
 __device__ __forceinline__ void pass_particle(double& z, double& e, double r, bool qe,
-                                              const PassConst& c, const GridConst& g,
+                                              const FusedConst& c, const GridConst& g,
                                               bool pending, bool upd_E0, double pmean,
                                               const double* __restrict__ pot, double& acc_z,
                                               double& acc_z2, double& acc_d, uint32_t& n_in,
                                               uint32_t* s_cnt, unsigned long long* s_cic) {
   if (pending) {
-    if (WAKE) e = __dsub_rn(e, wake_kick(z, g, pot));
-    if (upd_E0) e = __dsub_rn(e, pmean);
+    if (WAKE) e = e - wake_kick(z, g, pot);
+    if (upd_E0) e = e - pmean;
   }
   const double e_start = e;
   turn_particle(z, e, r, qe, c);
-  if (upd_E0) acc_d += __dsub_rn(e, e_start);
+  if (upd_E0) acc_d += e - e_start;
   if (WAKE) {
     acc_z += z;
     acc_z2 = fma(z, z, acc_z2);
     bool in;
-    int j = ngp_bin(z, g, in);
+    const int j = ngp_bin(z, g, in);
     if (in) {
       atomicAdd(&s_cnt[j], 1u);
       ++n_in;
@@ -127,12 +197,10 @@ __device__ __forceinline__ void pass_particle(double& z, double& e, double r, bo
       int idx;
       double w;
       cic_cell(z, g, idx, w);
-      unsigned long long q = __double2ull_rn(w * 4294967296.0);
-      if (!(w >= 0.0)) q = 0ull;  // NaN z: deposit in the first cell, flagged by the moments
-      atomicAdd(&s_cic[idx], (1ull << 32) - q);
-      atomicAdd(&s_cic[idx + 1], q);
+      unsigned long long q = (w >= 0.0) ? (unsigned long long)__double2uint_rn(w * 16777216.0) : 0ull;
+      atomicAdd(&s_cic[idx], (1ull << kCicSumBits) + q);
     } else {
-      atomicAdd(&s_cic[0], 1ull << 32);
+      atomicAdd(&s_cic[0], 1ull << kCicSumBits);
     }
   }
 }
@@ -167,7 +235,7 @@ __device__ __forceinline__ void block_sum4(double a0, double a1, double a2, doub
 }
 
 template <bool WAKE, int QE>
-__global__ void __launch_bounds__(kTrackThreads) k_track_pass(PassArgs a) {
+__global__ void __launch_bounds__(kTrackThreads, 1) k_track_pass(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned long long* s_cic = reinterpret_cast<unsigned long long*>(smem_raw);
   uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_cic + (WAKE ? a.B : 0));
@@ -179,10 +247,12 @@ __global__ void __launch_bounds__(kTrackThreads) k_track_pass(PassArgs a) {
   const int64_t turn = ts->turn;
   const bool upd_E0 = a.update_E0 != 0;
 
-  PassConst c;
+  FusedConst c;
   c.V = a.V;
   c.phi_s = a.phi_s;
   c.sin_phis = sc.sin_phis;
+  c.Vs = a.V * sc.sin_phis;
+  c.Vc = a.V * sc.cos_phis;
   c.k = sc.k;
   c.inv_k = sc.inv_k;
   c.excitation = sc.excitation;
@@ -190,8 +260,7 @@ __global__ void __launch_bounds__(kTrackThreads) k_track_pass(PassArgs a) {
   c.gamma0 = sc.gamma0;
   c.inv_mass = a.inv_mass;
   c.alpha_c = a.alpha_c;
-  c.two_pi_h = a.two_pi_h;
-  c.inv_b2E0 = sc.inv_b2E0;
+  c.K = a.two_pi_h * sc.inv_b2E0;
   c.coeff0 = sc.coeff0;
   c.drift_ok = sc.drift_ok;
   c.update_eta = a.update_eta;
@@ -213,6 +282,10 @@ __global__ void __launch_bounds__(kTrackThreads) k_track_pass(PassArgs a) {
       s_cic[i] = 0ull;
       s_cnt[i] = 0u;
     }
+    // zero the merged histograms k_hist_reduce accumulates into this turn
+    const int gstride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * a.B; i += gstride)
+      a.hist_out[i] = 0ull;
     __syncthreads();
   }
 
@@ -221,10 +294,24 @@ __global__ void __launch_bounds__(kTrackThreads) k_track_pass(PassArgs a) {
   const double* __restrict__ pot = a.pot;
   const int64_t nq = a.n >> 2;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double zn[4], en[4];
+  if (q < nq) {
+    ld4(a.z + 4 * q, zn);
+    ld4(a.dE + 4 * q, en);
+  }
+  for (; q < nq; q += stride) {
     double zz[4], ee[4], rr[4] = {0.0, 0.0, 0.0, 0.0};
-    ld4(a.z + 4 * q, zz);
-    ld4(a.dE + 4 * q, ee);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      zz[j] = zn[j];
+      ee[j] = en[j];
+    }
+    const int64_t qn = q + stride;
+    if (qn < nq) {               // prefetch the next quad while this one is computed
+      ld4(a.z + 4 * qn, zn);
+      ld4(a.dE + 4 * qn, en);
+    }
     if (QE == QE_PHILOX) {
       philox_normals4(a.seed, turn, q, rr);
     } else if (QE == QE_DRAWS) {
@@ -267,20 +354,29 @@ __global__ void __launch_bounds__(kTrackThreads) k_track_pass(PassArgs a) {
   }
 }
 
-// Deterministic reduction of the per-block histograms (fixed block order).
+// Merge of the per-block histograms.  Grid (bins/256, G): block column g sums
+// the partials of blocks g, g+G, ... and adds them to the merged arrays with
+// integer atomics (exact, so the result does not depend on their order).
+// out layout (u64): counts[B] | CIC counts[B] | CIC Σw·2^24 [B].
 __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
                               const unsigned long long* __restrict__ part_cic, int nblk, int B,
-                              unsigned long long* __restrict__ cnt,
-                              unsigned long long* __restrict__ cic) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
+                              unsigned long long* __restrict__ out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
-  unsigned long long sc = 0ull, sq = 0ull;
-  for (int k = 0; k < nblk; ++k) {
+  unsigned long long sc = 0ull, sn = 0ull, sw = 0ull;
+  for (int k = blockIdx.y; k < nblk; k += gridDim.y) {
     sc += __ldg(part_cnt + (size_t)k * B + b);
-    if (part_cic) sq += __ldg(part_cic + (size_t)k * B + b);
+    if (part_cic) {
+      const unsigned long long v = __ldg(part_cic + (size_t)k * B + b);
+      sn += v >> kCicSumBits;
+      sw += v & kCicSumMask;
+    }
   }
-  cnt[b] = sc;
-  if (cic) cic[b] = sq;
+  if (sc) atomicAdd(out + b, sc);
+  if (part_cic) {
+    if (sn) atomicAdd(out + B + b, sn);
+    if (sw) atomicAdd(out + 2 * B + b, sw);
+  }
 }
 
 // Pending kick + re-centring (optional), copy-out (optional) and the moments
@@ -366,7 +462,7 @@ __global__ void k_sr(double damping, double* __restrict__ dE, int64_t n) {
     dE[i] = __dmul_rn(dE[i], damping);
 }
 
-__global__ void k_phase_advance(PassConst c, const double* __restrict__ dE,
+__global__ void k_phase_advance(StepConst c, const double* __restrict__ dE,
                                 double* __restrict__ z, int64_t n) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -466,6 +562,9 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm) {
   int64_t g = (n + per_block - 1) / per_block;
   int64_t cap = (int64_t)num_sms * blocks_per_sm;
   if (g > cap) g = cap;
+  // the packed CIC counter holds at most kMaxBlockParticles per block and turn
+  const int64_t need = (n + kMaxBlockParticles - 1) / kMaxBlockParticles;
+  if (g < need) g = need;
   if (g < 1) g = 1;
   return (int)g;
 }
@@ -489,9 +588,15 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
 }
 
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
-                               int nblk, int B, unsigned long long* cnt,
-                               unsigned long long* cic, cudaStream_t st) {
-  k_hist_reduce<<<(B + 255) / 256, 256, 0, st>>>(part_cnt, part_cic, nblk, B, cnt, cic);
+                               int nblk, int B, unsigned long long* out, bool zero_first,
+                               cudaStream_t st) {
+  if (zero_first) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long) * (part_cic ? 3 : 1) * B, st);
+    if (e != cudaSuccess) return e;
+  }
+  const int G = nblk < 16 ? nblk : 16;
+  dim3 grid((B + 255) / 256, G > 0 ? G : 1);
+  k_hist_reduce<<<grid, 256, 0, st>>>(part_cnt, part_cic, nblk, B, out);
   return cudaGetLastError();
 }
 
@@ -537,7 +642,7 @@ cudaError_t launch_sr(double damping, double* dE, int64_t n, cudaStream_t st) {
 cudaError_t launch_phase_advance(int update_eta, TurnScalars s, double inv_mass,
                                  double alpha_c, double two_pi_h, double phi_s,
                                  const double* dE, double* z, int64_t n, cudaStream_t st) {
-  PassConst c{};
+  StepConst c{};
   c.phi_s = phi_s;
   c.k = s.k;
   c.inv_k = s.inv_k;

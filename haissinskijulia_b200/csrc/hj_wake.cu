@@ -43,40 +43,76 @@ __device__ __forceinline__ int bitrev(int n, int logH) {
   return (int)(__brev((unsigned)n) >> (32 - logH));
 }
 
-// In-place radix-2 decimation-in-time FFT of size H on shared memory that
-// holds its input in bit-reversed order.  twP[k] = exp(-2πi k/P); the
-// twiddle of a length-len butterfly group is twP[j * P/len].  inverse uses
-// conjugate twiddles and no normalisation.
-__device__ void smem_fft(double2* s, int H, int P, const double2* __restrict__ twP,
-                         bool inverse) {
-  for (int len = 2; len <= H; len <<= 1) {
-    const int half = len >> 1;
-    const int tstride = P / len;
+// In-place decimation-in-time FFT of size H on shared memory that holds its
+// input in bit-reversed order.  tw[j] = exp(-2πi j/H), j < H/2, also in shared
+// memory.  Pairs of radix-2 stages are fused into radix-4 passes (each thread
+// keeps the four points of two consecutive stages in registers), so a
+// length-8192 transform takes 7 passes over shared memory instead of 13.
+// inverse uses conjugate twiddles and no normalisation.
+__device__ void smem_fft(double2* s, const double2* tw, int H, int logH, bool inverse) {
+  int h = 1;
+  int stage = 0;
+  for (; stage + 2 <= logH; stage += 2, h <<= 2) {
+    const int sa = H / (2 * h), sb = H / (4 * h);
+    for (int b = threadIdx.x; b < (H >> 2); b += blockDim.x) {
+      const int j = b & (h - 1);
+      const int i0 = ((b - j) << 2) + j;
+      double2 x0 = s[i0], x1 = s[i0 + h], x2 = s[i0 + 2 * h], x3 = s[i0 + 3 * h];
+      double2 wa = tw[j * sa], wb = tw[j * sb];
+      if (inverse) {
+        wa.y = -wa.y;
+        wb.y = -wb.y;
+      }
+      // span h: (x0, x1) and (x2, x3) with w_{2h}^j
+      double2 t = cmul(x1, wa);
+      x1 = csub(x0, t);
+      x0 = cadd(x0, t);
+      t = cmul(x3, wa);
+      x3 = csub(x2, t);
+      x2 = cadd(x2, t);
+      // span 2h: (x0, x2) with w_{4h}^j, (x1, x3) with w_{4h}^{j+h} = w_{4h}^j (-i or +i)
+      t = cmul(x2, wb);
+      s[i0] = cadd(x0, t);
+      s[i0 + 2 * h] = csub(x0, t);
+      t = cmul(x3, wb);
+      t = inverse ? make_double2(-t.y, t.x) : make_double2(t.y, -t.x);
+      s[i0 + h] = cadd(x1, t);
+      s[i0 + 3 * h] = csub(x1, t);
+    }
+    __syncthreads();
+  }
+  if (stage < logH) {  // odd number of stages: final radix-2 pass, span H/2
     for (int b = threadIdx.x; b < (H >> 1); b += blockDim.x) {
-      const int j = b & (half - 1);
+      const int j = b & (h - 1);
       const int i0 = ((b - j) << 1) + j;
-      const int i1 = i0 + half;
-      double2 w = __ldg(&twP[j * tstride]);
+      double2 w = tw[j * (H / (2 * h))];
       if (inverse) w.y = -w.y;
       const double2 u = s[i0];
-      const double2 t = cmul(s[i1], w);
+      const double2 t = cmul(s[i0 + h], w);
       s[i0] = cadd(u, t);
-      s[i1] = csub(u, t);
+      s[i0 + h] = csub(u, t);
     }
     __syncthreads();
   }
 }
 
+// Twiddles of the length-H transform into shared memory: w_H^j = twP[4j].
+__device__ void load_twiddles(double2* tw, int H, const double2* __restrict__ twP) {
+  for (int j = threadIdx.x; j < (H >> 1); j += blockDim.x) tw[j] = __ldg(&twP[4 * j]);
+  __syncthreads();
+}
+
 // X[0..M) = FFT_M(x), x[n] = v(2n) + i v(2n+1), v(j) = 0 for j >= L (L <= M).
 template <typename Vals>
 __device__ void forward_packed(const Vals& v, int L, int P, int H, int logH,
-                               const double2* __restrict__ twP, double2* s, double2* Xg) {
+                               const double2* __restrict__ twP, double2* s, const double2* tw,
+                               double2* Xg) {
   for (int n = threadIdx.x; n < H; n += blockDim.x) {
     const int j = 2 * n;
     s[bitrev(n, logH)] = make_double2(j < L ? v(j) : 0.0, j + 1 < L ? v(j + 1) : 0.0);
   }
   __syncthreads();
-  smem_fft(s, H, P, twP, false);
+  smem_fft(s, tw, H, logH, false);
   for (int m = threadIdx.x; m < H; m += blockDim.x) Xg[2 * m] = s[m];
   __syncthreads();
   for (int n = threadIdx.x; n < H; n += blockDim.x) {
@@ -85,7 +121,7 @@ __device__ void forward_packed(const Vals& v, int L, int P, int H, int logH,
     s[bitrev(n, logH)] = cmul(a, __ldg(&twP[2 * n]));  // w_M^n = w_P^{2n}
   }
   __syncthreads();
-  smem_fft(s, H, P, twP, false);
+  smem_fft(s, tw, H, logH, false);
   for (int m = threadIdx.x; m < H; m += blockDim.x) Xg[2 * m + 1] = s[m];
   __syncthreads();
 }
@@ -153,7 +189,9 @@ __global__ void __launch_bounds__(kBinsThreads)
     k_wake_spectrum(const double* __restrict__ W, int B, int P, int M, int H, int logH,
                     const double2* __restrict__ twP, double2* Xg, double2* Wf) {
   extern __shared__ __align__(16) double2 s_fft[];
-  forward_packed(WakeVals{W}, B, P, H, logH, twP, s_fft, Xg);
+  double2* s_tw = s_fft + H;
+  load_twiddles(s_tw, H, twP);
+  forward_packed(WakeVals{W}, B, P, H, logH, twP, s_fft, s_tw, Xg);
   for (int k = threadIdx.x; k <= M; k += blockDim.x) Wf[k] = real_spectrum(Xg, k, M, twP);
 }
 
@@ -246,13 +284,15 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
     } else {
       const double inv_n = 1.0 / sh[3];                          // src/wakefield.jl:207
       if (a.H >= 4) {
+        double2* s_tw = s_fft + a.H;
+        load_twiddles(s_tw, a.H, a.twP);
         forward_packed(DensityVals{a.cnt, a.lam, inv_n}, a.B, a.P, a.H, a.logH, a.twP, s_fft,
-                       a.Xg);
+                       s_tw, a.Xg);
         // inverse, even half -> zE
         for (int m = threadIdx.x; m < a.H; m += blockDim.x)
           s_fft[bitrev(m, a.logH)] = packed_inverse_input(a.Xg, a.Wf, 2 * m, a.M, current, a.twP);
         __syncthreads();
-        smem_fft(s_fft, a.H, a.P, a.twP, true);
+        smem_fft(s_fft, s_tw, a.H, a.logH, true);
         for (int m = threadIdx.x; m < a.H; m += blockDim.x) a.zE[m] = s_fft[m];
         __syncthreads();
         // inverse, odd half, combine, potential and Σ H[k] pot[k]
@@ -260,21 +300,15 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
           s_fft[bitrev(m, a.logH)] =
               packed_inverse_input(a.Xg, a.Wf, 2 * m + 1, a.M, current, a.twP);
         __syncthreads();
-        smem_fft(s_fft, a.H, a.P, a.twP, true);
+        smem_fft(s_fft, s_tw, a.H, a.logH, true);
         const double invM = 1.0 / (double)a.M;
         for (int m = threadIdx.x; m < a.H; m += blockDim.x) {
           const double2 zo = cmul(s_fft[m], cconj(__ldg(&a.twP[2 * m])));
           const double2 ze = a.zE[m];
           const double re = (ze.x + zo.x) * invM, im = (ze.y + zo.y) * invM;
           const int j = 2 * m;
-          if (j < a.B) {
-            a.pot[j] = re;
-            if (a.cic) sum_kick += (double)a.cic[j] * re;
-          }
-          if (j + 1 < a.B) {
-            a.pot[j + 1] = im;
-            if (a.cic) sum_kick += (double)a.cic[j + 1] * im;
-          }
+          if (j < a.B) a.pot[j] = re;
+          if (j + 1 < a.B) a.pot[j + 1] = im;
         }
       } else {
         // Tiny grids (P < 16): direct causal convolution.
@@ -284,13 +318,25 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
             for (int j = 0; j <= i; ++j)
               acc += a.W[j] * (a.lam[i - j] * ((double)a.cnt[i - j] * inv_n));
             a.pot[i] = acc * current;
-            if (a.cic) sum_kick += (double)a.cic[i] * a.pot[i];
           }
+        }
+      }
+      // Σ_i lerp(pot, z_i) from the CIC deposit: with C[k] particles in cell k
+      // and S[k] = Σ w·2^24 over them,
+      //   Σ_i lerp = Σ_k C[k] pot[k] + 2^-24 Σ_k S[k] (pot[k+1] - pot[k]).
+      __syncthreads();
+      if (a.cic) {
+        const unsigned long long* C = a.cic;
+        const unsigned long long* S = a.cic + a.B;
+        for (int k = threadIdx.x; k < a.B; k += blockDim.x) {
+          double t = (double)C[k] * a.pot[k];
+          if (k + 1 < a.B) t += (double)S[k] * 5.9604644775390625e-08 * (a.pot[k + 1] - a.pot[k]);
+          sum_kick += t;
         }
       }
     }
   }
-  sum_kick = block_sum(sum_kick, red) * 2.3283064365386963e-10;  // CIC weights carry 2^32
+  sum_kick = block_sum(sum_kick, red);
 
   // 4. E0 update and next-turn scalars (src/evolution.jl:401-451, :300-304)
   if (threadIdx.x == 0 && !a.conv_only) {
@@ -322,7 +368,11 @@ cudaError_t prepare_wake_kernels(int max_smem) {
   return e;
 }
 
-size_t bins_smem_bytes(int H) { return (size_t)(H < 4 ? 4 : H) * sizeof(double2); }
+// FFT data (H complex) + twiddles (H/2 complex).
+size_t bins_smem_bytes(int H) {
+  const int h = H < 4 ? 4 : H;
+  return (size_t)(h + h / 2) * sizeof(double2);
+}
 
 cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, int logH,
                                  const double2* twP, double2* Xg, double2* Wf,

@@ -1,7 +1,8 @@
 """numpy restatement of the device random numbers (test infrastructure):
 Philox-4x32-10 (Salmon et al., SC'11) keyed by (seed_lo, seed_hi) over the
 counter (q_lo, q_hi, turn_lo, turn_hi), q = particle // 4, followed by the
-single-precision Box-Muller transform of haissinskijulia_b200/csrc/hj_device.cuh."""
+Box-Muller transform of haissinskijulia_b200/csrc/hj_device.cuh (evaluated
+here in double precision; the device evaluates it in single precision)."""
 import numpy as np
 
 _M = np.uint64(0xFFFFFFFF)
@@ -31,14 +32,15 @@ def philox_normals_reference(seed: int, turn: int, n: int) -> np.ndarray:
                                    seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
     s = np.float32(2.0 ** -32)
     h = np.float32(2.0 ** -33)
-    u = [x.astype(np.float32) * s + h for x in (x0, x1, x2, x3)]
-    ra = np.sqrt(np.float32(-2.0) * np.log(u[0]))
-    rb = np.sqrt(np.float32(-2.0) * np.log(u[2]))
-    ta = 2.0 * np.pi * u[1].astype(np.float64)
-    tb = 2.0 * np.pi * u[3].astype(np.float64)
+    u1 = x0.astype(np.float32) * s + h
+    u3 = x2.astype(np.float32) * s + h
+    ta = 2.0 * np.pi * (x1.astype(np.float64) * 2.0 ** -32 - 0.5)
+    tb = 2.0 * np.pi * (x3.astype(np.float64) * 2.0 ** -32 - 0.5)
+    ra = np.sqrt(-2.0 * np.log(u1.astype(np.float64)))
+    rb = np.sqrt(-2.0 * np.log(u3.astype(np.float64)))
     out = np.empty((nq, 4))
-    out[:, 0] = (ra * np.cos(ta).astype(np.float32)).astype(np.float64)
-    out[:, 1] = (ra * np.sin(ta).astype(np.float32)).astype(np.float64)
-    out[:, 2] = (rb * np.cos(tb).astype(np.float32)).astype(np.float64)
-    out[:, 3] = (rb * np.sin(tb).astype(np.float32)).astype(np.float64)
+    out[:, 0] = ra * np.cos(ta)
+    out[:, 1] = ra * np.sin(ta)
+    out[:, 2] = rb * np.cos(tb)
+    out[:, 3] = rb * np.sin(tb)
     return out.reshape(-1)[:n]
