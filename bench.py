@@ -45,6 +45,8 @@ def parse_args():
     ap.add_argument("--particles", type=float, default=1e8)
     ap.add_argument("--nbins", type=int, default=16384)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--layout", type=int, default=-1,
+                    help="thread layout of the fused pass (-1 = library default)")
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--e2e-turns", type=int, default=1000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
@@ -231,6 +233,7 @@ def run_ours(args) -> None:
     n, B, K, W = int(args.particles), args.nbins, args.steps, args.warmup
     cfg = benchmark_ring(n_turns=K, nbins=B)
     ctx = Context(local)
+    ctx.set_pass_layout(args.layout)
     stream = torch.cuda.current_stream()
     gen = torch.Generator(device="cuda").manual_seed(args.seed + 7919 * rank)
     z = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_z

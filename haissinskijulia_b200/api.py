@@ -225,6 +225,11 @@ class Context:
     def last_error(self) -> str:
         return self._lib.hj_last_error(self.handle).decode()
 
+    def set_pass_layout(self, layout: int) -> None:
+        """Thread layout of the fused pass for bunches created afterwards
+        (-1 = automatic; 0, 1, 2 = fixed layouts)."""
+        _check(self, self._lib.hj_set_pass_layout(self.handle, int(layout)))
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self._lib.hj_destroy(self.handle)

@@ -17,6 +17,13 @@ constexpr int64_t kMaxBins = 16384; // largest grid the shared-memory FFT holds 
 // counter keeps a 20-bit count per cell).
 constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 
+// Thread layouts of the fused pass: 0 = 4 particles/thread, 512 threads,
+// next group prefetched; 1 = 2 particles/thread, 1024 threads; 2 = 2
+// particles/thread, 512 threads.
+constexpr int kNumPassCfgs = 3;
+int pass_cfg_threads(int cfg);
+int pass_cfg_ppt(int cfg);
+
 // Quantum-excitation source of the particle pass.
 enum QeMode { QE_OFF = 0, QE_PHILOX = 1, QE_DRAWS = 2 };
 
@@ -26,7 +33,7 @@ struct PassArgs {
   double* dE;
   int64_t n;
   TurnState* ts;
-  const double* pot;       // potential of the previous turn at the bin centers
+  const double2* potd;     // (pot[k], pot[k+1]-pot[k]) of the previous turn
   // bin grid
   int32_t B;
   int32_t use_wake;
@@ -35,6 +42,7 @@ struct PassArgs {
   // physics constants of the run
   double V, phi_s, inv_mass, alpha_c, two_pi_h;
   int32_t update_eta, update_E0, sr, qe_mode;
+  int32_t cfg;             // thread layout (kNumPassCfgs)
   uint64_t seed;
   const double* draws;     // QE_DRAWS: turns x n, row = turn - draws_first_turn
   int64_t draws_first_turn;
@@ -65,6 +73,7 @@ struct BinsArgs {
   double2* Xg;                     // [M]
   double2* zE;                     // [H]
   double* pot;                     // [B]
+  double2* potd;                   // [B] (pot[k], pot[k+1]-pot[k]) for the next pass; NULL: not needed
   const double* W;                 // [B] wake table (direct path for tiny grids)
   // standalone convolution (hj_wake_potential): no turn-state update
   int32_t conv_only;
@@ -78,7 +87,7 @@ struct FlushArgs {
   double* dE;
   int64_t n;
   const TurnState* ts;
-  const double* pot;
+  const double2* potd;
   int32_t B;
   int32_t use_wake, update_E0;
   double c1, cB, inv_cstep;
@@ -91,8 +100,8 @@ struct FlushArgs {
 // ---- launchers (hj_track.cu) ----
 cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin);
 cudaError_t prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
-int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm);
-int track_blocks_per_sm(int B, int qe_mode, int use_wake);
+int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg);
+int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
 size_t track_smem_bytes(int B, int use_wake);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
 // out: counts[B] (| CIC counts[B] | CIC Σw·2^24 [B] when part_cic != NULL);

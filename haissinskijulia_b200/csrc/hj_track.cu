@@ -58,9 +58,15 @@ struct GridConst {
   double e0, eN, inv_e, c1, cB, inv_c;
 };
 
-// Packed CIC accumulator: particle count in the top 20 bits, Σ w·2^24 in the
-// low 44 bits.  A block deposits at most kMaxBlockParticles particles per
-// turn, so neither field can overflow.
+__device__ __forceinline__ int cic_hi(int B) { return B >= 2 ? B - 2 : 0; }
+
+// Packed CIC accumulator V = count·2^44 + Σ w·2^24 per cell (a block
+// deposits at most kMaxBlockParticles particles per turn, so neither field
+// overflows).  In shared memory V lives as two 32-bit words: 64-bit shared
+// atomics are several times slower than 32-bit ones on this GPU, so a deposit
+// adds q = w·2^24 to the low word with an atomic that returns the old value,
+// and 2^12 (one count) plus the carry out of the low word to the high word.
+// Every carry is counted exactly once, so the final words are exact.
 constexpr int kCicWeightBits = 24;
 constexpr int kCicSumBits = 44;
 constexpr unsigned long long kCicSumMask = (1ull << kCicSumBits) - 1ull;
@@ -85,20 +91,31 @@ __device__ __forceinline__ double rcp_approx(double x) {
 
 // Interpolation cell of z on the bin centers (src/wakefield.jl:64-78), 0-based:
 // idx = clamp(floor(u), 0, B-2), w = u - floor(u), u = (clamp(z,c1,cB)-c1)/Δc.
+// floor() is a round-down conversion to int (exact: u is within [0, B-1]).
 // The deposit of turn t and the kick applied in turn t+1 call this with the
 // same z, so they agree exactly.
 __device__ __forceinline__ void cic_cell(double z, const GridConst& g, int& idx, double& w) {
-  double cl = z > g.cB ? g.cB : (z < g.c1 ? g.c1 : z);
-  double u = __dmul_rn(__dsub_rn(cl, g.c1), g.inv_c);
-  double fl = floor(u);
-  double fi = (fl >= 0.0) ? (fl > (double)(g.B - 2) ? (double)(g.B - 2) : fl) : 0.0;
-  idx = (int)fi;
-  w = __dsub_rn(u, fl);
+  const double cl = fmin(fmax(z, g.c1), g.cB);
+  const double u = __dmul_rn(__dsub_rn(cl, g.c1), g.inv_c);
+  const int i = __double2int_rd(u);
+  w = __dsub_rn(u, (double)i);
+  idx = min(max(i, 0), cic_hi(g.B));
 }
 
-// lerp of the potential table (src/wakefield.jl:94-102).
+// Kick of the fused pass: lerp from the (pot[k], pot[k+1] - pot[k]) table.
 __device__ __forceinline__ double wake_kick(double z, const GridConst& g,
-                                            const double* __restrict__ pot) {
+                                            const double2* __restrict__ potd) {
+  int idx;
+  double w;
+  cic_cell(z, g, idx, w);
+  const double2 pd = __ldg(potd + idx);
+  return fma(w, pd.y, pd.x);
+}
+
+// Kick of the single-step kernel in the reference's form v1 (1 - w) + v2 w
+// (src/wakefield.jl:94-102).
+__device__ __forceinline__ double wake_kick_ref(double z, const GridConst& g,
+                                                const double* __restrict__ pot) {
   if (g.B < 2) return __ldg(pot);
   int idx;
   double w;
@@ -107,11 +124,12 @@ __device__ __forceinline__ double wake_kick(double z, const GridConst& g,
                    __dmul_rn(__ldg(pot + idx + 1), w));
 }
 
-// Histogram bin of z (src/utils.jl:387-397), 0-based: clamp(floor((z-e0)/Δe), 0, B-1).
+// Histogram bin of z (src/utils.jl:387-397), 0-based: clamp(floor((z-e0)/Δe), 0, B-1),
+// with (z - e0) and the product rounded exactly as the reference rounds them.
 __device__ __forceinline__ int ngp_bin(double z, const GridConst& g, bool& in) {
   in = (z >= g.e0) & (z <= g.eN);
-  double u = floor(__dmul_rn(__dsub_rn(z, g.e0), g.inv_e));
-  return (u >= 0.0) ? (u < (double)g.B ? (int)u : g.B - 1) : 0;
+  const int j = __double2int_rd(__dmul_rn(__dsub_rn(z, g.e0), g.inv_e));
+  return min(max(j, 0), g.B - 1);
 }
 
 // V(sin(ϕs - x) - sin ϕs) for |x| > 0.5, as the reference forms it.
@@ -174,11 +192,11 @@ template <bool WAKE>
 __device__ __forceinline__ void pass_particle(double& z, double& e, double r, bool qe,
                                               const FusedConst& c, const GridConst& g,
                                               bool pending, bool upd_E0, double pmean,
-                                              const double* __restrict__ pot, double& acc_z,
+                                              const double2* __restrict__ potd, double& acc_z,
                                               double& acc_z2, double& acc_d, uint32_t& n_in,
-                                              uint32_t* s_cnt, unsigned long long* s_cic) {
+                                              uint32_t* s_cnt, uint32_t* s_lo, uint32_t* s_hi) {
   if (pending) {
-    if (WAKE) e = e - wake_kick(z, g, pot);
+    if (WAKE) e = e - wake_kick(z, g, potd);
     if (upd_E0) e = e - pmean;
   }
   const double e_start = e;
@@ -193,15 +211,12 @@ __device__ __forceinline__ void pass_particle(double& z, double& e, double r, bo
       atomicAdd(&s_cnt[j], 1u);
       ++n_in;
     }
-    if (g.B >= 2) {
-      int idx;
-      double w;
-      cic_cell(z, g, idx, w);
-      unsigned long long q = (w >= 0.0) ? (unsigned long long)__double2uint_rn(w * 16777216.0) : 0ull;
-      atomicAdd(&s_cic[idx], (1ull << kCicSumBits) + q);
-    } else {
-      atomicAdd(&s_cic[0], 1ull << kCicSumBits);
-    }
+    int idx;
+    double w;
+    cic_cell(z, g, idx, w);
+    const uint32_t q = __double2uint_rn(w * 16777216.0);
+    const uint32_t old = atomicAdd(&s_lo[idx], q);
+    atomicAdd(&s_hi[idx], (1u << (kCicSumBits - 32)) + (old + q < old ? 1u : 0u));
   }
 }
 
@@ -212,9 +227,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Fixed-order block reduction of four accumulators into out[0..3] (thread 0).
+template <int THREADS>
 __device__ __forceinline__ void block_sum4(double a0, double a1, double a2, double a3,
                                            double* out) {
-  __shared__ double red[kTrackThreads / 32][4];
+  __shared__ double red[THREADS / 32][4];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   a0 = warp_sum(a0);
   a1 = warp_sum(a1);
@@ -234,11 +250,54 @@ __device__ __forceinline__ void block_sum4(double a0, double a1, double a2, doub
   }
 }
 
-template <bool WAKE, int QE>
-__global__ void __launch_bounds__(kTrackThreads, 1) k_track_pass(PassArgs a) {
+// Particle loads/stores of PPT = 2 or 4 consecutive particles.
+template <int PPT>
+__device__ __forceinline__ void ldp(const double* p, double v[PPT]) {
+  if (PPT == 4) {
+    asm("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+        : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+        : "l"(p));
+  } else {
+    asm("ld.global.v2.f64 {%0,%1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
+  }
+}
+
+template <int PPT>
+__device__ __forceinline__ void stp(double* p, const double v[PPT]) {
+  if (PPT == 4) {
+    asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
+                 "d"(v[2]), "d"(v[3])
+                 : "memory");
+  } else {
+    asm volatile("st.global.v2.f64 [%0], {%1,%2};" ::"l"(p), "d"(v[0]), "d"(v[1]) : "memory");
+  }
+}
+
+// Normals of particles PPT*g .. PPT*g+PPT-1 (the Philox quad of particle i is
+// i/4, its lane i%4; a pair uses half of its quad).
+template <int PPT>
+__device__ __forceinline__ void group_normals(uint64_t seed, int64_t turn, int64_t g,
+                                              double r[PPT]) {
+  double q4[4];
+  philox_normals4(seed, turn, PPT == 4 ? g : (g >> 1), q4);
+  if (PPT == 4) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) r[j] = q4[j];
+  } else {
+    const int h = (int)(g & 1) * 2;
+    r[0] = q4[h];
+    r[1] = q4[h + 1];
+  }
+}
+
+// One turn over the bunch.  PPT particles per thread per iteration (4 with the
+// next group prefetched in registers, or 2 with twice the threads per SM).
+template <bool WAKE, int QE, int PPT, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned long long* s_cic = reinterpret_cast<unsigned long long*>(smem_raw);
-  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_cic + (WAKE ? a.B : 0));
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem_raw);
+  uint32_t* s_lo = s_cnt + (WAKE ? a.B : 0);
+  uint32_t* s_hi = s_lo + (WAKE ? a.B : 0);
 
   TurnState* ts = a.ts;
   const TurnScalars sc = ts->cur;
@@ -278,78 +337,88 @@ __global__ void __launch_bounds__(kTrackThreads, 1) k_track_pass(PassArgs a) {
   }
 
   if (WAKE) {
-    for (int i = threadIdx.x; i < a.B; i += blockDim.x) {
-      s_cic[i] = 0ull;
+    for (int i = threadIdx.x; i < a.B; i += THREADS) {
       s_cnt[i] = 0u;
+      s_lo[i] = 0u;
+      s_hi[i] = 0u;
     }
     // zero the merged histograms k_hist_reduce accumulates into this turn
-    const int gstride = gridDim.x * blockDim.x;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * a.B; i += gstride)
+    const int gstride = gridDim.x * THREADS;
+    for (int i = blockIdx.x * THREADS + threadIdx.x; i < 3 * a.B; i += gstride)
       a.hist_out[i] = 0ull;
     __syncthreads();
   }
 
   double acc_z = 0.0, acc_z2 = 0.0, acc_d = 0.0;
   uint32_t n_in = 0;
-  const double* __restrict__ pot = a.pot;
-  const int64_t nq = a.n >> 2;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double zn[4], en[4];
-  if (q < nq) {
-    ld4(a.z + 4 * q, zn);
-    ld4(a.dE + 4 * q, en);
+  const double2* __restrict__ potd = a.potd;
+  const int64_t ng = a.n / PPT;
+  const int64_t stride = (int64_t)gridDim.x * THREADS;
+  int64_t q = (int64_t)blockIdx.x * THREADS + threadIdx.x;
+  constexpr bool kPrefetch = (PPT == 4);
+  double zn[PPT], en[PPT];
+  if (kPrefetch && q < ng) {
+    ldp<PPT>(a.z + PPT * q, zn);
+    ldp<PPT>(a.dE + PPT * q, en);
   }
-  for (; q < nq; q += stride) {
-    double zz[4], ee[4], rr[4] = {0.0, 0.0, 0.0, 0.0};
+  for (; q < ng; q += stride) {
+    double zz[PPT], ee[PPT], rr[PPT];
+    if (kPrefetch) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      zz[j] = zn[j];
-      ee[j] = en[j];
+      for (int j = 0; j < PPT; ++j) {
+        zz[j] = zn[j];
+        ee[j] = en[j];
+      }
+      const int64_t qn = q + stride;
+      if (qn < ng) {  // the next group streams in while this one is computed
+        ldp<PPT>(a.z + PPT * qn, zn);
+        ldp<PPT>(a.dE + PPT * qn, en);
+      }
+    } else {
+      ldp<PPT>(a.z + PPT * q, zz);
+      ldp<PPT>(a.dE + PPT * q, ee);
     }
-    const int64_t qn = q + stride;
-    if (qn < nq) {               // prefetch the next quad while this one is computed
-      ld4(a.z + 4 * qn, zn);
-      ld4(a.dE + 4 * qn, en);
-    }
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
     if (QE == QE_PHILOX) {
-      philox_normals4(a.seed, turn, q, rr);
+      group_normals<PPT>(a.seed, turn, q, rr);
     } else if (QE == QE_DRAWS) {
       if (drow) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) rr[j] = __ldg(drow + 4 * q + j);
+        for (int j = 0; j < PPT; ++j) rr[j] = __ldg(drow + PPT * q + j);
       }
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < PPT; ++j)
       pass_particle<WAKE>(zz[j], ee[j], rr[j], QE != QE_OFF, c, g, pending, upd_E0, pmean,
-                          pot, acc_z, acc_z2, acc_d, n_in, s_cnt, s_cic);
-    st4(a.z + 4 * q, zz);
-    st4(a.dE + 4 * q, ee);
+                          potd, acc_z, acc_z2, acc_d, n_in, s_cnt, s_lo, s_hi);
+    stp<PPT>(a.z + PPT * q, zz);
+    stp<PPT>(a.dE + PPT * q, ee);
   }
-  // Tail of n % 4 particles: threads 0..2 of block 0, scalar.
-  if (blockIdx.x == 0 && threadIdx.x < (int)(a.n & 3)) {
-    const int64_t i = nq * 4 + threadIdx.x;
-    double rr[4] = {0.0, 0.0, 0.0, 0.0};
-    if (QE == QE_PHILOX) philox_normals4(a.seed, turn, nq, rr);
-    double r = rr[threadIdx.x];
+  // Tail of n % PPT particles: the first threads of block 0, scalar.
+  if (blockIdx.x == 0 && threadIdx.x < (int)(a.n % PPT)) {
+    const int64_t i = ng * PPT + threadIdx.x;
+    double rr4[4] = {0.0, 0.0, 0.0, 0.0};
+    if (QE == QE_PHILOX) philox_normals4(a.seed, turn, i >> 2, rr4);
+    double r = rr4[i & 3];
     if (QE == QE_DRAWS && drow) r = __ldg(drow + i);
     double z = a.z[i], e = a.dE[i];
-    pass_particle<WAKE>(z, e, r, QE != QE_OFF, c, g, pending, upd_E0, pmean, pot, acc_z,
-                        acc_z2, acc_d, n_in, s_cnt, s_cic);
+    pass_particle<WAKE>(z, e, r, QE != QE_OFF, c, g, pending, upd_E0, pmean, potd, acc_z,
+                        acc_z2, acc_d, n_in, s_cnt, s_lo, s_hi);
     a.z[i] = z;
     a.dE[i] = e;
   }
 
-  block_sum4(acc_z, acc_z2, acc_d, (double)n_in, a.part_sum + (size_t)blockIdx.x * kNumSums);
+  block_sum4<THREADS>(acc_z, acc_z2, acc_d, (double)n_in,
+                      a.part_sum + (size_t)blockIdx.x * kNumSums);
 
   if (WAKE) {
     __syncthreads();
     uint32_t* pc = a.part_cnt + (size_t)blockIdx.x * a.B;
     unsigned long long* pq = a.part_cic + (size_t)blockIdx.x * a.B;
-    for (int i = threadIdx.x; i < a.B; i += blockDim.x) {
+    for (int i = threadIdx.x; i < a.B; i += THREADS) {
       pc[i] = s_cnt[i];
-      pq[i] = s_cic[i];
+      pq[i] = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
     }
   }
 }
@@ -390,7 +459,7 @@ __global__ void __launch_bounds__(kTrackThreads) k_flush(FlushArgs a) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
     double z = a.z[i], e = a.dE[i];
     if (apply) {
-      if (a.use_wake) e = __dsub_rn(e, wake_kick(z, g, a.pot));
+      if (a.use_wake) e = e - wake_kick(z, g, a.potd);
       if (a.update_E0) e = __dsub_rn(e, pmean);
     }
     if (a.z_out) a.z_out[i] = z;
@@ -400,7 +469,7 @@ __global__ void __launch_bounds__(kTrackThreads) k_flush(FlushArgs a) {
     s2 += e;
     s3 = fma(e, e, s3);
   }
-  block_sum4(s0, s1, s2, s3, a.part + (size_t)blockIdx.x * 4);
+  block_sum4<kTrackThreads>(s0, s1, s2, s3, a.part + (size_t)blockIdx.x * 4);
 }
 
 // NGP histogram only (hj_histogram, hj_apply_wakefield).
@@ -426,7 +495,7 @@ __global__ void k_interp_kick(const double* __restrict__ z, double* __restrict__
                               const double* __restrict__ pot, GridConst g) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-    dE[i] = __dsub_rn(dE[i], wake_kick(__ldg(z + i), g, pot));
+    dE[i] = __dsub_rn(dE[i], wake_kick_ref(__ldg(z + i), g, pot));
 }
 
 __global__ void k_rf_kick(double V, double sin_phis, double k, double phi_s,
@@ -516,48 +585,60 @@ cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn > 0 ? dyn : 0);
 }
 
-cudaError_t prepare_track_kernels(int max_smem) {
-  const void* fns[] = {(const void*)k_track_pass<true, QE_OFF>,
-                       (const void*)k_track_pass<true, QE_PHILOX>,
-                       (const void*)k_track_pass<true, QE_DRAWS>,
-                       (const void*)k_track_pass<false, QE_OFF>,
-                       (const void*)k_track_pass<false, QE_PHILOX>,
-                       (const void*)k_track_pass<false, QE_DRAWS>,
-                       (const void*)k_histogram};
-  for (const void* f : fns) {
-    cudaError_t e = allow_dynamic_smem(f, max_smem);
-    if (e != cudaSuccess) return e;
+namespace {
+template <bool W, int Q>
+const void* pass_fn_wq(int cfg) {
+  switch (cfg) {
+    case 0: return (const void*)k_track_pass<W, Q, 4, 512>;
+    case 1: return (const void*)k_track_pass<W, Q, 2, 1024>;
+    default: return (const void*)k_track_pass<W, Q, 2, 512>;
   }
-  return cudaSuccess;
+}
+
+template <bool W>
+const void* pass_fn_w(int qe, int cfg) {
+  switch (qe) {
+    case QE_PHILOX: return pass_fn_wq<W, QE_PHILOX>(cfg);
+    case QE_DRAWS: return pass_fn_wq<W, QE_DRAWS>(cfg);
+    default: return pass_fn_wq<W, QE_OFF>(cfg);
+  }
+}
+
+const void* pass_fn(int wake, int qe, int cfg) {
+  return wake ? pass_fn_w<true>(qe, cfg) : pass_fn_w<false>(qe, cfg);
+}
+}  // namespace
+
+int pass_cfg_threads(int cfg) { return cfg == 1 ? 1024 : 512; }
+int pass_cfg_ppt(int cfg) { return cfg == 0 ? 4 : 2; }
+
+cudaError_t prepare_track_kernels(int max_smem) {
+  for (int w = 0; w < 2; ++w)
+    for (int q = 0; q < 3; ++q)
+      for (int c = 0; c < kNumPassCfgs; ++c) {
+        cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
+        if (e != cudaSuccess) return e;
+      }
+  return allow_dynamic_smem((const void*)k_histogram, max_smem);
 }
 
 size_t track_smem_bytes(int B, int use_wake) {
   return use_wake ? (size_t)B * (sizeof(unsigned long long) + sizeof(uint32_t)) : 0;
 }
 
-int track_blocks_per_sm(int B, int qe_mode, int use_wake) {
-  size_t smem = track_smem_bytes(B, use_wake);
+int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
+  const size_t smem = track_smem_bytes(B, use_wake);
   int bps = 0;
-  const void* fn = nullptr;
-  if (use_wake) {
-    fn = qe_mode == QE_PHILOX ? (const void*)k_track_pass<true, QE_PHILOX>
-         : qe_mode == QE_DRAWS ? (const void*)k_track_pass<true, QE_DRAWS>
-                               : (const void*)k_track_pass<true, QE_OFF>;
-  } else {
-    fn = qe_mode == QE_PHILOX ? (const void*)k_track_pass<false, QE_PHILOX>
-         : qe_mode == QE_DRAWS ? (const void*)k_track_pass<false, QE_DRAWS>
-                               : (const void*)k_track_pass<false, QE_OFF>;
-  }
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, kTrackThreads, smem) !=
-      cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pass_fn(use_wake, qe_mode, cfg),
+                                                    pass_cfg_threads(cfg), smem) != cudaSuccess)
     bps = 1;
   return bps < 1 ? 1 : bps;
 }
 
 // Blocks of the particle pass: enough to fill the GPU, but each block should
 // own at least ~2 bins' worth of histogram traffic per particle it moves.
-int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm) {
-  int64_t per_block = 4 * (int64_t)kTrackThreads;
+int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg) {
+  int64_t per_block = (int64_t)pass_cfg_ppt(cfg) * pass_cfg_threads(cfg);
   if (per_block < 2 * (int64_t)B) per_block = 2 * (int64_t)B;
   int64_t g = (n + per_block - 1) / per_block;
   int64_t cap = (int64_t)num_sms * blocks_per_sm;
@@ -570,21 +651,10 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm) {
 }
 
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
-  size_t smem = track_smem_bytes(a.B, a.use_wake);
-  if (a.use_wake) {
-    switch (a.qe_mode) {
-      case QE_PHILOX: k_track_pass<true, QE_PHILOX><<<grid, kTrackThreads, smem, st>>>(a); break;
-      case QE_DRAWS: k_track_pass<true, QE_DRAWS><<<grid, kTrackThreads, smem, st>>>(a); break;
-      default: k_track_pass<true, QE_OFF><<<grid, kTrackThreads, smem, st>>>(a); break;
-    }
-  } else {
-    switch (a.qe_mode) {
-      case QE_PHILOX: k_track_pass<false, QE_PHILOX><<<grid, kTrackThreads, 0, st>>>(a); break;
-      case QE_DRAWS: k_track_pass<false, QE_DRAWS><<<grid, kTrackThreads, 0, st>>>(a); break;
-      default: k_track_pass<false, QE_OFF><<<grid, kTrackThreads, 0, st>>>(a); break;
-    }
-  }
-  return cudaGetLastError();
+  const size_t smem = track_smem_bytes(a.B, a.use_wake);
+  void* args[] = {const_cast<PassArgs*>(&a)};
+  return cudaLaunchKernel(pass_fn(a.use_wake, a.qe_mode, a.cfg), dim3(grid),
+                          dim3(pass_cfg_threads(a.cfg)), args, smem, st);
 }
 
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,

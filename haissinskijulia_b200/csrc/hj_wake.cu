@@ -39,61 +39,125 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) {
   return make_double2(a.x - b.x, a.y - b.y);
 }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-__device__ __forceinline__ int bitrev(int n, int logH) {
-  return (int)(__brev((unsigned)n) >> (32 - logH));
+// ---------------------------------------------------------------- FFT
+// Self-sorting (Stockham) FFT of size N = 2^logN in shared memory, natural
+// order in and out (Govindaraju et al., "High performance discrete Fourier
+// transforms on graphics processors", SC'08): radix-8 passes, then one
+// radix-4 or radix-2 pass.  Each thread loads its R points with unit stride
+// across threads (conflict-free), applies the twiddles, does the R-point DFT
+// in registers, and after a barrier stores them to their self-sorted
+// positions in the same buffer.  tw[j] = w_N^j, j < N/2, in shared memory.
+
+// w_N^m, 0 <= m < N, from the half table (w^{m+N/2} = -w^m).
+__device__ __forceinline__ double2 twiddle(const double2* tw, int m, int halfN, bool inverse) {
+  double2 w = (m < halfN) ? tw[m] : make_double2(-tw[m - halfN].x, -tw[m - halfN].y);
+  if (inverse) w.y = -w.y;
+  return w;
 }
 
-// In-place decimation-in-time FFT of size H on shared memory that holds its
-// input in bit-reversed order.  tw[j] = exp(-2πi j/H), j < H/2, also in shared
-// memory.  Pairs of radix-2 stages are fused into radix-4 passes (each thread
-// keeps the four points of two consecutive stages in registers), so a
-// length-8192 transform takes 7 passes over shared memory instead of 13.
-// inverse uses conjugate twiddles and no normalisation.
-__device__ void smem_fft(double2* s, const double2* tw, int H, int logH, bool inverse) {
-  int h = 1;
-  int stage = 0;
-  for (; stage + 2 <= logH; stage += 2, h <<= 2) {
-    const int sa = H / (2 * h), sb = H / (4 * h);
-    for (int b = threadIdx.x; b < (H >> 2); b += blockDim.x) {
-      const int j = b & (h - 1);
-      const int i0 = ((b - j) << 2) + j;
-      double2 x0 = s[i0], x1 = s[i0 + h], x2 = s[i0 + 2 * h], x3 = s[i0 + 3 * h];
-      double2 wa = tw[j * sa], wb = tw[j * sb];
-      if (inverse) {
-        wa.y = -wa.y;
-        wb.y = -wb.y;
-      }
-      // span h: (x0, x1) and (x2, x3) with w_{2h}^j
-      double2 t = cmul(x1, wa);
-      x1 = csub(x0, t);
-      x0 = cadd(x0, t);
-      t = cmul(x3, wa);
-      x3 = csub(x2, t);
-      x2 = cadd(x2, t);
-      // span 2h: (x0, x2) with w_{4h}^j, (x1, x3) with w_{4h}^{j+h} = w_{4h}^j (-i or +i)
-      t = cmul(x2, wb);
-      s[i0] = cadd(x0, t);
-      s[i0 + 2 * h] = csub(x0, t);
-      t = cmul(x3, wb);
-      t = inverse ? make_double2(-t.y, t.x) : make_double2(t.y, -t.x);
-      s[i0 + h] = cadd(x1, t);
-      s[i0 + 3 * h] = csub(x1, t);
-    }
-    __syncthreads();
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ double2 rot_q(double2 a) {
+  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft2(double2* v) {
+  const double2 t = v[0];
+  v[0] = cadd(t, v[1]);
+  v[1] = csub(t, v[1]);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(double2* v) {
+  const double2 d0 = cadd(v[0], v[2]), d1 = csub(v[0], v[2]);
+  const double2 d2 = cadd(v[1], v[3]), d3 = rot_q<INV>(csub(v[1], v[3]));
+  v[0] = cadd(d0, d2);
+  v[2] = csub(d0, d2);
+  v[1] = cadd(d1, d3);
+  v[3] = csub(d1, d3);
+}
+
+// 8-point DFT: one radix-2 decimation-in-frequency split into two 4-point DFTs.
+template <bool INV>
+__device__ __forceinline__ void dft8(double2* v) {
+  const double r = 0.70710678118654752440;  // 1/sqrt(2)
+  double2 a[4], b[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    a[k] = cadd(v[k], v[k + 4]);
+    b[k] = csub(v[k], v[k + 4]);
   }
-  if (stage < logH) {  // odd number of stages: final radix-2 pass, span H/2
-    for (int b = threadIdx.x; b < (H >> 1); b += blockDim.x) {
-      const int j = b & (h - 1);
-      const int i0 = ((b - j) << 1) + j;
-      double2 w = tw[j * (H / (2 * h))];
-      if (inverse) w.y = -w.y;
-      const double2 u = s[i0];
-      const double2 t = cmul(s[i0 + h], w);
-      s[i0] = cadd(u, t);
-      s[i0 + h] = csub(u, t);
-    }
-    __syncthreads();
+  // b[k] *= w_8^k
+  if (!INV) {
+    b[1] = make_double2(r * (b[1].x + b[1].y), r * (b[1].y - b[1].x));
+    b[3] = make_double2(r * (b[3].y - b[3].x), -r * (b[3].x + b[3].y));
+  } else {
+    b[1] = make_double2(r * (b[1].x - b[1].y), r * (b[1].x + b[1].y));
+    b[3] = make_double2(-r * (b[3].x + b[3].y), r * (b[3].x - b[3].y));
   }
+  b[2] = rot_q<INV>(b[2]);
+  dft4<INV>(a);
+  dft4<INV>(b);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[2 * k] = a[k];
+    v[2 * k + 1] = b[k];
+  }
+}
+
+template <int LR, bool INV>
+__device__ __forceinline__ void dftR(double2* v) {
+  if (LR == 3) dft8<INV>(v);
+  else if (LR == 2) dft4<INV>(v);
+  else dft2<INV>(v);
+}
+
+constexpr int kMaxFftH = 8192;   // largest shared-memory transform (B = 16384)
+
+template <int LR, bool INV>
+__device__ __forceinline__ void stockham_pass(double2* s, const double2* tw, int N, int Ns) {
+  constexpr int R = 1 << LR;
+  constexpr int PER = (kMaxFftH / R + kBinsThreads - 1) / kBinsThreads;
+  const int nb = N >> LR;
+  const int step = N / (Ns * R);
+  double2 v[PER][R];
+#pragma unroll
+  for (int t = 0; t < PER; ++t) {
+    const int j = threadIdx.x + t * kBinsThreads;
+    if (j < nb) {
+      const int jm = j & (Ns - 1);
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[t][q] = s[j + q * nb];
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[t][q] = cmul(v[t][q], twiddle(tw, q * jm * step, N >> 1, INV));
+      dftR<LR, INV>(v[t]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < PER; ++t) {
+    const int j = threadIdx.x + t * kBinsThreads;
+    if (j < nb) {
+      const int jm = j & (Ns - 1);
+      const int base = ((j - jm) << LR) + jm;
+#pragma unroll
+      for (int q = 0; q < R; ++q) s[base + q * Ns] = v[t][q];
+    }
+  }
+  __syncthreads();
+}
+
+template <bool INV>
+__device__ void smem_fft(double2* s, const double2* tw, int N, int logN) {
+  int Ns = 1, rem = logN;
+  while (rem >= 3) {
+    stockham_pass<3, INV>(s, tw, N, Ns);
+    Ns <<= 3;
+    rem -= 3;
+  }
+  if (rem == 2) stockham_pass<2, INV>(s, tw, N, Ns);
+  else if (rem == 1) stockham_pass<1, INV>(s, tw, N, Ns);
 }
 
 // Twiddles of the length-H transform into shared memory: w_H^j = twP[4j].
@@ -102,27 +166,30 @@ __device__ void load_twiddles(double2* tw, int H, const double2* __restrict__ tw
   __syncthreads();
 }
 
-// X[0..M) = FFT_M(x), x[n] = v(2n) + i v(2n+1), v(j) = 0 for j >= L (L <= M).
+// X[0..M) = FFT_M(x), x[n] = v(2n) + i v(2n+1), v(j) = 0 for j >= L (L <= M):
+// X[2m] = FFT_H(x)[m] and X[2m+1] = FFT_H(x[n] w_M^n)[m], since x[n] = 0 for n >= H.
 template <typename Vals>
-__device__ void forward_packed(const Vals& v, int L, int P, int H, int logH,
+__device__ void forward_packed(const Vals& v, int L, int H, int logH,
                                const double2* __restrict__ twP, double2* s, const double2* tw,
                                double2* Xg) {
-  for (int n = threadIdx.x; n < H; n += blockDim.x) {
+#pragma unroll 8
+  for (int n = threadIdx.x; n < H; n += kBinsThreads) {
     const int j = 2 * n;
-    s[bitrev(n, logH)] = make_double2(j < L ? v(j) : 0.0, j + 1 < L ? v(j + 1) : 0.0);
+    s[n] = make_double2(j < L ? v(j) : 0.0, j + 1 < L ? v(j + 1) : 0.0);
   }
   __syncthreads();
-  smem_fft(s, tw, H, logH, false);
-  for (int m = threadIdx.x; m < H; m += blockDim.x) Xg[2 * m] = s[m];
+  smem_fft<false>(s, tw, H, logH);
+  for (int m = threadIdx.x; m < H; m += kBinsThreads) Xg[2 * m] = s[m];
   __syncthreads();
-  for (int n = threadIdx.x; n < H; n += blockDim.x) {
+#pragma unroll 8
+  for (int n = threadIdx.x; n < H; n += kBinsThreads) {
     const int j = 2 * n;
-    double2 a = make_double2(j < L ? v(j) : 0.0, j + 1 < L ? v(j + 1) : 0.0);
-    s[bitrev(n, logH)] = cmul(a, __ldg(&twP[2 * n]));  // w_M^n = w_P^{2n}
+    const double2 a = make_double2(j < L ? v(j) : 0.0, j + 1 < L ? v(j + 1) : 0.0);
+    s[n] = cmul(a, __ldg(&twP[2 * n]));  // w_M^n = w_P^{2n}
   }
   __syncthreads();
-  smem_fft(s, tw, H, logH, false);
-  for (int m = threadIdx.x; m < H; m += blockDim.x) Xg[2 * m + 1] = s[m];
+  smem_fft<false>(s, tw, H, logH);
+  for (int m = threadIdx.x; m < H; m += kBinsThreads) Xg[2 * m + 1] = s[m];
   __syncthreads();
 }
 
@@ -138,24 +205,44 @@ __device__ __forceinline__ double2 real_spectrum(const double2* __restrict__ Xg,
   return cadd(E, cmul(__ldg(&twP[k]), O));
 }
 
-// Packed inverse input Z[k] (0 <= k < M) for the real inverse transform of
-// the Hermitian spectrum Y: E' = (Y[k] + conj Y[M-k])/2,
-// O' = (Y[k] - conj Y[M-k]) conj(w_P^k)/2, Z = E' + i O'.
-__device__ __forceinline__ double2 packed_inverse_input(const double2* __restrict__ Xg,
-                                                        const double2* __restrict__ Wf, int k,
-                                                        int M, double current,
-                                                        const double2* __restrict__ twP) {
-  double2 yk = cmul(real_spectrum(Xg, k, M, twP), __ldg(&Wf[k]));
-  yk.x *= current;
-  yk.y *= current;
-  double2 ym = cmul(real_spectrum(Xg, M - k, M, twP), __ldg(&Wf[M - k]));
-  ym.x *= current;
-  ym.y *= current;
-  const double2 yc = cconj(ym);
-  const double2 E = make_double2(0.5 * (yk.x + yc.x), 0.5 * (yk.y + yc.y));
-  const double2 D = make_double2(0.5 * (yk.x - yc.x), 0.5 * (yk.y - yc.y));
-  const double2 O = cmul(D, cconj(__ldg(&twP[k])));
-  return make_double2(E.x - O.y, E.y + O.x);
+// In-place pre-inverse phase: from the packed forward transform X of g
+// (in Xg) form, for each pair (k, M-k), the spectrum of g (G = E + w_P^k O),
+// the product Y = G FFT(W) current, and the packed inverse input
+// Z[k] = (Y[k] + conj Y[M-k])/2 + i (Y[k] - conj Y[M-k]) conj(w_P^k)/2, written
+// back over X[k] and X[M-k].  X[M] is X[0]; w_P^{M-k} = -conj(w_P^k).
+__device__ void spectrum_to_inverse_input(double2* Xg, const double2* __restrict__ Wf, int M,
+                                          double current, const double2* __restrict__ twP) {
+  for (int k = threadIdx.x; k <= M / 2; k += kBinsThreads) {
+    const int km = (k == 0) ? 0 : M - k;
+    const double2 xk = Xg[k], xm = Xg[km];
+    const double2 tk = __ldg(&twP[k]);
+    const double2 tm = make_double2(-tk.x, tk.y);             // w_P^{M-k}
+    // G[k] and G[M-k]
+    double2 E = make_double2(0.5 * (xk.x + xm.x), 0.5 * (xk.y - xm.y));
+    double2 D = make_double2(0.5 * (xk.x - xm.x), 0.5 * (xk.y + xm.y));
+    const double2 Gk = cadd(E, cmul(tk, make_double2(D.y, -D.x)));
+    E = make_double2(0.5 * (xm.x + xk.x), 0.5 * (xm.y - xk.y));
+    D = make_double2(0.5 * (xm.x - xk.x), 0.5 * (xm.y + xk.y));
+    const double2 Gm = cadd(E, cmul(tm, make_double2(D.y, -D.x)));
+    double2 Yk = cmul(Gk, __ldg(&Wf[k]));
+    double2 Ym = cmul(Gm, __ldg(&Wf[M - k]));
+    Yk.x *= current;
+    Yk.y *= current;
+    Ym.x *= current;
+    Ym.y *= current;
+    // Z[k]
+    double2 Ez = make_double2(0.5 * (Yk.x + Ym.x), 0.5 * (Yk.y - Ym.y));
+    double2 Dz = make_double2(0.5 * (Yk.x - Ym.x), 0.5 * (Yk.y + Ym.y));
+    double2 Oz = cmul(Dz, cconj(tk));
+    Xg[k] = make_double2(Ez.x - Oz.y, Ez.y + Oz.x);
+    if (k != 0 && km != k) {
+      // Z[M-k]
+      Ez = make_double2(0.5 * (Ym.x + Yk.x), 0.5 * (Ym.y - Yk.y));
+      Dz = make_double2(0.5 * (Ym.x - Yk.x), 0.5 * (Ym.y + Yk.y));
+      Oz = cmul(Dz, cconj(tm));
+      Xg[km] = make_double2(Ez.x - Oz.y, Ez.y + Oz.x);
+    }
+  }
 }
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -191,7 +278,7 @@ __global__ void __launch_bounds__(kBinsThreads)
   extern __shared__ __align__(16) double2 s_fft[];
   double2* s_tw = s_fft + H;
   load_twiddles(s_tw, H, twP);
-  forward_packed(WakeVals{W}, B, P, H, logH, twP, s_fft, s_tw, Xg);
+  forward_packed(WakeVals{W}, B, H, logH, twP, s_fft, s_tw, Xg);
   for (int k = threadIdx.x; k <= M; k += blockDim.x) Wf[k] = real_spectrum(Xg, k, M, twP);
 }
 
@@ -286,23 +373,25 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
       if (a.H >= 4) {
         double2* s_tw = s_fft + a.H;
         load_twiddles(s_tw, a.H, a.twP);
-        forward_packed(DensityVals{a.cnt, a.lam, inv_n}, a.B, a.P, a.H, a.logH, a.twP, s_fft,
+        forward_packed(DensityVals{a.cnt, a.lam, inv_n}, a.B, a.H, a.logH, a.twP, s_fft,
                        s_tw, a.Xg);
-        // inverse, even half -> zE
-        for (int m = threadIdx.x; m < a.H; m += blockDim.x)
-          s_fft[bitrev(m, a.logH)] = packed_inverse_input(a.Xg, a.Wf, 2 * m, a.M, current, a.twP);
+        spectrum_to_inverse_input(a.Xg, a.Wf, a.M, current, a.twP);
         __syncthreads();
-        smem_fft(s_fft, s_tw, a.H, a.logH, true);
-        for (int m = threadIdx.x; m < a.H; m += blockDim.x) a.zE[m] = s_fft[m];
+        // inverse of the even half -> zE
+#pragma unroll 8
+        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) s_fft[m] = a.Xg[2 * m];
         __syncthreads();
-        // inverse, odd half, combine, potential and Σ H[k] pot[k]
-        for (int m = threadIdx.x; m < a.H; m += blockDim.x)
-          s_fft[bitrev(m, a.logH)] =
-              packed_inverse_input(a.Xg, a.Wf, 2 * m + 1, a.M, current, a.twP);
+        smem_fft<true>(s_fft, s_tw, a.H, a.logH);
+        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) a.zE[m] = s_fft[m];
         __syncthreads();
-        smem_fft(s_fft, s_tw, a.H, a.logH, true);
+        // inverse of the odd half, combined with the even half into the potential
+#pragma unroll 8
+        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) s_fft[m] = a.Xg[2 * m + 1];
+        __syncthreads();
+        smem_fft<true>(s_fft, s_tw, a.H, a.logH);
         const double invM = 1.0 / (double)a.M;
-        for (int m = threadIdx.x; m < a.H; m += blockDim.x) {
+#pragma unroll 8
+        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) {
           const double2 zo = cmul(s_fft[m], cconj(__ldg(&a.twP[2 * m])));
           const double2 ze = a.zE[m];
           const double re = (ze.x + zo.x) * invM, im = (ze.y + zo.y) * invM;
@@ -321,18 +410,18 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
           }
         }
       }
-      // Σ_i lerp(pot, z_i) from the CIC deposit: with C[k] particles in cell k
-      // and S[k] = Σ w·2^24 over them,
-      //   Σ_i lerp = Σ_k C[k] pot[k] + 2^-24 Σ_k S[k] (pot[k+1] - pot[k]).
-      __syncthreads();
-      if (a.cic) {
-        const unsigned long long* C = a.cic;
-        const unsigned long long* S = a.cic + a.B;
-        for (int k = threadIdx.x; k < a.B; k += blockDim.x) {
-          double t = (double)C[k] * a.pot[k];
-          if (k + 1 < a.B) t += (double)S[k] * 5.9604644775390625e-08 * (a.pot[k + 1] - a.pot[k]);
-          sum_kick += t;
-        }
+    }
+    // The next pass kicks with lerp = pot[k] + w (pot[k+1] - pot[k]); the same
+    // table gives Σ_i lerp(pot, z_i) from the CIC deposit: with C[k] particles
+    // in cell k and S[k] = Σ w·2^24 over them,
+    //   Σ_i lerp = Σ_k C[k] pot[k] + 2^-24 Σ_k S[k] (pot[k+1] - pot[k]).
+    __syncthreads();
+    if (a.potd || a.cic) {
+      for (int k = threadIdx.x; k < a.B; k += blockDim.x) {
+        const double p0 = a.pot[k];
+        const double d = (k + 1 < a.B) ? a.pot[k + 1] - p0 : 0.0;
+        if (a.potd) a.potd[k] = make_double2(p0, d);
+        if (a.cic) sum_kick += (double)a.cic[k] * p0 + (double)a.cic[a.B + k] * 5.9604644775390625e-08 * d;
       }
     }
   }

@@ -134,6 +134,12 @@ hj_status hj_create(int32_t device, hj_ctx** out);
 void hj_destroy(hj_ctx* ctx);
 /* Message of the last failure on this context ("" if none). */
 const char* hj_last_error(const hj_ctx* ctx);
+/* Thread layout of the fused particle pass for bunches created afterwards on
+ * this context: -1 = chosen by the library (default), 0 = 4 particles per
+ * thread x 512 threads, 1 = 2 x 1024, 2 = 2 x 512.  Results do not depend on
+ * the layout beyond floating-point summation order.  No reference
+ * counterpart. */
+hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout);
 
 /* ---------------------------------------------------------------- set-up helpers */
 

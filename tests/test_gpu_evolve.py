@@ -84,6 +84,16 @@ def test_reference_ring_reference_wake(gpu_ctx, oracle):
     run_turn_by_turn(gpu_ctx, oracle, cfg, 100_000, 30, seed=1234)
 
 
+@pytest.mark.parametrize("layout", [0, 1, 2])
+def test_thread_layouts(oracle, layout):
+    """Every thread layout of the fused pass keeps per-particle parity."""
+    from haissinskijulia_b200 import Context
+    ctx = Context(0)
+    ctx.set_pass_layout(layout)
+    cfg = benchmark_ring(n_turns=20, nbins=4096)
+    run_turn_by_turn(ctx, oracle, cfg, 100_003, 20, seed=40 + layout, check_every=4)
+
+
 @pytest.mark.parametrize("flag", ["use_wakefield", "update_E0", "update_eta", "SR_damping",
                                   "use_excitation"])
 def test_physics_switches(gpu_ctx, oracle, flag):
