@@ -24,6 +24,8 @@
 // deposit of the particle pass, the mean energy change of the turn
 // (src/evolution.jl:401-429), the new E0 and the scalars of the next turn,
 // so a turn needs no host round trip.
+#include <cooperative_groups.h>
+
 #include "hj_internal.h"
 
 namespace hj {
@@ -115,54 +117,85 @@ __device__ __forceinline__ void dftR(double2* v) {
 
 constexpr int kMaxFftH = 8192;   // largest shared-memory transform (B = 16384)
 
+// Twiddle tables of a length-H transform in shared memory:
+//   tw[j] = w_H^j, j < H/2 (the last, radix-2 or radix-4, pass reads it with
+//           unit stride);
+//   ct[(Ns-1)/7 + jm] = w_{8 Ns}^jm, jm < Ns, one compact row per radix-8
+//           pass (Ns = 1, 8, 64, ...), so that pass also reads unit stride.
+// A butterfly's q-th twiddle is w1^q, w1 = w_{Ns R}^jm (a few complex
+// multiplications instead of R-1 scattered table reads).
+struct FftTables {
+  const double2* tw;
+  const double2* ct;
+};
+
+__device__ __forceinline__ int compact_table_size(int H) { return H / 7 + 2; }
+
 template <int LR, bool INV>
-__device__ __forceinline__ void stockham_pass(double2* s, const double2* tw, int N, int Ns) {
+__device__ __forceinline__ void stockham_pass(double2* s, FftTables t, int N, int Ns) {
   constexpr int R = 1 << LR;
   constexpr int PER = (kMaxFftH / R + kBinsThreads - 1) / kBinsThreads;
   const int nb = N >> LR;
-  const int step = N / (Ns * R);
   double2 v[PER][R];
 #pragma unroll
-  for (int t = 0; t < PER; ++t) {
-    const int j = threadIdx.x + t * kBinsThreads;
+  for (int u = 0; u < PER; ++u) {
+    const int j = threadIdx.x + u * kBinsThreads;
     if (j < nb) {
       const int jm = j & (Ns - 1);
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[t][q] = s[j + q * nb];
-#pragma unroll
-      for (int q = 1; q < R; ++q) v[t][q] = cmul(v[t][q], twiddle(tw, q * jm * step, N >> 1, INV));
-      dftR<LR, INV>(v[t]);
+      for (int q = 0; q < R; ++q) v[u][q] = s[j + q * nb];
+      double2 w1 = (LR == 3) ? t.ct[(Ns - 1) / 7 + jm] : t.tw[jm];   // last pass: Ns R = N
+      if (INV) w1.y = -w1.y;
+      if (LR >= 1) v[u][1] = cmul(v[u][1], w1);
+      if (LR >= 2) {
+        const double2 w2 = cmul(w1, w1);
+        v[u][2] = cmul(v[u][2], w2);
+        const double2 w3 = cmul(w2, w1);
+        v[u][3] = cmul(v[u][3], w3);
+        if (LR == 3) {
+          const double2 w4 = cmul(w2, w2);
+          v[u][4] = cmul(v[u][4], w4);
+          v[u][5] = cmul(v[u][5], cmul(w4, w1));
+          v[u][6] = cmul(v[u][6], cmul(w4, w2));
+          v[u][7] = cmul(v[u][7], cmul(w4, w3));
+        }
+      }
+      dftR<LR, INV>(v[u]);
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int t = 0; t < PER; ++t) {
-    const int j = threadIdx.x + t * kBinsThreads;
+  for (int u = 0; u < PER; ++u) {
+    const int j = threadIdx.x + u * kBinsThreads;
     if (j < nb) {
       const int jm = j & (Ns - 1);
       const int base = ((j - jm) << LR) + jm;
 #pragma unroll
-      for (int q = 0; q < R; ++q) s[base + q * Ns] = v[t][q];
+      for (int q = 0; q < R; ++q) s[base + q * Ns] = v[u][q];
     }
   }
   __syncthreads();
 }
 
 template <bool INV>
-__device__ void smem_fft(double2* s, const double2* tw, int N, int logN) {
+__device__ void smem_fft(double2* s, FftTables t, int N, int logN) {
   int Ns = 1, rem = logN;
   while (rem >= 3) {
-    stockham_pass<3, INV>(s, tw, N, Ns);
+    stockham_pass<3, INV>(s, t, N, Ns);
     Ns <<= 3;
     rem -= 3;
   }
-  if (rem == 2) stockham_pass<2, INV>(s, tw, N, Ns);
-  else if (rem == 1) stockham_pass<1, INV>(s, tw, N, Ns);
+  if (rem == 2) stockham_pass<2, INV>(s, t, N, Ns);
+  else if (rem == 1) stockham_pass<1, INV>(s, t, N, Ns);
 }
 
-// Twiddles of the length-H transform into shared memory: w_H^j = twP[4j].
-__device__ void load_twiddles(double2* tw, int H, const double2* __restrict__ twP) {
+// Twiddle tables of the length-H transform into shared memory (w_H^j = twP[4j]).
+__device__ void load_twiddles(double2* tw, double2* ct, int H, const double2* __restrict__ twP) {
   for (int j = threadIdx.x; j < (H >> 1); j += blockDim.x) tw[j] = __ldg(&twP[4 * j]);
+  for (int Ns = 1; 8 * Ns <= H; Ns <<= 3) {
+    const int off = (Ns - 1) / 7, stride = H / (8 * Ns);
+    for (int jm = threadIdx.x; jm < Ns; jm += blockDim.x) ct[off + jm] = __ldg(&twP[4 * jm * stride]);
+  }
   __syncthreads();
 }
 
@@ -170,7 +203,7 @@ __device__ void load_twiddles(double2* tw, int H, const double2* __restrict__ tw
 // X[2m] = FFT_H(x)[m] and X[2m+1] = FFT_H(x[n] w_M^n)[m], since x[n] = 0 for n >= H.
 template <typename Vals>
 __device__ void forward_packed(const Vals& v, int L, int H, int logH,
-                               const double2* __restrict__ twP, double2* s, const double2* tw,
+                               const double2* __restrict__ twP, double2* s, FftTables tb,
                                double2* Xg) {
 #pragma unroll 8
   for (int n = threadIdx.x; n < H; n += kBinsThreads) {
@@ -178,7 +211,7 @@ __device__ void forward_packed(const Vals& v, int L, int H, int logH,
     s[n] = make_double2(j < L ? v(j) : 0.0, j + 1 < L ? v(j + 1) : 0.0);
   }
   __syncthreads();
-  smem_fft<false>(s, tw, H, logH);
+  smem_fft<false>(s, tb, H, logH);
   for (int m = threadIdx.x; m < H; m += kBinsThreads) Xg[2 * m] = s[m];
   __syncthreads();
 #pragma unroll 8
@@ -188,7 +221,7 @@ __device__ void forward_packed(const Vals& v, int L, int H, int logH,
     s[n] = cmul(a, __ldg(&twP[2 * n]));  // w_M^n = w_P^{2n}
   }
   __syncthreads();
-  smem_fft<false>(s, tw, H, logH);
+  smem_fft<false>(s, tb, H, logH);
   for (int m = threadIdx.x; m < H; m += kBinsThreads) Xg[2 * m + 1] = s[m];
   __syncthreads();
 }
@@ -203,46 +236,6 @@ __device__ __forceinline__ double2 real_spectrum(const double2* __restrict__ Xg,
   const double2 D = make_double2(0.5 * (xk.x - xc.x), 0.5 * (xk.y - xc.y));
   const double2 O = make_double2(D.y, -D.x);
   return cadd(E, cmul(__ldg(&twP[k]), O));
-}
-
-// In-place pre-inverse phase: from the packed forward transform X of g
-// (in Xg) form, for each pair (k, M-k), the spectrum of g (G = E + w_P^k O),
-// the product Y = G FFT(W) current, and the packed inverse input
-// Z[k] = (Y[k] + conj Y[M-k])/2 + i (Y[k] - conj Y[M-k]) conj(w_P^k)/2, written
-// back over X[k] and X[M-k].  X[M] is X[0]; w_P^{M-k} = -conj(w_P^k).
-__device__ void spectrum_to_inverse_input(double2* Xg, const double2* __restrict__ Wf, int M,
-                                          double current, const double2* __restrict__ twP) {
-  for (int k = threadIdx.x; k <= M / 2; k += kBinsThreads) {
-    const int km = (k == 0) ? 0 : M - k;
-    const double2 xk = Xg[k], xm = Xg[km];
-    const double2 tk = __ldg(&twP[k]);
-    const double2 tm = make_double2(-tk.x, tk.y);             // w_P^{M-k}
-    // G[k] and G[M-k]
-    double2 E = make_double2(0.5 * (xk.x + xm.x), 0.5 * (xk.y - xm.y));
-    double2 D = make_double2(0.5 * (xk.x - xm.x), 0.5 * (xk.y + xm.y));
-    const double2 Gk = cadd(E, cmul(tk, make_double2(D.y, -D.x)));
-    E = make_double2(0.5 * (xm.x + xk.x), 0.5 * (xm.y - xk.y));
-    D = make_double2(0.5 * (xm.x - xk.x), 0.5 * (xm.y + xk.y));
-    const double2 Gm = cadd(E, cmul(tm, make_double2(D.y, -D.x)));
-    double2 Yk = cmul(Gk, __ldg(&Wf[k]));
-    double2 Ym = cmul(Gm, __ldg(&Wf[M - k]));
-    Yk.x *= current;
-    Yk.y *= current;
-    Ym.x *= current;
-    Ym.y *= current;
-    // Z[k]
-    double2 Ez = make_double2(0.5 * (Yk.x + Ym.x), 0.5 * (Yk.y - Ym.y));
-    double2 Dz = make_double2(0.5 * (Yk.x - Ym.x), 0.5 * (Yk.y + Ym.y));
-    double2 Oz = cmul(Dz, cconj(tk));
-    Xg[k] = make_double2(Ez.x - Oz.y, Ez.y + Oz.x);
-    if (k != 0 && km != k) {
-      // Z[M-k]
-      Ez = make_double2(0.5 * (Ym.x + Yk.x), 0.5 * (Ym.y - Yk.y));
-      Dz = make_double2(0.5 * (Ym.x - Yk.x), 0.5 * (Ym.y + Yk.y));
-      Oz = cmul(Dz, cconj(tm));
-      Xg[km] = make_double2(Ez.x - Oz.y, Ez.y + Oz.x);
-    }
-  }
 }
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
@@ -277,8 +270,9 @@ __global__ void __launch_bounds__(kBinsThreads)
                     const double2* __restrict__ twP, double2* Xg, double2* Wf) {
   extern __shared__ __align__(16) double2 s_fft[];
   double2* s_tw = s_fft + H;
-  load_twiddles(s_tw, H, twP);
-  forward_packed(WakeVals{W}, B, H, logH, twP, s_fft, s_tw, Xg);
+  double2* s_ct = s_tw + H / 2;
+  load_twiddles(s_tw, s_ct, H, twP);
+  forward_packed(WakeVals{W}, B, H, logH, twP, s_fft, FftTables{s_tw, s_ct}, Xg);
   for (int k = threadIdx.x; k <= M; k += blockDim.x) Wf[k] = real_spectrum(Xg, k, M, twP);
 }
 
@@ -320,12 +314,22 @@ __device__ __forceinline__ double global_std(double s, double s2, int64_t n) {
   return sqrt(sv);
 }
 
-__global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
+// The bins step as a cluster of two CTAs.  With k even (CTA 0) or odd (CTA 1),
+// X[k], its partner X[M-k], the spectrum product and the inverse input Z[k]
+// all have the same parity, so each CTA runs one forward length-H FFT, its
+// half of the spectrum and one inverse length-H FFT in its own shared memory;
+// the halves are combined through distributed shared memory.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1)
+    k_bins(BinsArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
   extern __shared__ __align__(16) double2 s_fft[];
   __shared__ double red[kBinsThreads / 32];
   __shared__ double sh[8];
+  __shared__ double s_peer_sum;
 
-  // 1. partial sums of the particle pass, fixed block order
+  // 1. partial sums of the particle pass, fixed block order (both CTAs)
   //    sh[0..3] = Σz, Σz², Σ(ΔE - ΔE_start), particles inside the bin range
   if (!a.conv_only) {
     double t[kNumSums] = {0.0, 0.0, 0.0, 0.0};
@@ -366,58 +370,95 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
   double sum_kick = 0.0;
 
   if (a.use_wake) {
-    if (!do_conv) {
-      for (int i = threadIdx.x; i < a.B; i += blockDim.x) a.pot[i] = 0.0;
-    } else {
+    if (do_conv && a.H >= 4) {
+      const int H = a.H, M = a.M;
+      double2* s = s_fft;
+      double2* s_tw = s_fft + H;
+      double2* s_ct = s_tw + H / 2;
+      const FftTables tb{s_tw, s_ct};
+      load_twiddles(s_tw, s_ct, H, a.twP);
       const double inv_n = 1.0 / sh[3];                          // src/wakefield.jl:207
-      if (a.H >= 4) {
-        double2* s_tw = s_fft + a.H;
-        load_twiddles(s_tw, a.H, a.twP);
-        forward_packed(DensityVals{a.cnt, a.lam, inv_n}, a.B, a.H, a.logH, a.twP, s_fft,
-                       s_tw, a.Xg);
-        spectrum_to_inverse_input(a.Xg, a.Wf, a.M, current, a.twP);
-        __syncthreads();
-        // inverse of the even half -> zE
+      const DensityVals g{a.cnt, a.lam, inv_n};
+      // x[n] = g[2n] + i g[2n+1] (times w_M^n in the odd CTA)
 #pragma unroll 8
-        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) s_fft[m] = a.Xg[2 * m];
-        __syncthreads();
-        smem_fft<true>(s_fft, s_tw, a.H, a.logH);
-        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) a.zE[m] = s_fft[m];
-        __syncthreads();
-        // inverse of the odd half, combined with the even half into the potential
-#pragma unroll 8
-        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) s_fft[m] = a.Xg[2 * m + 1];
-        __syncthreads();
-        smem_fft<true>(s_fft, s_tw, a.H, a.logH);
-        const double invM = 1.0 / (double)a.M;
-#pragma unroll 8
-        for (int m = threadIdx.x; m < a.H; m += kBinsThreads) {
-          const double2 zo = cmul(s_fft[m], cconj(__ldg(&a.twP[2 * m])));
-          const double2 ze = a.zE[m];
-          const double re = (ze.x + zo.x) * invM, im = (ze.y + zo.y) * invM;
-          const int j = 2 * m;
-          if (j < a.B) a.pot[j] = re;
-          if (j + 1 < a.B) a.pot[j + 1] = im;
+      for (int n = threadIdx.x; n < H; n += kBinsThreads) {
+        const int j = 2 * n;
+        const double2 x = make_double2(j < a.B ? g(j) : 0.0, j + 1 < a.B ? g(j + 1) : 0.0);
+        s[n] = rank ? cmul(x, __ldg(&a.twP[2 * n])) : x;
+      }
+      __syncthreads();
+      smem_fft<false>(s, tb, H, a.logH);                         // s[m] = X[2m + rank]
+      // spectrum pairs (k, M-k) of this parity, in place
+      const int mlast = rank ? H / 2 - 1 : H / 2;
+      for (int m = threadIdx.x; m <= mlast; m += kBinsThreads) {
+        const int k = 2 * m + rank;
+        const int mp = rank ? H - 1 - m : (m == 0 ? 0 : H - m);  // X[M-k] = s[mp]
+        const double2 xk = s[m], xm = s[mp];
+        const double2 tk = __ldg(&a.twP[k]);
+        const double2 tm = make_double2(-tk.x, tk.y);           // w_P^{M-k}
+        double2 E = make_double2(0.5 * (xk.x + xm.x), 0.5 * (xk.y - xm.y));
+        double2 D = make_double2(0.5 * (xk.x - xm.x), 0.5 * (xk.y + xm.y));
+        const double2 Gk = cadd(E, cmul(tk, make_double2(D.y, -D.x)));
+        E = make_double2(0.5 * (xm.x + xk.x), 0.5 * (xm.y - xk.y));
+        D = make_double2(0.5 * (xm.x - xk.x), 0.5 * (xm.y + xk.y));
+        const double2 Gm = cadd(E, cmul(tm, make_double2(D.y, -D.x)));
+        double2 Yk = cmul(Gk, __ldg(&a.Wf[k]));
+        double2 Ym = cmul(Gm, __ldg(&a.Wf[M - k]));
+        Yk.x *= current;
+        Yk.y *= current;
+        Ym.x *= current;
+        Ym.y *= current;
+        double2 Ez = make_double2(0.5 * (Yk.x + Ym.x), 0.5 * (Yk.y - Ym.y));
+        double2 Dz = make_double2(0.5 * (Yk.x - Ym.x), 0.5 * (Yk.y + Ym.y));
+        double2 Oz = cmul(Dz, cconj(tk));
+        const double2 Zk = make_double2(Ez.x - Oz.y, Ez.y + Oz.x);
+        if (mp != m && !(rank == 0 && m == 0)) {
+          Ez = make_double2(0.5 * (Ym.x + Yk.x), 0.5 * (Ym.y - Yk.y));
+          Dz = make_double2(0.5 * (Ym.x - Yk.x), 0.5 * (Ym.y + Yk.y));
+          Oz = cmul(Dz, cconj(tm));
+          s[mp] = make_double2(Ez.x - Oz.y, Ez.y + Oz.x);
         }
-      } else {
-        // Tiny grids (P < 16): direct causal convolution.
-        if (threadIdx.x == 0) {
-          for (int i = 0; i < a.B; ++i) {
-            double acc = 0.0;
-            for (int j = 0; j <= i; ++j)
-              acc += a.W[j] * (a.lam[i - j] * ((double)a.cnt[i - j] * inv_n));
-            a.pot[i] = acc * current;
-          }
+        s[m] = Zk;
+      }
+      __syncthreads();
+      smem_fft<true>(s, tb, H, a.logH);                          // unnormalised inverse
+      cluster.sync();
+      // z[n] = (zE[n] + conj(w_M^n) zO[n]) / M, pot[2n] = Re z, pot[2n+1] = Im z
+      const double2* sE = cluster.map_shared_rank(s_fft, 0);
+      const double2* sO = cluster.map_shared_rank(s_fft, 1);
+      const double invM = 1.0 / (double)M;
+      const int n0 = rank * (H / 2), n1 = n0 + H / 2;
+#pragma unroll 4
+      for (int n = n0 + threadIdx.x; n < n1; n += kBinsThreads) {
+        const double2 zo = cmul(sO[n], cconj(__ldg(&a.twP[2 * n])));
+        const double2 ze = sE[n];
+        const int j = 2 * n;
+        if (j < a.B) a.pot[j] = (ze.x + zo.x) * invM;
+        if (j + 1 < a.B) a.pot[j + 1] = (ze.y + zo.y) * invM;
+      }
+    } else if (do_conv) {
+      // Tiny grids (P < 16): direct causal convolution in CTA 0.
+      if (rank == 0 && threadIdx.x == 0) {
+        const double inv_n = 1.0 / sh[3];
+        for (int i = 0; i < a.B; ++i) {
+          double acc = 0.0;
+          for (int j = 0; j <= i; ++j)
+            acc += a.W[j] * (a.lam[i - j] * ((double)a.cnt[i - j] * inv_n));
+          a.pot[i] = acc * current;
         }
       }
+    } else {
+      for (int i = rank * kBinsThreads + threadIdx.x; i < a.B; i += 2 * kBinsThreads) a.pot[i] = 0.0;
     }
+    cluster.sync();   // pot complete; the peer is done reading this CTA's shared memory
     // The next pass kicks with lerp = pot[k] + w (pot[k+1] - pot[k]); the same
     // table gives Σ_i lerp(pot, z_i) from the CIC deposit: with C[k] particles
     // in cell k and S[k] = Σ w·2^24 over them,
     //   Σ_i lerp = Σ_k C[k] pot[k] + 2^-24 Σ_k S[k] (pot[k+1] - pot[k]).
-    __syncthreads();
     if (a.potd || a.cic) {
-      for (int k = threadIdx.x; k < a.B; k += blockDim.x) {
+      const int half = (a.B + 1) / 2;
+      const int k1 = min(a.B, (rank + 1) * half);
+      for (int k = rank * half + threadIdx.x; k < k1; k += blockDim.x) {
         const double p0 = a.pot[k];
         const double d = (k + 1 < a.B) ? a.pot[k + 1] - p0 : 0.0;
         if (a.potd) a.potd[k] = make_double2(p0, d);
@@ -426,9 +467,12 @@ __global__ void __launch_bounds__(kBinsThreads) k_bins(BinsArgs a) {
     }
   }
   sum_kick = block_sum(sum_kick, red);
+  if (rank == 1 && threadIdx.x == 0) *cluster.map_shared_rank(&s_peer_sum, 0) = sum_kick;
+  cluster.sync();
 
-  // 4. E0 update and next-turn scalars (src/evolution.jl:401-451, :300-304)
-  if (threadIdx.x == 0 && !a.conv_only) {
+  // E0 update and next-turn scalars (src/evolution.jl:401-451, :300-304)
+  if (rank == 0 && threadIdx.x == 0 && !a.conv_only) {
+    sum_kick += s_peer_sum;
     const double E0 = ts->cur.E0;
     double mean = 0.0;
     if (a.params.update_E0) mean = (sh[2] - sum_kick) / (double)a.n;
@@ -457,10 +501,10 @@ cudaError_t prepare_wake_kernels(int max_smem) {
   return e;
 }
 
-// FFT data (H complex) + twiddles (H/2 complex).
+// FFT data (H complex) + twiddles (H/2) + compact radix-8 twiddle rows.
 size_t bins_smem_bytes(int H) {
   const int h = H < 4 ? 4 : H;
-  return (size_t)(h + h / 2) * sizeof(double2);
+  return (size_t)(h + h / 2 + h / 7 + 2) * sizeof(double2);
 }
 
 cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, int logH,
@@ -473,7 +517,7 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
 
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st) {
   size_t smem = bins_smem_bytes(a.H);
-  k_bins<<<1, kBinsThreads, smem, st>>>(a);
+  k_bins<<<2, kBinsThreads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
