@@ -5,6 +5,8 @@
 // (particle pass, histogram reduction, bins step) whose turn-to-turn state
 // (E0, pending kick, turn counter) lives in device memory, so turns never
 // wait for the host.
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -38,6 +40,10 @@ struct hj_bunch {
   int use_wake = 0;
   int B = 0, P = 0, M = 0, H = 0, logH = 0;
   double e0 = 0, eN = 0, estep = 0, inv_e = 0, c1 = 0, cB = 0, inv_c = 0;
+  // interpolation the reference applies to every z >= cB (src/wakefield.jl:80-102):
+  // u = (cB - c1)/Δc, cell clamp(floor(u), 0, B-2), weight u - floor(u)
+  int hi_idx = 0;
+  double hi_w = 0;
   std::vector<double> centers;
   double sigma_E0_initial = 0, sigma_z0_initial = 0;
   uint64_t seed = 0;
@@ -49,9 +55,9 @@ struct hj_bunch {
   // device buffers
   TurnState* ts = nullptr;
   double* pot = nullptr;
-  double2* potd = nullptr;              // (pot[k], pot[k+1]-pot[k])
+  double2* potd = nullptr;              // [B+1] kick table (cell j: pot[j-1], step)
   int cfg = 0;                          // thread layout of the fused pass
-  unsigned long long* hist = nullptr;   // counts[B] | CIC counts[B] | CIC Σw·2^24 [B]
+  unsigned long long* hist = nullptr;   // counts[B] | cell counts[B+1] | cell Σw·2^24 [B+1]
   double* lam = nullptr;
   double* W = nullptr;
   double2* Wf = nullptr;
@@ -60,6 +66,7 @@ struct hj_bunch {
   double2* zE = nullptr;
   uint32_t* part_cnt = nullptr;
   unsigned long long* part_cic = nullptr;
+  unsigned long long* ngp_ovf = nullptr;   // [B] overflow of the pass's 16-bit counters
   double* part_sum = nullptr;
   double* part_mom = nullptr;
   double* h_mom = nullptr;    // pinned
@@ -206,6 +213,8 @@ hj_status launch_moments(hj_bunch* b, int apply, double* z_out, double* dE_out) 
   f.c1 = b->c1;
   f.cB = b->cB;
   f.inv_cstep = b->inv_c;
+  f.e0 = b->e0;
+  f.inv_estep = b->inv_e;
   f.apply = apply;
   f.z_out = z_out;
   f.dE_out = dE_out;
@@ -229,13 +238,13 @@ hj_status read_state(hj_bunch* b) {
   return HJ_OK;
 }
 
-// Thread layout of the fused pass when the context does not pin one: two
-// particles per thread and 1024 threads per block (32 warps per SM) measured
-// fastest at 4096-16384 bins and 1e8 particles on B200.
+// Thread layout of the fused pass when the context does not pin one: four
+// particles per thread with the next four prefetched, 512 threads per block,
+// measured fastest at 4096 and 16384 bins and 1e8 particles on B200.
 int default_pass_layout(int B, int64_t n) {
   (void)B;
   (void)n;
-  return 1;
+  return 0;
 }
 
 void fill_result(hj_bunch* b, const double m[4], hj_result* res) {
@@ -331,7 +340,7 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   cudaStreamSynchronize(b->stream);
   void* dev[] = {b->ts,       b->pot,      b->potd,     b->hist,    b->lam,
                  b->W,        b->Wf,       b->twP,      b->Xg,      b->zE,
-                 b->part_cnt, b->part_cic, b->part_sum, b->part_mom};
+                 b->part_cnt, b->part_cic, b->part_sum, b->part_mom, b->ngp_ovf};
   for (void* p : dev)
     if (p) cudaFree(p);
   if (b->h_mom) cudaFreeHost(b->h_mom);
@@ -403,6 +412,11 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     if (B >= 2) {
       const double step = (b->cB - b->c1) / (double)(B - 1);  // src/wakefield.jl:41-42
       b->inv_c = 1.0 / step;
+      const double u = (b->cB - b->c1) * b->inv_c;          // src/wakefield.jl:81-91
+      const double fl = std::floor(u);
+      const int64_t idx1 = std::min<int64_t>(std::max<int64_t>((int64_t)fl + 1, 1), B - 1);
+      b->hi_idx = (int)(idx1 - 1);
+      b->hi_w = u - fl;
     }
     b->P = (int)next_pow2(2 * (int64_t)B);               // src/evolution.jl:265
     b->M = b->P / 2;
@@ -418,14 +432,15 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     HJ_TRY(dalloc(ctx, &b->Xg, b->M));
     HJ_TRY(dalloc(ctx, &b->zE, std::max(b->H, 1)));
     HJ_TRY(dalloc(ctx, &b->pot, B));
-    HJ_TRY(dalloc(ctx, &b->potd, B));
-    HJ_TRY(dalloc(ctx, &b->hist, 3 * (size_t)B));
+    HJ_TRY(dalloc(ctx, &b->potd, (size_t)B + 1));
+    HJ_TRY(dalloc(ctx, &b->hist, 3 * (size_t)B + 2));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->W, W.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, lam.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->twP, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->pot, 0, sizeof(double) * B, b->stream));
-    HJ_CUDA(ctx, cudaMemsetAsync(b->potd, 0, sizeof(double2) * B, b->stream));
-    HJ_CUDA(ctx, cudaMemsetAsync(b->hist, 0, sizeof(unsigned long long) * 3 * B, b->stream));
+    HJ_CUDA(ctx, cudaMemsetAsync(b->potd, 0, sizeof(double2) * ((size_t)B + 1), b->stream));
+    HJ_CUDA(ctx, cudaMemsetAsync(b->hist, 0, sizeof(unsigned long long) * (3 * (size_t)B + 2),
+                                 b->stream));
     if (b->H >= 4)
       HJ_CUDA(ctx, launch_wake_spectrum(b->W, B, b->P, b->M, b->H, b->logH, b->twP, b->Xg,
                                         b->Wf, b->stream));
@@ -438,7 +453,9 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
   HJ_TRY(dalloc(ctx, &b->part_sum, (size_t)kNumSums * b->nblk));
   if (b->use_wake) {
     HJ_TRY(dalloc(ctx, &b->part_cnt, (size_t)b->nblk * b->B));
-    HJ_TRY(dalloc(ctx, &b->part_cic, (size_t)b->nblk * b->B));
+    HJ_TRY(dalloc(ctx, &b->part_cic, (size_t)b->nblk * ((size_t)b->B + 1)));
+    HJ_TRY(dalloc(ctx, &b->ngp_ovf, (size_t)b->B));
+    HJ_CUDA(ctx, cudaMemsetAsync(b->ngp_ovf, 0, sizeof(unsigned long long) * b->B, b->stream));
   }
 
   TurnState t{};
@@ -510,6 +527,8 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   a.inv_cstep = b->inv_c;
   a.V = b->p.voltage;
   a.phi_s = b->p.phi_s;
+  a.Vs = b->p.voltage * std::sin(b->p.phi_s);
+  a.Vc = b->p.voltage * std::cos(b->p.phi_s);
   a.inv_mass = 1.0 / b->p.mass;
   a.alpha_c = b->p.alpha_c;
   a.two_pi_h = kTwoPi * (double)b->p.harmonic;
@@ -526,6 +545,7 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   a.part_cic = b->part_cic;
   a.part_sum = b->part_sum;
   a.hist_out = b->hist;
+  a.ngp_ovf = b->ngp_ovf;
 
   BinsArgs g{};
   g.ts = b->ts;
@@ -550,6 +570,8 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   g.zE = b->zE;
   g.pot = b->pot;
   g.potd = b->potd;
+  g.hi_idx = b->hi_idx;
+  g.hi_w = b->hi_w;
   g.W = b->W;
   g.conv_only = 0;
 
@@ -569,7 +591,7 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
     if (b->profiling) HJ_CUDA(ctx, cudaEventRecord(ev[1], b->stream));
     if (b->use_wake)
       HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->hist, false,
-                                      b->stream));
+                                      b->stream, b->ngp_ovf));
     HJ_CUDA(ctx, launch_bins(g, b->stream));
     if (b->profiling) {
       HJ_CUDA(ctx, cudaEventRecord(ev[2], b->stream));
@@ -626,9 +648,12 @@ extern "C" hj_status hj_bunch_finish(hj_bunch* b, hj_result* res) {
   if (!b) return HJ_ERR_ARG;
   HJ_TRY(ctx_ok(b->ctx));
   HJ_TRY(launch_moments(b, 1, b->z, b->dE));
+  // nothing is pending any more: the next pass must see a zero kick table
   const int32_t zero = 0;
   HJ_CUDA(b->ctx, cudaMemcpyAsync(&b->ts->pending, &zero, sizeof(int32_t),
                                   cudaMemcpyHostToDevice, b->stream));
+  if (b->potd)
+    HJ_CUDA(b->ctx, cudaMemsetAsync(b->potd, 0, sizeof(double2) * ((size_t)b->B + 1), b->stream));
   double m[4];
   HJ_TRY(read_moments(b, m));
   HJ_TRY(read_state(b));

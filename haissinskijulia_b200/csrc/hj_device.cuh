@@ -3,9 +3,9 @@
 // Per-turn scalars follow src/evolution.jl:300-304 and the step functions
 // src/rf_kick.jl:84-87, src/quantum_excitation.jl:58-71,
 // src/synchrotron_radiation.jl:44-56 of the reference.  The random numbers
-// are Philox-4x32-10 (Salmon, Moraes, Dror & Shaw, "Parallel random numbers:
-// as easy as 1, 2, 3", SC'11) turned into normals by the Box-Muller
-// transform.
+// are Philox-2x32-10 (Salmon, Moraes, Dror & Shaw, "Parallel random numbers:
+// as easy as 1, 2, 3", SC'11), one counter per pair of particles, turned into
+// normals by the Box-Muller transform.
 #pragma once
 
 #include <cstdint>
@@ -34,6 +34,8 @@ struct TurnScalars {
   double damping;     // 1 - ∂U/∂E
   double inv_b2E0;    // 1 / (β0² E0)
   double coeff0;      // 2π h η0 / (β0² E0)  (constant-η drift)
+  double Kz;          // 2π h / (β0² E0 k): drift z -= Kz η_i ΔE
+  double coeff0z;     // coeff0 / k
   int32_t drift_ok;   // apply_phase_advance! runs (β0 > 0, E0 != 0, k != 0)
   int32_t _pad;
 };
@@ -74,6 +76,8 @@ __host__ __device__ inline TurnScalars make_turn_scalars(double E0, const hj_par
   double b2E0 = s.beta0 * s.beta0 * E0;
   s.inv_b2E0 = 1.0 / b2E0;
   s.coeff0 = (kTwoPi * (double)p.harmonic * s.eta0 / b2E0);
+  s.Kz = kTwoPi * (double)p.harmonic * s.inv_b2E0 * s.inv_k;
+  s.coeff0z = s.coeff0 * s.inv_k;
   s.drift_ok = !(s.beta0 <= 0 || E0 == 0 || s.k == 0);
   s._pad = 0;
   return s;
@@ -81,63 +85,45 @@ __host__ __device__ inline TurnScalars make_turn_scalars(double E0, const hj_par
 
 // ------------------------------------------------------------------ Philox
 
-struct U32x4 {
-  uint32_t x, y, z, w;
-};
-
-// Philox-4x32 with 10 rounds: multipliers 0xD2511F53 / 0xCD9E8D57, Weyl key
-// increments 0x9E3779B9 / 0xBB67AE85 (the published constants).
-__host__ __device__ inline U32x4 philox4x32_10(U32x4 c, uint32_t k0, uint32_t k1) {
+// Philox-2x32 with 10 rounds: multiplier 0xD256D193, Weyl key increment
+// 0x9E3779B9 (the published constants).
+__host__ __device__ inline void philox2x32_10(uint32_t& c0, uint32_t& c1, uint32_t k) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
 #if defined(__CUDA_ARCH__)
-    uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
-    uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    const uint32_t hi = __umulhi(0xD256D193u, c0), lo = 0xD256D193u * c0;
 #else
-    uint64_t p0 = (uint64_t)0xD2511F53u * c.x, p1 = (uint64_t)0xCD9E8D57u * c.z;
-    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    const uint64_t pr = (uint64_t)0xD256D193u * c0;
+    const uint32_t hi = (uint32_t)(pr >> 32), lo = (uint32_t)pr;
 #endif
-    U32x4 n;
-    n.x = hi1 ^ c.y ^ k0;
-    n.y = lo1;
-    n.z = hi0 ^ c.w ^ k1;
-    n.w = lo0;
-    c = n;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
+    c0 = hi ^ k ^ c1;
+    c1 = lo;
+    k += 0x9E3779B9u;
   }
-  return c;
 }
 
-// Four standard normals for particles 4q..4q+3 at `turn`: counter
-// (q_lo, q_hi, turn_lo, turn_hi), key (seed_lo, seed_hi); Box-Muller on
-// (x,y) and (z,w) with uniforms u in (0,1): r = sqrt(-2 ln u1),
-// θ = 2π (u2 - 1/2) in (-π, π).  The transform runs in single precision on the
+// Two standard normals for particles 2p and 2p+1 at `turn`: Philox-2x32-10
+// with key = (seed ^ seed >> 32) folded to 32 bits and counter
+// (p mod 2^32, (turn mod 2^24) | (p >> 32) << 24), then the Box-Muller
+// transform of its two uniforms u in (0,1): r = sqrt(-2 ln u1),
+// θ = 2π (u2 - 1/2).  The transform runs in single precision on the
 // special-function unit (__logf, __sincosf: absolute error below 2^-21 on
-// these ranges), and the normals are widened to double before they scale the
-// Float64 kick; the statistical quality of the variates is unaffected at the
-// 1e-6 level.
-__device__ __forceinline__ void philox_normals4(uint64_t seed, int64_t turn, int64_t q,
-                                                double out[4]) {
-  U32x4 c{(uint32_t)q, (uint32_t)((uint64_t)q >> 32), (uint32_t)turn,
-          (uint32_t)((uint64_t)turn >> 32)};
-  U32x4 r = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+// these ranges); the normals are widened to double before they scale the
+// Float64 kick, and their statistics are unaffected at the 1e-6 level.
+__device__ __forceinline__ void philox_normals2(uint64_t seed, int64_t turn, int64_t p,
+                                                double out[2]) {
+  uint32_t c0 = (uint32_t)p;
+  uint32_t c1 = ((uint32_t)turn & 0xFFFFFFu) | ((uint32_t)((uint64_t)p >> 32) << 24);
+  philox2x32_10(c0, c1, (uint32_t)(seed ^ (seed >> 32)));
   const float kScale = 2.3283064365386963e-10f;  // 2^-32
-  const float kTwoPiF = 6.2831853071795865f;
-  const float u1 = fmaf((float)r.x, kScale, 0.5f * kScale);
-  const float u3 = fmaf((float)r.z, kScale, 0.5f * kScale);
-  const float ta = kTwoPiF * fmaf((float)r.y, kScale, -0.5f);
-  const float tb = kTwoPiF * fmaf((float)r.w, kScale, -0.5f);
-  const float ra = sqrtf(-2.0f * __logf(u1));
-  const float rb = sqrtf(-2.0f * __logf(u3));
-  float sa, ca, sb, cb;
-  __sincosf(ta, &sa, &ca);
-  __sincosf(tb, &sb, &cb);
-  out[0] = (double)(ra * ca);
-  out[1] = (double)(ra * sa);
-  out[2] = (double)(rb * cb);
-  out[3] = (double)(rb * sb);
+  const float u1 = fmaf((float)c0, kScale, 0.5f * kScale);
+  const float th = 6.2831853071795865f * fmaf((float)c1, kScale, -0.5f);
+  const float m2l = fmaxf(-2.0f * __logf(u1), 1e-30f);
+  const float rad = m2l * rsqrtf(m2l);                        // sqrt without a slow path
+  float sn, cs;
+  __sincosf(th, &sn, &cs);
+  out[0] = (double)(rad * cs);
+  out[1] = (double)(rad * sn);
 }
 
 }  // namespace hj

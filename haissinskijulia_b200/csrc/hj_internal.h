@@ -20,7 +20,7 @@ constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 // Thread layouts of the fused pass: 0 = 4 particles/thread, 512 threads,
 // next group prefetched; 1 = 2 particles/thread, 1024 threads; 2 = 2
 // particles/thread, 512 threads.
-constexpr int kNumPassCfgs = 3;
+constexpr int kNumPassCfgs = 4;
 int pass_cfg_threads(int cfg);
 int pass_cfg_ppt(int cfg);
 
@@ -33,7 +33,7 @@ struct PassArgs {
   double* dE;
   int64_t n;
   TurnState* ts;
-  const double2* potd;     // (pot[k], pot[k+1]-pot[k]) of the previous turn
+  const double2* potd;     // [B+1] kick table of the previous turn (cell j: pot[j-1], step)
   // bin grid
   int32_t B;
   int32_t use_wake;
@@ -41,6 +41,7 @@ struct PassArgs {
   double c1, cB, inv_cstep;       // interpolation (centers)
   // physics constants of the run
   double V, phi_s, inv_mass, alpha_c, two_pi_h;
+  double Vs, Vc;           // V sin ϕs, V cos ϕs
   int32_t update_eta, update_E0, sr, qe_mode;
   int32_t cfg;             // thread layout (kNumPassCfgs)
   uint64_t seed;
@@ -49,9 +50,10 @@ struct PassArgs {
   int64_t draws_turns;
   // per-block outputs
   uint32_t* part_cnt;              // [grid][B]
-  unsigned long long* part_cic;    // [grid][B] packed CIC (count << 44 | Σw·2^24)
+  unsigned long long* part_cic;    // [grid][B+1] packed cell deposit (count << 44 | Σw·2^24)
   double* part_sum;                // [grid][kNumSums]
-  unsigned long long* hist_out;    // [3B] merged histograms, zeroed by the pass
+  unsigned long long* hist_out;    // [3B+2] merged histograms, zeroed by the pass
+  unsigned long long* ngp_ovf;     // [B] counts beyond the 16-bit per-block counters
 };
 
 // Arguments of the per-turn bins step (single CTA).
@@ -66,14 +68,17 @@ struct BinsArgs {
   int32_t use_wake;
   int32_t B, P, M, H, logH;
   const unsigned long long* cnt;   // [B] bin counts
-  const unsigned long long* cic;   // [2B] CIC counts | CIC Σw·2^24 (NULL: not needed)
+  const unsigned long long* cic;   // [2(B+1)] cell counts | cell Σw·2^24 (NULL: not needed)
   const double* lam;               // [B]
   const double2* Wf;               // [M+1]
   const double2* twP;              // [P]
   double2* Xg;                     // [M]
   double2* zE;                     // [H]
   double* pot;                     // [B]
-  double2* potd;                   // [B] (pot[k], pot[k+1]-pot[k]) for the next pass; NULL: not needed
+  double2* potd;                   // [B+1] kick table for the next pass; NULL: not needed
+  // the reference's interpolation at z >= cB: pot[hi_idx] (1 - hi_w) + pot[hi_idx+1] hi_w
+  int32_t hi_idx;
+  double hi_w;
   const double* W;                 // [B] wake table (direct path for tiny grids)
   // standalone convolution (hj_wake_potential): no turn-state update
   int32_t conv_only;
@@ -91,6 +96,7 @@ struct FlushArgs {
   int32_t B;
   int32_t use_wake, update_E0;
   double c1, cB, inv_cstep;
+  double e0, inv_estep;   // kick-table cell coordinate
   int32_t apply;      // 1: apply pending ops
   double* z_out;      // destination (may alias z/dE); NULL -> not written
   double* dE_out;
@@ -104,11 +110,11 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg);
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
 size_t track_smem_bytes(int B, int use_wake);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
-// out: counts[B] (| CIC counts[B] | CIC Σw·2^24 [B] when part_cic != NULL);
+// out: counts[B] (| cell counts[B+1] | cell Σw·2^24 [B+1] when part_cic != NULL);
 // zero_first clears out before the merge (the fused pass clears it itself).
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
                                int nblk, int B, unsigned long long* out, bool zero_first,
-                               cudaStream_t st);
+                               cudaStream_t st, unsigned long long* ovf = nullptr);
 cudaError_t launch_flush(const FlushArgs& a, int grid, cudaStream_t st);
 cudaError_t launch_histogram_only(const double* z, int64_t n, int B, double e0, double eN,
                                   double inv_estep, uint32_t* part_cnt, int grid,

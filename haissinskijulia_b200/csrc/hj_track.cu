@@ -24,13 +24,27 @@
 //
 // Per-particle arithmetic of the fused pass (the single-step kernels further
 // down keep the reference's exact operation order instead):
-//   * RF kick: V(sin(ϕs - x) - sin ϕs) = V sin ϕs (cos x - 1) - V cos ϕs sin x with
-//     x = z k, sin x and cos x - 1 from their Taylor series through x^15 and
-//     x^16 when |x| <= 0.5 (truncation error < 3e-20); the general sin() path
-//     otherwise.  This avoids the cancellation of sin(ϕ) - sin ϕs.
-//   * 1/γ² of the drift: rcp.approx.ftz.f64 refined by two Newton steps
-//     (relative error at double rounding level).
-//   * reciprocals of k, mass and β0²E0 are precomputed per turn.
+//   * RF kick: V(sin(ϕs - x) - sin ϕs) with x = z k.  x is reduced to
+//     r = x - n π/2, |r| <= π/4 (Cody-Waite with a two-word π/2; n = 0 for
+//     every particle within ±π/(4k) of the synchronous one), and
+//     sin(ϕs - x) = sin θn cos r - cos θn sin r, θn = ϕs - n π/2 (a 4-entry
+//     shared-memory table), with sin r and cos r - 1 from their Taylor series
+//     through r^15 and r^16 (truncation error below 5e-17).  For n = 0 the
+//     kick is V sin ϕs (cos r - 1) - V cos ϕs sin r, free of the cancellation
+//     in sin(ϕ) - sin ϕs.  No branches.
+//   * 1/γ² of the drift: rcp.approx.ftz.f64 refined by one Newton step
+//     (relative error ~1e-14 on a term 5e-5 of η, i.e. ~1e-18 on η).
+//   * drift: z' = z - (2π h / (β0² E0 k)) η_i ΔE, the reference's
+//     z' = (ϕs - (ϕs - z k + coeff ΔE)) / k without its cancellation against
+//     ϕs (the two agree to the reference's own rounding, ~1e-14 of z).
+//   * floor() and round-to-nearest as integers use the 1.5·2^52 addition
+//     (directed-rounding add for floor), the integer read from the low word.
+//   * clamps are compare-and-select (Julia clamp semantics, NaN stays NaN).
+//   * reciprocals of mass and β0²E0 and the RF coefficients V sin ϕs,
+//     V cos ϕs are precomputed.
+//   * switches that are off act through neutral values (a zero kick table
+//     and mean before the first turn, damping 1 without SR, r = 0 without
+//     QE), all exact, so the pass has no per-particle branches on them.
 #include "hj_internal.h"
 
 namespace hj {
@@ -39,12 +53,11 @@ namespace {
 // Run- and turn-constants of the fused pass.
 struct FusedConst {
   double Vs, Vc;            // V sin ϕs, V cos ϕs
-  double V, phi_s, sin_phis;
-  double k, inv_k;
+  double k;
   double excitation, damping;
-  double gamma0, inv_mass, alpha_c, K;   // K = 2π h / (β0² E0)
-  double coeff0;            // K η0 (constant-η drift)
-  int drift_ok, update_eta, sr;
+  double gamma0, inv_mass, alpha_c, Kz;  // Kz = 2π h / (β0² E0 k)
+  double coeff0z;           // Kz η0 (constant-η drift)
+  int drift_ok, update_eta;
 };
 
 // Constants of the single-step phase-advance kernel (reference operation order).
@@ -56,7 +69,13 @@ struct StepConst {
 struct GridConst {
   int B;
   double e0, eN, inv_e, c1, cB, inv_c;
+  double v_off;   // 1/2 - e0/Δe: v = z/Δe + v_off is the cell coordinate of the kick table
 };
+
+// 1/2 - e0/Δe, rounded the same way by every kernel that forms cell coordinates.
+__device__ __forceinline__ double kick_offset(double e0, double inv_e) {
+  return __dsub_rn(0.5, __dmul_rn(e0, inv_e));
+}
 
 __device__ __forceinline__ int cic_hi(int B) { return B >= 2 ? B - 2 : 0; }
 
@@ -89,26 +108,75 @@ __device__ __forceinline__ double rcp_approx(double x) {
   return r;
 }
 
+constexpr double kMagic = 6755399441055744.0;   // 1.5·2^52: unit ulp, integer in the low word
+
+// Julia's clamp(x, lo, hi) by compare-and-select (NaN stays NaN).
+__device__ __forceinline__ double clamp_sel(double x, double lo, double hi) {
+  x = (x < lo) ? lo : x;
+  return (x > hi) ? hi : x;
+}
+
 // Interpolation cell of z on the bin centers (src/wakefield.jl:64-78), 0-based:
 // idx = clamp(floor(u), 0, B-2), w = u - floor(u), u = (clamp(z,c1,cB)-c1)/Δc.
-// floor() is a round-down conversion to int (exact: u is within [0, B-1]).
+// floor(u) = (u + 1.5·2^52 rounded down) - 1.5·2^52, exact for 0 <= u < 2^51.
 // The deposit of turn t and the kick applied in turn t+1 call this with the
 // same z, so they agree exactly.
 __device__ __forceinline__ void cic_cell(double z, const GridConst& g, int& idx, double& w) {
-  const double cl = fmin(fmax(z, g.c1), g.cB);
+  const double cl = clamp_sel(z, g.c1, g.cB);
   const double u = __dmul_rn(__dsub_rn(cl, g.c1), g.inv_c);
-  const int i = __double2int_rd(u);
-  w = __dsub_rn(u, (double)i);
-  idx = min(max(i, 0), cic_hi(g.B));
+  const double fm = __dadd_rd(u, kMagic);
+  w = __dsub_rn(u, __dsub_rn(fm, kMagic));
+  idx = min(max(__double2loint(fm), 0), cic_hi(g.B));
 }
 
-// Kick of the fused pass: lerp from the (pot[k], pot[k+1] - pot[k]) table.
+// Cell of the kick table (B + 1 cells): v = z/Δe + 1/2 - e0/Δe (one FMA),
+// j = floor(v) clamped to [0, B], w = v - floor(v).  Cell j >= 1 is the
+// reference's interpolation cell j-1 between centres c[j-1] and c[j]
+// (src/wakefield.jl:64-78); cells 0 and B hold the flat ends pot[0] and pot[B-1]
+// that the reference's clamp of z to [c1, cB] gives, so out-of-range particles need
+// no clamp of z.  v agrees with the reference's (z - c1)/Δc to ~1e-15 of the bin
+// count, so the kick agrees to that fraction of a bin-to-bin potential step.
+// floor(v): the low word of (v + 1.5·2^52 rounded down) when the high word is
+// 0x43380000 (0 <= v < 2^32); other high words mean v < 0 (cell 0) or v >= 2^32,
+// +inf and NaN (cell B) -- every z lands in a valid cell.
+__device__ __forceinline__ void kick_cell(double z, const GridConst& g, int& j, double& w) {
+  const double v = fma(z, g.inv_e, g.v_off);
+  const double fm = __dadd_rd(v, kMagic);
+  w = __dsub_rn(v, __dsub_rn(fm, kMagic));
+  const int t = __double2hiint(fm) - 0x43380000;
+  const unsigned lo = (unsigned)__double2loint(fm);
+  j = (t == 0) ? (int)min(lo, (unsigned)g.B) : (t > 0 ? g.B : 0);
+}
+
+__device__ __forceinline__ double2 ld_table(const double2* p) {
+  double2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f64 {%0,%1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+
+// Table entry and weight of the kick of z (issued early: the gather's latency
+// overlaps the RF and QE arithmetic of the pass).
+struct KickFetch {
+  double2 pd;
+  double w;
+};
+__device__ __forceinline__ KickFetch kick_fetch(double z, const GridConst& g,
+                                                const double2* __restrict__ potd) {
+  int j;
+  KickFetch f;
+  kick_cell(z, g, j, f.w);
+  f.pd = ld_table(potd + j);
+  return f;
+}
+
+// Kick of the fused pass: lerp from the kick table, cell j holding
+// (pot at its left centre, pot step to its right centre), zero step in cells 0 and B.
 __device__ __forceinline__ double wake_kick(double z, const GridConst& g,
                                             const double2* __restrict__ potd) {
-  int idx;
+  int j;
   double w;
-  cic_cell(z, g, idx, w);
-  const double2 pd = __ldg(potd + idx);
+  kick_cell(z, g, j, w);
+  const double2 pd = ld_table(potd + j);
   return fma(w, pd.y, pd.x);
 }
 
@@ -126,24 +194,24 @@ __device__ __forceinline__ double wake_kick_ref(double z, const GridConst& g,
 
 // Histogram bin of z (src/utils.jl:387-397), 0-based: clamp(floor((z-e0)/Δe), 0, B-1),
 // with (z - e0) and the product rounded exactly as the reference rounds them.
+// Only in-range particles are counted, and for them 0 <= u <= B.
 __device__ __forceinline__ int ngp_bin(double z, const GridConst& g, bool& in) {
+  in = (z >= g.e0) & (z <= g.eN);
+  const double u = __dmul_rn(__dsub_rn(z, g.e0), g.inv_e);
+  return min(max(__double2loint(__dadd_rd(u, kMagic)), 0), g.B - 1);
+}
+
+// Reference-form bin for the single-step histogram kernel (any z).
+__device__ __forceinline__ int ngp_bin_any(double z, const GridConst& g, bool& in) {
   in = (z >= g.e0) & (z <= g.eN);
   const int j = __double2int_rd(__dmul_rn(__dsub_rn(z, g.e0), g.inv_e));
   return min(max(j, 0), g.B - 1);
 }
 
-// V(sin(ϕs - x) - sin ϕs) for |x| > 0.5, as the reference forms it.
-__device__ __noinline__ double rf_kick_general(double z, double k, double phi_s,
-                                               double sin_phis, double V) {
-  return V * (sin(fma(-z, k, phi_s)) - sin_phis);
-}
-
-// V(sin(ϕs - x) - sin ϕs), x = z k, by angle addition and Taylor series.
-__device__ __forceinline__ double rf_kick_term(double z, const FusedConst& c) {
-  const double x = z * c.k;
-  if (!(fabs(x) <= 0.5)) return rf_kick_general(z, c.k, c.phi_s, c.sin_phis, c.V);
-  const double t = x * x;
-  // sin x = x + x^3 P(t): coefficients (-1)^n / (2n+1)!, n = 1..7
+// sin r and cos r - 1 for |r| <= π/4: Taylor series through r^15 and r^16.
+__device__ __forceinline__ void sincm1_poly(double r, double& sn, double& cm1) {
+  const double t = r * r;
+  // sin r = r + r^3 P(t): coefficients (-1)^m / (2m+1)!, m = 1..7
   double p = -7.647163731819816e-13;          // -1/15!
   p = fma(t, p, 1.6059043836821613e-10);      // +1/13!
   p = fma(t, p, -2.505210838544172e-08);      // -1/11!
@@ -151,8 +219,8 @@ __device__ __forceinline__ double rf_kick_term(double z, const FusedConst& c) {
   p = fma(t, p, -1.984126984126984e-04);      // -1/7!
   p = fma(t, p, 8.333333333333333e-03);       // +1/5!
   p = fma(t, p, -1.6666666666666666e-01);     // -1/3!
-  const double sn = fma(t * x, p, x);
-  // cos x - 1 = t Q(t): coefficients (-1)^n / (2n)!, n = 1..8
+  sn = fma(t * r, p, r);
+  // cos r - 1 = t Q(t): coefficients (-1)^m / (2m)!, m = 1..8
   double q = 4.779477332387385e-14;           // +1/16!
   q = fma(t, q, -1.1470745597729725e-11);     // -1/14!
   q = fma(t, q, 2.08767569878681e-09);        // +1/12!
@@ -161,62 +229,88 @@ __device__ __forceinline__ double rf_kick_term(double z, const FusedConst& c) {
   q = fma(t, q, -1.388888888888889e-03);      // -1/6!
   q = fma(t, q, 4.1666666666666664e-02);      // +1/4!
   q = fma(t, q, -0.5);                        // -1/2!
-  const double cm1 = t * q;
-  return fma(c.Vs, cm1, -c.Vc * sn);
+  cm1 = t * q;
 }
 
-// RF kick, QE, SR and drift of one particle for one turn (fused-pass arithmetic).
-__device__ __forceinline__ void turn_particle(double& z, double& e, double r, bool qe,
-                                              const FusedConst& c) {
-  e = e + rf_kick_term(z, c);
-  if (qe) e = fma(c.excitation, r, e);
-  if (c.sr) e = e * c.damping;
-  double coeff;
-  if (c.update_eta) {
-    const double gp = fma(e, c.inv_mass, c.gamma0);   // γ0 + ΔE/m
-    const double g2 = gp * gp;
-    double ri = rcp_approx(g2);
-    ri = fma(ri, fma(-g2, ri, 1.0), ri);
-    ri = fma(ri, fma(-g2, ri, 1.0), ri);
-    coeff = c.K * (c.alpha_c - ri);                    // 2π h η_i / (β0² E0)
-  } else {
-    if (!c.drift_ok) return;                           // apply_phase_advance! skip
-    coeff = c.coeff0;
+// V(sin(ϕs - x) - sin ϕs), x = z k (see the header comment).  When every
+// active lane of the warp has |x| <= π/4 (the bunch core: n = 0) the series
+// runs on x directly; otherwise x = n π/2 + r with n = rint(2x/π) from the
+// 1.5·2^52 addition and r by Cody-Waite with a two-word π/2, and
+// rot[n mod 4] = (V sin θn, V cos θn), θn = ϕs - n π/2, from a shared-memory
+// table; the kick is V sin θn (cos r - 1) - V cos θn sin r + (V sin θn - V sin ϕs).
+__device__ __forceinline__ double rf_term(double z, const FusedConst& c,
+                                          const double2* __restrict__ s_rot) {
+  double r = z * c.k;
+  double sv = c.Vs, cv = c.Vc, off = 0.0;
+  if (!__all_sync(__activemask(), fabs(r) <= 0.78539816339744831)) {
+    const double x = r;
+    const double y = fma(x, 0.63661977236758134, kMagic);  // 2x/π + 1.5·2^52
+    const double nd = y - kMagic;
+    r = fma(-nd, 1.5707963267948966, x);
+    r = fma(-nd, 6.123233995736766e-17, r);
+    const double2 rot = s_rot[__double2loint(y) & 3];
+    sv = rot.x;
+    cv = rot.y;
+    off = sv - c.Vs;
   }
-  double ph = fma(-z, c.k, c.phi_s);                   // ϕ = -(z k - ϕs)
-  ph = fma(coeff, e, ph);
-  z = (c.phi_s - ph) * c.inv_k;                        // z = (-ϕ + ϕs)/k
+  double sn, cm1;
+  sincm1_poly(r, sn, cm1);
+  return fma(sv, cm1, -cv * sn) + off;
 }
 
+// One particle for one turn, given its wake kick (lerp of the previous turn's
+// potential; 0 without the wake) and its RF kick increment rf_term(z), both
+// formed from the z this pass starts from: previous turn's kick and E0
+// re-centring (zero table / zero mean when nothing is pending), RF kick, QE,
+// SR, drift, moments and the deposits.  Without update_η the drift
+// coefficient is the constant-η one (zero when apply_phase_advance! would
+// skip the advance).
 template <bool WAKE>
-__device__ __forceinline__ void pass_particle(double& z, double& e, double r, bool qe,
-                                              const FusedConst& c, const GridConst& g,
-                                              bool pending, bool upd_E0, double pmean,
-                                              const double2* __restrict__ potd, double& acc_z,
+__device__ __forceinline__ void pass_particle(double& z, double& e, double r, double kick,
+                                              double rf, const FusedConst& c,
+                                              const GridConst& g, double pmean, double& acc_z,
                                               double& acc_z2, double& acc_d, uint32_t& n_in,
-                                              uint32_t* s_cnt, uint32_t* s_lo, uint32_t* s_hi) {
-  if (pending) {
-    if (WAKE) e = e - wake_kick(z, g, potd);
-    if (upd_E0) e = e - pmean;
-  }
+                                              uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
+                                              unsigned long long* __restrict__ ngp_ovf) {
+  if (WAKE) e = e - kick;
+  e = e - pmean;
   const double e_start = e;
-  turn_particle(z, e, r, qe, c);
-  if (upd_E0) acc_d += e - e_start;
+  e = e + rf;
+  e = fma(c.excitation, r, e);                         // r = 0 without QE
+  e = e * c.damping;                                   // damping = 1 without SR
+  const double gp = fma(e, c.inv_mass, c.gamma0);     // γ0 + ΔE/m
+  const double g2 = gp * gp;
+  double ri = rcp_approx(g2);
+  ri = fma(ri, fma(-g2, ri, 1.0), ri);
+  const double coeff = c.update_eta ? c.Kz * (c.alpha_c - ri) : c.coeff0z;
+  z = fma(-coeff, e, z);
+  acc_d += e - e_start;
   if (WAKE) {
     acc_z += z;
     acc_z2 = fma(z, z, acc_z2);
     bool in;
     const int j = ngp_bin(z, g, in);
     if (in) {
-      atomicAdd(&s_cnt[j], 1u);
+      // 16-bit counters, two bins per word; the increment that takes a counter
+      // to 2^15 moves 2^15 counts to the global overflow array (at most 1024
+      // more increments can land before the move, so the counter never wraps)
+      const int sh = (j & 1) << 4;
+      const uint32_t old = atomicAdd(&s_ngp[j >> 1], 1u << sh);
+      if (((old >> sh) & 0xFFFFu) == 0x7FFFu) {
+        atomicSub(&s_ngp[j >> 1], 0x8000u << sh);
+        atomicAdd(ngp_ovf + j, 0x8000ull);
+      }
       ++n_in;
     }
-    int idx;
+    // deposit in the kick-table cell the next pass will read for this z
+    int j2;
     double w;
-    cic_cell(z, g, idx, w);
-    const uint32_t q = __double2uint_rn(w * 16777216.0);
-    const uint32_t old = atomicAdd(&s_lo[idx], q);
-    atomicAdd(&s_hi[idx], (1u << (kCicSumBits - 32)) + (old + q < old ? 1u : 0u));
+    kick_cell(z, g, j2, w);
+    // w·2^24 rounded to nearest (at most 2^24; a NaN z lands in cell B with
+    // any q and is flagged by the moments)
+    const uint32_t q = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
+    const uint32_t old = atomicAdd(&s_lo[j2], q);
+    atomicAdd(&s_hi[j2], (1u << (kCicSumBits - 32)) + (old + q < old ? 1u : 0u));
   }
 }
 
@@ -254,11 +348,11 @@ __device__ __forceinline__ void block_sum4(double a0, double a1, double a2, doub
 template <int PPT>
 __device__ __forceinline__ void ldp(const double* p, double v[PPT]) {
   if (PPT == 4) {
-    asm("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+    asm("ld.global.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];"
         : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
         : "l"(p));
   } else {
-    asm("ld.global.v2.f64 {%0,%1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
+    asm("ld.global.L1::no_allocate.v2.f64 {%0,%1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
   }
 }
 
@@ -273,21 +367,12 @@ __device__ __forceinline__ void stp(double* p, const double v[PPT]) {
   }
 }
 
-// Normals of particles PPT*g .. PPT*g+PPT-1 (the Philox quad of particle i is
-// i/4, its lane i%4; a pair uses half of its quad).
+// Normals of particles PPT*g .. PPT*g+PPT-1 (one Philox-2x32 counter per pair).
 template <int PPT>
 __device__ __forceinline__ void group_normals(uint64_t seed, int64_t turn, int64_t g,
                                               double r[PPT]) {
-  double q4[4];
-  philox_normals4(seed, turn, PPT == 4 ? g : (g >> 1), q4);
-  if (PPT == 4) {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) r[j] = q4[j];
-  } else {
-    const int h = (int)(g & 1) * 2;
-    r[0] = q4[h];
-    r[1] = q4[h + 1];
-  }
+  philox_normals2(seed, turn, (PPT / 2) * g, r);
+  if (PPT == 4) philox_normals2(seed, turn, 2 * g + 1, r + 2);
 }
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
@@ -295,36 +380,39 @@ __device__ __forceinline__ void group_normals(uint64_t seed, int64_t turn, int64
 template <bool WAKE, int QE, int PPT, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem_raw);
-  uint32_t* s_lo = s_cnt + (WAKE ? a.B : 0);
-  uint32_t* s_hi = s_lo + (WAKE ? a.B : 0);
+  __shared__ double2 s_rot[4];
+  const int nc = a.B + 1;                 // kick-table cells
+  const int nw = (a.B + 1) / 2;           // words of 16-bit NGP counters
+  uint32_t* s_ngp = reinterpret_cast<uint32_t*>(smem_raw);
+  uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
+  uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
+  if (threadIdx.x == 0) {                 // (V sin θn, V cos θn), θn = ϕs - n π/2
+    s_rot[0] = make_double2(a.Vs, a.Vc);
+    s_rot[1] = make_double2(-a.Vc, a.Vs);
+    s_rot[2] = make_double2(-a.Vs, -a.Vc);
+    s_rot[3] = make_double2(a.Vc, -a.Vs);
+  }
 
   TurnState* ts = a.ts;
   const TurnScalars sc = ts->cur;
-  const bool pending = ts->pending != 0;
-  const double pmean = ts->pending_mean;
+  const double pmean = ts->pending ? ts->pending_mean : 0.0;
   const int64_t turn = ts->turn;
-  const bool upd_E0 = a.update_E0 != 0;
 
   FusedConst c;
-  c.V = a.V;
-  c.phi_s = a.phi_s;
-  c.sin_phis = sc.sin_phis;
-  c.Vs = a.V * sc.sin_phis;
-  c.Vc = a.V * sc.cos_phis;
+  c.Vs = a.Vs;
+  c.Vc = a.Vc;
   c.k = sc.k;
-  c.inv_k = sc.inv_k;
   c.excitation = sc.excitation;
-  c.damping = sc.damping;
+  c.damping = a.sr ? sc.damping : 1.0;
   c.gamma0 = sc.gamma0;
   c.inv_mass = a.inv_mass;
   c.alpha_c = a.alpha_c;
-  c.K = a.two_pi_h * sc.inv_b2E0;
-  c.coeff0 = sc.coeff0;
+  c.Kz = sc.Kz;
+  c.coeff0z = sc.drift_ok ? sc.coeff0z : 0.0;
   c.drift_ok = sc.drift_ok;
   c.update_eta = a.update_eta;
-  c.sr = a.sr;
-  GridConst g{a.B, a.e0, a.eN, a.inv_estep, a.c1, a.cB, a.inv_cstep};
+  GridConst g{a.B, a.e0, a.eN, a.inv_estep, a.c1, a.cB, a.inv_cstep,
+              kick_offset(a.e0, a.inv_estep)};
 
   const double* drow = nullptr;
   if (QE == QE_DRAWS) {
@@ -337,17 +425,17 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   }
 
   if (WAKE) {
-    for (int i = threadIdx.x; i < a.B; i += THREADS) {
-      s_cnt[i] = 0u;
+    for (int i = threadIdx.x; i < nc; i += THREADS) {
+      if (i < nw) s_ngp[i] = 0u;
       s_lo[i] = 0u;
       s_hi[i] = 0u;
     }
     // zero the merged histograms k_hist_reduce accumulates into this turn
     const int gstride = gridDim.x * THREADS;
-    for (int i = blockIdx.x * THREADS + threadIdx.x; i < 3 * a.B; i += gstride)
+    for (int i = blockIdx.x * THREADS + threadIdx.x; i < a.B + 2 * nc; i += gstride)
       a.hist_out[i] = 0ull;
-    __syncthreads();
   }
+  __syncthreads();
 
   double acc_z = 0.0, acc_z2 = 0.0, acc_d = 0.0;
   uint32_t n_in = 0;
@@ -378,6 +466,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
       ldp<PPT>(a.z + PPT * q, zz);
       ldp<PPT>(a.dE + PPT * q, ee);
     }
+    KickFetch kf[PPT];
+    if (WAKE) {
+#pragma unroll
+      for (int j = 0; j < PPT; ++j) kf[j] = kick_fetch(zz[j], g, potd);
+    }
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
     if (QE == QE_PHILOX) {
@@ -388,23 +481,28 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
         for (int j = 0; j < PPT; ++j) rr[j] = __ldg(drow + PPT * q + j);
       }
     }
+    double rf[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rot);
 #pragma unroll
     for (int j = 0; j < PPT; ++j)
-      pass_particle<WAKE>(zz[j], ee[j], rr[j], QE != QE_OFF, c, g, pending, upd_E0, pmean,
-                          potd, acc_z, acc_z2, acc_d, n_in, s_cnt, s_lo, s_hi);
+      pass_particle<WAKE>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].pd.y, kf[j].pd.x) : 0.0,
+                          rf[j], c, g, pmean, acc_z, acc_z2, acc_d, n_in, s_ngp, s_lo, s_hi,
+                          a.ngp_ovf);
     stp<PPT>(a.z + PPT * q, zz);
     stp<PPT>(a.dE + PPT * q, ee);
   }
   // Tail of n % PPT particles: the first threads of block 0, scalar.
   if (blockIdx.x == 0 && threadIdx.x < (int)(a.n % PPT)) {
     const int64_t i = ng * PPT + threadIdx.x;
-    double rr4[4] = {0.0, 0.0, 0.0, 0.0};
-    if (QE == QE_PHILOX) philox_normals4(a.seed, turn, i >> 2, rr4);
-    double r = rr4[i & 3];
-    if (QE == QE_DRAWS && drow) r = __ldg(drow + i);
+    double r2[2] = {0.0, 0.0};
+    if (QE == QE_PHILOX) philox_normals2(a.seed, turn, i >> 1, r2);
+    double r = r2[i & 1];
+    if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
     double z = a.z[i], e = a.dE[i];
-    pass_particle<WAKE>(z, e, r, QE != QE_OFF, c, g, pending, upd_E0, pmean, potd, acc_z,
-                        acc_z2, acc_d, n_in, s_cnt, s_lo, s_hi);
+    const double kick = WAKE ? wake_kick(z, g, potd) : 0.0;
+    pass_particle<WAKE>(z, e, r, kick, rf_term(z, c, s_rot), c, g, pmean, acc_z, acc_z2, acc_d,
+                        n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
     a.z[i] = z;
     a.dE[i] = e;
   }
@@ -415,9 +513,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   if (WAKE) {
     __syncthreads();
     uint32_t* pc = a.part_cnt + (size_t)blockIdx.x * a.B;
-    unsigned long long* pq = a.part_cic + (size_t)blockIdx.x * a.B;
-    for (int i = threadIdx.x; i < a.B; i += THREADS) {
-      pc[i] = s_cnt[i];
+    unsigned long long* pq = a.part_cic + (size_t)blockIdx.x * nc;
+    for (int i = threadIdx.x; i < nc; i += THREADS) {
+      if (i < a.B) pc[i] = (s_ngp[i >> 1] >> ((i & 1) << 4)) & 0xFFFFu;
       pq[i] = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
     }
   }
@@ -426,17 +524,25 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
 // Merge of the per-block histograms.  Grid (bins/256, G): block column g sums
 // the partials of blocks g, g+G, ... and adds them to the merged arrays with
 // integer atomics (exact, so the result does not depend on their order).
-// out layout (u64): counts[B] | CIC counts[B] | CIC Σw·2^24 [B].
+// out layout (u64): counts[B] | cell counts[B+1] | cell Σw·2^24 [B+1].
+// ovf (optional): counts the pass moved out of its 16-bit counters; folded in
+// and cleared for the next turn.
 __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
                               const unsigned long long* __restrict__ part_cic, int nblk, int B,
-                              unsigned long long* __restrict__ out) {
+                              unsigned long long* __restrict__ out,
+                              unsigned long long* __restrict__ ovf) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
+  const int nc = B + 1;
+  if (b >= (part_cic ? nc : B)) return;
   unsigned long long sc = 0ull, sn = 0ull, sw = 0ull;
+  if (ovf && blockIdx.y == 0 && b < B) {
+    sc = ovf[b];
+    ovf[b] = 0ull;
+  }
   for (int k = blockIdx.y; k < nblk; k += gridDim.y) {
-    sc += __ldg(part_cnt + (size_t)k * B + b);
+    if (b < B) sc += __ldg(part_cnt + (size_t)k * B + b);
     if (part_cic) {
-      const unsigned long long v = __ldg(part_cic + (size_t)k * B + b);
+      const unsigned long long v = __ldg(part_cic + (size_t)k * nc + b);
       sn += v >> kCicSumBits;
       sw += v & kCicSumMask;
     }
@@ -444,7 +550,7 @@ __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
   if (sc) atomicAdd(out + b, sc);
   if (part_cic) {
     if (sn) atomicAdd(out + B + b, sn);
-    if (sw) atomicAdd(out + 2 * B + b, sw);
+    if (sw) atomicAdd(out + B + nc + b, sw);
   }
 }
 
@@ -453,7 +559,8 @@ __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
 __global__ void __launch_bounds__(kTrackThreads) k_flush(FlushArgs a) {
   const bool apply = a.apply && a.ts && a.ts->pending;
   const double pmean = apply ? a.ts->pending_mean : 0.0;
-  GridConst g{a.B, 0.0, 0.0, 0.0, a.c1, a.cB, a.inv_cstep};
+  GridConst g{a.B, a.e0, 0.0, a.inv_estep, a.c1, a.cB, a.inv_cstep,
+              kick_offset(a.e0, a.inv_estep)};
   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
@@ -483,7 +590,7 @@ __global__ void __launch_bounds__(kTrackThreads) k_histogram(const double* __res
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     bool in;
-    int j = ngp_bin(__ldg(z + i), g, in);
+    int j = ngp_bin_any(__ldg(z + i), g, in);
     if (in) atomicAdd(&s_cnt[j], 1u);
   }
   __syncthreads();
@@ -510,15 +617,15 @@ __global__ void k_rf_kick(double V, double sin_phis, double k, double phi_s,
 __global__ void k_qe(double excitation, const double* __restrict__ draws, uint64_t seed,
                      int64_t turn, double* __restrict__ dE, int64_t n) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t nq = (n + 3) >> 2;
-  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
-    double rr[4];
-    if (!draws) philox_normals4(seed, turn, q, rr);
+  const int64_t np = (n + 1) >> 1;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += stride) {
+    double rr[2];
+    if (!draws) philox_normals2(seed, turn, p, rr);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int64_t i = 4 * q + j;
+    for (int j = 0; j < 2; ++j) {
+      const int64_t i = 2 * p + j;
       if (i < n) {
-        double r = draws ? __ldg(draws + i) : rr[j];
+        const double r = draws ? __ldg(draws + i) : rr[j];
         dE[i] = __dadd_rn(dE[i], __dmul_rn(excitation, r));
       }
     }
@@ -556,13 +663,12 @@ __global__ void k_phase_advance(StepConst c, const double* __restrict__ dE,
 
 __global__ void k_gaussian(uint64_t seed, int64_t turn, int64_t n, double* __restrict__ out) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t nq = (n + 3) >> 2;
-  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
-    double rr[4];
-    philox_normals4(seed, turn, q, rr);
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if (4 * q + j < n) out[4 * q + j] = rr[j];
+  const int64_t np = (n + 1) >> 1;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += stride) {
+    double rr[2];
+    philox_normals2(seed, turn, p, rr);
+    out[2 * p] = rr[0];
+    if (2 * p + 1 < n) out[2 * p + 1] = rr[1];
   }
 }
 
@@ -591,6 +697,7 @@ const void* pass_fn_wq(int cfg) {
   switch (cfg) {
     case 0: return (const void*)k_track_pass<W, Q, 4, 512>;
     case 1: return (const void*)k_track_pass<W, Q, 2, 1024>;
+    case 3: return (const void*)k_track_pass<W, Q, 2, 768>;
     default: return (const void*)k_track_pass<W, Q, 2, 512>;
   }
 }
@@ -609,7 +716,7 @@ const void* pass_fn(int wake, int qe, int cfg) {
 }
 }  // namespace
 
-int pass_cfg_threads(int cfg) { return cfg == 1 ? 1024 : 512; }
+int pass_cfg_threads(int cfg) { return cfg == 1 ? 1024 : (cfg == 3 ? 768 : 512); }
 int pass_cfg_ppt(int cfg) { return cfg == 0 ? 4 : 2; }
 
 cudaError_t prepare_track_kernels(int max_smem) {
@@ -622,8 +729,11 @@ cudaError_t prepare_track_kernels(int max_smem) {
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
 }
 
+// 16-bit NGP counts [B] (two per word) + two 32-bit words per kick-table cell [B+1].
 size_t track_smem_bytes(int B, int use_wake) {
-  return use_wake ? (size_t)B * (sizeof(unsigned long long) + sizeof(uint32_t)) : 0;
+  return use_wake ? (size_t)((B + 1) / 2) * sizeof(uint32_t) +
+                        (size_t)(B + 1) * sizeof(unsigned long long)
+                  : 0;
 }
 
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
@@ -659,14 +769,15 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
 
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
                                int nblk, int B, unsigned long long* out, bool zero_first,
-                               cudaStream_t st) {
+                               cudaStream_t st, unsigned long long* ovf) {
   if (zero_first) {
-    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long) * (part_cic ? 3 : 1) * B, st);
+    cudaError_t e = cudaMemsetAsync(
+        out, 0, sizeof(unsigned long long) * (part_cic ? 3 * (size_t)B + 2 : (size_t)B), st);
     if (e != cudaSuccess) return e;
   }
   const int G = nblk < 16 ? nblk : 16;
-  dim3 grid((B + 255) / 256, G > 0 ? G : 1);
-  k_hist_reduce<<<grid, 256, 0, st>>>(part_cnt, part_cic, nblk, B, out);
+  dim3 grid((B + 1 + 255) / 256, G > 0 ? G : 1);
+  k_hist_reduce<<<grid, 256, 0, st>>>(part_cnt, part_cic, nblk, B, out, ovf);
   return cudaGetLastError();
 }
 
@@ -700,7 +811,7 @@ cudaError_t launch_rf_kick(double V, double sin_phis, double k, double phi_s,
 
 cudaError_t launch_qe(double excitation, const double* draws, uint64_t seed, int64_t turn,
                       double* dE, int64_t n, cudaStream_t st) {
-  k_qe<<<elementwise_grid((n + 3) / 4), 256, 0, st>>>(excitation, draws, seed, turn, dE, n);
+  k_qe<<<elementwise_grid((n + 1) / 2), 256, 0, st>>>(excitation, draws, seed, turn, dE, n);
   return cudaGetLastError();
 }
 
@@ -730,7 +841,7 @@ cudaError_t launch_phase_advance(int update_eta, TurnScalars s, double inv_mass,
 
 cudaError_t launch_gaussian(uint64_t seed, int64_t turn, int64_t n, double* out,
                             cudaStream_t st) {
-  k_gaussian<<<elementwise_grid((n + 3) / 4), 256, 0, st>>>(seed, turn, n, out);
+  k_gaussian<<<elementwise_grid((n + 1) / 2), 256, 0, st>>>(seed, turn, n, out);
   return cudaGetLastError();
 }
 

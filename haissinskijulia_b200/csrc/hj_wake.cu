@@ -451,18 +451,26 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1)
       for (int i = rank * kBinsThreads + threadIdx.x; i < a.B; i += 2 * kBinsThreads) a.pot[i] = 0.0;
     }
     cluster.sync();   // pot complete; the peer is done reading this CTA's shared memory
-    // The next pass kicks with lerp = pot[k] + w (pot[k+1] - pot[k]); the same
-    // table gives Σ_i lerp(pot, z_i) from the CIC deposit: with C[k] particles
-    // in cell k and S[k] = Σ w·2^24 over them,
-    //   Σ_i lerp = Σ_k C[k] pot[k] + 2^-24 Σ_k S[k] (pot[k+1] - pot[k]).
+    // Kick table of the next pass, B + 1 cells: cell j in 1..B-1 spans centres
+    // c[j-1]..c[j] and holds (pot[j-1], pot[j] - pot[j-1]); cells 0 and B are
+    // flat: pot[0] below c1, and above cB the value the reference's clamped
+    // interpolation takes there, pot[hi] (1 - w) + pot[hi+1] w with u =
+    // (cB - c1)/Δc rounded as it rounds it (pot[B-2] when u is exactly B-1,
+    // src/wakefield.jl:80-102).  With C[j] particles
+    // deposited in cell j and S[j] = Σ w·2^24 over them, the same table gives
+    //   Σ_i lerp(pot, z_i) = Σ_j C[j] pot_j + 2^-24 Σ_j S[j] step_j.
     if (a.potd || a.cic) {
-      const int half = (a.B + 1) / 2;
-      const int k1 = min(a.B, (rank + 1) * half);
-      for (int k = rank * half + threadIdx.x; k < k1; k += blockDim.x) {
-        const double p0 = a.pot[k];
-        const double d = (k + 1 < a.B) ? a.pot[k + 1] - p0 : 0.0;
-        if (a.potd) a.potd[k] = make_double2(p0, d);
-        if (a.cic) sum_kick += (double)a.cic[k] * p0 + (double)a.cic[a.B + k] * 5.9604644775390625e-08 * d;
+      const int nc = a.B + 1;
+      const int half = (nc + 1) / 2;
+      const int j1 = min(nc, (rank + 1) * half);
+      for (int j = rank * half + threadIdx.x; j < j1; j += blockDim.x) {
+        double p0 = a.pot[j > 0 ? j - 1 : 0];
+        if (j == a.B && a.B >= 2)
+          p0 = __dadd_rn(__dmul_rn(a.pot[a.hi_idx], __dsub_rn(1.0, a.hi_w)),
+                         __dmul_rn(a.pot[a.hi_idx + 1], a.hi_w));
+        const double d = (j > 0 && j < a.B) ? a.pot[j] - p0 : 0.0;
+        if (a.potd) a.potd[j] = make_double2(p0, d);
+        if (a.cic) sum_kick += (double)a.cic[j] * p0 + (double)a.cic[nc + j] * 5.9604644775390625e-08 * d;
       }
     }
   }

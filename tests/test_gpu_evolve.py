@@ -84,7 +84,7 @@ def test_reference_ring_reference_wake(gpu_ctx, oracle):
     run_turn_by_turn(gpu_ctx, oracle, cfg, 100_000, 30, seed=1234)
 
 
-@pytest.mark.parametrize("layout", [0, 1, 2])
+@pytest.mark.parametrize("layout", [0, 1, 2, 3])
 def test_thread_layouts(oracle, layout):
     """Every thread layout of the fused pass keeps per-particle parity."""
     from haissinskijulia_b200 import Context
@@ -100,6 +100,61 @@ def test_physics_switches(gpu_ctx, oracle, flag):
     cfg = benchmark_ring(n_turns=20, nbins=1024)
     cfg.params = cfg.params.replace(**{flag: False})
     run_turn_by_turn(gpu_ctx, oracle, cfg, 20_001, 20, seed=7, check_every=5)
+
+
+def test_far_particles_take_the_reduced_rf_path(gpu_ctx, oracle):
+    """Particles far from the synchronous one (|z k| > π/4, outside the bins)
+    go through the fused pass's argument reduction of the RF kick; they must
+    match the oracle's sin() like the rest of the bunch."""
+    cfg = benchmark_ring(n_turns=3, nbins=1024)
+    n = 4099
+    p = synthetic_bunch(n, cfg.sigma_z, cfg.sigma_E, 77)
+    far = np.array([0.05, -0.05, 0.0749, 0.0751, -0.0751, 0.1, -0.15, 0.2, 0.5, -1.0, 3.0, -3.0])
+    p.coordinates.z[::300][: far.size] = far
+    draws = np.random.default_rng(9).normal(size=(3, n))
+    grid = _shared_grid(oracle, p.coordinates.z, cfg)
+    zo, eo = p.coordinates.z.copy(), p.coordinates.dE.copy()
+    buf = create_simulation_buffers(n, cfg.nbins, ctx=gpu_ctx)
+    longitudinal_evolve(p, cfg.params, buf, wake=cfg.wake, grid=grid, qe_draws=draws)
+    rc, _ = oracle.evolve(zo, eo, cfg.params.to_c(), cfg.wake.to_c(), cfg.nbins, grid.to_c(),
+                          np.ascontiguousarray(draws))
+    assert rc == 0
+    assert_close(p.coordinates.z, zo, cfg.sigma_z, what="z")
+    assert_close(p.coordinates.dE, eo, cfg.sigma_E, what="dE")
+
+
+def test_crowded_bin_overflows_the_16bit_counters(gpu_ctx, oracle):
+    """6e6 particles share one bin (every block deposits > 2^15 counts into it),
+    so the pass's 16-bit shared counters overflow into the global array; the
+    counts stay bit-exact and the bunch keeps per-particle parity."""
+    cfg = benchmark_ring(n_turns=3, nbins=256)
+    cfg.params.use_excitation = False
+    n = 6_000_000
+    rng = np.random.default_rng(5)
+    z0 = np.zeros(n)
+    dE0 = np.zeros(n)
+    m = n // 100                      # a Gaussian 1 % keeps σ_z finite
+    z0[:m] = rng.normal(0.0, cfg.sigma_z, m)
+    dE0[:m] = rng.normal(0.0, cfg.sigma_E, m)
+    grid = BinGrid.make(cfg.sigma_z, cfg.nbins, cfg.wake.half_width_sigmas)
+    dz, de = device_pair(z0, dE0)
+    b = ResidentBunch(gpu_ctx, dz.data_ptr(), de.data_ptr(), n, cfg.params, cfg.nbins,
+                      wake=cfg.wake, grid=grid, seed=1)
+    zo, eo = z0.copy(), dE0.copy()
+    st = oracle.state(zo, eo, cfg.params.to_c(), cfg.wake.to_c(), cfg.nbins, grid.to_c())
+    zout, eout = torch.empty_like(dz), torch.empty_like(de)
+    for t in range(1, 4):
+        b.advance(1)
+        assert st.turn(None) == 0
+        b.observe(zout.data_ptr(), eout.data_ptr())
+        zg, eg = zout.cpu().numpy(), eout.cpu().numpy()
+        counts = b.histogram()
+        assert counts.max() >= n - m, "the crowded bin must hold the cold particles"
+        assert np.array_equal(counts, oracle.histogram(zg, grid.to_c())), f"counts turn {t}"
+        assert np.array_equal(counts, st.counts()), f"counts vs oracle bunch, turn {t}"
+        assert_close(zg, zo, cfg.sigma_z, what=f"z turn {t}")
+        assert_close(eg, eo, cfg.sigma_E, what=f"dE turn {t}")
+    b.close()
 
 
 @pytest.mark.parametrize("n", [2, 3, 5, 33, 1001])
