@@ -67,6 +67,8 @@ struct hj_bunch {
   uint32_t* part_cnt = nullptr;
   unsigned long long* part_cic = nullptr;
   unsigned long long* ngp_ovf = nullptr;   // [B] overflow of the pass's 16-bit counters
+  double2* rf_table = nullptr;             // [kRfTableSize] RF kick table of the pass
+  double rf_Vs = 0;                        // its entry 0: V sin ϕs
   double* part_sum = nullptr;
   double* part_mom = nullptr;
   double* h_mom = nullptr;    // pinned
@@ -340,7 +342,8 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   cudaStreamSynchronize(b->stream);
   void* dev[] = {b->ts,       b->pot,      b->potd,     b->hist,    b->lam,
                  b->W,        b->Wf,       b->twP,      b->Xg,      b->zE,
-                 b->part_cnt, b->part_cic, b->part_sum, b->part_mom, b->ngp_ovf};
+                 b->part_cnt, b->part_cic, b->part_sum, b->part_mom, b->ngp_ovf,
+                 b->rf_table};
   for (void* p : dev)
     if (p) cudaFree(p);
   if (b->h_mom) cudaFreeHost(b->h_mom);
@@ -458,6 +461,16 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     HJ_CUDA(ctx, cudaMemsetAsync(b->ngp_ovf, 0, sizeof(unsigned long long) * b->B, b->stream));
   }
 
+  {
+    std::vector<double> rf(2 * kRfTableSize);
+    host_rf_table(params->voltage, params->phi_s, kRfTableSize, rf.data());
+    b->rf_Vs = rf[0];
+    HJ_TRY(dalloc(ctx, &b->rf_table, kRfTableSize));
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->rf_table, rf.data(), sizeof(double) * rf.size(),
+                                 cudaMemcpyHostToDevice, b->stream));
+    HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
+  }
+
   TurnState t{};
   t.cur = make_turn_scalars(params->E0, *params, b->sigma_E0_initial);
   t.pending = 0;
@@ -527,8 +540,17 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   a.inv_cstep = b->inv_c;
   a.V = b->p.voltage;
   a.phi_s = b->p.phi_s;
-  a.Vs = b->p.voltage * std::sin(b->p.phi_s);
-  a.Vc = b->p.voltage * std::cos(b->p.phi_s);
+  {
+    const long double kPiL = 3.141592653589793238462643383279502884L;
+    const long double h = 2.0L * kPiL / (long double)kRfTableSize;
+    a.rf_table = b->rf_table;
+    a.Vs = b->rf_Vs;
+    a.rf_inv_h = (double)(1.0L / h);
+    a.rf_h_hi = (double)h;
+    a.rf_h_lo = (double)(h - (long double)a.rf_h_hi);
+    const uint32_t key = (uint32_t)(b->seed ^ (b->seed >> 32));
+    for (int r = 0; r < 10; ++r) a.philox_rk[r] = key + (uint32_t)r * 0x9E3779B9u;
+  }
   a.inv_mass = 1.0 / b->p.mass;
   a.alpha_c = b->p.alpha_c;
   a.two_pi_h = kTwoPi * (double)b->p.harmonic;

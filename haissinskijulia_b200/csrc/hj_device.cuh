@@ -102,6 +102,39 @@ __host__ __device__ inline void philox2x32_10(uint32_t& c0, uint32_t& c1, uint32
   }
 }
 
+// Philox-2x32-10 with its round keys given: rk[r] = key + r·0x9E3779B9.
+__device__ __forceinline__ void philox2x32_10_rk(uint32_t& c0, uint32_t& c1,
+                                                 const uint32_t (&rk)[10]) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi = __umulhi(0xD256D193u, c0), lo = 0xD256D193u * c0;
+    c0 = hi ^ rk[r] ^ c1;
+    c1 = lo;
+  }
+}
+
+// Box-Muller transform of one Philox output pair (see philox_normals2).
+__device__ __forceinline__ void box_muller2(uint32_t x0, uint32_t x1, double out[2]) {
+  const float kScale = 2.3283064365386963e-10f;  // 2^-32
+  const float u1 = fmaf((float)x0, kScale, 0.5f * kScale);
+  const float th = 6.2831853071795865f * fmaf((float)x1, kScale, -0.5f);
+  const float m2l = fmaxf(-2.0f * __logf(u1), 1e-30f);
+  const float rad = m2l * rsqrtf(m2l);                        // sqrt without a slow path
+  float sn, cs;
+  __sincosf(th, &sn, &cs);
+  out[0] = (double)(rad * cs);
+  out[1] = (double)(rad * sn);
+}
+
+// philox_normals2 with the round keys of (seed ^ seed >> 32) precomputed.
+__device__ __forceinline__ void philox_normals2_rk(const uint32_t (&rk)[10], int64_t turn,
+                                                   int64_t p, double out[2]) {
+  uint32_t c0 = (uint32_t)p;
+  uint32_t c1 = ((uint32_t)turn & 0xFFFFFFu) | ((uint32_t)((uint64_t)p >> 32) << 24);
+  philox2x32_10_rk(c0, c1, rk);
+  box_muller2(c0, c1, out);
+}
+
 // Two standard normals for particles 2p and 2p+1 at `turn`: Philox-2x32-10
 // with key = (seed ^ seed >> 32) folded to 32 bits and counter
 // (p mod 2^32, (turn mod 2^24) | (p >> 32) << 24), then the Box-Muller
@@ -115,15 +148,7 @@ __device__ __forceinline__ void philox_normals2(uint64_t seed, int64_t turn, int
   uint32_t c0 = (uint32_t)p;
   uint32_t c1 = ((uint32_t)turn & 0xFFFFFFu) | ((uint32_t)((uint64_t)p >> 32) << 24);
   philox2x32_10(c0, c1, (uint32_t)(seed ^ (seed >> 32)));
-  const float kScale = 2.3283064365386963e-10f;  // 2^-32
-  const float u1 = fmaf((float)c0, kScale, 0.5f * kScale);
-  const float th = 6.2831853071795865f * fmaf((float)c1, kScale, -0.5f);
-  const float m2l = fmaxf(-2.0f * __logf(u1), 1e-30f);
-  const float rad = m2l * rsqrtf(m2l);                        // sqrt without a slow path
-  float sn, cs;
-  __sincosf(th, &sn, &cs);
-  out[0] = (double)(rad * cs);
-  out[1] = (double)(rad * sn);
+  box_muller2(c0, c1, out);
 }
 
 }  // namespace hj

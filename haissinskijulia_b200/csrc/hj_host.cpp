@@ -98,6 +98,17 @@ void host_wake_tables(const double* centers, int64_t B, const hj_wake& w, double
 }
 
 // tw[k] = exp(-2πi k/P) in long double, rounded once.
+// RF kick table of the fused pass: (V sin θm, V cos θm), θm = ϕs - 2π m / M,
+// m = 0..M-1, in extended precision and rounded once.
+void host_rf_table(double V, double phi_s, int64_t M, double* tab_interleaved) {
+  const long double kPiL = 3.141592653589793238462643383279502884L;
+  for (int64_t m = 0; m < M; ++m) {
+    const long double a = (long double)phi_s - 2.0L * kPiL * (long double)m / (long double)M;
+    tab_interleaved[2 * m] = (double)((long double)V * sinl(a));
+    tab_interleaved[2 * m + 1] = (double)((long double)V * cosl(a));
+  }
+}
+
 void host_twiddles(int64_t P, double* tw_interleaved) {
   const long double kPiL = 3.141592653589793238462643383279502884L;
   for (int64_t k = 0; k < P; ++k) {

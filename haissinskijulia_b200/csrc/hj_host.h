@@ -11,4 +11,5 @@ double host_delta(double x, double sigma);
 void host_wake_tables(const double* centers, int64_t B, const hj_wake& w, double* W,
                       double* lam);
 void host_twiddles(int64_t P, double* tw_interleaved);
+void host_rf_table(double V, double phi_s, int64_t M, double* tab_interleaved);
 }  // namespace hj

@@ -19,8 +19,9 @@ constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 
 // Thread layouts of the fused pass: 0 = 4 particles/thread, 512 threads,
 // next group prefetched; 1 = 2 particles/thread, 1024 threads; 2 = 2
-// particles/thread, 512 threads.
+// particles/thread, 512 threads; 3 = 2 particles/thread, 768 threads.
 constexpr int kNumPassCfgs = 4;
+constexpr int kRfTableSize = 128;    // entries of the fused pass's RF kick table
 int pass_cfg_threads(int cfg);
 int pass_cfg_ppt(int cfg);
 
@@ -41,7 +42,11 @@ struct PassArgs {
   double c1, cB, inv_cstep;       // interpolation (centers)
   // physics constants of the run
   double V, phi_s, inv_mass, alpha_c, two_pi_h;
-  double Vs, Vc;           // V sin ϕs, V cos ϕs
+  // RF kick: x = z k = m h + t, h = 2π / kRfTableSize (h_hi + h_lo), and
+  // rf_table[m mod kRfTableSize] = (V sin(ϕs - m h), V cos(ϕs - m h)); Vs = V sin ϕs
+  const double2* rf_table;
+  double rf_inv_h, rf_h_hi, rf_h_lo, Vs;
+  uint32_t philox_rk[10];  // Philox-2x32 round keys: key + r·0x9E3779B9
   int32_t update_eta, update_E0, sr, qe_mode;
   int32_t cfg;             // thread layout (kNumPassCfgs)
   uint64_t seed;

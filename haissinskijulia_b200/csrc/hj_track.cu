@@ -24,14 +24,13 @@
 //
 // Per-particle arithmetic of the fused pass (the single-step kernels further
 // down keep the reference's exact operation order instead):
-//   * RF kick: V(sin(ϕs - x) - sin ϕs) with x = z k.  x is reduced to
-//     r = x - n π/2, |r| <= π/4 (Cody-Waite with a two-word π/2; n = 0 for
-//     every particle within ±π/(4k) of the synchronous one), and
-//     sin(ϕs - x) = sin θn cos r - cos θn sin r, θn = ϕs - n π/2 (a 4-entry
-//     shared-memory table), with sin r and cos r - 1 from their Taylor series
-//     through r^15 and r^16 (truncation error below 5e-17).  For n = 0 the
-//     kick is V sin ϕs (cos r - 1) - V cos ϕs sin r, free of the cancellation
-//     in sin(ϕ) - sin ϕs.  No branches.
+//   * RF kick: V(sin(ϕs - x) - sin ϕs) with x = z k = m h + t, h = 2π/128,
+//     |t| <= π/128, and sin(ϕs - x) = sin θm cos t - cos θm sin t with
+//     θm = ϕs - m h from a 128-entry shared-memory table (computed in
+//     extended precision on the host) and sin t, cos t - 1 from their Taylor
+//     series through t^7 and t^6.  For m = 0 the kick is V sin ϕs (cos t - 1)
+//     - V cos ϕs sin t, free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
+//   * Philox round keys are precomputed on the host (kernel parameters).
 //   * 1/γ² of the drift: rcp.approx.ftz.f64 refined by one Newton step
 //     (relative error ~1e-14 on a term 5e-5 of η, i.e. ~1e-18 on η).
 //   * drift: z' = z - (2π h / (β0² E0 k)) η_i ΔE, the reference's
@@ -52,7 +51,8 @@ namespace {
 
 // Run- and turn-constants of the fused pass.
 struct FusedConst {
-  double Vs, Vc;            // V sin ϕs, V cos ϕs
+  double Vs;                // V sin ϕs
+  double rf_inv_h, rf_h_hi, rf_h_lo;   // RF table step h = 2π/128: 1/h, h (two words)
   double k;
   double excitation, damping;
   double gamma0, inv_mass, alpha_c, Kz;  // Kz = 2π h / (β0² E0 k)
@@ -208,54 +208,29 @@ __device__ __forceinline__ int ngp_bin_any(double z, const GridConst& g, bool& i
   return min(max(j, 0), g.B - 1);
 }
 
-// sin r and cos r - 1 for |r| <= π/4: Taylor series through r^15 and r^16.
-__device__ __forceinline__ void sincm1_poly(double r, double& sn, double& cm1) {
-  const double t = r * r;
-  // sin r = r + r^3 P(t): coefficients (-1)^m / (2m+1)!, m = 1..7
-  double p = -7.647163731819816e-13;          // -1/15!
-  p = fma(t, p, 1.6059043836821613e-10);      // +1/13!
-  p = fma(t, p, -2.505210838544172e-08);      // -1/11!
-  p = fma(t, p, 2.7557319223985893e-06);      // +1/9!
-  p = fma(t, p, -1.984126984126984e-04);      // -1/7!
-  p = fma(t, p, 8.333333333333333e-03);       // +1/5!
-  p = fma(t, p, -1.6666666666666666e-01);     // -1/3!
-  sn = fma(t * r, p, r);
-  // cos r - 1 = t Q(t): coefficients (-1)^m / (2m)!, m = 1..8
-  double q = 4.779477332387385e-14;           // +1/16!
-  q = fma(t, q, -1.1470745597729725e-11);     // -1/14!
-  q = fma(t, q, 2.08767569878681e-09);        // +1/12!
-  q = fma(t, q, -2.755731922398589e-07);      // -1/10!
-  q = fma(t, q, 2.48015873015873e-05);        // +1/8!
-  q = fma(t, q, -1.388888888888889e-03);      // -1/6!
-  q = fma(t, q, 4.1666666666666664e-02);      // +1/4!
-  q = fma(t, q, -0.5);                        // -1/2!
-  cm1 = t * q;
-}
-
-// V(sin(ϕs - x) - sin ϕs), x = z k (see the header comment).  When every
-// active lane of the warp has |x| <= π/4 (the bunch core: n = 0) the series
-// runs on x directly; otherwise x = n π/2 + r with n = rint(2x/π) from the
-// 1.5·2^52 addition and r by Cody-Waite with a two-word π/2, and
-// rot[n mod 4] = (V sin θn, V cos θn), θn = ϕs - n π/2, from a shared-memory
-// table; the kick is V sin θn (cos r - 1) - V cos θn sin r + (V sin θn - V sin ϕs).
+// V(sin(ϕs - x) - sin ϕs), x = z k (see the header comment): x = m h + t with
+// m = rint(x/h) from the 1.5·2^52 addition, h = 2π/128, t by Cody-Waite with
+// a two-word h (|t| <= π/128), and rot = (V sin θm, V cos θm), θm = ϕs - m h,
+// from the shared-memory table (entry m mod 128).  sin t and cos t - 1 are
+// their Taylor series through t^7 and t^6 (truncation below 1e-20); the kick
+// V sin θm (cos t - 1) - V cos θm sin t + (V sin θm - V sin ϕs) is, for m = 0,
+// free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
 __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
-                                          const double2* __restrict__ s_rot) {
-  double r = z * c.k;
-  double sv = c.Vs, cv = c.Vc, off = 0.0;
-  if (!__all_sync(__activemask(), fabs(r) <= 0.78539816339744831)) {
-    const double x = r;
-    const double y = fma(x, 0.63661977236758134, kMagic);  // 2x/π + 1.5·2^52
-    const double nd = y - kMagic;
-    r = fma(-nd, 1.5707963267948966, x);
-    r = fma(-nd, 6.123233995736766e-17, r);
-    const double2 rot = s_rot[__double2loint(y) & 3];
-    sv = rot.x;
-    cv = rot.y;
-    off = sv - c.Vs;
-  }
-  double sn, cm1;
-  sincm1_poly(r, sn, cm1);
-  return fma(sv, cm1, -cv * sn) + off;
+                                          const double2* __restrict__ s_rf) {
+  const double x = z * c.k;
+  const double y = fma(x, c.rf_inv_h, kMagic);
+  const double md = y - kMagic;
+  double t = fma(-md, c.rf_h_hi, x);
+  t = fma(-md, c.rf_h_lo, t);
+  const double2 rot = s_rf[__double2loint(y) & (kRfTableSize - 1)];
+  const double t2 = t * t;
+  double p = fma(t2, -1.984126984126984e-04, 8.333333333333333e-03);   // -1/7!, 1/5!
+  p = fma(t2, p, -1.6666666666666666e-01);                               // -1/3!
+  const double sn = fma(t * t2, p, t);
+  double q = fma(t2, -1.388888888888889e-03, 4.1666666666666664e-02);  // -1/6!, 1/4!
+  q = fma(t2, q, -0.5);
+  const double cm1 = t2 * q;
+  return fma(rot.x, cm1, -rot.y * sn) + (rot.x - c.Vs);
 }
 
 // One particle for one turn, given its wake kick (lerp of the previous turn's
@@ -321,10 +296,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Fixed-order block reduction of four accumulators into out[0..3] (thread 0).
+// red: shared scratch of THREADS/32 x 4 doubles.
 template <int THREADS>
 __device__ __forceinline__ void block_sum4(double a0, double a1, double a2, double a3,
-                                           double* out) {
-  __shared__ double red[THREADS / 32][4];
+                                           double* out, double (*red)[4]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   a0 = warp_sum(a0);
   a1 = warp_sum(a1);
@@ -369,29 +344,25 @@ __device__ __forceinline__ void stp(double* p, const double v[PPT]) {
 
 // Normals of particles PPT*g .. PPT*g+PPT-1 (one Philox-2x32 counter per pair).
 template <int PPT>
-__device__ __forceinline__ void group_normals(uint64_t seed, int64_t turn, int64_t g,
+__device__ __forceinline__ void group_normals(const uint32_t (&rk)[10], int64_t turn, int64_t g,
                                               double r[PPT]) {
-  philox_normals2(seed, turn, (PPT / 2) * g, r);
-  if (PPT == 4) philox_normals2(seed, turn, 2 * g + 1, r + 2);
+  philox_normals2_rk(rk, turn, (PPT / 2) * g, r);
+  if (PPT == 4) philox_normals2_rk(rk, turn, 2 * g + 1, r + 2);
 }
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
 // next group prefetched in registers, or 2 with twice the threads per SM).
 template <bool WAKE, int QE, int PPT, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
+  // dynamic shared memory: RF table [128] | NGP counters [(B+1)/2] | cell words lo, hi [B+1]
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double2 s_rot[4];
   const int nc = a.B + 1;                 // kick-table cells
   const int nw = (a.B + 1) / 2;           // words of 16-bit NGP counters
-  uint32_t* s_ngp = reinterpret_cast<uint32_t*>(smem_raw);
+  double2* s_rf = reinterpret_cast<double2*>(smem_raw);
+  uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_rf + kRfTableSize);
   uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
   uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
-  if (threadIdx.x == 0) {                 // (V sin θn, V cos θn), θn = ϕs - n π/2
-    s_rot[0] = make_double2(a.Vs, a.Vc);
-    s_rot[1] = make_double2(-a.Vc, a.Vs);
-    s_rot[2] = make_double2(-a.Vs, -a.Vc);
-    s_rot[3] = make_double2(a.Vc, -a.Vs);
-  }
+  for (int i = threadIdx.x; i < kRfTableSize; i += THREADS) s_rf[i] = __ldg(a.rf_table + i);
 
   TurnState* ts = a.ts;
   const TurnScalars sc = ts->cur;
@@ -400,7 +371,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
 
   FusedConst c;
   c.Vs = a.Vs;
-  c.Vc = a.Vc;
+  c.rf_inv_h = a.rf_inv_h;
+  c.rf_h_hi = a.rf_h_hi;
+  c.rf_h_lo = a.rf_h_lo;
   c.k = sc.k;
   c.excitation = sc.excitation;
   c.damping = a.sr ? sc.damping : 1.0;
@@ -474,7 +447,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
     if (QE == QE_PHILOX) {
-      group_normals<PPT>(a.seed, turn, q, rr);
+      group_normals<PPT>(a.philox_rk, turn, q, rr);
     } else if (QE == QE_DRAWS) {
       if (drow) {
 #pragma unroll
@@ -483,7 +456,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
     }
     double rf[PPT];
 #pragma unroll
-    for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rot);
+    for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rf);
 #pragma unroll
     for (int j = 0; j < PPT; ++j)
       pass_particle<WAKE>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].pd.y, kf[j].pd.x) : 0.0,
@@ -496,19 +469,23 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   if (blockIdx.x == 0 && threadIdx.x < (int)(a.n % PPT)) {
     const int64_t i = ng * PPT + threadIdx.x;
     double r2[2] = {0.0, 0.0};
-    if (QE == QE_PHILOX) philox_normals2(a.seed, turn, i >> 1, r2);
+    if (QE == QE_PHILOX) philox_normals2_rk(a.philox_rk, turn, i >> 1, r2);
     double r = r2[i & 1];
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
     double z = a.z[i], e = a.dE[i];
     const double kick = WAKE ? wake_kick(z, g, potd) : 0.0;
-    pass_particle<WAKE>(z, e, r, kick, rf_term(z, c, s_rot), c, g, pmean, acc_z, acc_z2, acc_d,
+    pass_particle<WAKE>(z, e, r, kick, rf_term(z, c, s_rf), c, g, pmean, acc_z, acc_z2, acc_d,
                         n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
     a.z[i] = z;
     a.dE[i] = e;
   }
 
+  __syncthreads();                        // the RF table's space becomes the reduction scratch
+  static_assert(THREADS / 32 * 4 * sizeof(double) <= kRfTableSize * sizeof(double2),
+                "reduction scratch exceeds the RF table");
   block_sum4<THREADS>(acc_z, acc_z2, acc_d, (double)n_in,
-                      a.part_sum + (size_t)blockIdx.x * kNumSums);
+                      a.part_sum + (size_t)blockIdx.x * kNumSums,
+                      reinterpret_cast<double(*)[4]>(s_rf));
 
   if (WAKE) {
     __syncthreads();
@@ -576,7 +553,8 @@ __global__ void __launch_bounds__(kTrackThreads) k_flush(FlushArgs a) {
     s2 += e;
     s3 = fma(e, e, s3);
   }
-  block_sum4<kTrackThreads>(s0, s1, s2, s3, a.part + (size_t)blockIdx.x * 4);
+  __shared__ double red[kTrackThreads / 32][4];
+  block_sum4<kTrackThreads>(s0, s1, s2, s3, a.part + (size_t)blockIdx.x * 4, red);
 }
 
 // NGP histogram only (hj_histogram, hj_apply_wakefield).
@@ -729,11 +707,13 @@ cudaError_t prepare_track_kernels(int max_smem) {
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
 }
 
-// 16-bit NGP counts [B] (two per word) + two 32-bit words per kick-table cell [B+1].
+// RF table + 16-bit NGP counts [B] (two per word) + two 32-bit words per
+// kick-table cell [B+1].
 size_t track_smem_bytes(int B, int use_wake) {
-  return use_wake ? (size_t)((B + 1) / 2) * sizeof(uint32_t) +
+  const size_t rf = kRfTableSize * sizeof(double2);
+  return use_wake ? rf + (size_t)((B + 1) / 2) * sizeof(uint32_t) +
                         (size_t)(B + 1) * sizeof(unsigned long long)
-                  : 0;
+                  : rf;
 }
 
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
