@@ -240,13 +240,13 @@ hj_status read_state(hj_bunch* b) {
   return HJ_OK;
 }
 
-// Thread layout of the fused pass when the context does not pin one: four
-// particles per thread with the next four prefetched, 512 threads per block,
-// measured fastest at 4096 and 16384 bins and 1e8 particles on B200.
+// Thread layout of the fused pass when the context does not pin one, from
+// timings at 1e8 particles on B200: two particles per thread x 1024 threads
+// up to 4096 bins, four per thread x 512 threads above (both prefetching the
+// next group).
 int default_pass_layout(int B, int64_t n) {
-  (void)B;
   (void)n;
-  return 0;
+  return B <= 4096 ? 1 : 0;
 }
 
 void fill_result(hj_bunch* b, const double m[4], hj_result* res) {

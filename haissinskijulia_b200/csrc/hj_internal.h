@@ -17,9 +17,9 @@ constexpr int64_t kMaxBins = 16384; // largest grid the shared-memory FFT holds 
 // counter keeps a 20-bit count per cell).
 constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 
-// Thread layouts of the fused pass: 0 = 4 particles/thread, 512 threads,
-// next group prefetched; 1 = 2 particles/thread, 1024 threads; 2 = 2
-// particles/thread, 512 threads; 3 = 2 particles/thread, 768 threads.
+// Thread layouts of the fused pass (particles/thread x threads/block; the next
+// group prefetched into registers in 0-2): 0 = 4 x 512, 1 = 2 x 1024,
+// 2 = 2 x 768, 3 = 2 x 512 without prefetch.
 constexpr int kNumPassCfgs = 4;
 constexpr int kRfTableSize = 128;    // entries of the fused pass's RF kick table
 int pass_cfg_threads(int cfg);

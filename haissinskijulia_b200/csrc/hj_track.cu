@@ -352,7 +352,7 @@ __device__ __forceinline__ void group_normals(const uint32_t (&rk)[10], int64_t 
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
 // next group prefetched in registers, or 2 with twice the threads per SM).
-template <bool WAKE, int QE, int PPT, int THREADS>
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH>
 __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   // dynamic shared memory: RF table [128] | NGP counters [(B+1)/2] | cell words lo, hi [B+1]
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   const int64_t ng = a.n / PPT;
   const int64_t stride = (int64_t)gridDim.x * THREADS;
   int64_t q = (int64_t)blockIdx.x * THREADS + threadIdx.x;
-  constexpr bool kPrefetch = (PPT == 4);
+  constexpr bool kPrefetch = PREFETCH;
   double zn[PPT], en[PPT];
   if (kPrefetch && q < ng) {
     ldp<PPT>(a.z + PPT * q, zn);
@@ -673,10 +673,10 @@ namespace {
 template <bool W, int Q>
 const void* pass_fn_wq(int cfg) {
   switch (cfg) {
-    case 0: return (const void*)k_track_pass<W, Q, 4, 512>;
-    case 1: return (const void*)k_track_pass<W, Q, 2, 1024>;
-    case 3: return (const void*)k_track_pass<W, Q, 2, 768>;
-    default: return (const void*)k_track_pass<W, Q, 2, 512>;
+    case 0: return (const void*)k_track_pass<W, Q, 4, 512, true>;
+    case 1: return (const void*)k_track_pass<W, Q, 2, 1024, true>;
+    case 2: return (const void*)k_track_pass<W, Q, 2, 768, true>;
+    default: return (const void*)k_track_pass<W, Q, 2, 512, false>;
   }
 }
 
@@ -694,7 +694,7 @@ const void* pass_fn(int wake, int qe, int cfg) {
 }
 }  // namespace
 
-int pass_cfg_threads(int cfg) { return cfg == 1 ? 1024 : (cfg == 3 ? 768 : 512); }
+int pass_cfg_threads(int cfg) { return cfg == 1 ? 1024 : (cfg == 2 ? 768 : 512); }
 int pass_cfg_ppt(int cfg) { return cfg == 0 ? 4 : 2; }
 
 cudaError_t prepare_track_kernels(int max_smem) {
