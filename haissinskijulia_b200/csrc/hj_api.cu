@@ -352,10 +352,14 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   delete b;
 }
 
+// chunk > 0: a batch member, whose partial slots are its chunks of `chunk`
+// particles (the batch's chunk table) instead of one per block of the grid;
+// cfg >= 0 pins the pass layout.
 static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
                                    const hj_params* params, const hj_wake* wake,
                                    int64_t nbins, const hj_grid* grid, uint64_t seed,
-                                   void* stream, hj_bunch* b) {
+                                   void* stream, hj_bunch* b, int64_t chunk = 0,
+                                   int cfg = -1) {
   b->ctx = ctx;
   b->stream = (cudaStream_t)stream;
   b->z = d_z;
@@ -450,9 +454,13 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));     // host vectors go out of scope
   }
 
-  b->cfg = ctx->pass_layout >= 0 ? ctx->pass_layout : default_pass_layout(b->B, n);
-  const int bps = track_blocks_per_sm(b->B, b->qe_mode, b->use_wake, b->cfg);
-  b->nblk = track_grid_size(n, b->B, ctx->num_sms, bps, b->cfg);
+  b->cfg = cfg >= 0 ? cfg : (ctx->pass_layout >= 0 ? ctx->pass_layout : default_pass_layout(b->B, n));
+  if (chunk > 0) {
+    b->nblk = (int)std::max<int64_t>((n + chunk - 1) / chunk, 1);
+  } else {
+    const int bps = track_blocks_per_sm(b->B, b->qe_mode, b->use_wake, b->cfg);
+    b->nblk = track_grid_size(n, b->B, ctx->num_sms, bps, b->cfg);
+  }
   HJ_TRY(dalloc(ctx, &b->part_sum, (size_t)kNumSums * b->nblk));
   if (b->use_wake) {
     HJ_TRY(dalloc(ctx, &b->part_cnt, (size_t)b->nblk * b->B));
@@ -476,6 +484,7 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
   t.pending = 0;
   t.pending_mean = 0.0;
   t.turn = 1;
+  t.turns_left = INT64_MAX;   // a plain bunch runs until it is finished
   t.status = 0;
   *b->h_ts = t;
   HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice, b->stream));
@@ -519,12 +528,9 @@ extern "C" hj_status hj_bunch_set_draws(hj_bunch* b, const double* d_draws, int6
   return HJ_OK;
 }
 
-extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
-  if (!b) return HJ_ERR_ARG;
-  hj_ctx* ctx = b->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
-  PassArgs a{};
+// Arguments of the fused pass and of the bins step of bunch b.
+static void fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
+  a = PassArgs{};
   a.z = b->z;
   a.dE = b->dE;
   a.n = b->n;
@@ -569,7 +575,7 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   a.hist_out = b->hist;
   a.ngp_ovf = b->ngp_ovf;
 
-  BinsArgs g{};
+  g = BinsArgs{};
   g.ts = b->ts;
   g.part_sum = b->part_sum;
   g.nblk = b->nblk;
@@ -596,6 +602,18 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
   g.hi_w = b->hi_w;
   g.W = b->W;
   g.conv_only = 0;
+
+  a.n_parts = b->nblk;
+}
+
+extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
+  if (!b) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
+  PassArgs a;
+  BinsArgs g;
+  fill_turn_args(b, a, g);
 
   for (int64_t t = 0; t < turns; ++t) {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};

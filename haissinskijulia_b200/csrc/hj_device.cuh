@@ -54,6 +54,7 @@ struct TurnState {
   double last_mean;      // E0 change of the last turn
   double last_sum_kick;  // Σ_i lerp(pot, z_i) of the last turn
   double last_n_in;      // particles inside the bin range, last turn
+  int64_t turns_left;    // turns still to run (batches); a plain bunch never runs out
 };
 
 __host__ __device__ inline TurnScalars make_turn_scalars(double E0, const hj_params& p,

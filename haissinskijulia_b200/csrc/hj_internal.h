@@ -59,6 +59,17 @@ struct PassArgs {
   double* part_sum;                // [grid][kNumSums]
   unsigned long long* hist_out;    // [3B+2] merged histograms, zeroed by the pass
   unsigned long long* ngp_ovf;     // [B] counts beyond the 16-bit per-block counters
+  int32_t n_parts;                 // partial slots written per turn (batches)
+};
+
+// One entry of a batch's chunk table: particles [first, first + count) of
+// bunch `bunch`, deposited into that bunch's partial slot `part`.  first is a
+// multiple of 4, so the 32-byte particle loads stay aligned.
+struct BatchChunk {
+  int64_t first;
+  int64_t count;
+  int32_t bunch;
+  int32_t part;
 };
 
 // Arguments of the per-turn bins step (single CTA).
@@ -115,6 +126,13 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg);
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
 size_t track_smem_bytes(int B, int use_wake);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
+// Batched pass over a chunk table (*d_n_chunks entries live, grid max_chunks)
+// and the per-bunch merge of its partials.
+cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
+                              const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
+                              int qe, int cfg, cudaStream_t st);
+cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const int32_t* d_n_bunches,
+                                int max_bunches, int max_B, cudaStream_t st);
 // out: counts[B] (| cell counts[B+1] | cell Σw·2^24 [B+1] when part_cic != NULL);
 // zero_first clears out before the merge (the fused pass clears it itself).
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
@@ -144,6 +162,8 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
                                  const double2* twP, double2* Xg, double2* Wf,
                                  cudaStream_t st);
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st);
+cudaError_t launch_batch_bins(const BinsArgs* d_bunches, const int32_t* d_n_bunches,
+                              int max_bunches, int max_H, cudaStream_t st);
 size_t bins_smem_bytes(int H);
 
 // ---- context access for entry points outside hj_api.cu ----

@@ -352,10 +352,19 @@ __device__ __forceinline__ void group_normals(const uint32_t (&rk)[10], int64_t 
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
 // next group prefetched in registers, or 2 with twice the threads per SM).
+// Particle groups (PPT particles each) one block processes: thread t takes
+// groups q_begin + t, + q_step, ... below q_end; its partial histograms and
+// sums go to slot `part`; the `tail` block also takes the n % PPT last particles.
+struct PassRange {
+  int64_t q_begin, q_step, q_end;
+  int32_t part;
+  bool tail;
+};
+
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH>
-__global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
+__device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
+                                          unsigned char* smem_raw) {
   // dynamic shared memory: RF table [128] | NGP counters [(B+1)/2] | cell words lo, hi [B+1]
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nc = a.B + 1;                 // kick-table cells
   const int nw = (a.B + 1) / 2;           // words of 16-bit NGP counters
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
@@ -392,7 +401,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
     int64_t row = turn - a.draws_first_turn;
     if (row >= 0 && row < a.draws_turns) {
       drow = a.draws + row * a.n;
-    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+    } else if (rg.part == 0 && threadIdx.x == 0) {
       atomicOr(&ts->status, 1 << HJ_ERR_ARG);
     }
   }
@@ -403,19 +412,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
       s_lo[i] = 0u;
       s_hi[i] = 0u;
     }
-    // zero the merged histograms k_hist_reduce accumulates into this turn
-    const int gstride = gridDim.x * THREADS;
-    for (int i = blockIdx.x * THREADS + threadIdx.x; i < a.B + 2 * nc; i += gstride)
-      a.hist_out[i] = 0ull;
   }
   __syncthreads();
 
   double acc_z = 0.0, acc_z2 = 0.0, acc_d = 0.0;
   uint32_t n_in = 0;
   const double2* __restrict__ potd = a.potd;
-  const int64_t ng = a.n / PPT;
-  const int64_t stride = (int64_t)gridDim.x * THREADS;
-  int64_t q = (int64_t)blockIdx.x * THREADS + threadIdx.x;
+  const int64_t ng = rg.q_end;
+  const int64_t stride = rg.q_step;
+  int64_t q = rg.q_begin + threadIdx.x;
   constexpr bool kPrefetch = PREFETCH;
   double zn[PPT], en[PPT];
   if (kPrefetch && q < ng) {
@@ -465,9 +470,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
     stp<PPT>(a.z + PPT * q, zz);
     stp<PPT>(a.dE + PPT * q, ee);
   }
-  // Tail of n % PPT particles: the first threads of block 0, scalar.
-  if (blockIdx.x == 0 && threadIdx.x < (int)(a.n % PPT)) {
-    const int64_t i = ng * PPT + threadIdx.x;
+  // Tail of n % PPT particles: the first threads of the tail block, scalar.
+  if (rg.tail && threadIdx.x < (int)(a.n % PPT)) {
+    const int64_t i = (a.n / PPT) * PPT + threadIdx.x;
     double r2[2] = {0.0, 0.0};
     if (QE == QE_PHILOX) philox_normals2_rk(a.philox_rk, turn, i >> 1, r2);
     double r = r2[i & 1];
@@ -484,18 +489,51 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
   static_assert(THREADS / 32 * 4 * sizeof(double) <= kRfTableSize * sizeof(double2),
                 "reduction scratch exceeds the RF table");
   block_sum4<THREADS>(acc_z, acc_z2, acc_d, (double)n_in,
-                      a.part_sum + (size_t)blockIdx.x * kNumSums,
+                      a.part_sum + (size_t)rg.part * kNumSums,
                       reinterpret_cast<double(*)[4]>(s_rf));
 
   if (WAKE) {
     __syncthreads();
-    uint32_t* pc = a.part_cnt + (size_t)blockIdx.x * a.B;
-    unsigned long long* pq = a.part_cic + (size_t)blockIdx.x * nc;
+    uint32_t* pc = a.part_cnt + (size_t)rg.part * a.B;
+    unsigned long long* pq = a.part_cic + (size_t)rg.part * nc;
     for (int i = threadIdx.x; i < nc; i += THREADS) {
       if (i < a.B) pc[i] = (s_ngp[i >> 1] >> ((i & 1) << 4)) & 0xFFFFu;
       pq[i] = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
     }
   }
+}
+
+// One turn over one bunch: block b takes groups b, b + grid, ... (THREADS
+// apart) and writes partial slot b; block 0 takes the tail.
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH>
+__global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (WAKE) {  // zero the merged histograms k_hist_reduce accumulates into this turn
+    const int gstride = gridDim.x * THREADS;
+    for (int i = blockIdx.x * THREADS + threadIdx.x; i < 3 * a.B + 2; i += gstride)
+      a.hist_out[i] = 0ull;
+  }
+  const PassRange rg{(int64_t)blockIdx.x * THREADS, (int64_t)gridDim.x * THREADS, a.n / PPT,
+                     (int32_t)blockIdx.x, blockIdx.x == 0};
+  pass_body<WAKE, QE, PPT, THREADS, PREFETCH>(a, rg, smem_raw);
+}
+
+// One turn over a batch of bunches: block c takes chunk c of the chunk table
+// (a contiguous run of one bunch's particles) and writes the bunch's partial
+// slot ch.part.  Blocks past the table's length, and chunks of bunches with
+// no turns left, return at once.
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_batch_pass(const PassArgs* __restrict__ bunches, const BatchChunk* __restrict__ chunks,
+                 const int32_t* __restrict__ n_chunks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if ((int)blockIdx.x >= *n_chunks) return;
+  const BatchChunk ch = chunks[blockIdx.x];
+  const PassArgs a = bunches[ch.bunch];
+  if (a.ts->turns_left <= 0) return;
+  const PassRange rg{ch.first / PPT, THREADS, (ch.first + ch.count) / PPT, ch.part,
+                     ch.first + ch.count == a.n};
+  pass_body<WAKE, QE, PPT, THREADS, PREFETCH>(a, rg, smem_raw);
 }
 
 // Merge of the per-block histograms.  Grid (bins/256, G): block column g sums
@@ -529,6 +567,33 @@ __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
     if (sn) atomicAdd(out + B + b, sn);
     if (sw) atomicAdd(out + B + nc + b, sw);
   }
+}
+
+// Merge of a batch's per-chunk histograms: block (x, b) sums, for 256 cells
+// of bunch b, the partial slots of all its chunks in slot order and writes
+// the merged arrays (no atomics, so no zeroing; exact integer sums).
+__global__ void k_batch_reduce(const PassArgs* __restrict__ bunches,
+                               const int32_t* __restrict__ n_bunches) {
+  if ((int)blockIdx.y >= *n_bunches) return;
+  const PassArgs& a = bunches[blockIdx.y];
+  if (a.ts->turns_left <= 0 || !a.use_wake) return;
+  const int B = a.B, nc = B + 1;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nc) return;
+  unsigned long long sc = 0ull, sn = 0ull, sw = 0ull;
+  if (b < B) {
+    sc = a.ngp_ovf[b];
+    a.ngp_ovf[b] = 0ull;
+  }
+  for (int k = 0; k < a.n_parts; ++k) {
+    if (b < B) sc += __ldg(a.part_cnt + (size_t)k * B + b);
+    const unsigned long long v = __ldg(a.part_cic + (size_t)k * nc + b);
+    sn += v >> kCicSumBits;
+    sw += v & kCicSumMask;
+  }
+  if (b < B) a.hist_out[b] = sc;
+  a.hist_out[B + b] = sn;
+  a.hist_out[B + nc + b] = sw;
 }
 
 // Pending kick + re-centring (optional), copy-out (optional) and the moments
@@ -692,6 +757,22 @@ const void* pass_fn_w(int qe, int cfg) {
 const void* pass_fn(int wake, int qe, int cfg) {
   return wake ? pass_fn_w<true>(qe, cfg) : pass_fn_w<false>(qe, cfg);
 }
+
+template <bool W, int Q>
+const void* batch_fn_wq(int cfg) {
+  switch (cfg) {
+    case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true>;
+    case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true>;
+    case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true>;
+    default: return (const void*)k_batch_pass<W, Q, 2, 512, false>;
+  }
+}
+
+// Batches draw QE normals on the device or not at all (no host-fed draws).
+const void* batch_fn(int wake, int qe, int cfg) {
+  if (wake) return qe == QE_PHILOX ? batch_fn_wq<true, QE_PHILOX>(cfg) : batch_fn_wq<true, QE_OFF>(cfg);
+  return qe == QE_PHILOX ? batch_fn_wq<false, QE_PHILOX>(cfg) : batch_fn_wq<false, QE_OFF>(cfg);
+}
 }  // namespace
 
 int pass_cfg_threads(int cfg) { return cfg == 1 ? 1024 : (cfg == 2 ? 768 : 512); }
@@ -702,6 +783,7 @@ cudaError_t prepare_track_kernels(int max_smem) {
     for (int q = 0; q < 3; ++q)
       for (int c = 0; c < kNumPassCfgs; ++c) {
         cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
+        if (e == cudaSuccess && q != QE_DRAWS) e = allow_dynamic_smem(batch_fn(w, q, c), max_smem);
         if (e != cudaSuccess) return e;
       }
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
@@ -745,6 +827,23 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
   void* args[] = {const_cast<PassArgs*>(&a)};
   return cudaLaunchKernel(pass_fn(a.use_wake, a.qe_mode, a.cfg), dim3(grid),
                           dim3(pass_cfg_threads(a.cfg)), args, smem, st);
+}
+
+cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
+                              const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
+                              int qe, int cfg, cudaStream_t st) {
+  const size_t smem = track_smem_bytes(max_B, wake);
+  void* args[] = {const_cast<PassArgs**>(&d_bunches), const_cast<BatchChunk**>(&d_chunks),
+                  const_cast<int32_t**>(&d_n_chunks)};
+  return cudaLaunchKernel(batch_fn(wake, qe, cfg), dim3(max_chunks > 0 ? max_chunks : 1),
+                          dim3(pass_cfg_threads(cfg)), args, smem, st);
+}
+
+cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const int32_t* d_n_bunches,
+                                int max_bunches, int max_B, cudaStream_t st) {
+  dim3 grid((max_B + 1 + 255) / 256, max_bunches > 0 ? max_bunches : 1);
+  k_batch_reduce<<<grid, 256, 0, st>>>(d_bunches, d_n_bunches);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,

@@ -319,8 +319,7 @@ __device__ __forceinline__ double global_std(double s, double s2, int64_t n) {
 // all have the same parity, so each CTA runs one forward length-H FFT, its
 // half of the spectrum and one inverse length-H FFT in its own shared memory;
 // the halves are combined through distributed shared memory.
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1)
-    k_bins(BinsArgs a) {
+__device__ __forceinline__ void bins_body(const BinsArgs& a) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
@@ -493,6 +492,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1)
     ts->last_sum_kick = sum_kick;
     ts->last_n_in = sh[3];
     ts->turn = ts->turn + 1;
+    ts->turns_left = ts->turns_left - 1;
     ts->cur = make_turn_scalars(E0n, a.params, a.sigma_E0_initial);
     // Flag what the turn actually used: a NaN current with no particle in
     // range never reaches the bunch (src/wakefield.jl:305-311).
@@ -501,10 +501,27 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1)
   }
 }
 
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins(BinsArgs a) {
+  bins_body(a);
+}
+
+// The bins step of a batch: cluster i (CTAs 2i, 2i+1) runs bunch i; slots
+// past the live count and bunches with no turns left return at once (both
+// CTAs of a cluster read the same state before either writes it, so they agree).
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1)
+    k_batch_bins(const BinsArgs* __restrict__ bunches, const int32_t* __restrict__ n_bunches) {
+  const int i = (int)(blockIdx.x >> 1);
+  if (i >= *n_bunches) return;
+  const BinsArgs& a = bunches[i];
+  if (a.ts->turns_left <= 0) return;
+  bins_body(a);
+}
+
 }  // namespace
 
 cudaError_t prepare_wake_kernels(int max_smem) {
   cudaError_t e = allow_dynamic_smem((const void*)k_bins, max_smem);
+  if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_batch_bins, max_smem);
   if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_wake_spectrum, max_smem);
   return e;
 }
@@ -526,6 +543,14 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st) {
   size_t smem = bins_smem_bytes(a.H);
   k_bins<<<2, kBinsThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_bins(const BinsArgs* d_bunches, const int32_t* d_n_bunches,
+                              int max_bunches, int max_H, cudaStream_t st) {
+  size_t smem = bins_smem_bytes(max_H);
+  k_batch_bins<<<2 * (max_bunches > 0 ? max_bunches : 1), kBinsThreads, smem, st>>>(
+      d_bunches, d_n_bunches);
   return cudaGetLastError();
 }
 
