@@ -8,6 +8,7 @@ from .api import (  # noqa: F401
     ELECTRON_CHARGE,
     MASS_ELECTRON,
     SPEED_LIGHT,
+    Batch,
     BinGrid,
     Context,
     EvolveResult,

@@ -24,6 +24,7 @@ HJ_ERR_NONFINITE = 8
 HJ_ERR_TIMEOUT = 9
 HJ_ERR_NO_DEVICE = 10
 HJ_ERR_STATE = 11
+HJ_ERR_FULL = 12
 
 
 class HjParams(ctypes.Structure):
@@ -118,6 +119,16 @@ SIGNATURES = {
     "hj_bunch_histogram": (c_int32, [_BUNCH, _IP]),
     "hj_bunch_potential": (c_int32, [_BUNCH, _DP]),
     "hj_bunch_destroy": (None, [_BUNCH]),
+    "hj_batch_create": (c_int32, [_CTX, c_int64, c_int32, c_int32, c_int64, c_int32,
+                                  POINTER(c_void_p)]),
+    "hj_batch_destroy": (None, [c_void_p]),
+    "hj_batch_set_graph_turns": (c_int32, [c_void_p, c_int32]),
+    "hj_batch_add": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, POINTER(HjParams),
+                               POINTER(HjWake), c_int64, c_uint64, c_int64, _IP]),
+    "hj_batch_advance": (c_int32, [c_void_p, c_int64]),
+    "hj_batch_poll": (c_int32, [c_void_p, _IP, c_int32, POINTER(c_int32)]),
+    "hj_batch_take": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, POINTER(HjResult)]),
+    "hj_batch_stats": (c_int32, [c_void_p, _IP]),
     "hj_rf_kick": (c_int32, [_CTX, c_double, c_double, c_double, c_double, _DP, _DP, c_int64]),
     "hj_quantum_excitation": (c_int32, [_CTX, c_double, c_double, c_double, _DP, c_uint64,
                                         c_int64, _DP, c_int64]),

@@ -591,3 +591,104 @@ class ResidentBunch:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Independent bunches advanced together on one GPU (hj_batch_*).
+
+    Each bunch has its own particles, RF voltage, wake intensity, bins, seed
+    and turn count; every turn is one batched particle pass, one histogram
+    merge and one batched bins step for all live bunches, and blocks of
+    `graph_turns` turns replay a captured CUDA graph.  A bunch's results do
+    not depend on which other bunches share the batch.
+
+    pool_particles: particle capacity (16 B each on the device); max_bunches:
+    bunch slots; max_nbins: largest bin count; chunk: particles per block of
+    the pass (multiple of 4); layout: pass thread layout (-1 = default).
+    """
+
+    def __init__(self, ctx: Context, pool_particles: int, max_bunches: int, max_nbins: int,
+                 chunk: int = 65536, layout: int = -1, graph_turns: int = 16):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        _check(ctx, ctx._lib.hj_batch_create(ctx.handle, int(pool_particles), int(max_bunches),
+                                             int(max_nbins), int(chunk), int(layout),
+                                             ctypes.byref(h)))
+        self.handle = h
+        self.sizes = {}
+        if graph_turns != 16:
+            self.set_graph_turns(graph_turns)
+
+    def set_graph_turns(self, turns: int) -> None:
+        _check(self.ctx, self.ctx._lib.hj_batch_set_graph_turns(self.handle, int(turns)))
+
+    def _add(self, zp, ep, n, params, nbins, wake, seed, turns) -> int:
+        p = params.to_c()
+        w = (wake or WakeModel.reference(params)).to_c()
+        out = np.zeros(1, dtype=np.int64)
+        nt = params.n_turns if turns is None else int(turns)
+        _check(self.ctx, self.ctx._lib.hj_batch_add(
+            self.handle, zp, ep, int(n), ctypes.byref(p), ctypes.byref(w), int(nbins),
+            int(seed) & 0xFFFFFFFFFFFFFFFF, nt, _ip(out)))
+        bid = int(out[0])
+        self.sizes[bid] = int(n)
+        return bid
+
+    def add(self, z, dE, params: SimulationParameters, nbins: int, *,
+            wake: Optional[WakeModel] = None, seed: int = 0, turns: Optional[int] = None) -> int:
+        """Admit a bunch from host arrays (copied); returns its id.  Raises
+        HaissinskiError with status HJ_ERR_FULL when the batch has no room."""
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        dE = np.ascontiguousarray(dE, dtype=np.float64)
+        if z.shape != dE.shape:
+            raise ValueError("z and dE differ in length")
+        return self._add(z.ctypes.data_as(ctypes.c_void_p), dE.ctypes.data_as(ctypes.c_void_p),
+                         z.size, params, nbins, wake, seed, turns)
+
+    def add_device(self, d_z: int, d_dE: int, n: int, params: SimulationParameters, nbins: int,
+                   *, wake: Optional[WakeModel] = None, seed: int = 0,
+                   turns: Optional[int] = None) -> int:
+        """As add(), from device pointers (ints), copied into the pool."""
+        return self._add(ctypes.c_void_p(d_z), ctypes.c_void_p(d_dE), n, params, nbins, wake,
+                         seed, turns)
+
+    def advance(self, turns: int) -> None:
+        _check(self.ctx, self.ctx._lib.hj_batch_advance(self.handle, int(turns)))
+
+    def poll(self, cap: int = 4096) -> list:
+        """Waits for the enqueued turns; ids of bunches that ran all their turns."""
+        ids = np.zeros(max(cap, 1), dtype=np.int64)
+        n = ctypes.c_int32(0)
+        _check(self.ctx, self.ctx._lib.hj_batch_poll(self.handle, _ip(ids), int(cap),
+                                                     ctypes.byref(n)))
+        return [int(x) for x in ids[: n.value]]
+
+    def take(self, bid: int, copy_out: bool = True):
+        """Finishes bunch `bid` and frees its slot; returns (z, dE, EvolveResult)
+        (z and dE are None without copy_out)."""
+        n = self.sizes.pop(bid)
+        z = np.empty(n) if copy_out else None
+        dE = np.empty(n) if copy_out else None
+        r = HjResult()
+        rc = self.ctx._lib.hj_batch_take(
+            self.handle, int(bid), z.ctypes.data_as(ctypes.c_void_p) if copy_out else None,
+            dE.ctypes.data_as(ctypes.c_void_p) if copy_out else None, ctypes.byref(r))
+        _check(self.ctx, rc)
+        return z, dE, EvolveResult.from_c(r)
+
+    def stats(self) -> dict:
+        out = np.zeros(4, dtype=np.int64)
+        _check(self.ctx, self.ctx._lib.hj_batch_stats(self.handle, _ip(out)))
+        return {"live": int(out[0]), "largest_free_particles": int(out[1]),
+                "free_slots": int(out[2]), "turns_enqueued": int(out[3])}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.ctx._lib.hj_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -294,6 +294,7 @@ extern "C" const char* hj_status_string(hj_status s) {
     case HJ_ERR_TIMEOUT: return "HJ_ERR_TIMEOUT";
     case HJ_ERR_NO_DEVICE: return "HJ_ERR_NO_DEVICE";
     case HJ_ERR_STATE: return "HJ_ERR_STATE";
+    case HJ_ERR_FULL: return "HJ_ERR_FULL";
     default: return "HJ_ERR_UNKNOWN";
   }
 }
@@ -1069,4 +1070,406 @@ extern "C" hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE
     HJ_CUDA(ctx, launch_interp_kick(ex[0], ex[1], n, cb.pot, B, c1, cB, inv_c, ctx->stream));
   }
   return unstage(ctx, n, dE, ex[1]);
+}
+
+// ====================================================================== batches
+//
+// A batch holds hj_bunch objects whose particles live in one pool and whose
+// turn state lives in one device array (slot per bunch), so a poll is one
+// copy.  Per turn: k_batch_pass over the chunk table, k_batch_reduce, and
+// k_batch_bins (one 2-CTA cluster per bunch); the kernels read the bunch
+// tables and the live counts from device memory and are launched over the
+// batch's capacity, so a captured graph stays valid as bunches come and go.
+// A bunch's chunking depends only on its own size and the batch's chunk size,
+// so its sums -- and its results -- do not depend on the other bunches.
+
+struct BatchMember {
+  int64_t id = 0;
+  hj_bunch* b = nullptr;
+  int64_t start = 0, cap = 0;   // pool range [start, start + cap)
+  int slot = 0;                 // index into the turn-state array
+  int64_t turns = 0;
+};
+
+struct hj_batch {
+  hj_ctx* ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  int cfg = 0;
+  int64_t chunk = 65536;
+  int max_bunches = 0, max_B = 0, max_H = 0, max_chunks = 0;
+  int wake = -1, qe = -1;                      // fixed by the first bunch
+  int64_t pool_n = 0;
+  double* pool_z = nullptr;
+  double* pool_dE = nullptr;
+  std::vector<std::pair<int64_t, int64_t>> free_ranges;   // (start, length), sorted
+  std::vector<BatchMember> members;            // dense: index = device table slot
+  std::vector<int> free_slots;
+  int64_t next_id = 1;
+  TurnState* d_ts = nullptr;                   // [max_bunches]
+  TurnState* h_ts = nullptr;                   // pinned copy for polls
+  PassArgs* d_pass = nullptr;
+  BinsArgs* d_bins = nullptr;
+  BatchChunk* d_chunks = nullptr;
+  int32_t* d_counts = nullptr;                 // [0] chunks, [1] bunches
+  PassArgs* h_pass = nullptr;                  // pinned staging
+  BinsArgs* h_bins = nullptr;
+  BatchChunk* h_chunks = nullptr;
+  int32_t* h_counts = nullptr;
+  bool dirty = true;
+  int graph_turns = 16;
+  cudaGraphExec_t graph = nullptr;
+  int64_t turns_enqueued = 0;
+};
+
+namespace {
+
+hj_status batch_alloc_range(hj_batch* bt, int64_t n, int64_t* start, int64_t* cap) {
+  const int64_t need = std::max<int64_t>((n + 3) / 4 * 4, 4);
+  for (size_t i = 0; i < bt->free_ranges.size(); ++i) {
+    auto& r = bt->free_ranges[i];
+    if (r.second >= need) {
+      *start = r.first;
+      *cap = need;
+      r.first += need;
+      r.second -= need;
+      if (r.second == 0) bt->free_ranges.erase(bt->free_ranges.begin() + i);
+      return HJ_OK;
+    }
+  }
+  return HJ_ERR_FULL;
+}
+
+void batch_free_range(hj_batch* bt, int64_t start, int64_t cap) {
+  auto& fr = bt->free_ranges;
+  auto it = std::lower_bound(fr.begin(), fr.end(), std::make_pair(start, (int64_t)0));
+  it = fr.insert(it, {start, cap});
+  // merge with the neighbours
+  size_t i = it - fr.begin();
+  if (i + 1 < fr.size() && fr[i].first + fr[i].second == fr[i + 1].first) {
+    fr[i].second += fr[i + 1].second;
+    fr.erase(fr.begin() + i + 1);
+  }
+  if (i > 0 && fr[i - 1].first + fr[i - 1].second == fr[i].first) {
+    fr[i - 1].second += fr[i].second;
+    fr.erase(fr.begin() + i);
+  }
+}
+
+int64_t batch_largest_free(const hj_batch* bt) {
+  int64_t m = 0;
+  for (auto& r : bt->free_ranges) m = std::max(m, r.second);
+  return m;
+}
+
+// Rebuild and upload the device tables (bunch arguments, chunk table, counts).
+hj_status batch_upload(hj_batch* bt) {
+  hj_ctx* ctx = bt->ctx;
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));   // staging buffers are free again
+  int nch = 0;
+  const int nb = (int)bt->members.size();
+  for (int k = 0; k < nb; ++k) {
+    hj_bunch* b = bt->members[k].b;
+    fill_turn_args(b, bt->h_pass[k], bt->h_bins[k]);
+    for (int c = 0; c < b->nblk; ++c) {
+      BatchChunk ch;
+      ch.first = (int64_t)c * bt->chunk;
+      ch.count = std::min<int64_t>(bt->chunk, b->n - ch.first);
+      ch.bunch = k;
+      ch.part = c;
+      if (nch >= bt->max_chunks) return set_err(ctx, HJ_ERR_STATE, "batch chunk table overflow");
+      bt->h_chunks[nch++] = ch;
+    }
+  }
+  bt->h_counts[0] = nch;
+  bt->h_counts[1] = nb;
+  if (nb > 0) {
+    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_pass, bt->h_pass, sizeof(PassArgs) * nb,
+                                 cudaMemcpyHostToDevice, bt->stream));
+    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_bins, bt->h_bins, sizeof(BinsArgs) * nb,
+                                 cudaMemcpyHostToDevice, bt->stream));
+  }
+  if (nch > 0)
+    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_chunks, bt->h_chunks, sizeof(BatchChunk) * nch,
+                                 cudaMemcpyHostToDevice, bt->stream));
+  HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_counts, bt->h_counts, sizeof(int32_t) * 2,
+                               cudaMemcpyHostToDevice, bt->stream));
+  bt->dirty = false;
+  return HJ_OK;
+}
+
+hj_status batch_launch_turn(hj_batch* bt) {
+  hj_ctx* ctx = bt->ctx;
+  HJ_CUDA(ctx, launch_batch_pass(bt->d_pass, bt->d_chunks, bt->d_counts, bt->max_chunks,
+                                 bt->max_B, bt->wake, bt->qe, bt->cfg, bt->stream));
+  if (bt->wake)
+    HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_counts + 1, bt->max_bunches, bt->max_B,
+                                     bt->stream));
+  HJ_CUDA(ctx, launch_batch_bins(bt->d_bins, bt->d_counts + 1, bt->max_bunches, bt->max_H,
+                                 bt->stream));
+  return HJ_OK;
+}
+
+hj_status batch_capture(hj_batch* bt) {
+  hj_ctx* ctx = bt->ctx;
+  cudaGraph_t g = nullptr;
+  HJ_CUDA(ctx, cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
+  hj_status s = HJ_OK;
+  for (int t = 0; t < bt->graph_turns && s == HJ_OK; ++t) s = batch_launch_turn(bt);
+  cudaError_t e = cudaStreamEndCapture(bt->stream, &g);
+  if (s != HJ_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  if (e != cudaSuccess)
+    return set_err(ctx, HJ_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&bt->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return set_err(ctx, HJ_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+  return HJ_OK;
+}
+
+int batch_find(const hj_batch* bt, int64_t id) {
+  for (size_t k = 0; k < bt->members.size(); ++k)
+    if (bt->members[k].id == id) return (int)k;
+  return -1;
+}
+
+}  // namespace
+
+extern "C" void hj_batch_destroy(hj_batch* bt) {
+  if (!bt) return;
+  cudaSetDevice(bt->ctx->device);
+  if (bt->stream) cudaStreamSynchronize(bt->stream);
+  for (auto& m : bt->members) {
+    m.b->ts = nullptr;   // lives in the batch's array
+    hj_bunch_destroy(m.b);
+  }
+  if (bt->graph) cudaGraphExecDestroy(bt->graph);
+  void* dev[] = {bt->pool_z, bt->pool_dE, bt->d_ts, bt->d_pass, bt->d_bins, bt->d_chunks,
+                 bt->d_counts};
+  for (void* p : dev)
+    if (p) cudaFree(p);
+  void* pinned[] = {bt->h_ts, bt->h_pass, bt->h_bins, bt->h_chunks, bt->h_counts};
+  for (void* p : pinned)
+    if (p) cudaFreeHost(p);
+  if (bt->stream) cudaStreamDestroy(bt->stream);
+  delete bt;
+}
+
+static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
+                                   int32_t max_nbins, int64_t chunk, int32_t layout,
+                                   hj_batch* bt) {
+  bt->ctx = ctx;
+  bt->chunk = chunk;
+  bt->max_bunches = max_bunches;
+  bt->max_B = max_nbins;
+  const int64_t P = next_pow2(2 * (int64_t)max_nbins);
+  bt->max_H = (int)std::max<int64_t>(P / 4, 4);
+  bt->cfg = layout >= 0 ? layout : default_pass_layout(max_nbins, pool_particles);
+  bt->pool_n = (pool_particles + 3) / 4 * 4;
+  bt->max_chunks = (int)std::min<int64_t>(bt->pool_n / chunk + max_bunches + 1, INT32_MAX);
+  HJ_CUDA(ctx, cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking));
+  HJ_TRY(dalloc(ctx, &bt->pool_z, (size_t)bt->pool_n));
+  HJ_TRY(dalloc(ctx, &bt->pool_dE, (size_t)bt->pool_n));
+  HJ_TRY(dalloc(ctx, &bt->d_ts, (size_t)max_bunches));
+  HJ_TRY(dalloc(ctx, &bt->d_pass, (size_t)max_bunches));
+  HJ_TRY(dalloc(ctx, &bt->d_bins, (size_t)max_bunches));
+  HJ_TRY(dalloc(ctx, &bt->d_chunks, (size_t)bt->max_chunks));
+  HJ_TRY(dalloc(ctx, &bt->d_counts, 2));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_ts, sizeof(TurnState) * max_bunches));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_pass, sizeof(PassArgs) * max_bunches));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_bins, sizeof(BinsArgs) * max_bunches));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_chunks, sizeof(BatchChunk) * bt->max_chunks));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_counts, sizeof(int32_t) * 2));
+  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_counts, 0, sizeof(int32_t) * 2, bt->stream));
+  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_ts, 0, sizeof(TurnState) * max_bunches, bt->stream));
+  bt->free_ranges.push_back({0, bt->pool_n});
+  for (int s = max_bunches - 1; s >= 0; --s) bt->free_slots.push_back(s);
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
+                                     int32_t max_nbins, int64_t chunk_particles,
+                                     int32_t layout, hj_batch** out) {
+  HJ_TRY(ctx_ok(ctx));
+  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (pool_particles <= 0 || max_bunches <= 0)
+    return set_err(ctx, HJ_ERR_ARG, "pool_particles and max_bunches must be positive");
+  if (max_nbins <= 0) return set_err(ctx, HJ_ERR_NBINS, "Buffer nbins invalid (must be > 0).");
+  if (max_nbins > kMaxBins)
+    return set_err(ctx, HJ_ERR_TOO_LARGE, "max_nbins = %d exceeds the supported %lld",
+                   max_nbins, (long long)kMaxBins);
+  if (chunk_particles == 0) chunk_particles = 65536;
+  if (chunk_particles < 4 || chunk_particles % 4)
+    return set_err(ctx, HJ_ERR_ARG, "chunk_particles must be a positive multiple of 4");
+  if (layout < -1 || layout >= kNumPassCfgs)
+    return set_err(ctx, HJ_ERR_ARG, "pass layout must be -1 (automatic) or 0..%d", kNumPassCfgs - 1);
+  hj_batch* bt = new hj_batch();
+  hj_status s = batch_create_impl(ctx, pool_particles, max_bunches, max_nbins, chunk_particles,
+                                  layout, bt);
+  if (s != HJ_OK) {
+    hj_batch_destroy(bt);
+    return s;
+  }
+  *out = bt;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns) {
+  if (!bt) return HJ_ERR_ARG;
+  if (turns < 0) return set_err(bt->ctx, HJ_ERR_ARG, "graph turns must be >= 0");
+  if (bt->graph) {
+    HJ_CUDA(bt->ctx, cudaStreamSynchronize(bt->stream));
+    cudaGraphExecDestroy(bt->graph);
+    bt->graph = nullptr;
+  }
+  bt->graph_turns = turns;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* dE, int64_t n,
+                                  const hj_params* params, const hj_wake* wake, int64_t nbins,
+                                  uint64_t seed, int64_t turns, int64_t* id_out) {
+  if (!bt) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (!id_out) return set_err(ctx, HJ_ERR_ARG, "id_out is NULL");
+  *id_out = 0;
+  HJ_TRY(check_params(ctx, params));
+  if (n <= 0) return set_err(ctx, HJ_ERR_ARG, "a batch bunch needs at least one particle");
+  if (!z || !dE) return set_err(ctx, HJ_ERR_ARG, "particle arrays are NULL");
+  if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
+  const int wake_on = params->use_wakefield ? 1 : 0;
+  const int qe = params->use_excitation ? QE_PHILOX : QE_OFF;
+  if ((bt->wake >= 0 && bt->wake != wake_on) || (bt->qe >= 0 && bt->qe != qe))
+    return set_err(ctx, HJ_ERR_ARG,
+                   "all bunches of a batch share the wakefield and quantum-excitation switches");
+  if (wake_on && nbins > bt->max_B)
+    return set_err(ctx, HJ_ERR_FULL, "nbins = %lld exceeds the batch's %d",
+                   (long long)nbins, bt->max_B);
+  if (bt->free_slots.empty()) return set_err(ctx, HJ_ERR_FULL, "the batch's bunch slots are full");
+  int64_t start = 0, cap = 0;
+  if (batch_alloc_range(bt, n, &start, &cap) != HJ_OK)
+    return set_err(ctx, HJ_ERR_FULL, "no free pool range of %lld particles", (long long)n);
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  double* dz = bt->pool_z + start;
+  double* de = bt->pool_dE + start;
+  cudaError_t e = cudaMemcpyAsync(dz, z, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(de, dE, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
+  if (e != cudaSuccess) {
+    batch_free_range(bt, start, cap);
+    return set_err(ctx, HJ_ERR_CUDA, "copying the bunch into the pool failed: %s",
+                   cudaGetErrorString(e));
+  }
+  hj_bunch* b = new hj_bunch();
+  hj_status s = bunch_create_impl(ctx, dz, de, n, params, wake, nbins, nullptr, seed,
+                                  (void*)bt->stream, b, bt->chunk, bt->cfg);
+  if (s == HJ_OK && b->nblk > bt->max_chunks) s = set_err(ctx, HJ_ERR_FULL, "chunk table full");
+  if (s != HJ_OK) {
+    hj_bunch_destroy(b);
+    batch_free_range(bt, start, cap);
+    return s;
+  }
+  // move the turn state into the batch's array, with this bunch's turn budget
+  const int slot = bt->free_slots.back();
+  bt->free_slots.pop_back();
+  b->h_ts->turns_left = turns;
+  cudaFree(b->ts);
+  b->ts = bt->d_ts + slot;
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
+                               bt->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  BatchMember m;
+  m.id = bt->next_id++;
+  m.b = b;
+  m.start = start;
+  m.cap = cap;
+  m.slot = slot;
+  m.turns = turns;
+  bt->members.push_back(m);
+  bt->wake = wake_on;
+  bt->qe = qe;
+  bt->dirty = true;
+  *id_out = m.id;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_advance(hj_batch* bt, int64_t turns) {
+  if (!bt) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
+  if (bt->members.empty() || turns == 0) return HJ_OK;
+  if (bt->dirty) HJ_TRY(batch_upload(bt));
+  int64_t t = 0;
+  if (bt->graph_turns > 0 && turns >= bt->graph_turns) {
+    if (!bt->graph) HJ_TRY(batch_capture(bt));
+    for (; t + bt->graph_turns <= turns; t += bt->graph_turns)
+      HJ_CUDA(ctx, cudaGraphLaunch(bt->graph, bt->stream));
+  }
+  for (; t < turns; ++t) HJ_TRY(batch_launch_turn(bt));
+  bt->turns_enqueued += turns;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_poll(hj_batch* bt, int64_t* ids, int32_t cap, int32_t* n_done) {
+  if (!bt || !n_done || (cap > 0 && !ids)) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  *n_done = 0;
+  HJ_CUDA(ctx, cudaMemcpyAsync(bt->h_ts, bt->d_ts, sizeof(TurnState) * bt->max_bunches,
+                               cudaMemcpyDeviceToHost, bt->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  for (auto& m : bt->members) {
+    if (bt->h_ts[m.slot].turns_left <= 0 && *n_done < cap) ids[(*n_done)++] = m.id;
+  }
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_take(hj_batch* bt, int64_t id, double* z_out, double* dE_out,
+                                   hj_result* res) {
+  if (!bt) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  const int k = batch_find(bt, id);
+  if (k < 0) return set_err(ctx, HJ_ERR_ARG, "no bunch %lld in the batch", (long long)id);
+  BatchMember m = bt->members[k];
+  hj_bunch* b = m.b;
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  HJ_TRY(launch_moments(b, 1, b->z, b->dE));     // pending kick and re-centring
+  double mom[4];
+  HJ_TRY(read_moments(b, mom));
+  hj_status st = read_state(b);
+  fill_result(b, mom, res);
+  if (z_out)
+    HJ_CUDA(ctx, cudaMemcpyAsync(z_out, b->z, sizeof(double) * b->n, cudaMemcpyDefault, bt->stream));
+  if (dE_out)
+    HJ_CUDA(ctx, cudaMemcpyAsync(dE_out, b->dE, sizeof(double) * b->n, cudaMemcpyDefault,
+                                 bt->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  // retire: this slot's state must read "no turns left" for the kernels
+  TurnState dead{};
+  dead.turns_left = 0;
+  HJ_CUDA(ctx, cudaMemcpy(b->ts, &dead, sizeof(TurnState), cudaMemcpyHostToDevice));
+  b->ts = nullptr;
+  hj_bunch_destroy(b);
+  batch_free_range(bt, m.start, m.cap);
+  bt->free_slots.push_back(m.slot);
+  bt->members[k] = bt->members.back();
+  bt->members.pop_back();
+  bt->dirty = true;
+  return st;
+}
+
+extern "C" hj_status hj_batch_stats(hj_batch* bt, int64_t* out4) {
+  if (!bt || !out4) return HJ_ERR_ARG;
+  out4[0] = (int64_t)bt->members.size();
+  out4[1] = batch_largest_free(bt);
+  out4[2] = (int64_t)bt->free_slots.size();
+  out4[3] = bt->turns_enqueued;
+  return HJ_OK;
 }

@@ -6,7 +6,8 @@ C = 215.9 m, h = 360 at 500 MHz, V = 5 MV, α_c = 3e-4, U0 = 0.5 MeV/turn,
 resonator Rs = 10 kΩ, Q = 1, f_r = 20 GHz, 1e10 electrons, bins over ±6σ_z).
 The reference API has no circumference or damping-time fields, so they are
 expressed through its own parameters:
-  * ϕs = π - asin(U0/V): the reference's above-transition convention
+  * ϕs = π - asin(U0/V) for the ring's voltage V: the reference's
+    above-transition convention
     (its benchmark uses ϕs = 5π/6, tests/benchmark_total.jl:152);
   * radius = 4·8.85e-5·(E0/1e9)^3 / 2e-4 = 113.28 m, so that the per-turn
     damping ∂U/∂E of src/synchrotron_radiation.jl:44 is 1/5000;
@@ -42,7 +43,7 @@ def benchmark_ring(n_turns: int = 100, nbins: int = 4096, population: float = 1e
     radius = 4 * 8.85e-5 * (E0 / 1e9) ** 3 * damping_turns
     params = SimulationParameters(
         E0=E0, mass=MASS_ELECTRON, voltage=voltage, harmonic=360, radius=radius,
-        pipe_radius=2.5e-4, alpha_c=3e-4, phi_s=math.pi - math.asin(U0 / 5e6),
+        pipe_radius=2.5e-4, alpha_c=3e-4, phi_s=math.pi - math.asin(U0 / voltage),
         freq_rf=500e6, n_turns=n_turns, use_wakefield=use_wakefield, update_eta=True,
         update_E0=True, SR_damping=True, use_excitation=use_excitation)
     wake = WakeModel.resonator(Rs=1e4, Q=1.0, fr=20e9, population=population,

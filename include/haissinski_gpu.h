@@ -45,7 +45,9 @@ enum {
   HJ_ERR_NONFINITE = 8,    /* a NaN/Inf appeared in the bunch moments */
   HJ_ERR_TIMEOUT = 9,      /* a bounded device-side wait gave up */
   HJ_ERR_NO_DEVICE = 10,   /* no CUDA device, or device index out of range */
-  HJ_ERR_STATE = 11        /* call out of order (e.g. advance after finish) */
+  HJ_ERR_STATE = 11,       /* call out of order (e.g. advance after finish) */
+  HJ_ERR_FULL = 12         /* a batch has no room for the bunch now (slots, particle
+                              pool or bins): retire finished bunches and retry */
 };
 
 /*
@@ -121,6 +123,7 @@ typedef struct hj_result {
 
 typedef struct hj_ctx hj_ctx;
 typedef struct hj_bunch hj_bunch;
+typedef struct hj_batch hj_batch;
 
 /* ---------------------------------------------------------------- context */
 
@@ -242,6 +245,46 @@ hj_status hj_bunch_histogram(hj_bunch* b, int64_t* counts_host);
 hj_status hj_bunch_potential(hj_bunch* b, double* pot_host);
 void hj_bunch_destroy(hj_bunch* b);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent bunches -- each with its own particle count, RF voltage,
+ * intensity, bins, seed and number of turns -- advanced together: every turn
+ * is one particle-pass launch over a chunk table of all live bunches, one
+ * histogram merge and one bins-step launch with a two-CTA cluster per bunch.
+ * Blocks of K turns replay a captured CUDA graph.  A bunch's results do not
+ * depend on which other bunches share the batch.  No reference counterpart:
+ * the reference runs parameter points one after another
+ * (src/parameter_sensitivity/scan.jl:182-184). */
+
+/* A batch on ctx's device with its own stream: a particle pool of
+ * pool_particles (16 B each), up to max_bunches bunches of up to max_nbins
+ * bins, chunk_particles particles per block of the pass (a multiple of 4;
+ * 0 = 65536) and pass layout `layout` (-1 = the default for max_nbins). */
+hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
+                          int32_t max_nbins, int64_t chunk_particles, int32_t layout,
+                          hj_batch** out);
+void hj_batch_destroy(hj_batch* bt);
+/* Turns per captured CUDA graph (0 = launch every turn directly; default 16). */
+hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns);
+/* Admit a bunch: z, dE (host or device, n each) are copied into the pool;
+ * params/wake/nbins/seed as for hj_bunch_create (the wakefield must be on);
+ * it runs `turns` turns.  *id_out names it.  HJ_ERR_FULL: no room now. */
+hj_status hj_batch_add(hj_batch* bt, const double* z, const double* dE, int64_t n,
+                       const hj_params* params, const hj_wake* wake, int64_t nbins,
+                       uint64_t seed, int64_t turns, int64_t* id_out);
+/* Enqueue `turns` turns of every live bunch (a bunch stops at its own count). */
+hj_status hj_batch_advance(hj_batch* bt, int64_t turns);
+/* Wait for the enqueued turns; ids[0..*n_done-1] = bunches that have run all
+ * their turns and are not taken yet (at most cap). */
+hj_status hj_batch_poll(hj_batch* bt, int64_t* ids, int32_t cap, int32_t* n_done);
+/* Finish bunch `id` (pending kick and re-centring applied), copy its (z, dE)
+ * to z_out/dE_out (host or device, either may be NULL), fill *res, and free
+ * its slot and pool range. */
+hj_status hj_batch_take(hj_batch* bt, int64_t id, double* z_out, double* dE_out,
+                        hj_result* res);
+/* out[0] live bunches, out[1] free pool particles (largest free range),
+ * out[2] free slots, out[3] turns enqueued so far. */
+hj_status hj_batch_stats(hj_batch* bt, int64_t* out4);
+
 /* ---------------------------------------------------------------- single steps (host buffers) */
 
 /* rf_kick!(voltage, sin_ϕs, rf_factor, ϕs, particles, buffers)
@@ -307,7 +350,7 @@ hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE, int64_t n
                              const hj_wake* wake, double current, double sigma_z,
                              const hj_grid* grid);
 
-/* The Philox-4x32-10 standard normals used for quantum excitation:
+/* The Philox-2x32-10 standard normals used for quantum excitation:
  * out[i] = N(0,1) draw of particle i at `turn` under `seed`.  No reference
  * counterpart (the reference calls randn!, src/quantum_excitation.jl:36). */
 hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64_t n, double* out);

@@ -1,0 +1,119 @@
+"""Batches of independent bunches (hj_batch_*) against the plain resident path.
+
+A bunch advanced in a batch sees the same arithmetic as alone: the same
+Philox draws (seed, particle, turn), the same per-particle code and the same
+bins step; only the blocking of its partial sums differs from the plain
+path's grid, so (z, ΔE) agree within 1e-12 relative, and a bunch's results are
+bit-identical whichever other bunches share the batch."""
+import numpy as np
+import pytest
+import torch
+
+from haissinskijulia_b200 import Batch, HaissinskiError, ResidentBunch, benchmark_ring
+from haissinskijulia_b200 import _lib
+
+from gpu_util import assert_close, device_pair
+
+pytestmark = pytest.mark.gpu
+
+
+def _bunch(n, seed, cfg):
+    rng = np.random.default_rng(seed)
+    return rng.normal(0.0, cfg.sigma_z, n), rng.normal(0.0, cfg.sigma_E, n)
+
+
+def _spec(i):
+    """Bunch i of the test sweep: own size, voltage, intensity, bins, seed."""
+    n = [5003, 40_000, 123_457, 777, 65_536][i]
+    volt = [3e6, 5e6, 7e6, 4e6, 6e6][i]
+    pop = [1e9, 1e10, 1e11, 3e10, 5e9][i]
+    nbins = [512, 1024, 2048, 256, 1024][i]
+    cfg = benchmark_ring(n_turns=1, nbins=nbins, population=pop, voltage=volt)
+    z, dE = _bunch(n, 100 + i, cfg)
+    return cfg, z, dE, nbins, 1000 + i
+
+
+def _plain(ctx, cfg, z, dE, nbins, seed, turns):
+    dz, de = device_pair(z, dE)
+    b = ResidentBunch(ctx, dz.data_ptr(), de.data_ptr(), z.size, cfg.params, nbins,
+                      wake=cfg.wake, seed=seed)
+    b.advance(turns)
+    r = b.finish()
+    b.close()
+    return dz.cpu().numpy(), de.cpu().numpy(), r
+
+
+def _check(a, b, cfg, what):
+    za, ea, ra = a
+    zb, eb, rb = b
+    assert_close(za, zb, cfg.sigma_z, what=f"z {what}")
+    assert_close(ea, eb, cfg.sigma_E, what=f"dE {what}")
+    assert ra.E0 == pytest.approx(rb.E0, rel=1e-12)
+    assert ra.sigma_E == pytest.approx(rb.sigma_E, rel=1e-12)
+    assert ra.sigma_z == pytest.approx(rb.sigma_z, rel=1e-12)
+
+
+def test_batch_matches_the_plain_path_with_ragged_turns(gpu_ctx):
+    turns = [20, 35, 27, 20, 40]
+    bt = Batch(gpu_ctx, pool_particles=300_000, max_bunches=8, max_nbins=2048, chunk=16384)
+    ids = {}
+    for i in range(5):
+        cfg, z, dE, nbins, seed = _spec(i)
+        ids[bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=turns[i])] = i
+    done = {}
+    for _ in range(5):                       # 5 x 8 turns, with a poll between blocks
+        bt.advance(8)
+        for bid in bt.poll():
+            done[ids[bid]] = bt.take(bid)
+    assert sorted(done) == list(range(5))
+    assert bt.stats()["live"] == 0
+    for i in range(5):
+        cfg, z, dE, nbins, seed = _spec(i)
+        _check(done[i], _plain(gpu_ctx, cfg, z, dE, nbins, seed, turns[i]), cfg, f"bunch {i}")
+    bt.close()
+
+
+def test_results_do_not_depend_on_the_mix(gpu_ctx):
+    """Bunch 2 alone, and in a batch with others admitted before and after it
+    (graph replays and direct launches mixed): bit-identical results."""
+    cfg, z, dE, nbins, seed = _spec(2)
+    alone = Batch(gpu_ctx, 200_000, 4, 2048, chunk=16384, graph_turns=0)
+    a = alone.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=30)
+    alone.advance(30)
+    assert alone.poll() == [a]
+    za, ea, ra = alone.take(a)
+    alone.close()
+
+    mix = Batch(gpu_ctx, 400_000, 6, 2048, chunk=16384, graph_turns=8)
+    for i in (0, 1):
+        c, zz, ee, nb, s = _spec(i)
+        mix.add(zz, ee, c.params, nb, wake=c.wake, seed=s, turns=50)
+    mix.advance(5)                                   # the others are already running
+    m = mix.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=30)
+    c, zz, ee, nb, s = _spec(4)
+    mix.add(zz, ee, c.params, nb, wake=c.wake, seed=s, turns=50)
+    mix.advance(17)
+    mix.advance(13)
+    assert m in mix.poll()
+    zm, em, rm = mix.take(m)
+    mix.close()
+    assert np.array_equal(za, zm) and np.array_equal(ea, em)
+    assert (ra.E0, ra.sigma_E, ra.sigma_z) == (rm.E0, rm.sigma_E, rm.sigma_z)
+
+
+def test_admission_is_refused_when_the_batch_is_full(gpu_ctx):
+    cfg, z, dE, nbins, seed = _spec(1)
+    bt = Batch(gpu_ctx, 50_000, 2, 1024)
+    bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=3)
+    with pytest.raises(HaissinskiError) as e:
+        bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=3)  # pool
+    assert e.value.status == _lib.HJ_ERR_FULL
+    c4, z4, e4, nb4, s4 = _spec(3)
+    with pytest.raises(HaissinskiError) as e:
+        bt.add(z4, e4, c4.params, 4096, wake=c4.wake, seed=s4, turns=3)      # bins
+    assert e.value.status == _lib.HJ_ERR_FULL
+    bt.advance(3)
+    (bid,) = bt.poll()
+    bt.take(bid, copy_out=False)
+    bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=3)      # room again
+    bt.close()
