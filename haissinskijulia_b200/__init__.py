@@ -22,6 +22,7 @@ from .api import (  # noqa: F401
     calc_rf_factor,
     calculate_local_histogram,
     create_simulation_buffers,
+    gaussian_bunch,
     gaussian_draws,
     longitudinal_evolve,
     next_power_of_two,

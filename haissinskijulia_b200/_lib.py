@@ -125,6 +125,11 @@ SIGNATURES = {
     "hj_batch_set_graph_turns": (c_int32, [c_void_p, c_int32]),
     "hj_batch_add": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, POINTER(HjParams),
                                POINTER(HjWake), c_int64, c_uint64, c_int64, _IP]),
+    "hj_batch_add_gaussian": (c_int32, [c_void_p, c_int64, c_double, c_double, c_uint64,
+                                        POINTER(HjParams), POINTER(HjWake), c_int64, c_uint64,
+                                        c_int64, _IP]),
+    "hj_gaussian_bunch": (c_int32, [_CTX, c_uint64, c_int64, c_double, c_double, c_void_p,
+                                    c_void_p, c_void_p]),
     "hj_batch_advance": (c_int32, [c_void_p, c_int64]),
     "hj_batch_poll": (c_int32, [c_void_p, _IP, c_int32, POINTER(c_int32)]),
     "hj_batch_take": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, POINTER(HjResult)]),

@@ -652,6 +652,24 @@ class Batch:
         return self._add(ctypes.c_void_p(d_z), ctypes.c_void_p(d_dE), n, params, nbins, wake,
                          seed, turns)
 
+    def add_gaussian(self, n: int, sigma_z: float, sigma_E: float, init_seed: int,
+                     params: SimulationParameters, nbins: int, *,
+                     wake: Optional[WakeModel] = None, seed: int = 0,
+                     turns: Optional[int] = None) -> int:
+        """Admit a bunch of n independent Gaussians generated on the device
+        (gaussian_bunch with init_seed); returns its id."""
+        p = params.to_c()
+        w = (wake or WakeModel.reference(params)).to_c()
+        out = np.zeros(1, dtype=np.int64)
+        nt = params.n_turns if turns is None else int(turns)
+        _check(self.ctx, self.ctx._lib.hj_batch_add_gaussian(
+            self.handle, int(n), float(sigma_z), float(sigma_E),
+            int(init_seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(p), ctypes.byref(w), int(nbins),
+            int(seed) & 0xFFFFFFFFFFFFFFFF, nt, _ip(out)))
+        bid = int(out[0])
+        self.sizes[bid] = int(n)
+        return bid
+
     def advance(self, turns: int) -> None:
         _check(self.ctx, self.ctx._lib.hj_batch_advance(self.handle, int(turns)))
 
@@ -692,3 +710,13 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def gaussian_bunch(ctx: Context, init_seed: int, n: int, sigma_z: float, sigma_E: float,
+                   d_z: int, d_dE: int, stream: int = 0) -> None:
+    """Fill device arrays (ints: pointers) with n independent Gaussians
+    z ~ N(0, sigma_z), dE ~ N(0, sigma_E) from init_seed, on `stream`."""
+    _check(ctx, ctx._lib.hj_gaussian_bunch(ctx.handle, int(init_seed) & 0xFFFFFFFFFFFFFFFF,
+                                           int(n), float(sigma_z), float(sigma_E),
+                                           ctypes.c_void_p(d_z), ctypes.c_void_p(d_dE),
+                                           ctypes.c_void_p(stream)))

@@ -1330,9 +1330,12 @@ extern "C" hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns) {
   return HJ_OK;
 }
 
-extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* dE, int64_t n,
-                                  const hj_params* params, const hj_wake* wake, int64_t nbins,
-                                  uint64_t seed, int64_t turns, int64_t* id_out) {
+// z, dE != NULL: copy them into the pool; else generate independent
+// Gaussians (σ_z, σ_E) from init_seed in place.
+static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE, int64_t n,
+                                const hj_params* params, const hj_wake* wake, int64_t nbins,
+                                uint64_t seed, int64_t turns, int64_t* id_out, double sigma_z,
+                                double sigma_E, uint64_t init_seed) {
   if (!bt) return HJ_ERR_ARG;
   hj_ctx* ctx = bt->ctx;
   HJ_TRY(ctx_ok(ctx));
@@ -1340,7 +1343,6 @@ extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* d
   *id_out = 0;
   HJ_TRY(check_params(ctx, params));
   if (n <= 0) return set_err(ctx, HJ_ERR_ARG, "a batch bunch needs at least one particle");
-  if (!z || !dE) return set_err(ctx, HJ_ERR_ARG, "particle arrays are NULL");
   if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
   const int wake_on = params->use_wakefield ? 1 : 0;
   const int qe = params->use_excitation ? QE_PHILOX : QE_OFF;
@@ -1357,9 +1359,14 @@ extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* d
   HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
   double* dz = bt->pool_z + start;
   double* de = bt->pool_dE + start;
-  cudaError_t e = cudaMemcpyAsync(dz, z, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(de, dE, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
+  cudaError_t e;
+  if (z) {
+    e = cudaMemcpyAsync(dz, z, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(de, dE, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
+  } else {
+    e = launch_gaussian_bunch(init_seed, n, 0.0, sigma_z, 0.0, sigma_E, dz, de, bt->stream);
+  }
   if (e != cudaSuccess) {
     batch_free_range(bt, start, cap);
     return set_err(ctx, HJ_ERR_CUDA, "copying the bunch into the pool failed: %s",
@@ -1395,6 +1402,36 @@ extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* d
   bt->qe = qe;
   bt->dirty = true;
   *id_out = m.id;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* dE, int64_t n,
+                                  const hj_params* params, const hj_wake* wake, int64_t nbins,
+                                  uint64_t seed, int64_t turns, int64_t* id_out) {
+  if (bt && (!z || !dE)) return set_err(bt->ctx, HJ_ERR_ARG, "particle arrays are NULL");
+  return batch_add_impl(bt, z, dE, n, params, wake, nbins, seed, turns, id_out, 0.0, 0.0, 0);
+}
+
+extern "C" hj_status hj_batch_add_gaussian(hj_batch* bt, int64_t n, double sigma_z,
+                                           double sigma_E, uint64_t init_seed,
+                                           const hj_params* params, const hj_wake* wake,
+                                           int64_t nbins, uint64_t seed, int64_t turns,
+                                           int64_t* id_out) {
+  if (bt && !(sigma_z >= 0.0 && sigma_E >= 0.0))
+    return set_err(bt->ctx, HJ_ERR_ARG, "spreads must be non-negative");
+  return batch_add_impl(bt, nullptr, nullptr, n, params, wake, nbins, seed, turns, id_out,
+                        sigma_z, sigma_E, init_seed);
+}
+
+extern "C" hj_status hj_gaussian_bunch(hj_ctx* ctx, uint64_t init_seed, int64_t n,
+                                       double sigma_z, double sigma_E, double* d_z,
+                                       double* d_dE, void* stream) {
+  HJ_TRY(ctx_ok(ctx));
+  if (n < 0 || (n > 0 && (!d_z || !d_dE))) return set_err(ctx, HJ_ERR_ARG, "bad particle arrays");
+  if (!(sigma_z >= 0.0 && sigma_E >= 0.0)) return set_err(ctx, HJ_ERR_ARG, "spreads must be non-negative");
+  if (n == 0) return HJ_OK;
+  HJ_CUDA(ctx, launch_gaussian_bunch(init_seed, n, 0.0, sigma_z, 0.0, sigma_E, d_z, d_dE,
+                                     (cudaStream_t)stream));
   return HJ_OK;
 }
 

@@ -155,6 +155,9 @@ cudaError_t launch_phase_advance(int update_eta, TurnScalars s, double inv_mass,
                                  const double* dE, double* z, int64_t n, cudaStream_t st);
 cudaError_t launch_gaussian(uint64_t seed, int64_t turn, int64_t n, double* out,
                             cudaStream_t st);
+cudaError_t launch_gaussian_bunch(uint64_t seed, int64_t n, double mu_z, double sigma_z,
+                                  double mu_E, double sigma_E, double* z, double* dE,
+                                  cudaStream_t st);
 
 // ---- launchers (hj_wake.cu) ----
 cudaError_t prepare_wake_kernels(int max_smem);    // once per device: dynamic smem limits

@@ -715,6 +715,22 @@ __global__ void k_gaussian(uint64_t seed, int64_t turn, int64_t n, double* __res
   }
 }
 
+// Independent Gaussian bunch: particle i gets the Philox pair (i, turn 0) of
+// seed ^ kInitTag (turn 0 is never a tracking turn, and the tag keeps the
+// stream apart from the quantum-excitation one of the same seed).
+constexpr uint64_t kInitTag = 0x6A09E667F3BCC909ull;
+__global__ void k_gaussian_bunch(uint64_t seed, int64_t n, double mu_z, double sigma_z,
+                                 double mu_E, double sigma_E, double* __restrict__ z,
+                                 double* __restrict__ dE) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double rr[2];
+    philox_normals2(seed ^ kInitTag, 0, i, rr);
+    z[i] = fma(sigma_z, rr[0], mu_z);
+    dE[i] = fma(sigma_E, rr[1], mu_E);
+  }
+}
+
 int elementwise_grid(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g < 1) g = 1;
@@ -921,6 +937,14 @@ cudaError_t launch_phase_advance(int update_eta, TurnScalars s, double inv_mass,
 cudaError_t launch_gaussian(uint64_t seed, int64_t turn, int64_t n, double* out,
                             cudaStream_t st) {
   k_gaussian<<<elementwise_grid((n + 1) / 2), 256, 0, st>>>(seed, turn, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gaussian_bunch(uint64_t seed, int64_t n, double mu_z, double sigma_z,
+                                  double mu_E, double sigma_E, double* z, double* dE,
+                                  cudaStream_t st) {
+  k_gaussian_bunch<<<elementwise_grid(n), 256, 0, st>>>(seed, n, mu_z, sigma_z, mu_E, sigma_E, z,
+                                                        dE);
   return cudaGetLastError();
 }
 

@@ -271,6 +271,12 @@ hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns);
 hj_status hj_batch_add(hj_batch* bt, const double* z, const double* dE, int64_t n,
                        const hj_params* params, const hj_wake* wake, int64_t nbins,
                        uint64_t seed, int64_t turns, int64_t* id_out);
+/* As hj_batch_add, with the bunch generated on the device: independent
+ * Gaussians z ~ N(0, sigma_z), dE ~ N(0, sigma_E) (hj_gaussian_bunch). */
+hj_status hj_batch_add_gaussian(hj_batch* bt, int64_t n, double sigma_z, double sigma_E,
+                                uint64_t init_seed, const hj_params* params,
+                                const hj_wake* wake, int64_t nbins, uint64_t seed,
+                                int64_t turns, int64_t* id_out);
 /* Enqueue `turns` turns of every live bunch (a bunch stops at its own count). */
 hj_status hj_batch_advance(hj_batch* bt, int64_t turns);
 /* Wait for the enqueued turns; ids[0..*n_done-1] = bunches that have run all
@@ -349,6 +355,16 @@ hj_status hj_wake_potential_noalloc(hj_ctx* ctx, const int64_t* d_counts, const 
 hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE, int64_t n,
                              const hj_wake* wake, double current, double sigma_z,
                              const hj_grid* grid);
+
+/* A bunch of independent Gaussians on the device: d_z[i] = sigma_z * N0,
+ * d_dE[i] = sigma_E * N1 with (N0, N1) the Philox-2x32-10 / Box-Muller pair of
+ * particle i under init_seed (a stream apart from the quantum-excitation
+ * draws).  Enqueued on `stream`.  The reference draws its bunches with
+ * Distributions.jl on the host (generate_particles, src/evolution.jl:42-133,
+ * with a covariance estimate; the benchmark configurations use independent
+ * Gaussians). */
+hj_status hj_gaussian_bunch(hj_ctx* ctx, uint64_t init_seed, int64_t n, double sigma_z,
+                            double sigma_E, double* d_z, double* d_dE, void* stream);
 
 /* The Philox-2x32-10 standard normals used for quantum excitation:
  * out[i] = N(0,1) draw of particle i at `turn` under `seed`.  No reference
