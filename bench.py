@@ -55,6 +55,12 @@ def parse_args():
                     help="bounded CPU work of the --impl reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true",
+                    help="skip the batched-sweep / serving measurements (single GPU only)")
+    ap.add_argument("--sweep-turns", type=int, default=5000)
+    ap.add_argument("--sweep-plain-points", type=int, default=8,
+                    help="points of the sweep also run one after another on the plain path")
+    ap.add_argument("--serve-requests", type=int, default=40)
     return ap.parse_args()
 
 
@@ -210,6 +216,70 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def measure_sweeps(ctx, args) -> dict:
+    """The ragged 256-point sweep (batched vs plain point by point), the
+    32-bunch intensity scan and a served request stream, host wall clock
+    around each (admission, turns, retirement and result read-back included)."""
+    import numpy as np
+    from haissinskijulia_b200.sweep import (autotune, intensity_scan, request_stream,
+                                            run_batched, run_plain, serve, sweep_points)
+    T = args.sweep_turns
+    pts = sweep_points(256, turns=T)
+    t0 = time.perf_counter()
+    tun = autotune(ctx, pts, trial_turns=32, sample=64)
+    t_tune = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bat = run_batched(ctx, pts, tuning=tun, block_turns=500)
+    t_bat = time.perf_counter() - t0
+    k = max(1, min(args.sweep_plain_points, len(pts)))
+    idx = list(range(0, len(pts), len(pts) // k))[:k]
+    t0 = time.perf_counter()
+    pla = run_plain(ctx, [pts[i] for i in idx])
+    t_pla = time.perf_counter() - t0
+    rel = 0.0
+    for j, i in enumerate(idx):
+        a, b = bat[i].result, pla[j].result
+        for key in ("E0", "sigma_E", "sigma_z"):
+            x, y = getattr(a, key), getattr(b, key)
+            rel = max(rel, abs(x - y) / abs(y))
+    pt = sum(p.n * p.turns for p in pts)
+    out = {
+        "config": f"256 points: V ~ U[3,7] MV, population log-U[1e9,1e11], particles "
+                  f"log-U[1e4,2e6] (total {sum(p.n for p in pts):.3e}), {T} turns, 4096 bins, "
+                  "own seed; bunches generated on the device",
+        "batched_solves_per_s": len(pts) / t_bat, "batched_seconds": t_bat,
+        "batched_particle_turns_per_s": pt / t_bat,
+        "plain_solves_per_s": k / t_pla, "plain_seconds": t_pla,
+        "plain_sample": f"{k} of the 256 points (every {len(pts) // k}th), all {T} turns each, "
+                        "one after another on the plain resident path",
+        "speedup_vs_plain": (len(pts) / t_bat) / (k / t_pla),
+        "max_rel_diff_vs_plain": rel,
+        "tuning": {"particles_per_block": tun.chunk, "layout": tun.layout,
+                   "graph_turns": tun.graph_turns, "autotune_seconds": t_tune},
+        "timing": "host wall clock: admission, every turn, retirement",
+    }
+    scan = intensity_scan(turns=T)
+    t0 = time.perf_counter()
+    run_batched(ctx, scan, tuning=tun, block_turns=500)
+    t_scan = time.perf_counter() - t0
+    out["intensity_scan"] = {
+        "config": f"32 bunches x 1e6 particles, populations log-spaced 1e9-1e11, {T} turns, "
+                  "8192 bins, one batch",
+        "solves_per_s": len(scan) / t_scan, "seconds": t_scan,
+        "particle_turns_per_s": sum(p.n * p.turns for p in scan) / t_scan}
+    if args.serve_requests > 0:
+        reqs = request_stream(args.serve_requests)
+        rep = serve(ctx, reqs, tuning=tun)
+        sm = rep.summary()
+        sm["config"] = (f"{args.serve_requests} requests, Poisson arrivals at 50/s, V ~ U[3,7] "
+                        "MV, population log-U[1e9,1e11], particles log-U[1e4,4e6], turns "
+                        "U[1000,20000], bins in {2048,4096,8192}; admission by footprint "
+                        "(8 GB budget), 200-turn blocks")
+        sm["particle_turns_per_s"] = sm["particle_turns"] / sm["wall_s"]
+        out["serving"] = sm
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -316,6 +386,10 @@ def run_ours(args) -> None:
                "d2h_bytes_per_step": 16 * n, "turns_per_step": E,
                "seconds_per_step": t_e2e, "api": "haissinskijulia_b200.longitudinal_evolve -> hj_evolve"}
 
+    sweep = None
+    if world == 1 and not args.no_sweep:
+        sweep = measure_sweeps(ctx, args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = cpu_cores()
@@ -330,7 +404,7 @@ def run_ours(args) -> None:
             "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload(n, B), parallelism="replicas" if world > 1 else "single GPU"),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "sweep": sweep,
             "gpu_launches": prof["launches"], "clocks": clock_info,
             "wall_seconds_timed": t_wall,
             "final": {"sigma_E": res.sigma_E, "sigma_z": res.sigma_z, "E0": res.E0},

@@ -1097,6 +1097,9 @@ struct hj_batch {
   int cfg = 0;
   int64_t chunk = 65536;
   int max_bunches = 0, max_B = 0, max_H = 0, max_chunks = 0;
+  // launch widths: the live counts rounded up to a power of two (a captured
+  // graph is re-captured only when the live counts outgrow them)
+  int grid_chunks = 0, grid_bunches = 0;
   int wake = -1, qe = -1;                      // fixed by the first bunch
   int64_t pool_n = 0;
   double* pool_z = nullptr;
@@ -1182,6 +1185,14 @@ hj_status batch_upload(hj_batch* bt) {
   }
   bt->h_counts[0] = nch;
   bt->h_counts[1] = nb;
+  if (nch > bt->grid_chunks || nb > bt->grid_bunches) {
+    bt->grid_chunks = std::max(bt->grid_chunks, (int)std::min<int64_t>(next_pow2(nch), bt->max_chunks));
+    bt->grid_bunches = std::max(bt->grid_bunches, (int)std::min<int64_t>(next_pow2(nb), bt->max_bunches));
+    if (bt->graph) {
+      cudaGraphExecDestroy(bt->graph);
+      bt->graph = nullptr;
+    }
+  }
   if (nb > 0) {
     HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_pass, bt->h_pass, sizeof(PassArgs) * nb,
                                  cudaMemcpyHostToDevice, bt->stream));
@@ -1199,12 +1210,12 @@ hj_status batch_upload(hj_batch* bt) {
 
 hj_status batch_launch_turn(hj_batch* bt) {
   hj_ctx* ctx = bt->ctx;
-  HJ_CUDA(ctx, launch_batch_pass(bt->d_pass, bt->d_chunks, bt->d_counts, bt->max_chunks,
+  HJ_CUDA(ctx, launch_batch_pass(bt->d_pass, bt->d_chunks, bt->d_counts, bt->grid_chunks,
                                  bt->max_B, bt->wake, bt->qe, bt->cfg, bt->stream));
   if (bt->wake)
-    HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_counts + 1, bt->max_bunches, bt->max_B,
+    HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_counts + 1, bt->grid_bunches, bt->max_B,
                                      bt->stream));
-  HJ_CUDA(ctx, launch_batch_bins(bt->d_bins, bt->d_counts + 1, bt->max_bunches, bt->max_H,
+  HJ_CUDA(ctx, launch_batch_bins(bt->d_bins, bt->d_counts + 1, bt->grid_bunches, bt->max_H,
                                  bt->stream));
   return HJ_OK;
 }
