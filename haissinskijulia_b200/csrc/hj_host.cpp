@@ -5,6 +5,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "../../include/haissinski_gpu.h"
 #include "hj_host.h"
@@ -109,13 +112,25 @@ void host_rf_table(double V, double phi_s, int64_t M, double* tab_interleaved) {
   }
 }
 
+// exp(-2πik/P), k = 0..P-1, interleaved (re, im), in extended precision and
+// rounded once.  Tables are computed once per length and reused (a batch
+// admits many bunches with the same bin count).
 void host_twiddles(int64_t P, double* tw_interleaved) {
-  const long double kPiL = 3.141592653589793238462643383279502884L;
-  for (int64_t k = 0; k < P; ++k) {
-    const long double a = -2.0L * kPiL * (long double)k / (long double)P;
-    tw_interleaved[2 * k] = (double)cosl(a);
-    tw_interleaved[2 * k + 1] = (double)sinl(a);
+  static std::mutex mu;
+  static std::map<int64_t, std::vector<double>> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(P);
+  if (it == cache.end()) {
+    std::vector<double> t(2 * (size_t)P);
+    const long double kPiL = 3.141592653589793238462643383279502884L;
+    for (int64_t k = 0; k < P; ++k) {
+      const long double a = -2.0L * kPiL * (long double)k / (long double)P;
+      t[2 * k] = (double)cosl(a);
+      t[2 * k + 1] = (double)sinl(a);
+    }
+    it = cache.emplace(P, std::move(t)).first;
   }
+  std::memcpy(tw_interleaved, it->second.data(), sizeof(double) * 2 * (size_t)P);
 }
 
 }  // namespace hj

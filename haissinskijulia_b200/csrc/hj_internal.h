@@ -18,9 +18,10 @@ constexpr int64_t kMaxBins = 16384; // largest grid the shared-memory FFT holds 
 constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 
 // Thread layouts of the fused pass (particles/thread x threads/block; the next
-// group prefetched into registers in 0-2): 0 = 4 x 512, 1 = 2 x 1024,
-// 2 = 2 x 768, 3 = 2 x 512 without prefetch.
-constexpr int kNumPassCfgs = 4;
+// group prefetched into registers except in 3): 0 = 4 x 512, 1 = 2 x 1024,
+// 2 = 2 x 768, 3 = 2 x 512 without prefetch, 4 = 2 x 512 at 64 registers (two
+// blocks per SM where shared memory allows).
+constexpr int kNumPassCfgs = 5;
 constexpr int kRfTableSize = 128;    // entries of the fused pass's RF kick table
 int pass_cfg_threads(int cfg);
 int pass_cfg_ppt(int cfg);

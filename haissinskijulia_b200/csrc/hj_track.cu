@@ -505,8 +505,8 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
 
 // One turn over one bunch: block b takes groups b, b + grid, ... (THREADS
 // apart) and writes partial slot b; block 0 takes the tail.
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH>
-__global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1>
+__global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (WAKE) {  // zero the merged histograms k_hist_reduce accumulates into this turn
     const int gstride = gridDim.x * THREADS;
@@ -522,8 +522,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_track_pass(PassArgs a) {
 // (a contiguous run of one bunch's particles) and writes the bunch's partial
 // slot ch.part.  Blocks past the table's length, and chunks of bunches with
 // no turns left, return at once.
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH>
-__global__ void __launch_bounds__(THREADS, 1)
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1>
+__global__ void __launch_bounds__(THREADS, MINB)
     k_batch_pass(const PassArgs* __restrict__ bunches, const BatchChunk* __restrict__ chunks,
                  const int32_t* __restrict__ n_chunks) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -585,7 +585,25 @@ __global__ void k_batch_reduce(const PassArgs* __restrict__ bunches,
     sc = a.ngp_ovf[b];
     a.ngp_ovf[b] = 0ull;
   }
-  for (int k = 0; k < a.n_parts; ++k) {
+  // four slots in flight per thread (the loads are independent)
+  const int np = a.n_parts;
+  int k = 0;
+  for (; k + 4 <= np; k += 4) {
+    unsigned long long v[4];
+    uint32_t c[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (b < B) c[u] = __ldg(a.part_cnt + (size_t)(k + u) * B + b);
+      v[u] = __ldg(a.part_cic + (size_t)(k + u) * nc + b);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      sc += c[u];
+      sn += v[u] >> kCicSumBits;
+      sw += v[u] & kCicSumMask;
+    }
+  }
+  for (; k < np; ++k) {
     if (b < B) sc += __ldg(a.part_cnt + (size_t)k * B + b);
     const unsigned long long v = __ldg(a.part_cic + (size_t)k * nc + b);
     sn += v >> kCicSumBits;
@@ -757,6 +775,7 @@ const void* pass_fn_wq(int cfg) {
     case 0: return (const void*)k_track_pass<W, Q, 4, 512, true>;
     case 1: return (const void*)k_track_pass<W, Q, 2, 1024, true>;
     case 2: return (const void*)k_track_pass<W, Q, 2, 768, true>;
+    case 4: return (const void*)k_track_pass<W, Q, 2, 512, true, 2>;
     default: return (const void*)k_track_pass<W, Q, 2, 512, false>;
   }
 }
@@ -780,6 +799,7 @@ const void* batch_fn_wq(int cfg) {
     case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true>;
     case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true>;
     case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true>;
+    case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2>;
     default: return (const void*)k_batch_pass<W, Q, 2, 512, false>;
   }
 }

@@ -131,15 +131,15 @@ struct FftTables {
 
 __device__ __forceinline__ int compact_table_size(int H) { return H / 7 + 2; }
 
-template <int LR, bool INV>
+template <int LR, bool INV, int NT, int MAXH>
 __device__ __forceinline__ void stockham_pass(double2* s, FftTables t, int N, int Ns) {
   constexpr int R = 1 << LR;
-  constexpr int PER = (kMaxFftH / R + kBinsThreads - 1) / kBinsThreads;
+  constexpr int PER = (MAXH / R + NT - 1) / NT;
   const int nb = N >> LR;
   double2 v[PER][R];
 #pragma unroll
   for (int u = 0; u < PER; ++u) {
-    const int j = threadIdx.x + u * kBinsThreads;
+    const int j = threadIdx.x + u * NT;
     if (j < nb) {
       const int jm = j & (Ns - 1);
 #pragma unroll
@@ -166,7 +166,7 @@ __device__ __forceinline__ void stockham_pass(double2* s, FftTables t, int N, in
   __syncthreads();
 #pragma unroll
   for (int u = 0; u < PER; ++u) {
-    const int j = threadIdx.x + u * kBinsThreads;
+    const int j = threadIdx.x + u * NT;
     if (j < nb) {
       const int jm = j & (Ns - 1);
       const int base = ((j - jm) << LR) + jm;
@@ -177,16 +177,17 @@ __device__ __forceinline__ void stockham_pass(double2* s, FftTables t, int N, in
   __syncthreads();
 }
 
-template <bool INV>
+// Length-N (N <= MAXH) transform by NT threads.
+template <bool INV, int NT = kBinsThreads, int MAXH = kMaxFftH>
 __device__ void smem_fft(double2* s, FftTables t, int N, int logN) {
   int Ns = 1, rem = logN;
   while (rem >= 3) {
-    stockham_pass<3, INV>(s, t, N, Ns);
+    stockham_pass<3, INV, NT, MAXH>(s, t, N, Ns);
     Ns <<= 3;
     rem -= 3;
   }
-  if (rem == 2) stockham_pass<2, INV>(s, t, N, Ns);
-  else if (rem == 1) stockham_pass<1, INV>(s, t, N, Ns);
+  if (rem == 2) stockham_pass<2, INV, NT, MAXH>(s, t, N, Ns);
+  else if (rem == 1) stockham_pass<1, INV, NT, MAXH>(s, t, N, Ns);
 }
 
 // Twiddle tables of the length-H transform into shared memory (w_H^j = twP[4j]).
@@ -319,12 +320,13 @@ __device__ __forceinline__ double global_std(double s, double s2, int64_t n) {
 // all have the same parity, so each CTA runs one forward length-H FFT, its
 // half of the spectrum and one inverse length-H FFT in its own shared memory;
 // the halves are combined through distributed shared memory.
+template <int NT, int MAXH = kMaxFftH>
 __device__ __forceinline__ void bins_body(const BinsArgs& a) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   extern __shared__ __align__(16) double2 s_fft[];
-  __shared__ double red[kBinsThreads / 32];
+  __shared__ double red[NT / 32];
   __shared__ double sh[8];
   __shared__ double s_peer_sum;
 
@@ -380,16 +382,16 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
       const DensityVals g{a.cnt, a.lam, inv_n};
       // x[n] = g[2n] + i g[2n+1] (times w_M^n in the odd CTA)
 #pragma unroll 8
-      for (int n = threadIdx.x; n < H; n += kBinsThreads) {
+      for (int n = threadIdx.x; n < H; n += NT) {
         const int j = 2 * n;
         const double2 x = make_double2(j < a.B ? g(j) : 0.0, j + 1 < a.B ? g(j + 1) : 0.0);
         s[n] = rank ? cmul(x, __ldg(&a.twP[2 * n])) : x;
       }
       __syncthreads();
-      smem_fft<false>(s, tb, H, a.logH);                         // s[m] = X[2m + rank]
+      smem_fft<false, NT, MAXH>(s, tb, H, a.logH);                         // s[m] = X[2m + rank]
       // spectrum pairs (k, M-k) of this parity, in place
       const int mlast = rank ? H / 2 - 1 : H / 2;
-      for (int m = threadIdx.x; m <= mlast; m += kBinsThreads) {
+      for (int m = threadIdx.x; m <= mlast; m += NT) {
         const int k = 2 * m + rank;
         const int mp = rank ? H - 1 - m : (m == 0 ? 0 : H - m);  // X[M-k] = s[mp]
         const double2 xk = s[m], xm = s[mp];
@@ -420,7 +422,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
         s[m] = Zk;
       }
       __syncthreads();
-      smem_fft<true>(s, tb, H, a.logH);                          // unnormalised inverse
+      smem_fft<true, NT, MAXH>(s, tb, H, a.logH);                          // unnormalised inverse
       cluster.sync();
       // z[n] = (zE[n] + conj(w_M^n) zO[n]) / M, pot[2n] = Re z, pot[2n+1] = Im z
       const double2* sE = cluster.map_shared_rank(s_fft, 0);
@@ -428,7 +430,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
       const double invM = 1.0 / (double)M;
       const int n0 = rank * (H / 2), n1 = n0 + H / 2;
 #pragma unroll 4
-      for (int n = n0 + threadIdx.x; n < n1; n += kBinsThreads) {
+      for (int n = n0 + threadIdx.x; n < n1; n += NT) {
         const double2 zo = cmul(sO[n], cconj(__ldg(&a.twP[2 * n])));
         const double2 ze = sE[n];
         const int j = 2 * n;
@@ -447,7 +449,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
         }
       }
     } else {
-      for (int i = rank * kBinsThreads + threadIdx.x; i < a.B; i += 2 * kBinsThreads) a.pot[i] = 0.0;
+      for (int i = rank * NT + threadIdx.x; i < a.B; i += 2 * NT) a.pot[i] = 0.0;
     }
     cluster.sync();   // pot complete; the peer is done reading this CTA's shared memory
     // Kick table of the next pass, B + 1 cells: cell j in 1..B-1 spans centres
@@ -502,26 +504,38 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins(BinsArgs a) {
-  bins_body(a);
+  bins_body<kBinsThreads>(a);
 }
 
 // The bins step of a batch: cluster i (CTAs 2i, 2i+1) runs bunch i; slots
 // past the live count and bunches with no turns left return at once (both
 // CTAs of a cluster read the same state before either writes it, so they agree).
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1)
+template <int NT, int MAXH, int MINB>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, MINB)
     k_batch_bins(const BinsArgs* __restrict__ bunches, const int32_t* __restrict__ n_bunches) {
   const int i = (int)(blockIdx.x >> 1);
   if (i >= *n_bunches) return;
   const BinsArgs& a = bunches[i];
   if (a.ts->turns_left <= 0) return;
-  bins_body(a);
+  bins_body<NT, MAXH>(a);
 }
+
+// The batched bins step for H <= 2048 (up to 4096 bins): a radix-8 pass of a
+// length-2048 transform has 256 butterflies, so 256 threads per CTA keep every
+// pass busy, and four CTAs share an SM -- a batch of bunches runs in a quarter
+// of the waves of the 1024-thread kernel.
+constexpr int kBatchBinsSmallThreads = 256;
+constexpr int kBatchBinsSmallMaxH = 2048;
 
 }  // namespace
 
 cudaError_t prepare_wake_kernels(int max_smem) {
   cudaError_t e = allow_dynamic_smem((const void*)k_bins, max_smem);
-  if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_batch_bins, max_smem);
+  if (e == cudaSuccess)
+    e = allow_dynamic_smem((const void*)k_batch_bins<kBinsThreads, kMaxFftH, 1>, max_smem);
+  if (e == cudaSuccess)
+    e = allow_dynamic_smem(
+        (const void*)k_batch_bins<kBatchBinsSmallThreads, kBatchBinsSmallMaxH, 4>, max_smem);
   if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_wake_spectrum, max_smem);
   return e;
 }
@@ -549,8 +563,13 @@ cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st) {
 cudaError_t launch_batch_bins(const BinsArgs* d_bunches, const int32_t* d_n_bunches,
                               int max_bunches, int max_H, cudaStream_t st) {
   size_t smem = bins_smem_bytes(max_H);
-  k_batch_bins<<<2 * (max_bunches > 0 ? max_bunches : 1), kBinsThreads, smem, st>>>(
-      d_bunches, d_n_bunches);
+  const int grid = 2 * (max_bunches > 0 ? max_bunches : 1);
+  if (max_H <= kBatchBinsSmallMaxH)
+    k_batch_bins<kBatchBinsSmallThreads, kBatchBinsSmallMaxH, 4>
+        <<<grid, kBatchBinsSmallThreads, smem, st>>>(d_bunches, d_n_bunches);
+  else
+    k_batch_bins<kBinsThreads, kMaxFftH, 1><<<grid, kBinsThreads, smem, st>>>(d_bunches,
+                                                                             d_n_bunches);
   return cudaGetLastError();
 }
 

@@ -140,7 +140,8 @@ const char* hj_last_error(const hj_ctx* ctx);
 /* Thread layout of the fused particle pass for bunches created afterwards on
  * this context: -1 = chosen by the library (default), 0 = 4 particles per
  * thread x 512 threads, 1 = 2 x 1024, 2 = 2 x 768 (each with the next group
- * prefetched), 3 = 2 x 512 without prefetch.  Results do not depend on
+ * prefetched), 3 = 2 x 512 without prefetch, 4 = 2 x 512 with prefetch at
+ * two blocks per SM.  Results do not depend on
  * the layout beyond floating-point summation order.  No reference
  * counterpart. */
 hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout);

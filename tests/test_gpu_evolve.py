@@ -84,7 +84,7 @@ def test_reference_ring_reference_wake(gpu_ctx, oracle):
     run_turn_by_turn(gpu_ctx, oracle, cfg, 100_000, 30, seed=1234)
 
 
-@pytest.mark.parametrize("layout", [0, 1, 2, 3])
+@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4])
 def test_thread_layouts(oracle, layout):
     """Every thread layout of the fused pass keeps per-particle parity."""
     from haissinskijulia_b200 import Context
