@@ -16,6 +16,7 @@ from .api import (  # noqa: F401
     Particles,
     ResidentBunch,
     SimulationBuffers,
+    ShardedBunch,
     SimulationParameters,
     WakeModel,
     apply_wakefield_inplace,

@@ -119,6 +119,15 @@ SIGNATURES = {
     "hj_bunch_histogram": (c_int32, [_BUNCH, _IP]),
     "hj_bunch_potential": (c_int32, [_BUNCH, _DP]),
     "hj_bunch_destroy": (None, [_BUNCH]),
+    "hj_bunch_create_shard": (c_int32, [_CTX, c_void_p, c_void_p, c_int64, c_int64, c_int64,
+                                        POINTER(HjParams), POINTER(HjWake), POINTER(HjGrid),
+                                        c_uint64, c_void_p, POINTER(_BUNCH)]),
+    "hj_bunch_local_moments": (c_int32, [_BUNCH, _DP]),
+    "hj_bunch_set_global_moments": (c_int32, [_BUNCH, _DP]),
+    "hj_bunch_pass": (c_int32, [_BUNCH]),
+    "hj_bunch_exchange_buffers": (c_int32, [_BUNCH, POINTER(c_void_p), _IP, POINTER(c_void_p),
+                                            _IP]),
+    "hj_bunch_bins": (c_int32, [_BUNCH]),
     "hj_batch_create": (c_int32, [_CTX, c_int64, c_int32, c_int32, c_int64, c_int32,
                                   POINTER(c_void_p)]),
     "hj_batch_destroy": (None, [c_void_p]),

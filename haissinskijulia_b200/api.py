@@ -720,3 +720,138 @@ def gaussian_bunch(ctx: Context, init_seed: int, n: int, sigma_z: float, sigma_E
                                            int(n), float(sigma_z), float(sigma_E),
                                            ctypes.c_void_p(d_z), ctypes.c_void_p(d_dE),
                                            ctypes.c_void_p(stream)))
+
+
+class _DeviceArray:
+    """A device buffer (pointer, length, numpy typestr) seen by torch.as_tensor."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3}
+
+
+class ShardedBunch:
+    """One shard of a bunch split over processes (hj_bunch_create_shard).
+
+    Particles [first_particle, first_particle + n_local) of n_global live on
+    this process's GPU (device pointers d_z, d_dE); per turn: `pass_()`, a SUM
+    all-reduce of `buffers()` across ranks, `bins()` -- which `advance()` does
+    with torch.distributed on the shard's stream (NCCL).  The grid must be the
+    same on every rank.  With the Philox draws of the whole bunch, the ranks
+    together reproduce the single-GPU run (sums in another order).
+    """
+
+    def __init__(self, ctx: Context, d_z: int, d_dE: int, n_local: int, first_particle: int,
+                 n_global: int, params: SimulationParameters, grid: "BinGrid", *,
+                 wake: Optional[WakeModel] = None, seed: int = 0, stream: int = 0,
+                 group=None, exchange_initial: bool = True):
+        self.ctx = ctx
+        self.n_local, self.n_global, self.nbins = int(n_local), int(n_global), grid.nbins
+        self.group = group
+        self.stream = stream
+        self._p = params.to_c()
+        self._w = (wake or WakeModel.reference(params)).to_c()
+        self._grid = grid
+        g = grid.to_c()
+        h = ctypes.c_void_p()
+        _check(ctx, ctx._lib.hj_bunch_create_shard(
+            ctx.handle, ctypes.c_void_p(d_z), ctypes.c_void_p(d_dE), self.n_local,
+            int(first_particle), self.n_global, ctypes.byref(self._p), ctypes.byref(self._w),
+            ctypes.byref(g), int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.c_void_p(stream),
+            ctypes.byref(h)))
+        self.handle = h
+        if exchange_initial:
+            self.set_global_moments(self._all_reduce_host(self.local_moments()))
+
+    # -- per-turn steps
+    def pass_(self) -> None:
+        _check(self.ctx, self.ctx._lib.hj_bunch_pass(self.handle))
+
+    def buffers(self):
+        """(counts, sums) as torch tensors viewing the device exchange buffers."""
+        import torch
+        cp, sp = ctypes.c_void_p(), ctypes.c_void_p()
+        nc, ns = np.zeros(1, dtype=np.int64), np.zeros(1, dtype=np.int64)
+        _check(self.ctx, self.ctx._lib.hj_bunch_exchange_buffers(
+            self.handle, ctypes.byref(cp), _ip(nc), ctypes.byref(sp), _ip(ns)))
+        counts = torch.as_tensor(_DeviceArray(cp.value, nc[0], "<i8"), device="cuda")
+        sums = torch.as_tensor(_DeviceArray(sp.value, ns[0], "<f8"), device="cuda")
+        return counts, sums
+
+    def bins(self) -> None:
+        _check(self.ctx, self.ctx._lib.hj_bunch_bins(self.handle))
+
+    def advance(self, turns: int) -> None:
+        import torch.distributed as dist
+        counts, sums = self.buffers()
+        for _ in range(int(turns)):
+            self.pass_()
+            dist.all_reduce(counts, group=self.group)
+            dist.all_reduce(sums, group=self.group)
+            self.bins()
+
+    # -- moments
+    def local_moments(self) -> np.ndarray:
+        out = np.zeros(4, dtype=np.float64)
+        _check(self.ctx, self.ctx._lib.hj_bunch_local_moments(self.handle, _dp(out)))
+        return out
+
+    def set_global_moments(self, sums4) -> None:
+        s = np.ascontiguousarray(sums4, dtype=np.float64)
+        _check(self.ctx, self.ctx._lib.hj_bunch_set_global_moments(self.handle, _dp(s)))
+
+    def _all_reduce_host(self, v: np.ndarray) -> np.ndarray:
+        import torch
+        import torch.distributed as dist
+        if not (dist.is_available() and dist.is_initialized()):
+            return v
+        dev = "cuda" if dist.get_backend(self.group) == "nccl" else "cpu"
+        t = torch.from_numpy(v.copy()).to(dev)
+        dist.all_reduce(t, group=self.group)
+        return t.cpu().numpy()
+
+    def global_result(self, sums4=None) -> EvolveResult:
+        """(σ_E, σ_z, E0, ...) of the whole bunch (pending kick applied), from
+        the moments summed over the ranks (or the given sums) with the
+        reference's single-pass formula (src/utils.jl:593-605)."""
+        m = self._all_reduce_host(self.local_moments()) if sums4 is None else np.asarray(sums4)
+        r = self.observe_local()
+        n = self.n_global
+
+        def gstd(s, s2):
+            if n <= 1:
+                return 0.0
+            mean = s / n
+            var = (s2 / n) - mean * mean
+            v = var * n / (n - 1)
+            return math.sqrt(v) if v > 0 else (v if v != v else 0.0)
+        return EvolveResult(gstd(m[2], m[3]), gstd(m[0], m[1]), r.E0, r.sigma_E0_initial,
+                            r.sigma_z0_initial, m[0] / n, m[2] / n, r.turns)
+
+    def observe_local(self, d_z_out: int = 0, d_dE_out: int = 0) -> EvolveResult:
+        r = HjResult()
+        _check(self.ctx, self.ctx._lib.hj_bunch_observe(
+            self.handle, ctypes.c_void_p(d_z_out or None), ctypes.c_void_p(d_dE_out or None),
+            ctypes.byref(r)))
+        return EvolveResult.from_c(r)
+
+    def finish(self) -> None:
+        """Apply the pending kick and re-centring to the shard's particles."""
+        r = HjResult()
+        _check(self.ctx, self.ctx._lib.hj_bunch_finish(self.handle, ctypes.byref(r)))
+
+    def histogram(self) -> np.ndarray:
+        out = np.zeros(self.nbins, dtype=np.int64)
+        _check(self.ctx, self.ctx._lib.hj_bunch_histogram(self.handle, _ip(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.ctx._lib.hj_bunch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

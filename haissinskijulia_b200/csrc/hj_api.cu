@@ -51,6 +51,12 @@ struct hj_bunch {
   const double* draws = nullptr;
   int64_t draws_first = 0, draws_turns = 0;
   int nblk = 1, nblk_m = 1;
+  // a shard of a bunch split over processes: its particles are
+  // [first_particle, first_particle + n) of n_global; the bins step reads the
+  // exchanged totals (d_sums, hist) instead of this shard's partials
+  bool shard = false;
+  int64_t n_global = 0, first_particle = 0;
+  double* d_sums = nullptr;
   int64_t turns_done = 0;
   // device buffers
   TurnState* ts = nullptr;
@@ -344,7 +350,7 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   void* dev[] = {b->ts,       b->pot,      b->potd,     b->hist,    b->lam,
                  b->W,        b->Wf,       b->twP,      b->Xg,      b->zE,
                  b->part_cnt, b->part_cic, b->part_sum, b->part_mom, b->ngp_ovf,
-                 b->rf_table};
+                 b->rf_table, b->d_sums};
   for (void* p : dev)
     if (p) cudaFree(p);
   if (b->h_mom) cudaFreeHost(b->h_mom);
@@ -578,9 +584,9 @@ static void fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
 
   g = BinsArgs{};
   g.ts = b->ts;
-  g.part_sum = b->part_sum;
-  g.nblk = b->nblk;
-  g.n = b->n;
+  g.part_sum = b->shard ? b->d_sums : b->part_sum;
+  g.nblk = b->shard ? 1 : b->nblk;
+  g.n = b->shard ? b->n_global : b->n;
   g.params = b->p;
   g.sigma_E0_initial = b->sigma_E0_initial;
   g.population = b->w.population;
@@ -605,6 +611,7 @@ static void fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
   g.conv_only = 0;
 
   a.n_parts = b->nblk;
+  a.pair_offset = b->first_particle / 2;
 }
 
 extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
@@ -1519,5 +1526,112 @@ extern "C" hj_status hj_batch_stats(hj_batch* bt, int64_t* out4) {
   out4[1] = batch_largest_free(bt);
   out4[2] = (int64_t)bt->free_slots.size();
   out4[3] = bt->turns_enqueued;
+  return HJ_OK;
+}
+
+// ====================================================================== shards
+//
+// A bunch split over processes (one GPU each), the reference's MPI mode
+// (src/evolution.jl:206-212 with use_mpi): every rank tracks its particles;
+// once per turn the ranks sum the merged histograms and the pass's sums
+// (exchange buffers, B*3+2 u64 and kNumSums doubles) -- one all-reduce -- and
+// every rank runs the bins step on the totals, so all ranks keep the same
+// potential and E0.  The Philox draws of particle i of a shard are those of
+// particle first_particle + i of the whole bunch.
+
+extern "C" hj_status hj_bunch_create_shard(hj_ctx* ctx, double* d_z, double* d_dE,
+                                           int64_t n_local, int64_t first_particle,
+                                           int64_t n_global, const hj_params* params,
+                                           const hj_wake* wake, const hj_grid* grid,
+                                           uint64_t seed, void* stream, hj_bunch** out) {
+  HJ_TRY(ctx_ok(ctx));
+  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  HJ_TRY(check_params(ctx, params));
+  if (!params->use_wakefield || !grid)
+    return set_err(ctx, HJ_ERR_ARG, "a shard needs the wakefield on and the shared bin grid");
+  if (n_local <= 0 || first_particle < 0 || (first_particle & 1) ||
+      first_particle + n_local > n_global)
+    return set_err(ctx, HJ_ERR_ARG,
+                   "shard [%lld, %lld) of %lld particles: non-empty, inside, even start",
+                   (long long)first_particle, (long long)(first_particle + n_local),
+                   (long long)n_global);
+  if (!d_z || !d_dE || ((((uintptr_t)d_z) | ((uintptr_t)d_dE)) & 31))
+    return set_err(ctx, HJ_ERR_ARG, "device particle arrays must be non-NULL and 32-byte aligned");
+  hj_bunch* b = new hj_bunch();
+  hj_status s = bunch_create_impl(ctx, d_z, d_dE, n_local, params, wake, grid->nbins, grid,
+                                  seed, stream, b);
+  if (s == HJ_OK) s = dalloc(ctx, &b->d_sums, kNumSums);
+  if (s != HJ_OK) {
+    hj_bunch_destroy(b);
+    return s;
+  }
+  b->shard = true;
+  b->n_global = n_global;
+  b->first_particle = first_particle;
+  *out = b;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_local_moments(hj_bunch* b, double* out4) {
+  if (!b || !out4) return HJ_ERR_ARG;
+  HJ_TRY(ctx_ok(b->ctx));
+  HJ_TRY(launch_moments(b, 1, nullptr, nullptr));
+  return read_moments(b, out4);
+}
+
+extern "C" hj_status hj_bunch_set_global_moments(hj_bunch* b, const double* sums4) {
+  if (!b || !sums4) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (b->turns_done != 0) return set_err(ctx, HJ_ERR_STATE, "global moments are set before the first turn");
+  const int64_t n = b->shard ? b->n_global : b->n;
+  b->sigma_z0_initial = global_std(sums4[0], sums4[1], n);
+  b->sigma_E0_initial = global_std(sums4[2], sums4[3], n);
+  HJ_TRY(read_state(b));
+  b->h_ts->cur = make_turn_scalars(b->p.E0, b->p, b->sigma_E0_initial);
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
+                               b->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_pass(hj_bunch* b) {
+  if (!b) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (!b->shard) return set_err(ctx, HJ_ERR_STATE, "hj_bunch_pass is for shards (use hj_bunch_advance)");
+  PassArgs a;
+  BinsArgs g;
+  fill_turn_args(b, a, g);
+  HJ_CUDA(ctx, launch_track_pass(a, b->nblk, b->stream));
+  HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->hist, false,
+                                  b->stream, b->ngp_ovf));
+  HJ_CUDA(ctx, launch_sum_parts(b->part_sum, b->nblk, b->d_sums, b->stream));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_exchange_buffers(hj_bunch* b, uint64_t** d_counts,
+                                               int64_t* n_counts, double** d_sums,
+                                               int64_t* n_sums) {
+  if (!b || !d_counts || !n_counts || !d_sums || !n_sums) return HJ_ERR_ARG;
+  if (!b->shard) return set_err(b->ctx, HJ_ERR_STATE, "not a shard");
+  *d_counts = (uint64_t*)b->hist;
+  *n_counts = 3 * (int64_t)b->B + 2;
+  *d_sums = b->d_sums;
+  *n_sums = kNumSums;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_bins(hj_bunch* b) {
+  if (!b) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (!b->shard) return set_err(ctx, HJ_ERR_STATE, "hj_bunch_bins is for shards (use hj_bunch_advance)");
+  PassArgs a;
+  BinsArgs g;
+  fill_turn_args(b, a, g);
+  HJ_CUDA(ctx, launch_bins(g, b->stream));
+  b->turns_done += 1;
   return HJ_OK;
 }

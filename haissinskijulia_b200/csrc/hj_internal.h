@@ -61,6 +61,7 @@ struct PassArgs {
   unsigned long long* hist_out;    // [3B+2] merged histograms, zeroed by the pass
   unsigned long long* ngp_ovf;     // [B] counts beyond the 16-bit per-block counters
   int32_t n_parts;                 // partial slots written per turn (batches)
+  int64_t pair_offset;             // Philox pair index of particle 0 (shards of a bunch)
 };
 
 // One entry of a batch's chunk table: particles [first, first + count) of
@@ -132,6 +133,7 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
 cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
                               const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
                               int qe, int cfg, cudaStream_t st);
+cudaError_t launch_sum_parts(const double* part, int nblk, double* out, cudaStream_t st);
 cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const int32_t* d_n_bunches,
                                 int max_bunches, int max_B, cudaStream_t st);
 // out: counts[B] (| cell counts[B+1] | cell Σw·2^24 [B+1] when part_cic != NULL);

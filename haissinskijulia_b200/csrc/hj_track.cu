@@ -342,12 +342,13 @@ __device__ __forceinline__ void stp(double* p, const double v[PPT]) {
   }
 }
 
-// Normals of particles PPT*g .. PPT*g+PPT-1 (one Philox-2x32 counter per pair).
+// Normals of the PPT particles of pairs pair0, pair0 + 1, ... (one Philox-2x32
+// counter per pair of particles).
 template <int PPT>
-__device__ __forceinline__ void group_normals(const uint32_t (&rk)[10], int64_t turn, int64_t g,
-                                              double r[PPT]) {
-  philox_normals2_rk(rk, turn, (PPT / 2) * g, r);
-  if (PPT == 4) philox_normals2_rk(rk, turn, 2 * g + 1, r + 2);
+__device__ __forceinline__ void group_normals(const uint32_t (&rk)[10], int64_t turn,
+                                              int64_t pair0, double r[PPT]) {
+  philox_normals2_rk(rk, turn, pair0, r);
+  if (PPT == 4) philox_normals2_rk(rk, turn, pair0 + 1, r + 2);
 }
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
@@ -452,7 +453,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
     if (QE == QE_PHILOX) {
-      group_normals<PPT>(a.philox_rk, turn, q, rr);
+      group_normals<PPT>(a.philox_rk, turn, (PPT / 2) * q + a.pair_offset, rr);
     } else if (QE == QE_DRAWS) {
       if (drow) {
 #pragma unroll
@@ -474,7 +475,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
   if (rg.tail && threadIdx.x < (int)(a.n % PPT)) {
     const int64_t i = (a.n / PPT) * PPT + threadIdx.x;
     double r2[2] = {0.0, 0.0};
-    if (QE == QE_PHILOX) philox_normals2_rk(a.philox_rk, turn, i >> 1, r2);
+    if (QE == QE_PHILOX) philox_normals2_rk(a.philox_rk, turn, (i >> 1) + a.pair_offset, r2);
     double r = r2[i & 1];
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
     double z = a.z[i], e = a.dE[i];
@@ -873,6 +874,20 @@ cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chu
                   const_cast<int32_t**>(&d_n_chunks)};
   return cudaLaunchKernel(batch_fn(wake, qe, cfg), dim3(max_chunks > 0 ? max_chunks : 1),
                           dim3(pass_cfg_threads(cfg)), args, smem, st);
+}
+
+// Fixed-order sum of nblk per-block sum vectors into out[kNumSums] (one block).
+__global__ void k_sum_parts(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+  if (threadIdx.x < kNumSums) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += part[(size_t)b * kNumSums + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+cudaError_t launch_sum_parts(const double* part, int nblk, double* out, cudaStream_t st) {
+  k_sum_parts<<<1, 32, 0, st>>>(part, nblk, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const int32_t* d_n_bunches,

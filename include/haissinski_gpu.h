@@ -246,6 +246,37 @@ hj_status hj_bunch_histogram(hj_bunch* b, int64_t* counts_host);
 hj_status hj_bunch_potential(hj_bunch* b, double* pot_host);
 void hj_bunch_destroy(hj_bunch* b);
 
+/* ---------------------------------------------------------------- shards
+ * One bunch split over processes, one GPU each -- the reference's MPI mode
+ * (longitudinal_evolve! with use_mpi, src/evolution.jl:206-212; the exchange
+ * sites of src/wakefield.jl:186-345 and src/evolution.jl:408-426).  Per turn:
+ * hj_bunch_pass on every rank, a SUM all-reduce across ranks of the two
+ * exchange buffers (u64 counts, double sums) on the shard's stream, then
+ * hj_bunch_bins on every rank.  No reference counterpart for the split calls. */
+
+/* Particles [first_particle, first_particle + n_local) of a bunch of n_global
+ * (first_particle even; the Philox draws are the whole bunch's).  The grid
+ * must be the same on every rank.  Before the first turn, sum
+ * hj_bunch_local_moments over the ranks and pass the totals to
+ * hj_bunch_set_global_moments. */
+hj_status hj_bunch_create_shard(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n_local,
+                                int64_t first_particle, int64_t n_global,
+                                const hj_params* params, const hj_wake* wake,
+                                const hj_grid* grid, uint64_t seed, void* stream,
+                                hj_bunch** out);
+/* out = (Σz, Σz², ΣdE, ΣdE²) of this bunch's particles (pending kick applied,
+ * state unchanged).  Synchronises the stream. */
+hj_status hj_bunch_local_moments(hj_bunch* b, double* out4);
+/* Initial spreads σ_z0, σ_E0 from the moments summed over all shards. */
+hj_status hj_bunch_set_global_moments(hj_bunch* b, const double* sums4);
+/* This turn's particle pass on the shard; fills the exchange buffers. */
+hj_status hj_bunch_pass(hj_bunch* b);
+/* Device buffers to SUM across ranks between hj_bunch_pass and hj_bunch_bins. */
+hj_status hj_bunch_exchange_buffers(hj_bunch* b, uint64_t** d_counts, int64_t* n_counts,
+                                    double** d_sums, int64_t* n_sums);
+/* This turn's bins step from the exchanged totals. */
+hj_status hj_bunch_bins(hj_bunch* b);
+
 /* ---------------------------------------------------------------- batches
  * Many independent bunches -- each with its own particle count, RF voltage,
  * intensity, bins, seed and number of turns -- advanced together: every turn

@@ -129,6 +129,14 @@ class Oracle:
         self.lib.or_gaussian(int(seed) & 0xFFFFFFFFFFFFFFFF, int(turn), n, _dp(out))
         return out
 
+    def wake_current(self, n_global, E0, mass, alpha_c, radius, sigma_z, sigma_E0_initial,
+                     population) -> float:
+        return self.lib.or_wake_current(int(n_global), E0, mass, alpha_c, radius, sigma_z,
+                                        sigma_E0_initial, population)
+
+    def rf_factor(self, freq_rf, beta) -> float:
+        return self.lib.or_calc_rf_factor(freq_rf, beta)
+
     def global_std(self, x) -> float:
         x = np.ascontiguousarray(x, dtype=np.float64)
         return self.lib.or_compute_global_std(_dp(x), x.shape[0])
