@@ -68,7 +68,8 @@ def workload(n: int, B: int) -> dict:
     return {
         "workload": f"plain single bunch at scale: {n:.0e} Float64 macroparticles, {B} bins, "
                     "4 GeV benchmark ring, resonator wake (Rs=10kOhm, Q=1, fr=20GHz, 1e10 e-), "
-                    "RF+QE(Philox)+SR+drift+wake+E0 update every turn",
+                    "RF+QE(Philox)+SR+drift+wake+E0 update every turn; moments and line density "
+                    "logged on the device every 100 turns",
         "particles": n,
         "nbins": B,
         "turns_per_step": 1,
@@ -310,6 +311,8 @@ def run_ours(args) -> None:
     dE = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_E
     bunch = ResidentBunch(ctx, z.data_ptr(), dE.data_ptr(), n, cfg.params, B, wake=cfg.wake,
                           seed=args.seed + rank, stream=stream.cuda_stream)
+    # moments and line density logged on the device every 100 turns
+    bunch.set_log(100, capacity=(K + W) // 100 + 1, density=True)
 
     def barrier():
         torch.cuda.synchronize()
@@ -331,6 +334,7 @@ def run_ours(args) -> None:
     clock_info = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     prof = bunch.read_profile()
+    log = bunch.read_log()
     res = bunch.finish()
     bunch.close()
     if world > 1:
@@ -407,6 +411,12 @@ def run_ours(args) -> None:
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "sweep": sweep,
             "gpu_launches": prof["launches"], "clocks": clock_info,
             "wall_seconds_timed": t_wall,
+            "turn_log": {"every": 100, "records": int(log.shape[0]),
+                         "content": "turn, E0, sigma_z, sigma_E, mean z, mean dE, wake current, "
+                                    f"particles in bins + {B} bin counts, written on the device",
+                         "last": {"turn": float(log[-1, 0]), "E0": float(log[-1, 1]),
+                                  "sigma_z": float(log[-1, 2]), "sigma_E": float(log[-1, 3])}
+                         if log.shape[0] else None},
             "final": {"sigma_E": res.sigma_E, "sigma_z": res.sigma_z, "E0": res.E0},
         }
         print(json.dumps(line), flush=True)

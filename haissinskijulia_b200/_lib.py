@@ -118,6 +118,8 @@ SIGNATURES = {
     "hj_bunch_read_profile": (c_int32, [_BUNCH, _DP]),
     "hj_bunch_histogram": (c_int32, [_BUNCH, _IP]),
     "hj_bunch_potential": (c_int32, [_BUNCH, _DP]),
+    "hj_bunch_set_log": (c_int32, [_BUNCH, c_int64, c_int64, c_int32]),
+    "hj_bunch_read_log": (c_int32, [_BUNCH, _DP, c_int64, _IP]),
     "hj_bunch_destroy": (None, [_BUNCH]),
     "hj_bunch_create_shard": (c_int32, [_CTX, c_void_p, c_void_p, c_int64, c_int64, c_int64,
                                         POINTER(HjParams), POINTER(HjWake), POINTER(HjGrid),

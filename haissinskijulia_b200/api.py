@@ -571,6 +571,22 @@ class ResidentBunch:
         return {"pass_ms": float(out[0]), "bins_ms": float(out[1]), "turns": int(out[2]),
                 "launches": int(out[3])}
 
+    def set_log(self, every: int, capacity: int = 1024, density: bool = False) -> None:
+        """Record [turn, E0, σ_z, σ_E, mean z, mean ΔE, current, n_in] (+ the bin
+        counts with density) every `every` turns on the device."""
+        self._log_density = bool(density)
+        _check(self.ctx, self.ctx._lib.hj_bunch_set_log(self.handle, int(every), int(capacity),
+                                                        int(bool(density))))
+
+    def read_log(self, max_records: int = 1 << 20) -> np.ndarray:
+        """The logged records, oldest first: rows of 8 (+ nbins) values."""
+        width = 8 + (self.nbins if getattr(self, "_log_density", False) else 0)
+        out = np.zeros((max_records, width), dtype=np.float64)
+        n = np.zeros(1, dtype=np.int64)
+        _check(self.ctx, self.ctx._lib.hj_bunch_read_log(self.handle, _dp(out), int(max_records),
+                                                         _ip(n)))
+        return out[: int(n[0])]
+
     def histogram(self) -> np.ndarray:
         out = np.zeros(self.nbins, dtype=np.int64)
         _check(self.ctx, self.ctx._lib.hj_bunch_histogram(self.handle, _ip(out)))

@@ -57,6 +57,10 @@ struct hj_bunch {
   bool shard = false;
   int64_t n_global = 0, first_particle = 0;
   double* d_sums = nullptr;
+  // turn log: a record every log_every turns into a ring of log_capacity
+  int64_t log_every = 0, log_capacity = 0, log_count = 0;
+  int log_density = 0;
+  double* d_log = nullptr;
   int64_t turns_done = 0;
   // device buffers
   TurnState* ts = nullptr;
@@ -350,7 +354,7 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   void* dev[] = {b->ts,       b->pot,      b->potd,     b->hist,    b->lam,
                  b->W,        b->Wf,       b->twP,      b->Xg,      b->zE,
                  b->part_cnt, b->part_cic, b->part_sum, b->part_mom, b->ngp_ovf,
-                 b->rf_table, b->d_sums};
+                 b->rf_table, b->d_sums, b->d_log};
   for (void* p : dev)
     if (p) cudaFree(p);
   if (b->h_mom) cudaFreeHost(b->h_mom);
@@ -645,6 +649,16 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
       HJ_CUDA(ctx, cudaEventRecord(ev[2], b->stream));
       b->profiled_turns += 1;
       b->profiled_launches += b->use_wake ? 3 : 2;
+    }
+    if (b->log_every > 0 && (b->turns_done + t + 1) % b->log_every == 0) {
+      const int64_t rec = kLogHeader + (b->log_density ? b->B : 0);
+      HJ_TRY(launch_moments(b, 1, nullptr, nullptr));
+      HJ_CUDA(ctx, launch_log_record(b->part_mom, b->nblk_m, b->n, b->ts,
+                                     b->log_density ? b->hist : nullptr, b->B,
+                                     b->d_log + (b->log_count % b->log_capacity) * rec,
+                                     b->stream));
+      b->log_count += 1;
+      if (b->profiling) b->profiled_launches += 2;
     }
   }
   b->turns_done += turns;
@@ -1633,5 +1647,48 @@ extern "C" hj_status hj_bunch_bins(hj_bunch* b) {
   fill_turn_args(b, a, g);
   HJ_CUDA(ctx, launch_bins(g, b->stream));
   b->turns_done += 1;
+  return HJ_OK;
+}
+
+// ====================================================================== turn log
+
+extern "C" hj_status hj_bunch_set_log(hj_bunch* b, int64_t every, int64_t capacity,
+                                      int32_t density) {
+  if (!b) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (every < 0 || (every > 0 && capacity <= 0))
+    return set_err(ctx, HJ_ERR_ARG, "log every >= 0 turns into capacity > 0 records");
+  if (density && !b->use_wake) return set_err(ctx, HJ_ERR_STATE, "no line density without the wakefield");
+  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
+  if (b->d_log) cudaFree(b->d_log);
+  b->d_log = nullptr;
+  b->log_every = every;
+  b->log_capacity = capacity;
+  b->log_density = density ? 1 : 0;
+  b->log_count = 0;
+  if (every > 0)
+    HJ_TRY(dalloc(ctx, &b->d_log, (size_t)capacity * (kLogHeader + (b->log_density ? b->B : 0))));
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_read_log(hj_bunch* b, double* out, int64_t max_records,
+                                       int64_t* n_records) {
+  if (!b || !n_records || (max_records > 0 && !out)) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  *n_records = 0;
+  if (!b->d_log) return HJ_OK;
+  const int64_t rec = kLogHeader + (b->log_density ? b->B : 0);
+  const int64_t held = std::min(b->log_count, b->log_capacity);
+  const int64_t n = std::min(held, max_records);
+  // the n most recent records, oldest first
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t idx = (b->log_count - n + k) % b->log_capacity;
+    HJ_CUDA(ctx, cudaMemcpyAsync(out + k * rec, b->d_log + idx * rec, sizeof(double) * rec,
+                                 cudaMemcpyDeviceToHost, b->stream));
+  }
+  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
+  *n_records = n;
   return HJ_OK;
 }

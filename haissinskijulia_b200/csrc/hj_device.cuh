@@ -84,6 +84,17 @@ __host__ __device__ inline TurnScalars make_turn_scalars(double E0, const hj_par
   return s;
 }
 
+// compute_global_std from single-pass sums (src/utils.jl:593-605).
+__host__ __device__ inline double global_std_of_sums(double s, double s2, int64_t n) {
+  if (n <= 1) return 0.0;
+  const double nd = (double)n;
+  const double mean = s / nd;
+  const double var = (s2 / nd) - (mean * mean);
+  double v = var * nd / (double)(n - 1);
+  if (!(v > 0.0)) v = (v != v) ? v : 0.0;
+  return sqrt(v);
+}
+
 // ------------------------------------------------------------------ Philox
 
 // Philox-2x32 with 10 rounds: multiplier 0xD256D193, Weyl key increment

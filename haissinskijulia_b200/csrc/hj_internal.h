@@ -23,6 +23,7 @@ constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 // blocks per SM where shared memory allows).
 constexpr int kNumPassCfgs = 5;
 constexpr int kRfTableSize = 128;    // entries of the fused pass's RF kick table
+constexpr int kLogHeader = 8;       // doubles before the bin counts in a turn-log record
 int pass_cfg_threads(int cfg);
 int pass_cfg_ppt(int cfg);
 
@@ -142,6 +143,9 @@ cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long lon
                                int nblk, int B, unsigned long long* out, bool zero_first,
                                cudaStream_t st, unsigned long long* ovf = nullptr);
 cudaError_t launch_flush(const FlushArgs& a, int grid, cudaStream_t st);
+cudaError_t launch_log_record(const double* part, int nblk, int64_t n, const TurnState* ts,
+                              const unsigned long long* counts, int B, double* rec,
+                              cudaStream_t st);
 cudaError_t launch_histogram_only(const double* z, int64_t n, int B, double e0, double eN,
                                   double inv_estep, uint32_t* part_cnt, int grid,
                                   cudaStream_t st);

@@ -641,6 +641,32 @@ __global__ void __launch_bounds__(kTrackThreads) k_flush(FlushArgs a) {
   block_sum4<kTrackThreads>(s0, s1, s2, s3, a.part + (size_t)blockIdx.x * 4, red);
 }
 
+// One record of a bunch's turn log: [turn, E0, σ_z, σ_E, mean z, mean ΔE, wake
+// current, particles in the bins] of the state after the last completed turn
+// (moments from k_flush with the pending kick applied), then the B bin
+// counts of that turn when `counts` is given.
+__global__ void k_log_record(const double* __restrict__ part, int nblk, int64_t n,
+                             const TurnState* __restrict__ ts,
+                             const unsigned long long* __restrict__ counts, int B,
+                             double* __restrict__ rec) {
+  if (threadIdx.x == 0) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < nblk; ++b)
+      for (int k = 0; k < 4; ++k) s[k] += part[(size_t)b * 4 + k];
+    const double nd = n > 0 ? (double)n : 1.0;
+    rec[0] = (double)(ts->turn - 1);
+    rec[1] = ts->cur.E0;
+    rec[2] = global_std_of_sums(s[0], s[1], n);
+    rec[3] = global_std_of_sums(s[2], s[3], n);
+    rec[4] = s[0] / nd;
+    rec[5] = s[2] / nd;
+    rec[6] = ts->last_current;
+    rec[7] = ts->last_n_in;
+  }
+  if (counts)
+    for (int i = threadIdx.x; i < B; i += blockDim.x) rec[kLogHeader + i] = (double)counts[i];
+}
+
 // NGP histogram only (hj_histogram, hj_apply_wakefield).
 __global__ void __launch_bounds__(kTrackThreads) k_histogram(const double* __restrict__ z,
                                                             int64_t n, GridConst g,
@@ -908,6 +934,13 @@ cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long lon
   const int G = nblk < 16 ? nblk : 16;
   dim3 grid((B + 1 + 255) / 256, G > 0 ? G : 1);
   k_hist_reduce<<<grid, 256, 0, st>>>(part_cnt, part_cic, nblk, B, out, ovf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_log_record(const double* part, int nblk, int64_t n, const TurnState* ts,
+                              const unsigned long long* counts, int B, double* rec,
+                              cudaStream_t st) {
+  k_log_record<<<1, 256, 0, st>>>(part, nblk, n, ts, counts, B, rec);
   return cudaGetLastError();
 }
 

@@ -240,6 +240,17 @@ hj_status hj_bunch_set_profiling(hj_bunch* b, int32_t enable);
  * out[2] = turns profiled, out[3] = kernel launches profiled.
  * Synchronises the bunch's stream. */
 hj_status hj_bunch_read_profile(hj_bunch* b, double* out4);
+/* Turn log: every `every` turns of hj_bunch_advance, one record of the state
+ * after that turn -- [turn, E0, σ_z, σ_E, mean z, mean ΔE, wake current,
+ * particles in the bins], then the nbins line-density counts when density != 0
+ * -- written on the device into a ring of `capacity` records (no host round
+ * trip; costs one moments pass over the particles per record).  every = 0
+ * stops.  The reference keeps per-turn observables in BeamTurn
+ * (src/data_structures.jl:52-54, src/utils.jl:42-50). */
+hj_status hj_bunch_set_log(hj_bunch* b, int64_t every, int64_t capacity, int32_t density);
+/* Copies the most recent min(held, max_records) records, oldest first, into
+ * out (8 [+ nbins] doubles each); *n_records = how many. */
+hj_status hj_bunch_read_log(hj_bunch* b, double* out, int64_t max_records, int64_t* n_records);
 /* Line density of the last completed turn: integer bin counts (nbins). */
 hj_status hj_bunch_histogram(hj_bunch* b, int64_t* counts_host);
 /* Potential at the bin centers from the last completed turn (nbins). */
