@@ -24,6 +24,8 @@ from .api import (  # noqa: F401
     calculate_local_histogram,
     create_simulation_buffers,
     gaussian_bunch,
+    generate_particles,
+    generate_particles_device,
     gaussian_draws,
     longitudinal_evolve,
     next_power_of_two,

@@ -159,6 +159,8 @@ SIGNATURES = {
     "hj_apply_wakefield": (c_int32, [_CTX, _DP, _DP, c_int64, POINTER(HjWake), c_double,
                                      c_double, POINTER(HjGrid)]),
     "hj_gaussian": (c_int32, [_CTX, c_uint64, c_int64, c_int64, _DP]),
+    "hj_generate_particles": (c_int32, [_CTX, c_double, c_double, c_double, c_double, c_int64,
+                                        c_uint64, c_void_p, c_void_p, c_void_p, _DP, _DP]),
 }
 
 _lib = None

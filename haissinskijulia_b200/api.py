@@ -871,3 +871,36 @@ class ShardedBunch:
             self.close()
         except Exception:
             pass
+
+
+def generate_particles_device(ctx: Context, mu_z: float, mu_E: float, sigma_z: float,
+                              sigma_E: float, n: int, d_z: int, d_dE: int, *, seed: int = 0,
+                              stream: int = 0):
+    """generate_particles (src/evolution.jl:42-133) into device arrays (ints:
+    pointers); returns (actual σ_E, actual σ_z)."""
+    sE = np.zeros(1)
+    sz = np.zeros(1)
+    _check(ctx, ctx._lib.hj_generate_particles(ctx.handle, float(mu_z), float(mu_E),
+                                               float(sigma_z), float(sigma_E), int(n),
+                                               int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                               ctypes.c_void_p(d_z), ctypes.c_void_p(d_dE),
+                                               ctypes.c_void_p(stream), _dp(sE), _dp(sz)))
+    return float(sE[0]), float(sz[0])
+
+
+def generate_particles(mu_z: float, mu_E: float, sigma_z: float, sigma_E: float,
+                       num_particles: int, energy: float, mass: float = MASS_ELECTRON,
+                       phi_s: float = 0.0, freq_rf: float = 0.0, *,
+                       ctx: Optional[Context] = None, seed: int = 0):
+    """The reference's generate_particles(μ_z, μ_E, σ_z, σ_E, num_particles,
+    energy, mass, ϕs, freq_rf) -> (particles, actual σ_E, actual σ_z, energy),
+    drawn on the GPU (mass, ϕs and freq_rf are accepted for signature parity
+    and, as in the reference, unused)."""
+    import torch
+    ctx = ctx or Context(0)
+    n = max(int(num_particles), 0)
+    dz = torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
+    de = torch.empty_like(dz)
+    sE, sz = generate_particles_device(ctx, mu_z, mu_E, sigma_z, sigma_E, n, dz.data_ptr(),
+                                       de.data_ptr(), seed=seed)
+    return Particles(dz[:n].cpu().numpy(), de[:n].cpu().numpy()), sE, sz, energy

@@ -1692,3 +1692,87 @@ extern "C" hj_status hj_bunch_read_log(hj_bunch* b, double* out, int64_t max_rec
   *n_records = n;
   return HJ_OK;
 }
+
+// ====================================================================== generate_particles
+
+namespace {
+// compute_std (src/utils.jl:531-544) of a device array: two passes, per-block
+// sums added on the host in block order.
+hj_status device_compute_std(hj_ctx* ctx, const double* x, int64_t n, double* part, int grid,
+                             cudaStream_t st, double* out) {
+  std::vector<double> h(grid);
+  HJ_CUDA(ctx, launch_std_parts(x, n, 0.0, 0, part, grid, st));
+  HJ_CUDA(ctx, cudaMemcpyAsync(h.data(), part, sizeof(double) * grid, cudaMemcpyDeviceToHost, st));
+  HJ_CUDA(ctx, cudaStreamSynchronize(st));
+  double s = 0.0;
+  for (double v : h) s += v;
+  const double mu = s / (double)n;
+  HJ_CUDA(ctx, launch_std_parts(x, n, mu, 1, part, grid, st));
+  HJ_CUDA(ctx, cudaMemcpyAsync(h.data(), part, sizeof(double) * grid, cudaMemcpyDeviceToHost, st));
+  HJ_CUDA(ctx, cudaStreamSynchronize(st));
+  double s2 = 0.0;
+  for (double v : h) s2 += v;
+  const double var = s2 / (double)(n - 1);
+  *out = std::sqrt(std::max(0.0, var));
+  return HJ_OK;
+}
+}  // namespace
+
+extern "C" hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E, double sigma_z,
+                                           double sigma_E, int64_t n, uint64_t seed,
+                                           double* d_z, double* d_dE, void* stream,
+                                           double* actual_sigma_E, double* actual_sigma_z) {
+  HJ_TRY(ctx_ok(ctx));
+  if (!actual_sigma_E || !actual_sigma_z) return set_err(ctx, HJ_ERR_ARG, "output spreads are NULL");
+  if (!(sigma_z >= 0.0 && sigma_E >= 0.0)) return set_err(ctx, HJ_ERR_ARG, "spreads must be non-negative");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n <= 0) {                                   // src/evolution.jl:47-53
+    *actual_sigma_E = 0.0;
+    *actual_sigma_z = 0.0;
+    return HJ_OK;
+  }
+  if (!d_z || !d_dE) return set_err(ctx, HJ_ERR_ARG, "particle arrays are NULL");
+  *actual_sigma_E = sigma_E;
+  *actual_sigma_z = sigma_z;
+  if (n < 2) {                                    // :62-67, independent draws, input spreads
+    HJ_CUDA(ctx, launch_gaussian_bunch(seed, n, mu_z, sigma_z, mu_E, sigma_E, d_z, d_dE, st));
+    HJ_CUDA(ctx, cudaStreamSynchronize(st));
+    return HJ_OK;
+  }
+  const int grid = (int)std::min<int64_t>((n + 1023) / 1024, 4 * (int64_t)ctx->num_sms);
+  double* dev = nullptr;
+  HJ_TRY(dalloc(ctx, &dev, (size_t)grid + 3));
+  hj_status s = HJ_OK;
+  do {
+    // covariance of a sample of min(n, 10000) independent draws (:69-81)
+    const int64_t S = std::min<int64_t>(n, 10000);
+    double c[3];
+    cudaError_t e = launch_gen_sample_cov(seed, S, mu_z, sigma_z, mu_E, sigma_E, dev + grid, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c, dev + grid, sizeof(c), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      s = set_err(ctx, HJ_ERR_CUDA, "covariance sample failed: %s", cudaGetErrorString(e));
+      break;
+    }
+    double a = std::max(1e-18, c[0]), b = c[2], d = std::max(1e-18, c[1]);
+    // positive semi-definite guard (:88-93): eigmin of [[a, b], [b, d]]
+    const double min_eig = 0.5 * (a + d) - std::sqrt(0.25 * (a - d) * (a - d) + b * b);
+    if (min_eig < 1e-12) {
+      const double add = std::max(0.0, 1e-12 - min_eig);
+      a += add;
+      d += add;
+    }
+    // MvNormal draw (:95-116): mu + L eps, L the lower Cholesky factor of the covariance
+    const double l00 = std::sqrt(a), l10 = b / l00, l11 = std::sqrt(std::max(0.0, d - l10 * l10));
+    e = launch_gen_correlated(seed, n, mu_z, mu_E, l00, l10, l11, d_z, d_dE, st);
+    if (e != cudaSuccess) {
+      s = set_err(ctx, HJ_ERR_CUDA, "bunch draw failed: %s", cudaGetErrorString(e));
+      break;
+    }
+    // actual spreads, compute_std (:119-121)
+    s = device_compute_std(ctx, d_z, n, dev, grid, st, actual_sigma_z);
+    if (s == HJ_OK) s = device_compute_std(ctx, d_dE, n, dev, grid, st, actual_sigma_E);
+  } while (false);
+  cudaFree(dev);
+  return s;
+}

@@ -143,6 +143,13 @@ cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long lon
                                int nblk, int B, unsigned long long* out, bool zero_first,
                                cudaStream_t st, unsigned long long* ovf = nullptr);
 cudaError_t launch_flush(const FlushArgs& a, int grid, cudaStream_t st);
+// generate_particles on the device (covariance sample, correlated bunch, two-pass std)
+cudaError_t launch_gen_sample_cov(uint64_t seed, int64_t S, double mu_z, double sz, double mu_E,
+                                  double sE, double* out, cudaStream_t st);
+cudaError_t launch_gen_correlated(uint64_t seed, int64_t n, double mu_z, double mu_E, double l00,
+                                  double l10, double l11, double* z, double* dE, cudaStream_t st);
+cudaError_t launch_std_parts(const double* x, int64_t n, double mean, int second, double* part,
+                             int grid, cudaStream_t st);
 cudaError_t launch_log_record(const double* part, int nblk, int64_t n, const TurnState* ts,
                               const unsigned long long* counts, int B, double* rec,
                               cudaStream_t st);

@@ -776,6 +776,86 @@ __global__ void k_gaussian_bunch(uint64_t seed, int64_t n, double mu_z, double s
   }
 }
 
+// ---- generate_particles (src/evolution.jl:42-133) on the device
+constexpr uint64_t kSampleTag = 0xBB67AE8584CAA73Bull;   // covariance-estimate sample
+constexpr uint64_t kCorrTag = 0x3C6EF372FE94F82Bull;     // the bunch itself
+
+__device__ __forceinline__ double block_sum_1024(double v, double* red) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+  return s;
+}
+
+// Sample covariance (two-pass, divisor S - 1) of S independent draws
+// z ~ N(mu_z, sz), E ~ N(mu_E, sE): out = (cov zz, cov EE, cov zE).  One block.
+__global__ void k_gen_sample_cov(uint64_t seed, int64_t S, double mu_z, double sz, double mu_E,
+                                 double sE, double* __restrict__ out) {
+  __shared__ double red[32];
+  double a = 0.0, b = 0.0;
+  for (int64_t i = threadIdx.x; i < S; i += blockDim.x) {
+    double r[2];
+    philox_normals2(seed ^ kSampleTag, 0, i, r);
+    a += fma(sz, r[0], mu_z);
+    b += fma(sE, r[1], mu_E);
+  }
+  const double mz = block_sum_1024(a, red) / (double)S;
+  const double mE = block_sum_1024(b, red) / (double)S;
+  double czz = 0.0, cEE = 0.0, czE = 0.0;
+  for (int64_t i = threadIdx.x; i < S; i += blockDim.x) {
+    double r[2];
+    philox_normals2(seed ^ kSampleTag, 0, i, r);
+    const double dz = fma(sz, r[0], mu_z) - mz, dEv = fma(sE, r[1], mu_E) - mE;
+    czz = fma(dz, dz, czz);
+    cEE = fma(dEv, dEv, cEE);
+    czE = fma(dz, dEv, czE);
+  }
+  czz = block_sum_1024(czz, red);
+  cEE = block_sum_1024(cEE, red);
+  czE = block_sum_1024(czE, red);
+  if (threadIdx.x == 0) {
+    out[0] = czz / (double)(S - 1);
+    out[1] = cEE / (double)(S - 1);
+    out[2] = czE / (double)(S - 1);
+  }
+}
+
+// (z, E) = mu + L eps with L = [[l00, 0], [l10, l11]] (the bunch's MvNormal draw).
+__global__ void k_gen_correlated(uint64_t seed, int64_t n, double mu_z, double mu_E, double l00,
+                                 double l10, double l11, double* __restrict__ z,
+                                 double* __restrict__ dE) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double r[2];
+    philox_normals2(seed ^ kCorrTag, 0, i, r);
+    z[i] = fma(l00, r[0], mu_z);
+    dE[i] = fma(l11, r[1], fma(l10, r[0], mu_E));
+  }
+}
+
+// Per-block sums for compute_std (src/utils.jl:531-544): of x (first pass,
+// mean = NaN) or of (x - mean)^2 (second pass).
+__global__ void k_std_parts(const double* __restrict__ x, int64_t n, double mean, int second,
+                            double* __restrict__ part) {
+  __shared__ double red[32];
+  double s = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double v = x[i];
+    if (second) {
+      const double d = v - mean;
+      s = fma(d, d, s);
+    } else {
+      s += v;
+    }
+  }
+  s = block_sum_1024(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
 int elementwise_grid(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g < 1) g = 1;
@@ -941,6 +1021,26 @@ cudaError_t launch_log_record(const double* part, int nblk, int64_t n, const Tur
                               const unsigned long long* counts, int B, double* rec,
                               cudaStream_t st) {
   k_log_record<<<1, 256, 0, st>>>(part, nblk, n, ts, counts, B, rec);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gen_sample_cov(uint64_t seed, int64_t S, double mu_z, double sz, double mu_E,
+                                  double sE, double* out, cudaStream_t st) {
+  k_gen_sample_cov<<<1, 1024, 0, st>>>(seed, S, mu_z, sz, mu_E, sE, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gen_correlated(uint64_t seed, int64_t n, double mu_z, double mu_E, double l00,
+                                  double l10, double l11, double* z, double* dE,
+                                  cudaStream_t st) {
+  k_gen_correlated<<<elementwise_grid(n), 256, 0, st>>>(seed, n, mu_z, mu_E, l00, l10, l11, z,
+                                                        dE);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_std_parts(const double* x, int64_t n, double mean, int second, double* part,
+                             int grid, cudaStream_t st) {
+  k_std_parts<<<grid, 1024, 0, st>>>(x, n, mean, second, part);
   return cudaGetLastError();
 }
 

@@ -409,6 +409,19 @@ hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE, int64_t n
 hj_status hj_gaussian_bunch(hj_ctx* ctx, uint64_t init_seed, int64_t n, double sigma_z,
                             double sigma_E, double* d_z, double* d_dE, void* stream);
 
+/* generate_particles(μ_z, μ_E, σ_z, σ_E, num_particles, ...)
+ * (src/evolution.jl:42-133) on the device: the covariance of a sample of
+ * min(n, 10000) independent Gaussians, its positive-definite guard, then n
+ * correlated draws mu + L eps (L its Cholesky factor) into d_z, d_dE, and the
+ * actual spreads by the two-pass compute_std (src/utils.jl:531-544).  Draws
+ * are Philox-2x32-10 / Box-Muller under `seed` (the reference's come from
+ * Julia's default RNG).  n <= 0: spreads 0; n = 1: one independent draw and
+ * the input spreads, as the reference returns them. */
+hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E, double sigma_z,
+                                double sigma_E, int64_t n, uint64_t seed, double* d_z,
+                                double* d_dE, void* stream, double* actual_sigma_E,
+                                double* actual_sigma_z);
+
 /* The Philox-2x32-10 standard normals used for quantum excitation:
  * out[i] = N(0,1) draw of particle i at `turn` under `seed`.  No reference
  * counterpart (the reference calls randn!, src/quantum_excitation.jl:36). */
