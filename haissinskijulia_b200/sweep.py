@@ -283,3 +283,36 @@ def serve(ctx: Context, requests: List[Point], *, memory_budget: int = 8 << 30,
         bt.close()
     rep.solves = [done[i] for i in sorted(done)]
     return rep
+
+
+def time_batch_turns(ctx: Context, points: List[Point], turns: int, tuning: Tuning) -> float:
+    """Seconds per turn of all `points` live in one Batch (after a warm-up of
+    one graph block); the points are given enough turns not to finish."""
+    bt = Batch(ctx, sum(p.n + 4 for p in points), len(points), max(p.nbins for p in points),
+               chunk=tuning.chunk, layout=tuning.layout, graph_turns=tuning.graph_turns)
+    try:
+        for p in points:
+            cfg = p.ring()
+            bt.add_gaussian(p.n, cfg.sigma_z, cfg.sigma_E, p.seed, cfg.params, p.nbins,
+                            wake=cfg.wake, seed=p.seed, turns=10 * turns + 10 * tuning.graph_turns)
+        bt.advance(max(tuning.graph_turns, 1))
+        bt.poll()
+        t0 = time.perf_counter()
+        bt.advance(turns)
+        bt.poll()
+        return (time.perf_counter() - t0) / turns
+    finally:
+        bt.close()
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="Time batched turns of the 256-point sweep")
+    ap.add_argument("--turns", type=int, default=64)
+    ap.add_argument("--chunk", type=int, default=65536)
+    ap.add_argument("--layout", type=int, default=1)
+    ap.add_argument("--graph-turns", type=int, default=8)
+    args = ap.parse_args()
+    s = time_batch_turns(Context(0), sweep_points(256), args.turns,
+                         Tuning(args.chunk, args.layout, args.graph_turns))
+    print(f"{s * 1e3:.3f} ms per batched turn of the 256-point sweep")
