@@ -1204,6 +1204,10 @@ hj_status batch_upload(hj_batch* bt) {
       bt->h_chunks[nch++] = ch;
     }
   }
+  // full chunks first, then the partial ones largest first: the last wave of
+  // blocks is made of the shortest chunks
+  std::stable_sort(bt->h_chunks, bt->h_chunks + nch,
+                   [](const BatchChunk& x, const BatchChunk& y) { return x.count > y.count; });
   bt->h_counts[0] = nch;
   bt->h_counts[1] = nb;
   if (nch > bt->grid_chunks || nb > bt->grid_bunches) {
