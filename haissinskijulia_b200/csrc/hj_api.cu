@@ -1120,7 +1120,7 @@ struct hj_batch {
   int max_bunches = 0, max_B = 0, max_H = 0, max_chunks = 0;
   // launch widths: the live counts rounded up to a power of two (a captured
   // graph is re-captured only when the live counts outgrow them)
-  int grid_chunks = 0, grid_bunches = 0;
+  int grid_chunks = 0, grid_bunches = 0, grid_items = 0;
   int wake = -1, qe = -1;                      // fixed by the first bunch
   int64_t pool_n = 0;
   double* pool_z = nullptr;
@@ -1134,10 +1134,12 @@ struct hj_batch {
   PassArgs* d_pass = nullptr;
   BinsArgs* d_bins = nullptr;
   BatchChunk* d_chunks = nullptr;
-  int32_t* d_counts = nullptr;                 // [0] chunks, [1] bunches
+  BatchChunk* d_items = nullptr;               // merge table: groups of a bunch's partial slots
+  int32_t* d_counts = nullptr;                 // [0] chunks, [1] bunches, [2] merge items
   PassArgs* h_pass = nullptr;                  // pinned staging
   BinsArgs* h_bins = nullptr;
   BatchChunk* h_chunks = nullptr;
+  BatchChunk* h_items = nullptr;
   int32_t* h_counts = nullptr;
   bool dirty = true;
   int graph_turns = 16;
@@ -1208,11 +1210,28 @@ hj_status batch_upload(hj_batch* bt) {
   // blocks is made of the shortest chunks
   std::stable_sort(bt->h_chunks, bt->h_chunks + nch,
                    [](const BatchChunk& x, const BatchChunk& y) { return x.count > y.count; });
+  // merge table: each bunch's partial slots in groups of kMergeGroup
+  constexpr int kMergeGroup = 4;
+  int nit = 0;
+  for (int k = 0; k < nb; ++k) {
+    const int np = bt->members[k].b->nblk;
+    for (int p0 = 0; p0 < np; p0 += kMergeGroup) {
+      if (nit >= bt->max_chunks) return set_err(ctx, HJ_ERR_STATE, "batch merge table overflow");
+      BatchChunk it;
+      it.first = p0;
+      it.count = std::min(kMergeGroup, np - p0);
+      it.bunch = k;
+      it.part = 0;
+      bt->h_items[nit++] = it;
+    }
+  }
   bt->h_counts[0] = nch;
   bt->h_counts[1] = nb;
-  if (nch > bt->grid_chunks || nb > bt->grid_bunches) {
+  bt->h_counts[2] = nit;
+  if (nch > bt->grid_chunks || nb > bt->grid_bunches || nit > bt->grid_items) {
     bt->grid_chunks = std::max(bt->grid_chunks, (int)std::min<int64_t>(next_pow2(nch), bt->max_chunks));
     bt->grid_bunches = std::max(bt->grid_bunches, (int)std::min<int64_t>(next_pow2(nb), bt->max_bunches));
+    bt->grid_items = std::max(bt->grid_items, (int)std::min<int64_t>(next_pow2(nit), bt->max_chunks));
     if (bt->graph) {
       cudaGraphExecDestroy(bt->graph);
       bt->graph = nullptr;
@@ -1227,7 +1246,10 @@ hj_status batch_upload(hj_batch* bt) {
   if (nch > 0)
     HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_chunks, bt->h_chunks, sizeof(BatchChunk) * nch,
                                  cudaMemcpyHostToDevice, bt->stream));
-  HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_counts, bt->h_counts, sizeof(int32_t) * 2,
+  if (nit > 0)
+    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_items, bt->h_items, sizeof(BatchChunk) * nit,
+                                 cudaMemcpyHostToDevice, bt->stream));
+  HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_counts, bt->h_counts, sizeof(int32_t) * 3,
                                cudaMemcpyHostToDevice, bt->stream));
   bt->dirty = false;
   return HJ_OK;
@@ -1238,8 +1260,8 @@ hj_status batch_launch_turn(hj_batch* bt) {
   HJ_CUDA(ctx, launch_batch_pass(bt->d_pass, bt->d_chunks, bt->d_counts, bt->grid_chunks,
                                  bt->max_B, bt->wake, bt->qe, bt->cfg, bt->stream));
   if (bt->wake)
-    HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_counts + 1, bt->grid_bunches, bt->max_B,
-                                     bt->stream));
+    HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_items, bt->d_counts + 2, bt->grid_items,
+                                     bt->max_B, bt->stream));
   HJ_CUDA(ctx, launch_batch_bins(bt->d_bins, bt->d_counts + 1, bt->grid_bunches, bt->max_H,
                                  bt->stream));
   return HJ_OK;
@@ -1283,10 +1305,10 @@ extern "C" void hj_batch_destroy(hj_batch* bt) {
   }
   if (bt->graph) cudaGraphExecDestroy(bt->graph);
   void* dev[] = {bt->pool_z, bt->pool_dE, bt->d_ts, bt->d_pass, bt->d_bins, bt->d_chunks,
-                 bt->d_counts};
+                 bt->d_items, bt->d_counts};
   for (void* p : dev)
     if (p) cudaFree(p);
-  void* pinned[] = {bt->h_ts, bt->h_pass, bt->h_bins, bt->h_chunks, bt->h_counts};
+  void* pinned[] = {bt->h_ts, bt->h_pass, bt->h_bins, bt->h_chunks, bt->h_items, bt->h_counts};
   for (void* p : pinned)
     if (p) cudaFreeHost(p);
   if (bt->stream) cudaStreamDestroy(bt->stream);
@@ -1312,13 +1334,15 @@ static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t 
   HJ_TRY(dalloc(ctx, &bt->d_pass, (size_t)max_bunches));
   HJ_TRY(dalloc(ctx, &bt->d_bins, (size_t)max_bunches));
   HJ_TRY(dalloc(ctx, &bt->d_chunks, (size_t)bt->max_chunks));
-  HJ_TRY(dalloc(ctx, &bt->d_counts, 2));
+  HJ_TRY(dalloc(ctx, &bt->d_items, (size_t)bt->max_chunks));
+  HJ_TRY(dalloc(ctx, &bt->d_counts, 3));
   HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_ts, sizeof(TurnState) * max_bunches));
   HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_pass, sizeof(PassArgs) * max_bunches));
   HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_bins, sizeof(BinsArgs) * max_bunches));
   HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_chunks, sizeof(BatchChunk) * bt->max_chunks));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_counts, sizeof(int32_t) * 2));
-  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_counts, 0, sizeof(int32_t) * 2, bt->stream));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_items, sizeof(BatchChunk) * bt->max_chunks));
+  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_counts, sizeof(int32_t) * 3));
+  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_counts, 0, sizeof(int32_t) * 3, bt->stream));
   HJ_CUDA(ctx, cudaMemsetAsync(bt->d_ts, 0, sizeof(TurnState) * max_bunches, bt->stream));
   bt->free_ranges.push_back({0, bt->pool_n});
   for (int s = max_bunches - 1; s >= 0; --s) bt->free_slots.push_back(s);

@@ -135,8 +135,9 @@ cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chu
                               const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
                               int qe, int cfg, cudaStream_t st);
 cudaError_t launch_sum_parts(const double* part, int nblk, double* out, cudaStream_t st);
-cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const int32_t* d_n_bunches,
-                                int max_bunches, int max_B, cudaStream_t st);
+cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const BatchChunk* d_items,
+                                const int32_t* d_n_items, int max_items, int max_B,
+                                cudaStream_t st);
 // out: counts[B] (| cell counts[B+1] | cell Σw·2^24 [B+1] when part_cic != NULL);
 // zero_first clears out before the merge (the fused pass clears it itself).
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,

@@ -532,6 +532,9 @@ __global__ void __launch_bounds__(THREADS, MINB)
   const BatchChunk ch = chunks[blockIdx.x];
   const PassArgs a = bunches[ch.bunch];
   if (a.ts->turns_left <= 0) return;
+  if (WAKE && ch.part == 0) {  // zero the merged histograms k_batch_reduce adds into
+    for (int i = threadIdx.x; i < 3 * a.B + 2; i += THREADS) a.hist_out[i] = 0ull;
+  }
   const PassRange rg{ch.first / PPT, THREADS, (ch.first + ch.count) / PPT, ch.part,
                      ch.first + ch.count == a.n};
   pass_body<WAKE, QE, PPT, THREADS, PREFETCH>(a, rg, smem_raw);
@@ -570,49 +573,35 @@ __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
   }
 }
 
-// Merge of a batch's per-chunk histograms: block (x, b) sums, for 256 cells
-// of bunch b, the partial slots of all its chunks in slot order and writes
-// the merged arrays (no atomics, so no zeroing; exact integer sums).
+// Merge of a batch's per-chunk histograms: block (x, i) takes item i of the
+// merge table -- partial slots [first, first + count) of one bunch -- sums
+// them for 256 cells and adds the sums to the merged arrays (zeroed by the
+// bunch's first chunk in the pass) with integer atomics: exact, so neither
+// the items' order nor their grouping matters.
 __global__ void k_batch_reduce(const PassArgs* __restrict__ bunches,
-                               const int32_t* __restrict__ n_bunches) {
-  if ((int)blockIdx.y >= *n_bunches) return;
-  const PassArgs& a = bunches[blockIdx.y];
+                               const BatchChunk* __restrict__ items,
+                               const int32_t* __restrict__ n_items) {
+  if ((int)blockIdx.y >= *n_items) return;
+  const BatchChunk it = items[blockIdx.y];
+  const PassArgs& a = bunches[it.bunch];
   if (a.ts->turns_left <= 0 || !a.use_wake) return;
   const int B = a.B, nc = B + 1;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nc) return;
   unsigned long long sc = 0ull, sn = 0ull, sw = 0ull;
-  if (b < B) {
+  if (b < B && it.first == 0) {
     sc = a.ngp_ovf[b];
     a.ngp_ovf[b] = 0ull;
   }
-  // four slots in flight per thread (the loads are independent)
-  const int np = a.n_parts;
-  int k = 0;
-  for (; k + 4 <= np; k += 4) {
-    unsigned long long v[4];
-    uint32_t c[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (b < B) c[u] = __ldg(a.part_cnt + (size_t)(k + u) * B + b);
-      v[u] = __ldg(a.part_cic + (size_t)(k + u) * nc + b);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      sc += c[u];
-      sn += v[u] >> kCicSumBits;
-      sw += v[u] & kCicSumMask;
-    }
-  }
-  for (; k < np; ++k) {
+  for (int64_t k = it.first; k < it.first + it.count; ++k) {
     if (b < B) sc += __ldg(a.part_cnt + (size_t)k * B + b);
     const unsigned long long v = __ldg(a.part_cic + (size_t)k * nc + b);
     sn += v >> kCicSumBits;
     sw += v & kCicSumMask;
   }
-  if (b < B) a.hist_out[b] = sc;
-  a.hist_out[B + b] = sn;
-  a.hist_out[B + nc + b] = sw;
+  if (sc) atomicAdd(a.hist_out + b, sc);
+  if (sn) atomicAdd(a.hist_out + B + b, sn);
+  if (sw) atomicAdd(a.hist_out + B + nc + b, sw);
 }
 
 // Pending kick + re-centring (optional), copy-out (optional) and the moments
@@ -996,10 +985,11 @@ cudaError_t launch_sum_parts(const double* part, int nblk, double* out, cudaStre
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const int32_t* d_n_bunches,
-                                int max_bunches, int max_B, cudaStream_t st) {
-  dim3 grid((max_B + 1 + 255) / 256, max_bunches > 0 ? max_bunches : 1);
-  k_batch_reduce<<<grid, 256, 0, st>>>(d_bunches, d_n_bunches);
+cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const BatchChunk* d_items,
+                                const int32_t* d_n_items, int max_items, int max_B,
+                                cudaStream_t st) {
+  dim3 grid((max_B + 1 + 255) / 256, max_items > 0 ? max_items : 1);
+  k_batch_reduce<<<grid, 256, 0, st>>>(d_bunches, d_items, d_n_items);
   return cudaGetLastError();
 }
 
