@@ -161,6 +161,7 @@ SIGNATURES = {
     "hj_gaussian": (c_int32, [_CTX, c_uint64, c_int64, c_int64, _DP]),
     "hj_generate_particles": (c_int32, [_CTX, c_double, c_double, c_double, c_double, c_int64,
                                         c_uint64, c_void_p, c_void_p, c_void_p, _DP, _DP]),
+    "hj_correlation": (c_int32, [_CTX, c_void_p, c_void_p, c_int64, c_void_p, _DP]),
 }
 
 _lib = None

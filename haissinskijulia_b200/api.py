@@ -505,7 +505,7 @@ def apply_wakefield_inplace(particles: Particles, buffers: SimulationBuffers, wa
 
 
 def gaussian_draws(seed: int, turn: int, n: int, buffers: SimulationBuffers) -> np.ndarray:
-    """The on-device Philox-4x32-10 normals of (seed, particle, turn)."""
+    """The on-device Philox-2x32-10 normals of (seed, particle, turn)."""
     ctx = buffers.context()
     out = np.empty(n, dtype=np.float64)
     _check(ctx, ctx._lib.hj_gaussian(ctx.handle, int(seed) & 0xFFFFFFFFFFFFFFFF, int(turn), n,
@@ -710,6 +710,14 @@ class Batch:
         _check(self.ctx, rc)
         return z, dE, EvolveResult.from_c(r)
 
+    def take_device(self, bid: int, d_z: int, d_dE: int) -> EvolveResult:
+        """As take(), with (z, dE) copied to device arrays (ints: pointers)."""
+        self.sizes.pop(bid)
+        r = HjResult()
+        _check(self.ctx, self.ctx._lib.hj_batch_take(self.handle, int(bid), ctypes.c_void_p(d_z),
+                                                     ctypes.c_void_p(d_dE), ctypes.byref(r)))
+        return EvolveResult.from_c(r)
+
     def stats(self) -> dict:
         out = np.zeros(4, dtype=np.int64)
         _check(self.ctx, self.ctx._lib.hj_batch_stats(self.handle, _ip(out)))
@@ -904,3 +912,13 @@ def generate_particles(mu_z: float, mu_E: float, sigma_z: float, sigma_E: float,
     sE, sz = generate_particles_device(ctx, mu_z, mu_E, sigma_z, sigma_E, n, dz.data_ptr(),
                                        de.data_ptr(), seed=seed)
     return Particles(dz[:n].cpu().numpy(), de[:n].cpu().numpy()), sE, sz, energy
+
+
+def correlation_device(ctx: Context, d_x: int, d_y: int, n: int, stream: int = 0) -> float:
+    """Pearson correlation of two device arrays of n doubles (ints: pointers),
+    two passes on the GPU (hj_correlation): the cor(z, ΔE) of EmittanceFoM
+    (src/parameter_sensitivity/figures_of_merit.jl:42)."""
+    out = np.zeros(1)
+    _check(ctx, ctx._lib.hj_correlation(ctx.handle, ctypes.c_void_p(d_x), ctypes.c_void_p(d_y),
+                                        int(n), ctypes.c_void_p(stream), _dp(out)))
+    return float(out[0])

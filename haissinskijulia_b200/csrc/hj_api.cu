@@ -1804,3 +1804,39 @@ extern "C" hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E
   cudaFree(dev);
   return s;
 }
+
+// ====================================================================== correlation
+
+// cor(particles.coordinates.z, particles.coordinates.ΔE) of EmittanceFoM
+// (src/parameter_sensitivity/figures_of_merit.jl:42, Julia's Statistics.cor):
+// two passes over the device arrays (means, then centred sums Sxx, Syy, Sxy),
+// per-block sums added on the host in block order, r = Sxy/(√Sxx √Syy)
+// clamped to [-1, 1].
+extern "C" hj_status hj_correlation(hj_ctx* ctx, const double* d_x, const double* d_y, int64_t n,
+                                    void* stream, double* out) {
+  HJ_TRY(ctx_ok(ctx));
+  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
+  if (n <= 0) return set_err(ctx, HJ_ERR_ARG, "correlation only defined for non-empty vectors");
+  if (!d_x || !d_y) return set_err(ctx, HJ_ERR_ARG, "arrays are NULL");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int grid = (int)std::min<int64_t>((n + 4095) / 4096, 4 * (int64_t)ctx->num_sms);
+  void* base = nullptr;
+  HJ_TRY(scratch(ctx, sizeof(double) * 3 * (size_t)grid, &base));
+  double* part = (double*)base;
+  std::vector<double> h(3 * (size_t)grid);
+  double s[2][3] = {};
+  double mx = 0.0, my = 0.0;
+  for (int pass = 0; pass < 2; ++pass) {
+    HJ_CUDA(ctx, launch_cor_parts(d_x, d_y, n, mx, my, pass, part, grid, st));
+    HJ_CUDA(ctx, cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(),
+                                 cudaMemcpyDeviceToHost, st));
+    HJ_CUDA(ctx, cudaStreamSynchronize(st));
+    for (int b = 0; b < grid; ++b)
+      for (int k = 0; k < 3; ++k) s[pass][k] += h[3 * (size_t)b + k];
+    mx = s[0][0] / (double)n;
+    my = s[0][1] / (double)n;
+  }
+  const double r = s[1][2] / (std::sqrt(s[1][0]) * std::sqrt(s[1][1]));
+  *out = r != r ? r : std::min(1.0, std::max(-1.0, r));
+  return HJ_OK;
+}

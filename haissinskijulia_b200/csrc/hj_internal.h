@@ -151,6 +151,8 @@ cudaError_t launch_gen_correlated(uint64_t seed, int64_t n, double mu_z, double 
                                   double l10, double l11, double* z, double* dE, cudaStream_t st);
 cudaError_t launch_std_parts(const double* x, int64_t n, double mean, int second, double* part,
                              int grid, cudaStream_t st);
+cudaError_t launch_cor_parts(const double* x, const double* y, int64_t n, double mx, double my,
+                             int second, double* part, int grid, cudaStream_t st);
 cudaError_t launch_log_record(const double* part, int nblk, int64_t n, const TurnState* ts,
                               const unsigned long long* counts, int B, double* rec,
                               cudaStream_t st);

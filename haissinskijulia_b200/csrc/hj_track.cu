@@ -845,6 +845,37 @@ __global__ void k_std_parts(const double* __restrict__ x, int64_t n, double mean
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
+// Per-block sums for the Pearson correlation of (x, y): first pass [Σx, Σy];
+// second pass [Σ(x-mx)², Σ(y-my)², Σ(x-mx)(y-my)] (Statistics.cor, two-pass).
+// part: 3 doubles per block.
+__global__ void k_cor_parts(const double* __restrict__ x, const double* __restrict__ y,
+                            int64_t n, double mx, double my, int second,
+                            double* __restrict__ part) {
+  __shared__ double red[32];
+  double a = 0.0, b = 0.0, c = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double u = x[i], v = y[i];
+    if (second) {
+      const double du = u - mx, dv = v - my;
+      a = fma(du, du, a);
+      b = fma(dv, dv, b);
+      c = fma(du, dv, c);
+    } else {
+      a += u;
+      b += v;
+    }
+  }
+  a = block_sum_1024(a, red);
+  b = block_sum_1024(b, red);
+  c = block_sum_1024(c, red);
+  if (threadIdx.x == 0) {
+    part[3 * (size_t)blockIdx.x] = a;
+    part[3 * (size_t)blockIdx.x + 1] = b;
+    part[3 * (size_t)blockIdx.x + 2] = c;
+  }
+}
+
 int elementwise_grid(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g < 1) g = 1;
@@ -1031,6 +1062,12 @@ cudaError_t launch_gen_correlated(uint64_t seed, int64_t n, double mu_z, double 
 cudaError_t launch_std_parts(const double* x, int64_t n, double mean, int second, double* part,
                              int grid, cudaStream_t st) {
   k_std_parts<<<grid, 1024, 0, st>>>(x, n, mean, second, part);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cor_parts(const double* x, const double* y, int64_t n, double mx, double my,
+                             int second, double* part, int grid, cudaStream_t st) {
+  k_cor_parts<<<grid, 1024, 0, st>>>(x, y, n, mx, my, second, part);
   return cudaGetLastError();
 }
 

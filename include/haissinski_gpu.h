@@ -183,7 +183,7 @@ hj_status hj_make_grid(double sigma_z0, double half_width_sigmas, int64_t nbins,
  *   nbins      bin count (length(buffers.λ) in the reference);
  *   grid       NULL -> grid built on the device's sigma_z0_initial with
  *              hj_make_grid; non-NULL -> used as given (nbins must match);
- *   qe_draws   NULL -> on-device Philox-4x32-10 Gaussians keyed by
+ *   qe_draws   NULL -> on-device Philox-2x32-10 Gaussians keyed by
  *              (seed, particle, turn); non-NULL -> host array of
  *              n_turns*n standard normals, turn-major, used in place of
  *              randn! (src/quantum_excitation.jl:36);
@@ -421,6 +421,14 @@ hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E, double si
                                 double sigma_E, int64_t n, uint64_t seed, double* d_z,
                                 double* d_dE, void* stream, double* actual_sigma_E,
                                 double* actual_sigma_z);
+
+/* cor(particles.coordinates.z, particles.coordinates.ΔE), the correlation
+ * EmittanceFoM computes (src/parameter_sensitivity/figures_of_merit.jl:42), of
+ * two device arrays of n doubles: Pearson r from two passes (means, then the
+ * centred sums), clamped to [-1, 1]; NaN when a spread is zero.  n <= 0 is
+ * HJ_ERR_ARG, as cor rejects empty vectors.  Synchronises `stream`. */
+hj_status hj_correlation(hj_ctx* ctx, const double* d_x, const double* d_y, int64_t n,
+                         void* stream, double* out);
 
 /* The Philox-2x32-10 standard normals used for quantum excitation:
  * out[i] = N(0,1) draw of particle i at `turn` under `seed`.  No reference
