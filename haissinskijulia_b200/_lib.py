@@ -97,6 +97,7 @@ SIGNATURES = {
     "hj_create": (c_int32, [c_int32, POINTER(_CTX)]),
     "hj_destroy": (None, [_CTX]),
     "hj_last_error": (c_char_p, [_CTX]),
+    "hj_trim": (c_int32, [_CTX]),
     "hj_set_pass_layout": (c_int32, [_CTX, c_int32]),
     "hj_wake_reference": (c_int32, [POINTER(HjParams), POINTER(HjWake)]),
     "hj_wake_resonator": (c_int32, [c_double, c_double, c_double, c_double, c_double,

@@ -230,6 +230,11 @@ class Context:
         (-1 = automatic; 0, 1, 2 = fixed layouts)."""
         _check(self, self._lib.hj_set_pass_layout(self.handle, int(layout)))
 
+    def trim(self) -> None:
+        """Free the device and pinned blocks this context keeps for reuse
+        (hj_trim)."""
+        _check(self, self._lib.hj_trim(self.handle))
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self._lib.hj_destroy(self.handle)

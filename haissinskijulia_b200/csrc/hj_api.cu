@@ -10,6 +10,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -27,6 +28,11 @@ struct hj_ctx {
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
   int pass_layout = -1;   // -1: chosen per bunch
+  // released blocks kept for reuse, by size class (device / pinned host)
+  std::multimap<size_t, void*> dev_free, host_free;
+  size_t dev_free_bytes = 0, host_free_bytes = 0;
+  // twiddle tables of the bins step by FFT length P, shared by all bunches
+  std::map<int, double2*> twiddles;
 };
 
 struct hj_bunch {
@@ -83,6 +89,12 @@ struct hj_bunch {
   double* part_mom = nullptr;
   double* h_mom = nullptr;    // pinned
   TurnState* h_ts = nullptr;  // pinned
+  // the buffers above are carved from one device block and one pinned block
+  // of the context's cache; twP is the context's shared table
+  void* arena = nullptr;
+  size_t arena_cap = 0;
+  void* harena = nullptr;
+  size_t harena_cap = 0;
   // profiling: three events per profiled turn (before pass, after pass, after bins)
   bool profiling = false;
   std::vector<cudaEvent_t> events;
@@ -183,6 +195,93 @@ hj_status scratch(hj_ctx* ctx, size_t bytes, void** out) {
 }
 
 size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
+
+// ---- block cache.  A bunch's buffers come from one device block and one
+// pinned block; released blocks are kept (up to a cap) for the next request
+// of the same size class, so admitting and retiring bunches of recurring
+// sizes allocates nothing.  Size classes: 2^k x {1, 1.25, 1.5, 1.75}.
+constexpr size_t kDevCacheCap = size_t(8) << 30;
+constexpr size_t kHostCacheCap = size_t(256) << 20;
+
+size_t size_class(size_t b) {
+  if (b <= 4096) return 4096;
+  const int lg = 63 - __builtin_clzll((unsigned long long)b);
+  const size_t step = size_t(1) << (lg - 2);
+  return (b + step - 1) / step * step;
+}
+
+hj_status cache_take(hj_ctx* ctx, bool host, size_t bytes, void** out, size_t* cap) {
+  const size_t c = size_class(bytes);
+  auto& fl = host ? ctx->host_free : ctx->dev_free;
+  auto it = fl.find(c);
+  if (it != fl.end()) {
+    *out = it->second;
+    fl.erase(it);
+    (host ? ctx->host_free_bytes : ctx->dev_free_bytes) -= c;
+  } else {
+    cudaError_t e = host ? cudaMallocHost(out, c) : cudaMalloc(out, c);
+    if (e != cudaSuccess) {
+      *out = nullptr;
+      return set_err(ctx, HJ_ERR_NOMEM, "%s(%zu bytes) failed: %s",
+                     host ? "cudaMallocHost" : "cudaMalloc", c, cudaGetErrorString(e));
+    }
+  }
+  *cap = c;
+  return HJ_OK;
+}
+
+// Returns a block to the cache (or frees it beyond the cap).  No queued work
+// may still use it.
+void cache_give(hj_ctx* ctx, bool host, void* p, size_t cap) {
+  if (!p) return;
+  size_t& held = host ? ctx->host_free_bytes : ctx->dev_free_bytes;
+  if (held + cap > (host ? kHostCacheCap : kDevCacheCap)) {
+    if (host) cudaFreeHost(p);
+    else cudaFree(p);
+    return;
+  }
+  (host ? ctx->host_free : ctx->dev_free).insert({cap, p});
+  held += cap;
+}
+
+void cache_clear(hj_ctx* ctx) {
+  for (auto& kv : ctx->dev_free) cudaFree(kv.second);
+  for (auto& kv : ctx->host_free) cudaFreeHost(kv.second);
+  ctx->dev_free.clear();
+  ctx->host_free.clear();
+  ctx->dev_free_bytes = ctx->host_free_bytes = 0;
+}
+
+// The twiddle table [P] of the bins step, built once per context and P.
+hj_status shared_twiddles(hj_ctx* ctx, int P, double2** out) {
+  auto it = ctx->twiddles.find(P);
+  if (it == ctx->twiddles.end()) {
+    std::vector<double> tw(2 * (size_t)P);
+    host_twiddles(P, tw.data());
+    double2* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, sizeof(double2) * P);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(d, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      if (d) cudaFree(d);
+      return set_err(ctx, HJ_ERR_CUDA, "twiddle table: %s", cudaGetErrorString(e));
+    }
+    it = ctx->twiddles.insert({P, d}).first;
+  }
+  *out = it->second;
+  return HJ_OK;
+}
+
+// Offsets of the buffers carved from one block (each 256-byte aligned).
+struct Carve {
+  size_t off = 0;
+  template <class T>
+  size_t add(size_t count) {
+    const size_t o = off;
+    off = align_up(off + sizeof(T) * (count ? count : 1));
+    return o;
+  }
+};
 
 hj_status check_params(hj_ctx* ctx, const hj_params* p) {
   if (!p) return set_err(ctx, HJ_ERR_ARG, "params is NULL");
@@ -332,10 +431,19 @@ extern "C" void hj_destroy(hj_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->scratch) cudaFree(ctx->scratch);
+  cache_clear(ctx);
+  for (auto& kv : ctx->twiddles) cudaFree(kv.second);
   delete ctx;
 }
 
 extern "C" const char* hj_last_error(const hj_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+extern "C" hj_status hj_trim(hj_ctx* ctx) {
+  HJ_TRY(ctx_ok(ctx));
+  HJ_CUDA(ctx, cudaDeviceSynchronize());
+  cache_clear(ctx);
+  return HJ_OK;
+}
 
 extern "C" hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout) {
   if (!ctx) return HJ_ERR_ARG;
@@ -350,15 +458,11 @@ extern "C" hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout) {
 extern "C" void hj_bunch_destroy(hj_bunch* b) {
   if (!b) return;
   cudaSetDevice(b->ctx->device);
-  cudaStreamSynchronize(b->stream);
-  void* dev[] = {b->ts,       b->pot,      b->potd,     b->hist,    b->lam,
-                 b->W,        b->Wf,       b->twP,      b->Xg,      b->zE,
-                 b->part_cnt, b->part_cic, b->part_sum, b->part_mom, b->ngp_ovf,
-                 b->rf_table, b->d_sums, b->d_log};
-  for (void* p : dev)
-    if (p) cudaFree(p);
-  if (b->h_mom) cudaFreeHost(b->h_mom);
-  if (b->h_ts) cudaFreeHost(b->h_ts);
+  cudaStreamSynchronize(b->stream);       // nothing queued still uses the blocks
+  cache_give(b->ctx, false, b->arena, b->arena_cap);
+  cache_give(b->ctx, true, b->harena, b->harena_cap);
+  if (b->d_sums) cudaFree(b->d_sums);
+  if (b->d_log) cudaFree(b->d_log);
   for (cudaEvent_t e : b->events) cudaEventDestroy(e);
   delete b;
 }
@@ -398,13 +502,71 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     b->B = (int)B;
   }
 
-  // Initial spreads, src/evolution.jl:247-249.
+  // sizes of every buffer, then one device and one pinned block for all
   b->nblk_m = (int)std::min<int64_t>(std::max<int64_t>((n + 4095) / 4096, 1),
                                      (int64_t)ctx->num_sms * 4);
-  HJ_TRY(dalloc(ctx, &b->part_mom, (size_t)4 * b->nblk_m));
-  HJ_TRY(dalloc(ctx, &b->ts, 1));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&b->h_mom, sizeof(double) * 4 * b->nblk_m));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&b->h_ts, sizeof(TurnState)));
+  if (b->use_wake) {
+    b->P = (int)next_pow2(2 * (int64_t)b->B);            // src/evolution.jl:265
+    b->M = b->P / 2;
+    b->H = b->M / 2;
+    b->logH = b->H >= 1 ? ilog2(b->H) : 0;
+  }
+  b->cfg = cfg >= 0 ? cfg : (ctx->pass_layout >= 0 ? ctx->pass_layout : default_pass_layout(b->B, n));
+  if (chunk > 0) {
+    b->nblk = (int)std::max<int64_t>((n + chunk - 1) / chunk, 1);
+  } else {
+    const int bps = track_blocks_per_sm(b->B, b->qe_mode, b->use_wake, b->cfg);
+    b->nblk = track_grid_size(n, b->B, ctx->num_sms, bps, b->cfg);
+  }
+  {
+    const size_t B = (size_t)b->B, nb = (size_t)b->nblk;
+    Carve c;
+    const size_t o_mom = c.add<double>(4 * (size_t)b->nblk_m);
+    const size_t o_ts = c.add<TurnState>(1);
+    const size_t o_sum = c.add<double>((size_t)kNumSums * nb);
+    const size_t o_rf = c.add<double2>(kRfTableSize);
+    size_t o[11] = {};
+    if (b->use_wake) {
+      o[0] = c.add<double>(B);                                   // W
+      o[1] = c.add<double>(B);                                   // lam
+      o[2] = c.add<double2>((size_t)b->M + 1);                   // Wf
+      o[3] = c.add<double2>((size_t)b->M);                       // Xg
+      o[4] = c.add<double2>((size_t)std::max(b->H, 1));          // zE
+      o[5] = c.add<double>(B);                                   // pot
+      o[6] = c.add<double2>(B + 1);                              // potd
+      o[7] = c.add<unsigned long long>(3 * B + 2);               // hist
+      o[8] = c.add<uint32_t>(nb * B);                            // part_cnt
+      o[9] = c.add<unsigned long long>(nb * (B + 1));            // part_cic
+      o[10] = c.add<unsigned long long>(B);                      // ngp_ovf
+    }
+    HJ_TRY(cache_take(ctx, false, c.off, &b->arena, &b->arena_cap));
+    char* a = (char*)b->arena;
+    b->part_mom = (double*)(a + o_mom);
+    b->ts = (TurnState*)(a + o_ts);
+    b->part_sum = (double*)(a + o_sum);
+    b->rf_table = (double2*)(a + o_rf);
+    if (b->use_wake) {
+      b->W = (double*)(a + o[0]);
+      b->lam = (double*)(a + o[1]);
+      b->Wf = (double2*)(a + o[2]);
+      b->Xg = (double2*)(a + o[3]);
+      b->zE = (double2*)(a + o[4]);
+      b->pot = (double*)(a + o[5]);
+      b->potd = (double2*)(a + o[6]);
+      b->hist = (unsigned long long*)(a + o[7]);
+      b->part_cnt = (uint32_t*)(a + o[8]);
+      b->part_cic = (unsigned long long*)(a + o[9]);
+      b->ngp_ovf = (unsigned long long*)(a + o[10]);
+    }
+    Carve hc;
+    const size_t h_mom = hc.add<double>(4 * (size_t)b->nblk_m);
+    const size_t h_ts = hc.add<TurnState>(1);
+    HJ_TRY(cache_take(ctx, true, hc.off, &b->harena, &b->harena_cap));
+    b->h_mom = (double*)((char*)b->harena + h_mom);
+    b->h_ts = (TurnState*)((char*)b->harena + h_ts);
+  }
+
+  // Initial spreads, src/evolution.jl:247-249.
   double m[4];
   HJ_TRY(launch_moments(b, 0, nullptr, nullptr));
   HJ_TRY(read_moments(b, m));
@@ -436,25 +598,11 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
       b->hi_idx = (int)(idx1 - 1);
       b->hi_w = u - fl;
     }
-    b->P = (int)next_pow2(2 * (int64_t)B);               // src/evolution.jl:265
-    b->M = b->P / 2;
-    b->H = b->M / 2;
-    b->logH = b->H >= 1 ? ilog2(b->H) : 0;
-    std::vector<double> W(B), lam(B), tw(2 * (size_t)b->P);
+    std::vector<double> W(B), lam(B);
     host_wake_tables(b->centers.data(), B, b->w, W.data(), lam.data());
-    host_twiddles(b->P, tw.data());
-    HJ_TRY(dalloc(ctx, &b->W, B));
-    HJ_TRY(dalloc(ctx, &b->lam, B));
-    HJ_TRY(dalloc(ctx, &b->twP, b->P));
-    HJ_TRY(dalloc(ctx, &b->Wf, (size_t)b->M + 1));
-    HJ_TRY(dalloc(ctx, &b->Xg, b->M));
-    HJ_TRY(dalloc(ctx, &b->zE, std::max(b->H, 1)));
-    HJ_TRY(dalloc(ctx, &b->pot, B));
-    HJ_TRY(dalloc(ctx, &b->potd, (size_t)B + 1));
-    HJ_TRY(dalloc(ctx, &b->hist, 3 * (size_t)B + 2));
+    HJ_TRY(shared_twiddles(ctx, b->P, &b->twP));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->W, W.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, lam.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
-    HJ_CUDA(ctx, cudaMemcpyAsync(b->twP, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->pot, 0, sizeof(double) * B, b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->potd, 0, sizeof(double2) * ((size_t)B + 1), b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->hist, 0, sizeof(unsigned long long) * (3 * (size_t)B + 2),
@@ -465,26 +613,13 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));     // host vectors go out of scope
   }
 
-  b->cfg = cfg >= 0 ? cfg : (ctx->pass_layout >= 0 ? ctx->pass_layout : default_pass_layout(b->B, n));
-  if (chunk > 0) {
-    b->nblk = (int)std::max<int64_t>((n + chunk - 1) / chunk, 1);
-  } else {
-    const int bps = track_blocks_per_sm(b->B, b->qe_mode, b->use_wake, b->cfg);
-    b->nblk = track_grid_size(n, b->B, ctx->num_sms, bps, b->cfg);
-  }
-  HJ_TRY(dalloc(ctx, &b->part_sum, (size_t)kNumSums * b->nblk));
-  if (b->use_wake) {
-    HJ_TRY(dalloc(ctx, &b->part_cnt, (size_t)b->nblk * b->B));
-    HJ_TRY(dalloc(ctx, &b->part_cic, (size_t)b->nblk * ((size_t)b->B + 1)));
-    HJ_TRY(dalloc(ctx, &b->ngp_ovf, (size_t)b->B));
+  if (b->use_wake)
     HJ_CUDA(ctx, cudaMemsetAsync(b->ngp_ovf, 0, sizeof(unsigned long long) * b->B, b->stream));
-  }
 
   {
     std::vector<double> rf(2 * kRfTableSize);
     host_rf_table(params->voltage, params->phi_s, kRfTableSize, rf.data());
     b->rf_Vs = rf[0];
-    HJ_TRY(dalloc(ctx, &b->rf_table, kRfTableSize));
     HJ_CUDA(ctx, cudaMemcpyAsync(b->rf_table, rf.data(), sizeof(double) * rf.size(),
                                  cudaMemcpyHostToDevice, b->stream));
     HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
@@ -787,8 +922,15 @@ extern "C" hj_status hj_evolve(hj_ctx* ctx, double* z, double* dE, int64_t n,
   if (n == 0) return evolve_empty(ctx, params, out);
   if (!z || !dE) return set_err(ctx, HJ_ERR_ARG, "particle arrays are NULL");
   double *d_z = nullptr, *d_dE = nullptr, *d_draws = nullptr;
-  hj_status s = dalloc(ctx, &d_z, (size_t)n);
-  if (s == HJ_OK) s = dalloc(ctx, &d_dE, (size_t)n);
+  // the particle arrays: one block of the context's cache, kept for the next call
+  void* blk = nullptr;
+  size_t blk_cap = 0;
+  const size_t half = align_up(sizeof(double) * (size_t)n);
+  hj_status s = cache_take(ctx, false, 2 * half, &blk, &blk_cap);
+  if (s == HJ_OK) {
+    d_z = (double*)blk;
+    d_dE = (double*)((char*)blk + half);
+  }
   const bool draws = qe_draws && params->use_excitation && params->n_turns > 0;
   if (s == HJ_OK && draws) s = dalloc(ctx, &d_draws, (size_t)n * (size_t)params->n_turns);
   cudaStream_t st = ctx->stream;
@@ -808,8 +950,8 @@ extern "C" hj_status hj_evolve(hj_ctx* ctx, double* z, double* dE, int64_t n,
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) s = set_err(ctx, HJ_ERR_CUDA, "device->host copy failed: %s", cudaGetErrorString(e));
   }
-  if (d_z) cudaFree(d_z);
-  if (d_dE) cudaFree(d_dE);
+  cudaStreamSynchronize(st);
+  cache_give(ctx, false, blk, blk_cap);
   if (d_draws) cudaFree(d_draws);
   return s;
 }
@@ -1445,8 +1587,7 @@ static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE,
   const int slot = bt->free_slots.back();
   bt->free_slots.pop_back();
   b->h_ts->turns_left = turns;
-  cudaFree(b->ts);
-  b->ts = bt->d_ts + slot;
+  b->ts = bt->d_ts + slot;           // the arena's own TurnState stays unused
   HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
                                bt->stream));
   HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));

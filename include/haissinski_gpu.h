@@ -137,6 +137,11 @@ hj_status hj_create(int32_t device, hj_ctx** out);
 void hj_destroy(hj_ctx* ctx);
 /* Message of the last failure on this context ("" if none). */
 const char* hj_last_error(const hj_ctx* ctx);
+/* A context keeps the device and pinned blocks of finished bunches and of
+ * hj_evolve's particle arrays (up to 8 GB device, 256 MB pinned) for reuse,
+ * so that admitting bunches of recurring sizes allocates nothing; hj_trim
+ * frees them now (hj_destroy frees them too).  No reference counterpart. */
+hj_status hj_trim(hj_ctx* ctx);
 /* Thread layout of the fused particle pass for bunches created afterwards on
  * this context: -1 = chosen by the library (default), 0 = 4 particles per
  * thread x 512 threads, 1 = 2 x 1024, 2 = 2 x 768 (each with the next group
