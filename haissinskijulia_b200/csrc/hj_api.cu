@@ -6,6 +6,7 @@
 // (E0, pending kick, turn counter) lives in device memory, so turns never
 // wait for the host.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -33,6 +34,18 @@ struct hj_ctx {
   size_t dev_free_bytes = 0, host_free_bytes = 0;
   // twiddle tables of the bins step by FFT length P, shared by all bunches
   std::map<int, double2*> twiddles;
+  // grids and wake tables built from an initial σ_z, by the bit patterns of
+  // (nbins, σ_z0, half width, F, s, cτ, sin coefficient, δ width): bunches
+  // of a scan start from the same particles and share them
+  struct WakeSet {
+    std::vector<double> centers;
+    double e0 = 0, eN = 0, estep = 0;
+    void* dev = nullptr;            // W[B] | λ[B] | FFT(W)[M+1], a block of the cache
+    size_t cap = 0;
+    uint64_t used = 0;
+  };
+  std::map<std::array<uint64_t, 8>, WakeSet> wake_sets;
+  uint64_t wake_clock = 0;
 };
 
 struct hj_bunch {
@@ -245,6 +258,8 @@ void cache_give(hj_ctx* ctx, bool host, void* p, size_t cap) {
 }
 
 void cache_clear(hj_ctx* ctx) {
+  for (auto& kv : ctx->wake_sets) cudaFree(kv.second.dev);
+  ctx->wake_sets.clear();
   for (auto& kv : ctx->dev_free) cudaFree(kv.second);
   for (auto& kv : ctx->host_free) cudaFreeHost(kv.second);
   ctx->dev_free.clear();
@@ -577,11 +592,29 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     const int B = b->B;
     b->centers.resize(B);
     hj_grid g{};
+    hj_ctx::WakeSet* cached = nullptr;
+    std::array<uint64_t, 8> key{};
     if (grid) {
       std::memcpy(b->centers.data(), grid->centers, sizeof(double) * B);
       g = *grid;
     } else {
-      HJ_TRY(hj_make_grid(b->sigma_z0_initial, b->w.half_width_sigmas, B, b->centers.data(), &g));
+      const double kv[7] = {b->sigma_z0_initial, b->w.half_width_sigmas, b->w.wake_factor,
+                            b->w.wake_sqrt, b->w.ctau, b->w.sin_coef, b->w.delta_std};
+      key[0] = (uint64_t)B;
+      std::memcpy(key.data() + 1, kv, sizeof(kv));
+      auto it = ctx->wake_sets.find(key);
+      if (it != ctx->wake_sets.end()) {
+        cached = &it->second;
+        cached->used = ++ctx->wake_clock;
+        b->centers = cached->centers;
+        g.nbins = B;
+        g.edge_first = cached->e0;
+        g.edge_last = cached->eN;
+        g.edge_step = cached->estep;
+      } else {
+        HJ_TRY(hj_make_grid(b->sigma_z0_initial, b->w.half_width_sigmas, B, b->centers.data(),
+                            &g));
+      }
     }
     b->e0 = g.edge_first;
     b->eN = g.edge_last;
@@ -598,18 +631,56 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
       b->hi_idx = (int)(idx1 - 1);
       b->hi_w = u - fl;
     }
-    std::vector<double> W(B), lam(B);
-    host_wake_tables(b->centers.data(), B, b->w, W.data(), lam.data());
     HJ_TRY(shared_twiddles(ctx, b->P, &b->twP));
-    HJ_CUDA(ctx, cudaMemcpyAsync(b->W, W.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
-    HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, lam.data(), sizeof(double) * B, cudaMemcpyHostToDevice, b->stream));
+    const size_t wbytes = sizeof(double) * B, fbytes = sizeof(double2) * ((size_t)b->M + 1);
+    std::vector<double> W, lam;
+    if (cached) {
+      const char* src = (const char*)cached->dev;
+      HJ_CUDA(ctx, cudaMemcpyAsync(b->W, src, wbytes, cudaMemcpyDeviceToDevice, b->stream));
+      HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, src + wbytes, wbytes, cudaMemcpyDeviceToDevice,
+                                   b->stream));
+      HJ_CUDA(ctx, cudaMemcpyAsync(b->Wf, src + 2 * wbytes, fbytes, cudaMemcpyDeviceToDevice,
+                                   b->stream));
+    } else {
+      W.resize(B);
+      lam.resize(B);
+      host_wake_tables(b->centers.data(), B, b->w, W.data(), lam.data());
+      HJ_CUDA(ctx, cudaMemcpyAsync(b->W, W.data(), wbytes, cudaMemcpyHostToDevice, b->stream));
+      HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, lam.data(), wbytes, cudaMemcpyHostToDevice, b->stream));
+      if (b->H >= 4)
+        HJ_CUDA(ctx, launch_wake_spectrum(b->W, B, b->P, b->M, b->H, b->logH, b->twP, b->Xg,
+                                          b->Wf, b->stream));
+      if (!grid) {
+        // keep this grid and its tables for the next bunch with the same key
+        // (at most 8 sets; the least recently used goes)
+        if (ctx->wake_sets.size() >= 8) {
+          auto lru = ctx->wake_sets.begin();
+          for (auto it = ctx->wake_sets.begin(); it != ctx->wake_sets.end(); ++it)
+            if (it->second.used < lru->second.used) lru = it;
+          HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
+          cache_give(ctx, false, lru->second.dev, lru->second.cap);
+          ctx->wake_sets.erase(lru);
+        }
+        hj_ctx::WakeSet ws;
+        ws.centers = b->centers;
+        ws.e0 = g.edge_first;
+        ws.eN = g.edge_last;
+        ws.estep = g.edge_step;
+        ws.used = ++ctx->wake_clock;
+        HJ_TRY(cache_take(ctx, false, 2 * wbytes + fbytes, &ws.dev, &ws.cap));
+        char* dst = (char*)ws.dev;
+        HJ_CUDA(ctx, cudaMemcpyAsync(dst, b->W, wbytes, cudaMemcpyDeviceToDevice, b->stream));
+        HJ_CUDA(ctx, cudaMemcpyAsync(dst + wbytes, b->lam, wbytes, cudaMemcpyDeviceToDevice,
+                                     b->stream));
+        HJ_CUDA(ctx, cudaMemcpyAsync(dst + 2 * wbytes, b->Wf, fbytes, cudaMemcpyDeviceToDevice,
+                                     b->stream));
+        ctx->wake_sets.insert({key, std::move(ws)});
+      }
+    }
     HJ_CUDA(ctx, cudaMemsetAsync(b->pot, 0, sizeof(double) * B, b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->potd, 0, sizeof(double2) * ((size_t)B + 1), b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->hist, 0, sizeof(unsigned long long) * (3 * (size_t)B + 2),
                                  b->stream));
-    if (b->H >= 4)
-      HJ_CUDA(ctx, launch_wake_spectrum(b->W, B, b->P, b->M, b->H, b->logH, b->twP, b->Xg,
-                                        b->Wf, b->stream));
     HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));     // host vectors go out of scope
   }
 

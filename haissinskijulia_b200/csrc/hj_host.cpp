@@ -54,6 +54,29 @@ extern "C" hj_status hj_wake_resonator(double Rs, double Q, double fr, double po
   return HJ_OK;
 }
 
+namespace {
+// The correctly rounded w·m/B (|m| < 2^53 / |w| headroom, B > 0) in double
+// arithmetic: w·m = ph + pl exactly (fma), q0 = ph/B with its exact
+// remainder, then the correction.  Returns false when the exact value lies
+// within 2^-30 of a half-gap of the candidate (a rounding boundary); the
+// caller then takes the quad-precision quotient, which such rare cases need.
+bool rounded_ratio(double w, int64_t m, int64_t B, double* out) {
+  const double md = (double)m, Bd = (double)B;
+  const double ph = w * md;
+  const double pl = std::fma(w, md, -ph);
+  const double q0 = ph / Bd;
+  const double r = std::fma(-q0, Bd, ph);            // exact: ph - q0·B
+  const double e = (r + pl) / Bd;                    // x - q0, relative error ~2^-52
+  const double q = q0 + e;
+  const double d = e - (q - q0);                     // x - q (q - q0 exact)
+  const double gap = d >= 0.0 ? std::nextafter(q, INFINITY) - q
+                              : q - std::nextafter(q, -INFINITY);
+  if (!(std::fabs(d) < 0.5 * gap * (1.0 - 0x1p-30))) return false;
+  *out = q;
+  return true;
+}
+}  // namespace
+
 extern "C" hj_status hj_make_grid(double sigma_z0, double half_width_sigmas, int64_t nbins,
                                   double* centers, hj_grid* out) {
   if (!centers || !out) return HJ_ERR_ARG;
@@ -61,11 +84,14 @@ extern "C" hj_status hj_make_grid(double sigma_z0, double half_width_sigmas, int
   double w = half_width_sigmas * sigma_z0;                   // src/evolution.jl:270
   if (w < 1e-9) w = 1e-6;                                    // :272
   // Julia's range(-w, w, length=B+1) and its midpoints hold the correctly
-  // rounded values of w(2k-B)/B and w(2k+1-B)/B; with B a power of two the
-  // quad-precision product below is exact before the single rounding.
+  // rounded values of w(2k-B)/B and w(2k+1-B)/B.
   const __float128 W = (__float128)w, Bq = (__float128)nbins;
-  for (int64_t k = 0; k < nbins; ++k)
-    centers[k] = (double)(W * (__float128)(2 * k + 1 - nbins) / Bq);
+  for (int64_t k = 0; k < nbins; ++k) {
+    const int64_t m = 2 * k + 1 - nbins;
+    double c;
+    if (!rounded_ratio(w, m, nbins, &c)) c = (double)(W * (__float128)m / Bq);
+    centers[k] = c;
+  }
   out->nbins = nbins;
   out->edge_first = -w;
   out->edge_last = w;

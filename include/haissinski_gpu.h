@@ -137,10 +137,13 @@ hj_status hj_create(int32_t device, hj_ctx** out);
 void hj_destroy(hj_ctx* ctx);
 /* Message of the last failure on this context ("" if none). */
 const char* hj_last_error(const hj_ctx* ctx);
-/* A context keeps the device and pinned blocks of finished bunches and of
- * hj_evolve's particle arrays (up to 8 GB device, 256 MB pinned) for reuse,
- * so that admitting bunches of recurring sizes allocates nothing; hj_trim
- * frees them now (hj_destroy frees them too).  No reference counterpart. */
+/* A context keeps, for reuse, the device and pinned blocks of finished
+ * bunches and of hj_evolve's particle arrays (up to 8 GB device, 256 MB
+ * pinned) and the last 8 bin grids with their wake tables built from an
+ * initial sigma_z (bunches of a scan start from the same particles), so that
+ * admitting bunches of recurring sizes allocates and recomputes nothing.
+ * hj_trim frees them now (hj_destroy frees them too).  No reference
+ * counterpart. */
 hj_status hj_trim(hj_ctx* ctx);
 /* Thread layout of the fused particle pass for bunches created afterwards on
  * this context: -1 = chosen by the library (default), 0 = 4 particles per

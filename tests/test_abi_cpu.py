@@ -74,6 +74,16 @@ def test_make_grid_correctly_rounded(lib, B):
         assert g.centers[k] == float(W * (2 * int(k) + 1 - B) / B)
 
 
+@pytest.mark.parametrize("B", [7, 2000, 4096, 10000])
+def test_make_grid_every_center_correctly_rounded(lib, B):
+    rng = np.random.default_rng(B)
+    for sigma in (0.0040123456789, *rng.uniform(1e-4, 1e-2, 3)):
+        g = BinGrid.make(float(sigma), B, 7.5)
+        W = Fraction(7.5 * float(sigma))
+        want = [float(W * (2 * k + 1 - B) / B) for k in range(B)]
+        assert np.array_equal(g.centers, np.array(want))
+
+
 def test_make_grid_width_floor_and_errors(lib):
     g = BinGrid.make(0.0, 8, 7.5)          # src/evolution.jl:272
     assert g.edge_last == 1e-6
