@@ -61,6 +61,10 @@ def parse_args():
     ap.add_argument("--sweep-plain-points", type=int, default=8,
                     help="points of the sweep also run one after another on the plain path")
     ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--scan-points", type=int, default=32,
+                    help="parameter-scan points (0: no scan measurement)")
+    ap.add_argument("--scan-samples", type=int, default=20)
+    ap.add_argument("--scan-sequential-points", type=int, default=4)
     return ap.parse_args()
 
 
@@ -278,7 +282,53 @@ def measure_sweeps(ctx, args) -> dict:
                         "(8 GB budget), 200-turn blocks")
         sm["particle_turns_per_s"] = sm["particle_turns"] / sm["wall_s"]
         out["serving"] = sm
+    if args.scan_points > 0:
+        out["parameter_scan"] = measure_scan(ctx, args)
     return out
+
+
+def measure_scan(ctx, args) -> dict:
+    """scan_parameter (src/parameter_sensitivity/scan.jl) over RF voltage with
+    the emittance figure of merit and derivative samples: every run in one
+    batch, against the same runs one after another on a sample of points."""
+    import numpy as np
+    from haissinskijulia_b200 import Particles, benchmark_ring
+    from haissinskijulia_b200.sensitivity import (EmittanceFoM, VoltageTransform,
+                                                  scan_parameter, scan_parameter_sequential)
+    n, P, S = 100_000, args.scan_points, args.scan_samples
+    cfg = benchmark_ring(n_turns=100, nbins=n // 10)
+    rng = np.random.default_rng(args.seed)
+    parts = Particles(rng.normal(0.0, cfg.sigma_z, n), rng.normal(0.0, cfg.sigma_E, n))
+    values = np.linspace(3e6, 7e6, P)
+    kw = dict(ctx=ctx, n_samples=S, seed=args.seed, return_runs=True)
+    times = []
+    for _ in range(2):            # the first scan also fills the context's block cache
+        t0 = time.perf_counter()
+        _, fb, gb, _, runs = scan_parameter(VoltageTransform(), EmittanceFoM(), values, parts,
+                                            cfg.params, block_turns=32, graph_turns=32, **kw)
+        times.append(time.perf_counter() - t0)
+    t_bat = times[-1]
+    k = max(1, min(args.scan_sequential_points, P))
+    idx = list(range(0, P, max(P // k, 1)))[:k]
+    t0 = time.perf_counter()
+    _, fs, gs, _, _ = scan_parameter_sequential(VoltageTransform(), EmittanceFoM(),
+                                                values[idx], parts, cfg.params, **kw)
+    t_seq = time.perf_counter() - t0
+    rel = float(np.max(np.abs(fb[idx] - fs) / np.abs(fs)))
+    return {
+        "config": f"{P} RF voltages in [3, 7] MV, EmittanceFoM, {S} derivative samples per "
+                  f"point ({1 + 2 * S} runs per point, {len(runs)} in all); 1e5 particles, "
+                  "1e4 bins (the reference's nbins = n/10), 100-turn point runs, 10-turn "
+                  "derivative runs",
+        "batched_points_per_s": P / t_bat, "batched_seconds": t_bat,
+        "batched_seconds_first_scan": times[0],
+        "sequential_points_per_s": k / t_seq, "sequential_seconds": t_seq,
+        "sequential_sample": f"{k} of the {P} points, all their runs one after another on "
+                             "the plain resident path",
+        "speedup_vs_sequential": (P / t_bat) / (k / t_seq),
+        "max_rel_diff_fom": rel,
+        "timing": "host wall clock: admission, every turn, retirement, figures of merit",
+    }
 
 
 def run_ours(args) -> None:

@@ -645,13 +645,13 @@ class Batch:
 
     def _add(self, zp, ep, n, params, nbins, wake, seed, turns) -> int:
         p = params.to_c()
-        w = (wake or WakeModel.reference(params)).to_c()
-        out = np.zeros(1, dtype=np.int64)
+        w = ctypes.byref(wake.to_c()) if wake is not None else None   # None: the reference's
+        out = ctypes.c_int64(0)
         nt = params.n_turns if turns is None else int(turns)
         _check(self.ctx, self.ctx._lib.hj_batch_add(
-            self.handle, zp, ep, int(n), ctypes.byref(p), ctypes.byref(w), int(nbins),
-            int(seed) & 0xFFFFFFFFFFFFFFFF, nt, _ip(out)))
-        bid = int(out[0])
+            self.handle, zp, ep, int(n), ctypes.byref(p), w, int(nbins),
+            int(seed) & 0xFFFFFFFFFFFFFFFF, nt, ctypes.byref(out)))
+        bid = int(out.value)
         self.sizes[bid] = int(n)
         return bid
 

@@ -102,6 +102,7 @@ struct hj_bunch {
   double* part_mom = nullptr;
   double* h_mom = nullptr;    // pinned
   TurnState* h_ts = nullptr;  // pinned
+  double* h_rf = nullptr;     // pinned staging of the RF table
   // the buffers above are carved from one device block and one pinned block
   // of the context's cache; twP is the context's shared table
   void* arena = nullptr;
@@ -316,13 +317,17 @@ hj_status check_grid(hj_ctx* ctx, const hj_grid* g) {
 }
 
 // Device sums of the moments kernel, reduced on the host in block order.
+void sum_moments(const hj_bunch* b, double m[4]) {
+  m[0] = m[1] = m[2] = m[3] = 0.0;
+  for (int i = 0; i < b->nblk_m; ++i)
+    for (int k = 0; k < 4; ++k) m[k] += b->h_mom[4 * i + k];
+}
+
 hj_status read_moments(hj_bunch* b, double m[4]) {
   HJ_CUDA(b->ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 4 * b->nblk_m,
                                   cudaMemcpyDeviceToHost, b->stream));
   HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
-  m[0] = m[1] = m[2] = m[3] = 0.0;
-  for (int i = 0; i < b->nblk_m; ++i)
-    for (int k = 0; k < 4; ++k) m[k] += b->h_mom[4 * i + k];
+  sum_moments(b, m);
   return HJ_OK;
 }
 
@@ -349,10 +354,8 @@ hj_status launch_moments(hj_bunch* b, int apply, double* z_out, double* dE_out) 
   return HJ_OK;
 }
 
-hj_status read_state(hj_bunch* b) {
-  HJ_CUDA(b->ctx, cudaMemcpyAsync(b->h_ts, b->ts, sizeof(TurnState), cudaMemcpyDeviceToHost,
-                                  b->stream));
-  HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
+// The sticky status of the turn state already copied to h_ts.
+hj_status state_status(hj_bunch* b) {
   int st = b->h_ts->status;
   if (st & (1 << HJ_ERR_NONFINITE))
     return set_err(b->ctx, HJ_ERR_NONFINITE,
@@ -362,6 +365,13 @@ hj_status read_state(hj_bunch* b) {
     return set_err(b->ctx, HJ_ERR_ARG, "host-fed draws do not cover turn %lld",
                    (long long)b->h_ts->turn - 1);
   return HJ_OK;
+}
+
+hj_status read_state(hj_bunch* b) {
+  HJ_CUDA(b->ctx, cudaMemcpyAsync(b->h_ts, b->ts, sizeof(TurnState), cudaMemcpyDeviceToHost,
+                                  b->stream));
+  HJ_CUDA(b->ctx, cudaStreamSynchronize(b->stream));
+  return state_status(b);
 }
 
 // Thread layout of the fused pass when the context does not pin one, from
@@ -576,9 +586,11 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     Carve hc;
     const size_t h_mom = hc.add<double>(4 * (size_t)b->nblk_m);
     const size_t h_ts = hc.add<TurnState>(1);
+    const size_t h_rf = hc.add<double>(2 * (size_t)kRfTableSize);
     HJ_TRY(cache_take(ctx, true, hc.off, &b->harena, &b->harena_cap));
     b->h_mom = (double*)((char*)b->harena + h_mom);
     b->h_ts = (TurnState*)((char*)b->harena + h_ts);
+    b->h_rf = (double*)((char*)b->harena + h_rf);
   }
 
   // Initial spreads, src/evolution.jl:247-249.
@@ -681,20 +693,17 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     HJ_CUDA(ctx, cudaMemsetAsync(b->potd, 0, sizeof(double2) * ((size_t)B + 1), b->stream));
     HJ_CUDA(ctx, cudaMemsetAsync(b->hist, 0, sizeof(unsigned long long) * (3 * (size_t)B + 2),
                                  b->stream));
-    HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));     // host vectors go out of scope
+    if (!cached) HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));   // host vectors W, lam
   }
 
   if (b->use_wake)
     HJ_CUDA(ctx, cudaMemsetAsync(b->ngp_ovf, 0, sizeof(unsigned long long) * b->B, b->stream));
 
-  {
-    std::vector<double> rf(2 * kRfTableSize);
-    host_rf_table(params->voltage, params->phi_s, kRfTableSize, rf.data());
-    b->rf_Vs = rf[0];
-    HJ_CUDA(ctx, cudaMemcpyAsync(b->rf_table, rf.data(), sizeof(double) * rf.size(),
-                                 cudaMemcpyHostToDevice, b->stream));
-    HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
-  }
+  // RF table, staged in the bunch's pinned block
+  host_rf_table(params->voltage, params->phi_s, kRfTableSize, b->h_rf);
+  b->rf_Vs = b->h_rf[0];
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->rf_table, b->h_rf, sizeof(double) * 2 * kRfTableSize,
+                               cudaMemcpyHostToDevice, b->stream));
 
   TurnState t{};
   t.cur = make_turn_scalars(params->E0, *params, b->sigma_E0_initial);
@@ -704,8 +713,9 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
   t.turns_left = INT64_MAX;   // a plain bunch runs until it is finished
   t.status = 0;
   *b->h_ts = t;
+  // staged in pinned memory that lives as long as the bunch; later work on
+  // the stream is ordered after the copy, host reads of h_ts synchronise first
   HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice, b->stream));
-  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
   return HJ_OK;
 }
 
@@ -1354,6 +1364,11 @@ struct hj_batch {
   BatchChunk* h_chunks = nullptr;
   BatchChunk* h_items = nullptr;
   int32_t* h_counts = nullptr;
+  // the buffers above are carved from one device and one pinned cached block
+  void* arena = nullptr;
+  size_t arena_cap = 0;
+  void* harena = nullptr;
+  size_t harena_cap = 0;
   bool dirty = true;
   int graph_turns = 16;
   cudaGraphExec_t graph = nullptr;
@@ -1517,13 +1532,8 @@ extern "C" void hj_batch_destroy(hj_batch* bt) {
     hj_bunch_destroy(m.b);
   }
   if (bt->graph) cudaGraphExecDestroy(bt->graph);
-  void* dev[] = {bt->pool_z, bt->pool_dE, bt->d_ts, bt->d_pass, bt->d_bins, bt->d_chunks,
-                 bt->d_items, bt->d_counts};
-  for (void* p : dev)
-    if (p) cudaFree(p);
-  void* pinned[] = {bt->h_ts, bt->h_pass, bt->h_bins, bt->h_chunks, bt->h_items, bt->h_counts};
-  for (void* p : pinned)
-    if (p) cudaFreeHost(p);
+  cache_give(bt->ctx, false, bt->arena, bt->arena_cap);
+  cache_give(bt->ctx, true, bt->harena, bt->harena_cap);
   if (bt->stream) cudaStreamDestroy(bt->stream);
   delete bt;
 }
@@ -1541,20 +1551,35 @@ static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t 
   bt->pool_n = (pool_particles + 3) / 4 * 4;
   bt->max_chunks = (int)std::min<int64_t>(bt->pool_n / chunk + max_bunches + 1, INT32_MAX);
   HJ_CUDA(ctx, cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking));
-  HJ_TRY(dalloc(ctx, &bt->pool_z, (size_t)bt->pool_n));
-  HJ_TRY(dalloc(ctx, &bt->pool_dE, (size_t)bt->pool_n));
-  HJ_TRY(dalloc(ctx, &bt->d_ts, (size_t)max_bunches));
-  HJ_TRY(dalloc(ctx, &bt->d_pass, (size_t)max_bunches));
-  HJ_TRY(dalloc(ctx, &bt->d_bins, (size_t)max_bunches));
-  HJ_TRY(dalloc(ctx, &bt->d_chunks, (size_t)bt->max_chunks));
-  HJ_TRY(dalloc(ctx, &bt->d_items, (size_t)bt->max_chunks));
-  HJ_TRY(dalloc(ctx, &bt->d_counts, 3));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_ts, sizeof(TurnState) * max_bunches));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_pass, sizeof(PassArgs) * max_bunches));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_bins, sizeof(BinsArgs) * max_bunches));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_chunks, sizeof(BatchChunk) * bt->max_chunks));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_items, sizeof(BatchChunk) * bt->max_chunks));
-  HJ_CUDA(ctx, cudaMallocHost((void**)&bt->h_counts, sizeof(int32_t) * 3));
+  // the pool and the tables: one device and one pinned block of the context's cache
+  const size_t nb = (size_t)max_bunches, nc = (size_t)bt->max_chunks;
+  Carve c;
+  const size_t o_z = c.add<double>((size_t)bt->pool_n), o_e = c.add<double>((size_t)bt->pool_n);
+  const size_t o_ts = c.add<TurnState>(nb), o_pass = c.add<PassArgs>(nb);
+  const size_t o_bins = c.add<BinsArgs>(nb), o_ch = c.add<BatchChunk>(nc);
+  const size_t o_it = c.add<BatchChunk>(nc), o_cnt = c.add<int32_t>(3);
+  HJ_TRY(cache_take(ctx, false, c.off, &bt->arena, &bt->arena_cap));
+  char* a = (char*)bt->arena;
+  bt->pool_z = (double*)(a + o_z);
+  bt->pool_dE = (double*)(a + o_e);
+  bt->d_ts = (TurnState*)(a + o_ts);
+  bt->d_pass = (PassArgs*)(a + o_pass);
+  bt->d_bins = (BinsArgs*)(a + o_bins);
+  bt->d_chunks = (BatchChunk*)(a + o_ch);
+  bt->d_items = (BatchChunk*)(a + o_it);
+  bt->d_counts = (int32_t*)(a + o_cnt);
+  Carve h;
+  const size_t p_ts = h.add<TurnState>(nb), p_pass = h.add<PassArgs>(nb);
+  const size_t p_bins = h.add<BinsArgs>(nb), p_ch = h.add<BatchChunk>(nc);
+  const size_t p_it = h.add<BatchChunk>(nc), p_cnt = h.add<int32_t>(3);
+  HJ_TRY(cache_take(ctx, true, h.off, &bt->harena, &bt->harena_cap));
+  char* q = (char*)bt->harena;
+  bt->h_ts = (TurnState*)(q + p_ts);
+  bt->h_pass = (PassArgs*)(q + p_pass);
+  bt->h_bins = (BinsArgs*)(q + p_bins);
+  bt->h_chunks = (BatchChunk*)(q + p_ch);
+  bt->h_items = (BatchChunk*)(q + p_it);
+  bt->h_counts = (int32_t*)(q + p_cnt);
   HJ_CUDA(ctx, cudaMemsetAsync(bt->d_counts, 0, sizeof(int32_t) * 3, bt->stream));
   HJ_CUDA(ctx, cudaMemsetAsync(bt->d_ts, 0, sizeof(TurnState) * max_bunches, bt->stream));
   bt->free_ranges.push_back({0, bt->pool_n});
@@ -1660,8 +1685,7 @@ static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE,
   b->h_ts->turns_left = turns;
   b->ts = bt->d_ts + slot;           // the arena's own TurnState stays unused
   HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
-                               bt->stream));
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+                               bt->stream));   // ordered before the next turn's kernels
   BatchMember m;
   m.id = bt->next_id++;
   m.b = b;
@@ -1748,22 +1772,28 @@ extern "C" hj_status hj_batch_take(hj_batch* bt, int64_t id, double* z_out, doub
   if (k < 0) return set_err(ctx, HJ_ERR_ARG, "no bunch %lld in the batch", (long long)id);
   BatchMember m = bt->members[k];
   hj_bunch* b = m.b;
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  HJ_TRY(launch_moments(b, 1, b->z, b->dE));     // pending kick and re-centring
-  double mom[4];
-  HJ_TRY(read_moments(b, mom));
-  hj_status st = read_state(b);
-  fill_result(b, mom, res);
+  // one round trip: pending kick and re-centring applied in place, moments
+  // and turn state read, particles copied out, and the slot's state set to
+  // "no turns left" for the kernels
+  HJ_TRY(launch_moments(b, 1, b->z, b->dE));
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 4 * b->nblk_m,
+                               cudaMemcpyDeviceToHost, bt->stream));
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->h_ts, b->ts, sizeof(TurnState), cudaMemcpyDeviceToHost,
+                               bt->stream));
   if (z_out)
     HJ_CUDA(ctx, cudaMemcpyAsync(z_out, b->z, sizeof(double) * b->n, cudaMemcpyDefault, bt->stream));
   if (dE_out)
     HJ_CUDA(ctx, cudaMemcpyAsync(dE_out, b->dE, sizeof(double) * b->n, cudaMemcpyDefault,
                                  bt->stream));
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  // retire: this slot's state must read "no turns left" for the kernels
   TurnState dead{};
   dead.turns_left = 0;
-  HJ_CUDA(ctx, cudaMemcpy(b->ts, &dead, sizeof(TurnState), cudaMemcpyHostToDevice));
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, &dead, sizeof(TurnState), cudaMemcpyHostToDevice,
+                               bt->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  double mom[4];
+  sum_moments(b, mom);
+  hj_status st = state_status(b);
+  fill_result(b, mom, res);
   b->ts = nullptr;
   hj_bunch_destroy(b);
   batch_free_range(bt, m.start, m.cap);

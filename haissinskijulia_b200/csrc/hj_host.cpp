@@ -129,12 +129,30 @@ void host_wake_tables(const double* centers, int64_t B, const hj_wake& w, double
 // tw[k] = exp(-2πi k/P) in long double, rounded once.
 // RF kick table of the fused pass: (V sin θm, V cos θm), θm = ϕs - 2π m / M,
 // m = 0..M-1, in extended precision and rounded once.
+// The extended-precision (sin θm, cos θm) of a phase are kept per (ϕs, M):
+// bunches of a voltage scan share ϕs.
 void host_rf_table(double V, double phi_s, int64_t M, double* tab_interleaved) {
-  const long double kPiL = 3.141592653589793238462643383279502884L;
+  static std::mutex mu;
+  static std::map<std::pair<uint64_t, int64_t>, std::vector<long double>> cache;
+  uint64_t bits;
+  std::memcpy(&bits, &phi_s, sizeof(bits));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find({bits, M});
+  if (it == cache.end()) {
+    if (cache.size() >= 64) cache.clear();
+    const long double kPiL = 3.141592653589793238462643383279502884L;
+    std::vector<long double> sc(2 * (size_t)M);
+    for (int64_t m = 0; m < M; ++m) {
+      const long double a = (long double)phi_s - 2.0L * kPiL * (long double)m / (long double)M;
+      sc[2 * m] = sinl(a);
+      sc[2 * m + 1] = cosl(a);
+    }
+    it = cache.insert({{bits, M}, std::move(sc)}).first;
+  }
+  const std::vector<long double>& sc = it->second;
   for (int64_t m = 0; m < M; ++m) {
-    const long double a = (long double)phi_s - 2.0L * kPiL * (long double)m / (long double)M;
-    tab_interleaved[2 * m] = (double)((long double)V * sinl(a));
-    tab_interleaved[2 * m + 1] = (double)((long double)V * cosl(a));
+    tab_interleaved[2 * m] = (double)((long double)V * sc[2 * m]);
+    tab_interleaved[2 * m + 1] = (double)((long double)V * sc[2 * m + 1]);
   }
 }
 
