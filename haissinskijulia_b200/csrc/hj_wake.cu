@@ -190,12 +190,15 @@ __device__ void smem_fft(double2* s, FftTables t, int N, int logN) {
   else if (rem == 1) stockham_pass<1, INV, NT, MAXH>(s, t, N, Ns);
 }
 
-// Twiddle tables of the length-H transform into shared memory (w_H^j = twP[4j]).
-__device__ void load_twiddles(double2* tw, double2* ct, int H, const double2* __restrict__ twP) {
-  for (int j = threadIdx.x; j < (H >> 1); j += blockDim.x) tw[j] = __ldg(&twP[4 * j]);
-  for (int Ns = 1; 8 * Ns <= H; Ns <<= 3) {
-    const int off = (Ns - 1) / 7, stride = H / (8 * Ns);
-    for (int jm = threadIdx.x; jm < Ns; jm += blockDim.x) ct[off + jm] = __ldg(&twP[4 * jm * stride]);
+// Twiddle tables of a length-N transform into shared memory, w_N^j =
+// twP[step j] with step = P/N (4 for the length-H transforms).
+__device__ void load_twiddles(double2* tw, double2* ct, int N, const double2* __restrict__ twP,
+                              int step = 4) {
+  for (int j = threadIdx.x; j < (N >> 1); j += blockDim.x) tw[j] = __ldg(&twP[step * j]);
+  for (int Ns = 1; 8 * Ns <= N; Ns <<= 3) {
+    const int off = (Ns - 1) / 7, stride = N / (8 * Ns);
+    for (int jm = threadIdx.x; jm < Ns; jm += blockDim.x)
+      ct[off + jm] = __ldg(&twP[step * jm * stride]);
   }
   __syncthreads();
 }
@@ -315,20 +318,25 @@ __device__ __forceinline__ double global_std(double s, double s2, int64_t n) {
   return sqrt(sv);
 }
 
-// The bins step as a cluster of two CTAs.  With k even (CTA 0) or odd (CTA 1),
-// X[k], its partner X[M-k], the spectrum product and the inverse input Z[k]
-// all have the same parity, so each CTA runs one forward length-H FFT, its
-// half of the spectrum and one inverse length-H FFT in its own shared memory;
-// the halves are combined through distributed shared memory.
-template <int NT, int MAXH = kMaxFftH>
+// The bins step as a cluster of C = 2 or 4 CTAs; CTA r owns the spectrum
+// entries k = r (mod C).  Since x[n] = 0 for n >= H = M/2,
+//   X[Cm + r] = FFT_L(y_r)[m],  y_r[n] = Σ_{t<C/2} x[n + tL] w_M^{(n + tL) r},
+// L = M/C, so each CTA runs one forward and one inverse length-L FFT in its own
+// shared memory.  The partner X[M-k] of a spectrum pair has residue -r: for
+// C = 2 it is in the same CTA (each pair is formed in place); for C = 4 CTAs 1
+// and 3 read each other's through distributed shared memory.  The inverse
+// outputs z[n] = Σ_r w_M^{-nr} ẑ_r[n mod L], n < H, are combined through
+// distributed shared memory, a quarter (C = 4) or half (C = 2) per CTA.
+template <int NT, int MAXH = kMaxFftH, int C = 2>
 __device__ __forceinline__ void bins_body(const BinsArgs& a) {
+  static_assert(C == 2 || C == 4, "two or four CTAs per cluster");
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   extern __shared__ __align__(16) double2 s_fft[];
   __shared__ double red[NT / 32];
   __shared__ double sh[8];
-  __shared__ double s_peer_sum;
+  __shared__ double s_peer_sum[C];
 
   // 1. partial sums of the particle pass, fixed block order (both CTAs)
   //    sh[0..3] = Σz, Σz², Σ(ΔE - ΔE_start), particles inside the bin range
@@ -371,24 +379,97 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
   double sum_kick = 0.0;
 
   if (a.use_wake) {
-    if (do_conv && a.H >= 4) {
+    if (do_conv && a.H >= (C == 2 ? 4 : 8)) {
       const int H = a.H, M = a.M;
+      const int L = M / C, logL = a.logH - (C == 2 ? 0 : 1);
       double2* s = s_fft;
-      double2* s_tw = s_fft + H;
-      double2* s_ct = s_tw + H / 2;
+      double2* s_tw = s_fft + L;
+      double2* s_ct = s_tw + L / 2;
       const FftTables tb{s_tw, s_ct};
-      load_twiddles(s_tw, s_ct, H, a.twP);
+      load_twiddles(s_tw, s_ct, L, a.twP, 2 * C);              // w_L^j = w_P^{2Cj}
       const double inv_n = 1.0 / sh[3];                          // src/wakefield.jl:207
       const DensityVals g{a.cnt, a.lam, inv_n};
-      // x[n] = g[2n] + i g[2n+1] (times w_M^n in the odd CTA)
+      // y_r[n] = Σ_t x[n + tL] w_M^{(n + tL) r}, x[n] = g[2n] + i g[2n+1]
 #pragma unroll 8
-      for (int n = threadIdx.x; n < H; n += NT) {
-        const int j = 2 * n;
-        const double2 x = make_double2(j < a.B ? g(j) : 0.0, j + 1 < a.B ? g(j + 1) : 0.0);
-        s[n] = rank ? cmul(x, __ldg(&a.twP[2 * n])) : x;
+      for (int n = threadIdx.x; n < L; n += NT) {
+        double2 y = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int t = 0; t < C / 2; ++t) {
+          const int nn = n + t * L;
+          const int j = 2 * nn;
+          const double2 x = make_double2(j < a.B ? g(j) : 0.0, j + 1 < a.B ? g(j + 1) : 0.0);
+          const double2 xr = rank ? cmul(x, __ldg(&a.twP[(2 * nn * rank) & (a.P - 1)])) : x;
+          if (t == 0) y = xr;
+          else y = cadd(y, xr);
+        }
+        s[n] = y;
       }
       __syncthreads();
-      smem_fft<false, NT, MAXH>(s, tb, H, a.logH);                         // s[m] = X[2m + rank]
+      smem_fft<false, NT, MAXH>(s, tb, L, logL);                           // s[m] = X[Cm + rank]
+      if constexpr (C == 4) {
+        // spectrum of this residue from X[k] here and X[M-k] in the CTA of
+        // residue -rank; Z[k] kept in registers until every CTA has read
+        constexpr int PER = (MAXH + NT - 1) / NT;                 // L <= MAXH
+        cluster.sync();
+        const int pr = (C - rank) % C;
+        const double2* sp = cluster.map_shared_rank(s_fft, pr);
+        double2 zk[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int m = threadIdx.x + u * NT;
+          if (m < L) {
+            const int k = C * m + rank;
+            const int kp = (M - k) & (M - 1);                     // M-k, X[M] = X[0]
+            const double2 xk = s[m], xm = sp[(kp - pr) / C];
+            const double2 tk = k <= M / 2 ? __ldg(&a.twP[k])
+                                          : make_double2(-__ldg(&a.twP[M - k]).x,
+                                                         __ldg(&a.twP[M - k]).y);
+            const double2 tm = make_double2(-tk.x, tk.y);       // w_P^{M-k}
+            double2 E = make_double2(0.5 * (xk.x + xm.x), 0.5 * (xk.y - xm.y));
+            double2 D = make_double2(0.5 * (xk.x - xm.x), 0.5 * (xk.y + xm.y));
+            const double2 Gk = cadd(E, cmul(tk, make_double2(D.y, -D.x)));
+            E = make_double2(0.5 * (xm.x + xk.x), 0.5 * (xm.y - xk.y));
+            D = make_double2(0.5 * (xm.x - xk.x), 0.5 * (xm.y + xk.y));
+            const double2 Gm = cadd(E, cmul(tm, make_double2(D.y, -D.x)));
+            double2 Yk = cmul(Gk, __ldg(&a.Wf[k]));
+            double2 Ym = cmul(Gm, __ldg(&a.Wf[M - k]));
+            Yk.x *= current;
+            Yk.y *= current;
+            Ym.x *= current;
+            Ym.y *= current;
+            const double2 Ez = make_double2(0.5 * (Yk.x + Ym.x), 0.5 * (Yk.y - Ym.y));
+            const double2 Dz = make_double2(0.5 * (Yk.x - Ym.x), 0.5 * (Yk.y + Ym.y));
+            const double2 Oz = cmul(Dz, cconj(tk));
+            zk[u] = make_double2(Ez.x - Oz.y, Ez.y + Oz.x);
+          }
+        }
+        cluster.sync();
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int m = threadIdx.x + u * NT;
+          if (m < L) s[m] = zk[u];
+        }
+        __syncthreads();
+        smem_fft<true, NT, MAXH>(s, tb, L, logL);                          // unnormalised inverse
+        cluster.sync();
+        // z[n] = Σ_r conj(w_M^{nr}) ẑ_r[n mod L] / M, n in this CTA's quarter of [0, H)
+        const double invM = 1.0 / (double)M;
+        const double2* sr[C];
+#pragma unroll
+        for (int r = 0; r < C; ++r) sr[r] = cluster.map_shared_rank(s_fft, r);
+        const int n0 = rank * (H / C), n1 = n0 + H / C;
+#pragma unroll 2
+        for (int n = n0 + threadIdx.x; n < n1; n += NT) {
+          const int nl = n & (L - 1);
+          double2 z = sr[0][nl];
+#pragma unroll
+          for (int r = 1; r < C; ++r)
+            z = cadd(z, cmul(sr[r][nl], cconj(__ldg(&a.twP[(2 * n * r) & (a.P - 1)]))));
+          const int j = 2 * n;
+          if (j < a.B) a.pot[j] = z.x * invM;
+          if (j + 1 < a.B) a.pot[j + 1] = z.y * invM;
+        }
+      } else {
       // spectrum pairs (k, M-k) of this parity, in place
       const int mlast = rank ? H / 2 - 1 : H / 2;
       for (int m = threadIdx.x; m <= mlast; m += NT) {
@@ -422,7 +503,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
         s[m] = Zk;
       }
       __syncthreads();
-      smem_fft<true, NT, MAXH>(s, tb, H, a.logH);                          // unnormalised inverse
+      smem_fft<true, NT, MAXH>(s, tb, L, logL);                            // unnormalised inverse
       cluster.sync();
       // z[n] = (zE[n] + conj(w_M^n) zO[n]) / M, pot[2n] = Re z, pot[2n+1] = Im z
       const double2* sE = cluster.map_shared_rank(s_fft, 0);
@@ -437,6 +518,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
         if (j < a.B) a.pot[j] = (ze.x + zo.x) * invM;
         if (j + 1 < a.B) a.pot[j + 1] = (ze.y + zo.y) * invM;
       }
+      }
     } else if (do_conv) {
       // Tiny grids (P < 16): direct causal convolution in CTA 0.
       if (rank == 0 && threadIdx.x == 0) {
@@ -449,7 +531,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
         }
       }
     } else {
-      for (int i = rank * NT + threadIdx.x; i < a.B; i += 2 * NT) a.pot[i] = 0.0;
+      for (int i = rank * NT + threadIdx.x; i < a.B; i += C * NT) a.pot[i] = 0.0;
     }
     cluster.sync();   // pot complete; the peer is done reading this CTA's shared memory
     // Kick table of the next pass, B + 1 cells: cell j in 1..B-1 spans centres
@@ -462,9 +544,9 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
     //   Σ_i lerp(pot, z_i) = Σ_j C[j] pot_j + 2^-24 Σ_j S[j] step_j.
     if (a.potd || a.cic) {
       const int nc = a.B + 1;
-      const int half = (nc + 1) / 2;
-      const int j1 = min(nc, (rank + 1) * half);
-      for (int j = rank * half + threadIdx.x; j < j1; j += blockDim.x) {
+      const int part = (nc + C - 1) / C;
+      const int j1 = min(nc, (rank + 1) * part);
+      for (int j = rank * part + threadIdx.x; j < j1; j += blockDim.x) {
         double p0 = a.pot[j > 0 ? j - 1 : 0];
         if (j == a.B && a.B >= 2)
           p0 = __dadd_rn(__dmul_rn(a.pot[a.hi_idx], __dsub_rn(1.0, a.hi_w)),
@@ -476,12 +558,12 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
     }
   }
   sum_kick = block_sum(sum_kick, red);
-  if (rank == 1 && threadIdx.x == 0) *cluster.map_shared_rank(&s_peer_sum, 0) = sum_kick;
+  if (rank > 0 && threadIdx.x == 0) *cluster.map_shared_rank(&s_peer_sum[rank], 0) = sum_kick;
   cluster.sync();
 
   // E0 update and next-turn scalars (src/evolution.jl:401-451, :300-304)
   if (rank == 0 && threadIdx.x == 0 && !a.conv_only) {
-    sum_kick += s_peer_sum;
+    for (int r = 1; r < C; ++r) sum_kick += s_peer_sum[r];
     const double E0 = ts->cur.E0;
     double mean = 0.0;
     if (a.params.update_E0) mean = (sh[2] - sum_kick) / (double)a.n;
@@ -505,6 +587,12 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins(BinsArgs a) {
   bins_body<kBinsThreads>(a);
+}
+
+// Four CTAs, length-L = M/4 transforms (at most kMaxFftH / 2).
+constexpr int kBins4MinH = 1024;
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins4(BinsArgs a) {
+  bins_body<kBinsThreads, kMaxFftH / 2, 4>(a);
 }
 
 // The bins step of a batch: cluster i (CTAs 2i, 2i+1) runs bunch i; slots
@@ -531,6 +619,7 @@ constexpr int kBatchBinsSmallMaxH = 2048;
 
 cudaError_t prepare_wake_kernels(int max_smem) {
   cudaError_t e = allow_dynamic_smem((const void*)k_bins, max_smem);
+  if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_bins4, max_smem);
   if (e == cudaSuccess)
     e = allow_dynamic_smem((const void*)k_batch_bins<kBinsThreads, kMaxFftH, 1>, max_smem);
   if (e == cudaSuccess)
@@ -555,8 +644,11 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
 }
 
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st) {
-  size_t smem = bins_smem_bytes(a.H);
-  k_bins<<<2, kBinsThreads, smem, st>>>(a);
+  if (a.H >= kBins4MinH) {
+    k_bins4<<<4, kBinsThreads, bins_smem_bytes(a.M / 4), st>>>(a);
+  } else {
+    k_bins<<<2, kBinsThreads, bins_smem_bytes(a.H), st>>>(a);
+  }
   return cudaGetLastError();
 }
 
