@@ -329,7 +329,8 @@ __device__ __forceinline__ double global_std(double s, double s2, int64_t n) {
 // distributed shared memory, a quarter (C = 4) or half (C = 2) per CTA.
 template <int NT, int MAXH = kMaxFftH, int C = 2>
 __device__ __forceinline__ void bins_body(const BinsArgs& a) {
-  static_assert(C == 2 || C == 4, "two or four CTAs per cluster");
+  static_assert(C == 2 || C == 4 || C == 8, "two, four or eight CTAs per cluster");
+  constexpr int kLogC = C == 2 ? 1 : (C == 4 ? 2 : 3);
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
@@ -379,9 +380,9 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
   double sum_kick = 0.0;
 
   if (a.use_wake) {
-    if (do_conv && a.H >= (C == 2 ? 4 : 8)) {
+    if (do_conv && a.H >= 2 * C) {
       const int H = a.H, M = a.M;
-      const int L = M / C, logL = a.logH - (C == 2 ? 0 : 1);
+      const int L = M / C, logL = a.logH + 1 - kLogC;
       double2* s = s_fft;
       double2* s_tw = s_fft + L;
       double2* s_ct = s_tw + L / 2;
@@ -406,7 +407,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
       }
       __syncthreads();
       smem_fft<false, NT, MAXH>(s, tb, L, logL);                           // s[m] = X[Cm + rank]
-      if constexpr (C == 4) {
+      if constexpr (C >= 4) {
         // spectrum of this residue from X[k] here and X[M-k] in the CTA of
         // residue -rank; Z[k] kept in registers until every CTA has read
         constexpr int PER = (MAXH + NT - 1) / NT;                 // L <= MAXH
@@ -595,6 +596,12 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kBinsThreads, 1) k_b
   bins_body<kBinsThreads, kMaxFftH / 2, 4>(a);
 }
 
+// Eight CTAs, length-L = M/8 transforms.
+constexpr int kBins8MinH = 4096;
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins8(BinsArgs a) {
+  bins_body<kBinsThreads, kMaxFftH / 4, 8>(a);
+}
+
 // The bins step of a batch: cluster i (CTAs 2i, 2i+1) runs bunch i; slots
 // past the live count and bunches with no turns left return at once (both
 // CTAs of a cluster read the same state before either writes it, so they agree).
@@ -620,6 +627,7 @@ constexpr int kBatchBinsSmallMaxH = 2048;
 cudaError_t prepare_wake_kernels(int max_smem) {
   cudaError_t e = allow_dynamic_smem((const void*)k_bins, max_smem);
   if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_bins4, max_smem);
+  if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_bins8, max_smem);
   if (e == cudaSuccess)
     e = allow_dynamic_smem((const void*)k_batch_bins<kBinsThreads, kMaxFftH, 1>, max_smem);
   if (e == cudaSuccess)
@@ -644,7 +652,9 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
 }
 
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st) {
-  if (a.H >= kBins4MinH) {
+  if (a.H >= kBins8MinH) {
+    k_bins8<<<8, kBinsThreads, bins_smem_bytes(a.M / 8), st>>>(a);
+  } else if (a.H >= kBins4MinH) {
     k_bins4<<<4, kBinsThreads, bins_smem_bytes(a.M / 4), st>>>(a);
   } else {
     k_bins<<<2, kBinsThreads, bins_smem_bytes(a.H), st>>>(a);
