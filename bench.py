@@ -265,13 +265,18 @@ def measure_sweeps(ctx, args) -> dict:
     }
     scan = intensity_scan(turns=T)
     t0 = time.perf_counter()
-    run_batched(ctx, scan, tuning=tun, block_turns=500)
+    tun_i = autotune(ctx, scan, trial_turns=32, sample=len(scan))
+    t_tune_i = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    run_batched(ctx, scan, tuning=tun_i, block_turns=500)
     t_scan = time.perf_counter() - t0
     out["intensity_scan"] = {
         "config": f"32 bunches x 1e6 particles, populations log-spaced 1e9-1e11, {T} turns, "
                   "8192 bins, one batch",
         "solves_per_s": len(scan) / t_scan, "seconds": t_scan,
-        "particle_turns_per_s": sum(p.n * p.turns for p in scan) / t_scan}
+        "particle_turns_per_s": sum(p.n * p.turns for p in scan) / t_scan,
+        "tuning": {"particles_per_block": tun_i.chunk, "layout": tun_i.layout,
+                   "graph_turns": tun_i.graph_turns, "autotune_seconds": t_tune_i}}
     if args.serve_requests > 0:
         reqs = request_stream(args.serve_requests)
         rep = serve(ctx, reqs, tuning=tun)

@@ -1370,6 +1370,7 @@ struct hj_batch {
   void* harena = nullptr;
   size_t harena_cap = 0;
   bool dirty = true;
+  int bins_ctas = 2;                           // CTAs per bunch in the bins step
   int graph_turns = 16;
   cudaGraphExec_t graph = nullptr;
   int64_t turns_enqueued = 0;
@@ -1491,7 +1492,7 @@ hj_status batch_launch_turn(hj_batch* bt) {
     HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_items, bt->d_counts + 2, bt->grid_items,
                                      bt->max_B, bt->stream));
   HJ_CUDA(ctx, launch_batch_bins(bt->d_bins, bt->d_counts + 1, bt->grid_bunches, bt->max_H,
-                                 bt->stream));
+                                 bt->bins_ctas, bt->stream));
   return HJ_OK;
 }
 
@@ -1547,6 +1548,7 @@ static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t 
   bt->max_B = max_nbins;
   const int64_t P = next_pow2(2 * (int64_t)max_nbins);
   bt->max_H = (int)std::max<int64_t>(P / 4, 4);
+  bt->bins_ctas = batch_bins_ctas(bt->max_H, max_bunches, ctx->num_sms);
   bt->cfg = layout >= 0 ? layout : default_pass_layout(max_nbins, pool_particles);
   bt->pool_n = (pool_particles + 3) / 4 * 4;
   bt->max_chunks = (int)std::min<int64_t>(bt->pool_n / chunk + max_bunches + 1, INT32_MAX);

@@ -182,8 +182,9 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
                                  const double2* twP, double2* Xg, double2* Wf,
                                  cudaStream_t st);
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st);
+int batch_bins_ctas(int max_H, int max_bunches, int num_sms);
 cudaError_t launch_batch_bins(const BinsArgs* d_bunches, const int32_t* d_n_bunches,
-                              int max_bunches, int max_H, cudaStream_t st);
+                              int max_bunches, int max_H, int ctas, cudaStream_t st);
 size_t bins_smem_bytes(int H);
 
 // ---- context access for entry points outside hj_api.cu ----

@@ -602,17 +602,17 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(kBinsThreads, 1) k_b
   bins_body<kBinsThreads, kMaxFftH / 4, 8>(a);
 }
 
-// The bins step of a batch: cluster i (CTAs 2i, 2i+1) runs bunch i; slots
-// past the live count and bunches with no turns left return at once (both
-// CTAs of a cluster read the same state before either writes it, so they agree).
-template <int NT, int MAXH, int MINB>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, MINB)
+// The bins step of a batch: cluster i (CTAs Ci .. Ci + C - 1) runs bunch i;
+// slots past the live count and bunches with no turns left return at once
+// (the CTAs of a cluster read the same state before any writes it, so they agree).
+template <int NT, int MAXH, int MINB, int C = 2>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, MINB)
     k_batch_bins(const BinsArgs* __restrict__ bunches, const int32_t* __restrict__ n_bunches) {
-  const int i = (int)(blockIdx.x >> 1);
+  const int i = (int)(blockIdx.x / C);
   if (i >= *n_bunches) return;
   const BinsArgs& a = bunches[i];
   if (a.ts->turns_left <= 0) return;
-  bins_body<NT, MAXH>(a);
+  bins_body<NT, MAXH, C>(a);
 }
 
 // The batched bins step for H <= 2048 (up to 4096 bins): a radix-8 pass of a
@@ -630,6 +630,9 @@ cudaError_t prepare_wake_kernels(int max_smem) {
   if (e == cudaSuccess) e = allow_dynamic_smem((const void*)k_bins8, max_smem);
   if (e == cudaSuccess)
     e = allow_dynamic_smem((const void*)k_batch_bins<kBinsThreads, kMaxFftH, 1>, max_smem);
+  if (e == cudaSuccess)
+    e = allow_dynamic_smem((const void*)k_batch_bins<kBinsThreads, kMaxFftH / 2, 1, 4>,
+                           max_smem);
   if (e == cudaSuccess)
     e = allow_dynamic_smem(
         (const void*)k_batch_bins<kBatchBinsSmallThreads, kBatchBinsSmallMaxH, 4>, max_smem);
@@ -662,11 +665,21 @@ cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// CTAs per bunch of a batch's bins step, fixed when the batch is created so
+// that a bunch's arithmetic does not depend on which bunches share it: four
+// for large grids when every slot's cluster still fits in one wave, else two.
+int batch_bins_ctas(int max_H, int max_bunches, int num_sms) {
+  return (max_H >= kBins4MinH && 4 * max_bunches <= num_sms) ? 4 : 2;
+}
+
 cudaError_t launch_batch_bins(const BinsArgs* d_bunches, const int32_t* d_n_bunches,
-                              int max_bunches, int max_H, cudaStream_t st) {
+                              int max_bunches, int max_H, int ctas, cudaStream_t st) {
   size_t smem = bins_smem_bytes(max_H);
   const int grid = 2 * (max_bunches > 0 ? max_bunches : 1);
-  if (max_H <= kBatchBinsSmallMaxH)
+  if (ctas == 4) {
+    k_batch_bins<kBinsThreads, kMaxFftH / 2, 1, 4>
+        <<<2 * grid, kBinsThreads, bins_smem_bytes(max_H / 2), st>>>(d_bunches, d_n_bunches);
+  } else if (max_H <= kBatchBinsSmallMaxH)
     k_batch_bins<kBatchBinsSmallThreads, kBatchBinsSmallMaxH, 4>
         <<<grid, kBatchBinsSmallThreads, smem, st>>>(d_bunches, d_n_bunches);
   else

@@ -181,12 +181,29 @@ def run_plain(ctx: Context, points: List[Point], copy_out: bool = False) -> List
     return out
 
 
+def wave_chunks(points: List[Point], num_sms: int, waves=(1, 2, 4)) -> List[int]:
+    """Particles per block that split the whole workload into `waves` full
+    waves of `num_sms` blocks (rounded up to a multiple of 4)."""
+    total = sum(p.n for p in points)
+    out = []
+    for w in waves:
+        c = -(-total // (num_sms * w))
+        c = min(max((c + 3) // 4 * 4, 4096), 1 << 22)
+        out.append(int(c))
+    return out
+
+
 def autotune(ctx: Context, points: List[Point], *, trial_turns: int = 64,
-             chunks=(16384, 65536, 262144), layouts=(0, 1), graph_turns=(8, 32),
+             chunks=None, layouts=(0, 1), graph_turns=(8, 32),
              sample: int = 64) -> Tuning:
     """Times each candidate (particles per block, pass layout, graph turns) on
     up to `sample` of the points for `trial_turns` turns after a warm-up and
-    returns the fastest."""
+    returns the fastest.  Default block sizes: 16K, 64K, 256K particles and
+    those that fill one, two or four waves of the GPU with the whole workload."""
+    if chunks is None:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        chunks = sorted(set((16384, 65536, 262144, *wave_chunks(points, sms))))
     pts = points[:sample]
     pool = sum(p.n + 4 for p in pts)
     best, best_t = Tuning(), float("inf")
