@@ -9,6 +9,29 @@
 
 namespace hj {
 
+// The per-turn kernels of a bunch are launched with programmatic stream
+// serialisation: each may be scheduled while the previous kernel on the
+// stream drains, and starts with grid_dependency_wait(), which returns once
+// that kernel has completed and its memory is visible.
+__device__ __forceinline__ void grid_dependency_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+struct PdlConfig {
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1];
+  PdlConfig(dim3 grid, dim3 block, size_t smem, cudaStream_t st) {
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+};
+
 constexpr int kNumSums = 4;         // per-block partial sums of the particle pass
 constexpr int kTrackThreads = 512;  // threads per block of the particle kernels
 constexpr int kBinsThreads = 1024;  // threads of the single-CTA bins kernel

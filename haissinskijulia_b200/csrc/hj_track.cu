@@ -509,6 +509,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1>
 __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  grid_dependency_wait();
   if (WAKE) {  // zero the merged histograms k_hist_reduce accumulates into this turn
     const int gstride = gridDim.x * THREADS;
     for (int i = blockIdx.x * THREADS + threadIdx.x; i < 3 * a.B + 2; i += gstride)
@@ -550,6 +551,7 @@ __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
                               const unsigned long long* __restrict__ part_cic, int nblk, int B,
                               unsigned long long* __restrict__ out,
                               unsigned long long* __restrict__ ovf) {
+  grid_dependency_wait();
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = B + 1;
   if (b >= (part_cic ? nc : B)) return;
@@ -988,8 +990,8 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg) {
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
   const size_t smem = track_smem_bytes(a.B, a.use_wake);
   void* args[] = {const_cast<PassArgs*>(&a)};
-  return cudaLaunchKernel(pass_fn(a.use_wake, a.qe_mode, a.cfg), dim3(grid),
-                          dim3(pass_cfg_threads(a.cfg)), args, smem, st);
+  PdlConfig l(dim3(grid), dim3(pass_cfg_threads(a.cfg)), smem, st);
+  return cudaLaunchKernelExC(&l.cfg, pass_fn(a.use_wake, a.qe_mode, a.cfg), args);
 }
 
 cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
@@ -1034,7 +1036,9 @@ cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long lon
   }
   const int G = nblk < 16 ? nblk : 16;
   dim3 grid((B + 1 + 255) / 256, G > 0 ? G : 1);
-  k_hist_reduce<<<grid, 256, 0, st>>>(part_cnt, part_cic, nblk, B, out, ovf);
+  PdlConfig l(grid, dim3(256), 0, st);
+  cudaError_t e = cudaLaunchKernelEx(&l.cfg, k_hist_reduce, part_cnt, part_cic, nblk, B, out, ovf);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

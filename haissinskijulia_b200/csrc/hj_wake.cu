@@ -587,18 +587,21 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins(BinsArgs a) {
+  grid_dependency_wait();
   bins_body<kBinsThreads>(a);
 }
 
 // Four CTAs, length-L = M/4 transforms (at most kMaxFftH / 2).
 constexpr int kBins4MinH = 1024;
 __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins4(BinsArgs a) {
+  grid_dependency_wait();
   bins_body<kBinsThreads, kMaxFftH / 2, 4>(a);
 }
 
 // Eight CTAs, length-L = M/8 transforms.
 constexpr int kBins8MinH = 4096;
 __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(kBinsThreads, 1) k_bins8(BinsArgs a) {
+  grid_dependency_wait();
   bins_body<kBinsThreads, kMaxFftH / 4, 8>(a);
 }
 
@@ -656,13 +659,15 @@ cudaError_t launch_wake_spectrum(const double* W, int B, int P, int M, int H, in
 
 cudaError_t launch_bins(const BinsArgs& a, cudaStream_t st) {
   if (a.H >= kBins8MinH) {
-    k_bins8<<<8, kBinsThreads, bins_smem_bytes(a.M / 8), st>>>(a);
-  } else if (a.H >= kBins4MinH) {
-    k_bins4<<<4, kBinsThreads, bins_smem_bytes(a.M / 4), st>>>(a);
-  } else {
-    k_bins<<<2, kBinsThreads, bins_smem_bytes(a.H), st>>>(a);
+    PdlConfig l(dim3(8), dim3(kBinsThreads), bins_smem_bytes(a.M / 8), st);
+    return cudaLaunchKernelEx(&l.cfg, k_bins8, a);
   }
-  return cudaGetLastError();
+  if (a.H >= kBins4MinH) {
+    PdlConfig l(dim3(4), dim3(kBinsThreads), bins_smem_bytes(a.M / 4), st);
+    return cudaLaunchKernelEx(&l.cfg, k_bins4, a);
+  }
+  PdlConfig l(dim3(2), dim3(kBinsThreads), bins_smem_bytes(a.H), st);
+  return cudaLaunchKernelEx(&l.cfg, k_bins, a);
 }
 
 // CTAs per bunch of a batch's bins step, fixed when the batch is created so
