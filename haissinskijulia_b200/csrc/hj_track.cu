@@ -973,10 +973,12 @@ int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
 }
 
 // Blocks of the particle pass: enough to fill the GPU, but each block should
-// own at least ~2 bins' worth of histogram traffic per particle it moves.
+// move at least B/2 particles, since it writes a B-bin partial histogram
+// that the merge reads back (B/2 measured best for 1e5-1e7 particles at 4096
+// and 16384 bins).
 int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg) {
   int64_t per_block = (int64_t)pass_cfg_ppt(cfg) * pass_cfg_threads(cfg);
-  if (per_block < 2 * (int64_t)B) per_block = 2 * (int64_t)B;
+  if (per_block < (int64_t)B / 2) per_block = (int64_t)B / 2;
   int64_t g = (n + per_block - 1) / per_block;
   int64_t cap = (int64_t)num_sms * blocks_per_sm;
   if (g > cap) g = cap;

@@ -255,6 +255,28 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;  // valid in thread 0
 }
 
+// Four block_sum's at once (one pair of barriers): each value is summed in
+// block_sum's order, so the results are the same.  Valid in thread 0.
+__device__ __forceinline__ void block_sum4(double (&v)[4], double (*red4)[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) red4[warp][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red4[w][k];
+      v[k] = s;
+    }
+}
+
 struct WakeVals {
   const double* W;
   __device__ double operator()(int j) const { return W[j]; }
@@ -342,14 +364,16 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
   // 1. partial sums of the particle pass, fixed block order (both CTAs)
   //    sh[0..3] = Σz, Σz², Σ(ΔE - ΔE_start), particles inside the bin range
   if (!a.conv_only) {
+    static_assert(kNumSums == 4, "four partial sums per block");
+    __shared__ double red4[NT / 32][4];
     double t[kNumSums] = {0.0, 0.0, 0.0, 0.0};
     for (int b = threadIdx.x; b < a.nblk; b += blockDim.x)
 #pragma unroll
       for (int k = 0; k < kNumSums; ++k) t[k] += a.part_sum[(size_t)b * kNumSums + k];
-    for (int k = 0; k < kNumSums; ++k) {
-      double v = block_sum(t[k], red);
-      if (threadIdx.x == 0) sh[k] = v;
-    }
+    block_sum4(t, red4);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int k = 0; k < kNumSums; ++k) sh[k] = t[k];
   } else {
     double t = 0.0;
     for (int i = threadIdx.x; i < a.B; i += blockDim.x) t += (double)a.cnt[i];
