@@ -198,12 +198,16 @@ def autotune(ctx: Context, points: List[Point], *, trial_turns: int = 64,
              sample: int = 64) -> Tuning:
     """Times each candidate (particles per block, pass layout, graph turns) on
     up to `sample` of the points for `trial_turns` turns after a warm-up and
-    returns the fastest.  Default block sizes: 16K, 64K, 256K particles and
-    those that fill one, two or four waves of the GPU with the whole workload."""
+    returns the fastest.  Default block sizes: 16K, 64K, 256K particles and,
+    when the trial runs the whole workload, those that fill one, two or four
+    waves of the GPU with it (on a sample they would be sized for the sample)."""
     if chunks is None:
-        import torch
-        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-        chunks = sorted(set((16384, 65536, 262144, *wave_chunks(points, sms))))
+        chunks = [16384, 65536, 262144]
+        if len(points) <= sample:
+            import torch
+            dev = torch.cuda.current_device()
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            chunks = sorted(set(chunks + wave_chunks(points, sms)))
     pts = points[:sample]
     pool = sum(p.n + 4 for p in pts)
     best, best_t = Tuning(), float("inf")
