@@ -227,7 +227,8 @@ class Context:
 
     def set_pass_layout(self, layout: int) -> None:
         """Thread layout of the fused pass for bunches created afterwards
-        (-1 = automatic; 0, 1, 2 = fixed layouts)."""
+        (-1 = automatic; 0-4 = fixed layouts with 16-bit bin counters, 8-12
+        the same with 32-bit counters; see hj_set_pass_layout)."""
         _check(self, self._lib.hj_set_pass_layout(self.handle, int(layout)))
 
     def trim(self) -> None:

@@ -44,10 +44,13 @@ constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 // group prefetched into registers except in 3): 0 = 4 x 512, 1 = 2 x 1024,
 // 2 = 2 x 768, 3 = 2 x 512 without prefetch, 4 = 2 x 512 at 64 registers (two
 // blocks per SM where shared memory allows).
-constexpr int kNumPassCfgs = 5;
+constexpr int kNumPassCfgs = 5;       // thread layouts of the fused pass
+constexpr int kPassLayoutMask = 7;    // layout bits of a pass configuration
+constexpr int kPassN32 = 8;           // + one 32-bit NGP counter per bin (else 16-bit pairs)
 constexpr int kRfTableSize = 128;    // entries of the fused pass's RF kick table
 constexpr int kLogHeader = 8;       // doubles before the bin counts in a turn-log record
 int pass_cfg_threads(int cfg);
+bool pass_cfg_valid(int cfg);
 int pass_cfg_ppt(int cfg);
 
 // Quantum-excitation source of the particle pass.
@@ -150,7 +153,7 @@ cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin);
 cudaError_t prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
 int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg);
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
-size_t track_smem_bytes(int B, int use_wake);
+size_t track_smem_bytes(int B, int use_wake, int cfg);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
 // Batched pass over a chunk table (*d_n_chunks entries live, grid max_chunks)
 // and the per-bunch merge of its partials.

@@ -240,7 +240,7 @@ __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
 // SR, drift, moments and the deposits.  Without update_η the drift
 // coefficient is the constant-η one (zero when apply_phase_advance! would
 // skip the advance).
-template <bool WAKE>
+template <bool WAKE, bool N32>
 __device__ __forceinline__ void pass_particle(double& z, double& e, double r, double kick,
                                               double rf, const FusedConst& c,
                                               const GridConst& g, double pmean, double& acc_z,
@@ -266,14 +266,18 @@ __device__ __forceinline__ void pass_particle(double& z, double& e, double r, do
     bool in;
     const int j = ngp_bin(z, g, in);
     if (in) {
-      // 16-bit counters, two bins per word; the increment that takes a counter
-      // to 2^15 moves 2^15 counts to the global overflow array (at most 1024
-      // more increments can land before the move, so the counter never wraps)
-      const int sh = (j & 1) << 4;
-      const uint32_t old = atomicAdd(&s_ngp[j >> 1], 1u << sh);
-      if (((old >> sh) & 0xFFFFu) == 0x7FFFu) {
-        atomicSub(&s_ngp[j >> 1], 0x8000u << sh);
-        atomicAdd(ngp_ovf + j, 0x8000ull);
+      if (N32) {
+        atomicAdd(&s_ngp[j], 1u);   // one 32-bit counter per bin, no return value used
+      } else {
+        // 16-bit counters, two bins per word; the increment that takes a counter
+        // to 2^15 moves 2^15 counts to the global overflow array (at most 1024
+        // more increments can land before the move, so the counter never wraps)
+        const int sh = (j & 1) << 4;
+        const uint32_t old = atomicAdd(&s_ngp[j >> 1], 1u << sh);
+        if (((old >> sh) & 0xFFFFu) == 0x7FFFu) {
+          atomicSub(&s_ngp[j >> 1], 0x8000u << sh);
+          atomicAdd(ngp_ovf + j, 0x8000ull);
+        }
       }
       ++n_in;
     }
@@ -362,12 +366,13 @@ struct PassRange {
   bool tail;
 };
 
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH>
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = false>
 __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
                                           unsigned char* smem_raw) {
-  // dynamic shared memory: RF table [128] | NGP counters [(B+1)/2] | cell words lo, hi [B+1]
+  // dynamic shared memory: RF table [128] | NGP counters | cell words lo, hi [B+1];
+  // NGP counters: (B+1)/2 words of two 16-bit counters, or B 32-bit ones (N32)
   const int nc = a.B + 1;                 // kick-table cells
-  const int nw = (a.B + 1) / 2;           // words of 16-bit NGP counters
+  const int nw = N32 ? a.B : (a.B + 1) / 2;
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
   uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_rf + kRfTableSize);
   uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
@@ -465,7 +470,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rf);
 #pragma unroll
     for (int j = 0; j < PPT; ++j)
-      pass_particle<WAKE>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].pd.y, kf[j].pd.x) : 0.0,
+      pass_particle<WAKE, N32>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].pd.y, kf[j].pd.x) : 0.0,
                           rf[j], c, g, pmean, acc_z, acc_z2, acc_d, n_in, s_ngp, s_lo, s_hi,
                           a.ngp_ovf);
     stp<PPT>(a.z + PPT * q, zz);
@@ -480,7 +485,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
     double z = a.z[i], e = a.dE[i];
     const double kick = WAKE ? wake_kick(z, g, potd) : 0.0;
-    pass_particle<WAKE>(z, e, r, kick, rf_term(z, c, s_rf), c, g, pmean, acc_z, acc_z2, acc_d,
+    pass_particle<WAKE, N32>(z, e, r, kick, rf_term(z, c, s_rf), c, g, pmean, acc_z, acc_z2, acc_d,
                         n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
     a.z[i] = z;
     a.dE[i] = e;
@@ -498,7 +503,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     uint32_t* pc = a.part_cnt + (size_t)rg.part * a.B;
     unsigned long long* pq = a.part_cic + (size_t)rg.part * nc;
     for (int i = threadIdx.x; i < nc; i += THREADS) {
-      if (i < a.B) pc[i] = (s_ngp[i >> 1] >> ((i & 1) << 4)) & 0xFFFFu;
+      if (i < a.B) pc[i] = N32 ? s_ngp[i] : (s_ngp[i >> 1] >> ((i & 1) << 4)) & 0xFFFFu;
       pq[i] = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
     }
   }
@@ -506,7 +511,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
 
 // One turn over one bunch: block b takes groups b, b + grid, ... (THREADS
 // apart) and writes partial slot b; block 0 takes the tail.
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1>
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   grid_dependency_wait();
@@ -517,14 +522,14 @@ __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
   }
   const PassRange rg{(int64_t)blockIdx.x * THREADS, (int64_t)gridDim.x * THREADS, a.n / PPT,
                      (int32_t)blockIdx.x, blockIdx.x == 0};
-  pass_body<WAKE, QE, PPT, THREADS, PREFETCH>(a, rg, smem_raw);
+  pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
 }
 
 // One turn over a batch of bunches: block c takes chunk c of the chunk table
 // (a contiguous run of one bunch's particles) and writes the bunch's partial
 // slot ch.part.  Blocks past the table's length, and chunks of bunches with
 // no turns left, return at once.
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1>
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_batch_pass(const PassArgs* __restrict__ bunches, const BatchChunk* __restrict__ chunks,
                  const int32_t* __restrict__ n_chunks) {
@@ -538,7 +543,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
   }
   const PassRange rg{ch.first / PPT, THREADS, (ch.first + ch.count) / PPT, ch.part,
                      ch.first + ch.count == a.n};
-  pass_body<WAKE, QE, PPT, THREADS, PREFETCH>(a, rg, smem_raw);
+  pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
 }
 
 // Merge of the per-block histograms.  Grid (bins/256, G): block column g sums
@@ -898,15 +903,22 @@ cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin) {
 }
 
 namespace {
+// cfg: thread layout (bits 0-2) | kPassN32 (32-bit NGP counters)
+template <bool W, int Q, bool N>
+const void* pass_fn_wqn(int layout) {
+  switch (layout) {
+    case 0: return (const void*)k_track_pass<W, Q, 4, 512, true, 1, N>;
+    case 1: return (const void*)k_track_pass<W, Q, 2, 1024, true, 1, N>;
+    case 2: return (const void*)k_track_pass<W, Q, 2, 768, true, 1, N>;
+    case 4: return (const void*)k_track_pass<W, Q, 2, 512, true, 2, N>;
+    default: return (const void*)k_track_pass<W, Q, 2, 512, false, 1, N>;
+  }
+}
+
 template <bool W, int Q>
 const void* pass_fn_wq(int cfg) {
-  switch (cfg) {
-    case 0: return (const void*)k_track_pass<W, Q, 4, 512, true>;
-    case 1: return (const void*)k_track_pass<W, Q, 2, 1024, true>;
-    case 2: return (const void*)k_track_pass<W, Q, 2, 768, true>;
-    case 4: return (const void*)k_track_pass<W, Q, 2, 512, true, 2>;
-    default: return (const void*)k_track_pass<W, Q, 2, 512, false>;
-  }
+  if (W && (cfg & kPassN32)) return pass_fn_wqn<W, Q, true>(cfg & kPassLayoutMask);
+  return pass_fn_wqn<W, Q, false>(cfg & kPassLayoutMask);
 }
 
 template <bool W>
@@ -922,15 +934,21 @@ const void* pass_fn(int wake, int qe, int cfg) {
   return wake ? pass_fn_w<true>(qe, cfg) : pass_fn_w<false>(qe, cfg);
 }
 
+template <bool W, int Q, bool N>
+const void* batch_fn_wqn(int layout) {
+  switch (layout) {
+    case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true, 1, N>;
+    case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true, 1, N>;
+    case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true, 1, N>;
+    case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2, N>;
+    default: return (const void*)k_batch_pass<W, Q, 2, 512, false, 1, N>;
+  }
+}
+
 template <bool W, int Q>
 const void* batch_fn_wq(int cfg) {
-  switch (cfg) {
-    case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true>;
-    case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true>;
-    case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true>;
-    case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2>;
-    default: return (const void*)k_batch_pass<W, Q, 2, 512, false>;
-  }
+  if (W && (cfg & kPassN32)) return batch_fn_wqn<W, Q, true>(cfg & kPassLayoutMask);
+  return batch_fn_wqn<W, Q, false>(cfg & kPassLayoutMask);
 }
 
 // Batches draw QE normals on the device or not at all (no host-fed draws).
@@ -940,31 +958,40 @@ const void* batch_fn(int wake, int qe, int cfg) {
 }
 }  // namespace
 
-int pass_cfg_threads(int cfg) { return cfg == 1 ? 1024 : (cfg == 2 ? 768 : 512); }
-int pass_cfg_ppt(int cfg) { return cfg == 0 ? 4 : 2; }
+int pass_cfg_threads(int cfg) {
+  const int l = cfg & kPassLayoutMask;
+  return l == 1 ? 1024 : (l == 2 ? 768 : 512);
+}
+int pass_cfg_ppt(int cfg) { return (cfg & kPassLayoutMask) == 0 ? 4 : 2; }
+bool pass_cfg_valid(int cfg) {
+  return cfg >= 0 && (cfg & ~(kPassLayoutMask | kPassN32)) == 0 &&
+         (cfg & kPassLayoutMask) < kNumPassCfgs;
+}
 
 cudaError_t prepare_track_kernels(int max_smem) {
   for (int w = 0; w < 2; ++w)
     for (int q = 0; q < 3; ++q)
-      for (int c = 0; c < kNumPassCfgs; ++c) {
-        cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
-        if (e == cudaSuccess && q != QE_DRAWS) e = allow_dynamic_smem(batch_fn(w, q, c), max_smem);
-        if (e != cudaSuccess) return e;
-      }
+      for (int n = 0; n < 2; ++n)
+        for (int l = 0; l < kNumPassCfgs; ++l) {
+          const int c = l | (n ? kPassN32 : 0);
+          cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
+          if (e == cudaSuccess && q != QE_DRAWS) e = allow_dynamic_smem(batch_fn(w, q, c), max_smem);
+          if (e != cudaSuccess) return e;
+        }
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
 }
 
-// RF table + 16-bit NGP counts [B] (two per word) + two 32-bit words per
-// kick-table cell [B+1].
-size_t track_smem_bytes(int B, int use_wake) {
+// RF table + NGP counts [B] (16-bit, two per word, or 32-bit with kPassN32)
+// + two 32-bit words per kick-table cell [B+1].
+size_t track_smem_bytes(int B, int use_wake, int cfg) {
   const size_t rf = kRfTableSize * sizeof(double2);
-  return use_wake ? rf + (size_t)((B + 1) / 2) * sizeof(uint32_t) +
-                        (size_t)(B + 1) * sizeof(unsigned long long)
+  const size_t nw = (cfg & kPassN32) ? (size_t)B : (size_t)((B + 1) / 2);
+  return use_wake ? rf + nw * sizeof(uint32_t) + (size_t)(B + 1) * sizeof(unsigned long long)
                   : rf;
 }
 
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
-  const size_t smem = track_smem_bytes(B, use_wake);
+  const size_t smem = track_smem_bytes(B, use_wake, cfg);
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pass_fn(use_wake, qe_mode, cfg),
                                                     pass_cfg_threads(cfg), smem) != cudaSuccess)
@@ -990,7 +1017,7 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg) {
 }
 
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
-  const size_t smem = track_smem_bytes(a.B, a.use_wake);
+  const size_t smem = track_smem_bytes(a.B, a.use_wake, a.cfg);
   void* args[] = {const_cast<PassArgs*>(&a)};
   PdlConfig l(dim3(grid), dim3(pass_cfg_threads(a.cfg)), smem, st);
   return cudaLaunchKernelExC(&l.cfg, pass_fn(a.use_wake, a.qe_mode, a.cfg), args);
@@ -999,7 +1026,7 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
 cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
                               const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
                               int qe, int cfg, cudaStream_t st) {
-  const size_t smem = track_smem_bytes(max_B, wake);
+  const size_t smem = track_smem_bytes(max_B, wake, cfg);
   void* args[] = {const_cast<PassArgs**>(&d_bunches), const_cast<BatchChunk**>(&d_chunks),
                   const_cast<int32_t**>(&d_n_chunks)};
   return cudaLaunchKernel(batch_fn(wake, qe, cfg), dim3(max_chunks > 0 ? max_chunks : 1),

@@ -13,8 +13,9 @@ batched bins step per turn, turn blocks replayed from a CUDA graph.
   blocks of K turns, retires finished points.
 * `run_plain`: the same points one after another on the plain resident path
   (the baseline the batch is measured against).
-* `autotune`: times candidate (particles per block, pass layout, K) on a
-  sample of the workload and keeps the fastest.
+* `autotune`: times candidate (particles per block, pass layout with the
+  width of the shared-memory bin counters -- the histogram privatisation --,
+  K) on a sample of the workload and keeps the fastest.
 * `serve`: a request stream with arrival times; requests are admitted by
   device-memory footprint (16 B per particle plus bin tables) while others
   run, and per-request latency percentiles are reported with solves/s.
@@ -194,7 +195,7 @@ def wave_chunks(points: List[Point], num_sms: int, waves=(1, 2, 4)) -> List[int]
 
 
 def autotune(ctx: Context, points: List[Point], *, trial_turns: int = 64,
-             chunks=None, layouts=(0, 1), graph_turns=(8, 32),
+             chunks=None, layouts=(0, 1, 8, 9), graph_turns=(8, 32),
              sample: int = 64) -> Tuning:
     """Times each candidate (particles per block, pass layout, graph turns) on
     up to `sample` of the points for `trial_turns` turns after a warm-up and
@@ -331,7 +332,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser(description="Time batched turns of the 256-point sweep")
     ap.add_argument("--turns", type=int, default=64)
     ap.add_argument("--chunk", type=int, default=65536)
-    ap.add_argument("--layout", type=int, default=1)
+    ap.add_argument("--layout", type=int, default=-1)
     ap.add_argument("--graph-turns", type=int, default=8)
     args = ap.parse_args()
     s = time_batch_turns(Context(0), sweep_points(256), args.turns,

@@ -149,9 +149,11 @@ hj_status hj_trim(hj_ctx* ctx);
  * this context: -1 = chosen by the library (default), 0 = 4 particles per
  * thread x 512 threads, 1 = 2 x 1024, 2 = 2 x 768 (each with the next group
  * prefetched), 3 = 2 x 512 without prefetch, 4 = 2 x 512 with prefetch at
- * two blocks per SM.  Results do not depend on
- * the layout beyond floating-point summation order.  No reference
- * counterpart. */
+ * two blocks per SM; plus 8 (8..12): the same layout with one 32-bit
+ * shared-memory counter per bin instead of two 16-bit ones per word (more
+ * shared memory, no overflow check; the default up to 8192 bins).  Results do
+ * not depend on the layout beyond floating-point summation order; bin counts
+ * are the same.  No reference counterpart. */
 hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout);
 
 /* ---------------------------------------------------------------- set-up helpers */
@@ -309,7 +311,8 @@ hj_status hj_bunch_bins(hj_bunch* b);
 /* A batch on ctx's device with its own stream: a particle pool of
  * pool_particles (16 B each), up to max_bunches bunches of up to max_nbins
  * bins, chunk_particles particles per block of the pass (a multiple of 4;
- * 0 = 65536) and pass layout `layout` (-1 = the default for max_nbins). */
+ * 0 = 65536) and pass layout `layout` (-1 = the default for max_nbins; values
+ * as for hj_set_pass_layout). */
 hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
                           int32_t max_nbins, int64_t chunk_particles, int32_t layout,
                           hj_batch** out);

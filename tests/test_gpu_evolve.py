@@ -84,9 +84,10 @@ def test_reference_ring_reference_wake(gpu_ctx, oracle):
     run_turn_by_turn(gpu_ctx, oracle, cfg, 100_000, 30, seed=1234)
 
 
-@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4, 8, 9, 10, 11, 12])
 def test_thread_layouts(oracle, layout):
-    """Every thread layout of the fused pass keeps per-particle parity."""
+    """Every thread layout of the fused pass, with 16-bit (0-4) or 32-bit (8-12)
+    bin counters, keeps per-particle parity and bit-exact counts."""
     from haissinskijulia_b200 import Context
     ctx = Context(0)
     ctx.set_pass_layout(layout)
