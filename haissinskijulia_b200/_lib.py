@@ -146,6 +146,11 @@ SIGNATURES = {
     "hj_batch_poll": (c_int32, [c_void_p, _IP, c_int32, POINTER(c_int32)]),
     "hj_batch_take": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, POINTER(HjResult)]),
     "hj_batch_stats": (c_int32, [c_void_p, _IP]),
+    "hj_batch_add_many": (c_int32, [c_void_p, c_int32, POINTER(c_void_p), POINTER(c_void_p), _IP,
+                                    POINTER(HjParams), POINTER(HjWake), _IP, POINTER(c_uint64),
+                                    _IP, _IP, POINTER(c_int32)]),
+    "hj_batch_take_many": (c_int32, [c_void_p, c_int32, _IP, POINTER(c_void_p),
+                                     POINTER(c_void_p), POINTER(HjResult), _DP]),
     "hj_rf_kick": (c_int32, [_CTX, c_double, c_double, c_double, c_double, _DP, _DP, c_int64]),
     "hj_quantum_excitation": (c_int32, [_CTX, c_double, c_double, c_double, _DP, c_uint64,
                                         c_int64, _DP, c_int64]),

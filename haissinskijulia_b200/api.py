@@ -724,6 +724,53 @@ class Batch:
                                                      ctypes.c_void_p(d_dE), ctypes.byref(r)))
         return EvolveResult.from_c(r)
 
+    def add_many(self, z, dE, n, params, nbins, seeds, turns, wakes=None):
+        """Admit bunches in order with one synchronisation (hj_batch_add_many).
+        z, dE: per-bunch particle arrays as pointers (ints, host or device) or
+        numpy arrays (host, kept alive by the caller until the call returns);
+        n, params, nbins, seeds, turns: per-bunch values; wakes: None (each
+        params' reference wake) or a list of WakeModel.  Returns (ids of the
+        admitted bunches -- the first ones --, the HaissinskiError that stopped
+        admission, or None)."""
+        k = len(n)
+        def ptrs(a):
+            arr = (ctypes.c_void_p * max(k, 1))()
+            for i, x in enumerate(a):
+                arr[i] = x if isinstance(x, int) else x.ctypes.data
+            return arr
+        zp, ep = ptrs(z), ptrs(dE)
+        nn = np.ascontiguousarray(n, dtype=np.int64)
+        pc = (HjParams * max(k, 1))(*[p.to_c() for p in params])
+        wc = None if wakes is None else (HjWake * max(k, 1))(*[w.to_c() for w in wakes])
+        nb = np.ascontiguousarray(nbins, dtype=np.int64)
+        sd = (ctypes.c_uint64 * max(k, 1))(*[int(x) & 0xFFFFFFFFFFFFFFFF for x in seeds])
+        tt = np.ascontiguousarray(turns, dtype=np.int64)
+        ids = np.zeros(max(k, 1), dtype=np.int64)
+        added = ctypes.c_int32(0)
+        rc = self.ctx._lib.hj_batch_add_many(self.handle, k, zp, ep, _ip(nn), pc, wc, _ip(nb), sd,
+                                             _ip(tt), _ip(ids), ctypes.byref(added))
+        out = [int(x) for x in ids[: added.value]]
+        for bid, size in zip(out, nn):
+            self.sizes[bid] = int(size)
+        err = None
+        if rc != 0:
+            err = HaissinskiError(rc, self.ctx.last_error())
+        return out, err
+
+    def take_many(self, ids, correlation: bool = False):
+        """Finish and free bunches `ids` with one synchronisation
+        (hj_batch_take_many); returns (results, correlations or None)."""
+        k = len(ids)
+        idv = np.ascontiguousarray(ids, dtype=np.int64)
+        res = (HjResult * max(k, 1))()
+        corr = np.zeros(max(k, 1)) if correlation else None
+        _check(self.ctx, self.ctx._lib.hj_batch_take_many(
+            self.handle, k, _ip(idv), None, None, res, _dp(corr) if correlation else None))
+        for b in ids:
+            self.sizes.pop(int(b), None)
+        results = [EvolveResult.from_c(res[i]) for i in range(k)]
+        return results, ([float(c) for c in corr[:k]] if correlation else None)
+
     def stats(self) -> dict:
         out = np.zeros(4, dtype=np.int64)
         _check(self.ctx, self.ctx._lib.hj_batch_stats(self.handle, _ip(out)))

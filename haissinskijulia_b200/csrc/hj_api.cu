@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "hj_host.h"
@@ -32,6 +33,13 @@ struct hj_ctx {
   // released blocks kept for reuse, by size class (device / pinned host)
   std::multimap<size_t, void*> dev_free, host_free;
   size_t dev_free_bytes = 0, host_free_bytes = 0;
+  // device blocks up to kSlabBlockMax are carved from large slabs (a
+  // cudaMalloc of a megabyte costs ~0.6 ms); carved blocks are reused through
+  // dev_free and released with their slabs by hj_destroy
+  std::vector<void*> dev_slabs;
+  char* slab_cur = nullptr;
+  size_t slab_left = 0;
+  std::unordered_set<void*> carved;
   // twiddle tables of the bins step by FFT length P, shared by all bunches
   std::map<int, double2*> twiddles;
   // grids and wake tables built from an initial σ_z, by the bit patterns of
@@ -224,6 +232,9 @@ size_t size_class(size_t b) {
   return (b + step - 1) / step * step;
 }
 
+constexpr size_t kSlabBlockMax = size_t(16) << 20;
+constexpr size_t kSlabSize = size_t(256) << 20;
+
 hj_status cache_take(hj_ctx* ctx, bool host, size_t bytes, void** out, size_t* cap) {
   const size_t c = size_class(bytes);
   auto& fl = host ? ctx->host_free : ctx->dev_free;
@@ -231,7 +242,24 @@ hj_status cache_take(hj_ctx* ctx, bool host, size_t bytes, void** out, size_t* c
   if (it != fl.end()) {
     *out = it->second;
     fl.erase(it);
-    (host ? ctx->host_free_bytes : ctx->dev_free_bytes) -= c;
+    if (host || !ctx->carved.count(*out)) (host ? ctx->host_free_bytes : ctx->dev_free_bytes) -= c;
+  } else if (!host && c <= kSlabBlockMax) {
+    if (ctx->slab_left < c) {
+      void* slab = nullptr;
+      cudaError_t e = cudaMalloc(&slab, kSlabSize);
+      if (e != cudaSuccess) {
+        *out = nullptr;
+        return set_err(ctx, HJ_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", kSlabSize,
+                       cudaGetErrorString(e));
+      }
+      ctx->dev_slabs.push_back(slab);
+      ctx->slab_cur = (char*)slab;
+      ctx->slab_left = kSlabSize;
+    }
+    *out = ctx->slab_cur;                 // size classes are multiples of 256 bytes
+    ctx->slab_cur += c;
+    ctx->slab_left -= c;
+    ctx->carved.insert(*out);
   } else {
     cudaError_t e = host ? cudaMallocHost(out, c) : cudaMalloc(out, c);
     if (e != cudaSuccess) {
@@ -248,6 +276,10 @@ hj_status cache_take(hj_ctx* ctx, bool host, size_t bytes, void** out, size_t* c
 // may still use it.
 void cache_give(hj_ctx* ctx, bool host, void* p, size_t cap) {
   if (!p) return;
+  if (!host && ctx->carved.count(p)) {
+    ctx->dev_free.insert({cap, p});
+    return;
+  }
   size_t& held = host ? ctx->host_free_bytes : ctx->dev_free_bytes;
   if (held + cap > (host ? kHostCacheCap : kDevCacheCap)) {
     if (host) cudaFreeHost(p);
@@ -258,14 +290,28 @@ void cache_give(hj_ctx* ctx, bool host, void* p, size_t cap) {
   held += cap;
 }
 
-void cache_clear(hj_ctx* ctx) {
-  for (auto& kv : ctx->wake_sets) cudaFree(kv.second.dev);
+// Frees the kept blocks (carved ones stay for reuse unless `slabs` is set,
+// which also frees the slabs: only when no bunch or batch holds a block).
+void cache_clear(hj_ctx* ctx, bool slabs = false) {
+  for (auto& kv : ctx->wake_sets) cache_give(ctx, false, kv.second.dev, kv.second.cap);
   ctx->wake_sets.clear();
-  for (auto& kv : ctx->dev_free) cudaFree(kv.second);
+  std::multimap<size_t, void*> keep;
+  for (auto& kv : ctx->dev_free) {
+    if (ctx->carved.count(kv.second)) keep.insert(kv);
+    else cudaFree(kv.second);
+  }
   for (auto& kv : ctx->host_free) cudaFreeHost(kv.second);
-  ctx->dev_free.clear();
+  ctx->dev_free.swap(keep);
   ctx->host_free.clear();
   ctx->dev_free_bytes = ctx->host_free_bytes = 0;
+  if (slabs) {
+    for (void* s : ctx->dev_slabs) cudaFree(s);
+    ctx->dev_slabs.clear();
+    ctx->carved.clear();
+    ctx->dev_free.clear();
+    ctx->slab_cur = nullptr;
+    ctx->slab_left = 0;
+  }
 }
 
 // The twiddle table [P] of the bins step, built once per context and P.
@@ -458,7 +504,7 @@ extern "C" void hj_destroy(hj_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->scratch) cudaFree(ctx->scratch);
-  cache_clear(ctx);
+  cache_clear(ctx, true);
   for (auto& kv : ctx->twiddles) cudaFree(kv.second);
   delete ctx;
 }
@@ -495,14 +541,19 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   delete b;
 }
 
+// Creation of a bunch in two halves, so that a batch can admit many bunches
+// with one synchronisation: bunch_create_begin validates, lays out the
+// buffers and enqueues the initial moments and their copy to the host;
+// bunch_create_end (after the stream has reached them) builds the grid, the
+// wake tables, the RF table and the turn state.
 // chunk > 0: a batch member, whose partial slots are its chunks of `chunk`
 // particles (the batch's chunk table) instead of one per block of the grid;
 // cfg >= 0 pins the pass layout.
-static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
-                                   const hj_params* params, const hj_wake* wake,
-                                   int64_t nbins, const hj_grid* grid, uint64_t seed,
-                                   void* stream, hj_bunch* b, int64_t chunk = 0,
-                                   int cfg = -1) {
+static hj_status bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                    const hj_params* params, const hj_wake* wake,
+                                    int64_t nbins, const hj_grid* grid, uint64_t seed,
+                                    void* stream, hj_bunch* b, int64_t chunk = 0,
+                                    int cfg = -1) {
   b->ctx = ctx;
   b->stream = (cudaStream_t)stream;
   b->z = d_z;
@@ -596,10 +647,19 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
     b->h_rf = (double*)((char*)b->harena + h_rf);
   }
 
-  // Initial spreads, src/evolution.jl:247-249.
-  double m[4];
+  // Initial spreads, src/evolution.jl:247-249: enqueued here, read in
+  // bunch_create_end
   HJ_TRY(launch_moments(b, 0, nullptr, nullptr));
-  HJ_TRY(read_moments(b, m));
+  HJ_CUDA(ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 4 * b->nblk_m,
+                               cudaMemcpyDeviceToHost, b->stream));
+  return HJ_OK;
+}
+
+static hj_status bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid) {
+  const int64_t n = b->n;
+  const hj_params* params = &b->p;
+  double m[4];
+  sum_moments(b, m);
   b->sigma_z0_initial = global_std(m[0], m[1], n);
   b->sigma_E0_initial = global_std(m[2], m[3], n);
 
@@ -720,6 +780,17 @@ static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64
   // the stream is ordered after the copy, host reads of h_ts synchronise first
   HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice, b->stream));
   return HJ_OK;
+}
+
+static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                   const hj_params* params, const hj_wake* wake,
+                                   int64_t nbins, const hj_grid* grid, uint64_t seed,
+                                   void* stream, hj_bunch* b, int64_t chunk = 0,
+                                   int cfg = -1) {
+  HJ_TRY(bunch_create_begin(ctx, d_z, d_dE, n, params, wake, nbins, grid, seed, stream, b,
+                            chunk, cfg));
+  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
+  return bunch_create_end(ctx, b, grid);
 }
 
 extern "C" hj_status hj_bunch_create(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
@@ -1636,15 +1707,28 @@ extern "C" hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns) {
 
 // z, dE != NULL: copy them into the pool; else generate independent
 // Gaussians (σ_z, σ_E) from init_seed in place.
-static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE, int64_t n,
-                                const hj_params* params, const hj_wake* wake, int64_t nbins,
-                                uint64_t seed, int64_t turns, int64_t* id_out, double sigma_z,
-                                double sigma_E, uint64_t init_seed) {
-  if (!bt) return HJ_ERR_ARG;
+// Admission in two halves (see bunch_create_begin): the first checks the
+// bunch, reserves its slot and pool range, fills its particles and enqueues
+// its initial moments; the second, after the stream has reached them,
+// completes the bunch and makes it a member.
+struct PendingAdd {
+  hj_bunch* b = nullptr;
+  int64_t start = 0, cap = 0, turns = 0;
+  int slot = -1;
+};
+
+static void batch_add_abort(hj_batch* bt, PendingAdd& p) {
+  if (p.b) hj_bunch_destroy(p.b);
+  if (p.cap) batch_free_range(bt, p.start, p.cap);
+  if (p.slot >= 0) bt->free_slots.push_back(p.slot);
+  p = PendingAdd{};
+}
+
+static hj_status batch_add_begin(hj_batch* bt, const double* z, const double* dE, int64_t n,
+                                 const hj_params* params, const hj_wake* wake, int64_t nbins,
+                                 uint64_t seed, int64_t turns, double sigma_z, double sigma_E,
+                                 uint64_t init_seed, PendingAdd* out) {
   hj_ctx* ctx = bt->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (!id_out) return set_err(ctx, HJ_ERR_ARG, "id_out is NULL");
-  *id_out = 0;
   HJ_TRY(check_params(ctx, params));
   if (n <= 0) return set_err(ctx, HJ_ERR_ARG, "a batch bunch needs at least one particle");
   if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
@@ -1657,12 +1741,14 @@ static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE,
     return set_err(ctx, HJ_ERR_FULL, "nbins = %lld exceeds the batch's %d",
                    (long long)nbins, bt->max_B);
   if (bt->free_slots.empty()) return set_err(ctx, HJ_ERR_FULL, "the batch's bunch slots are full");
-  int64_t start = 0, cap = 0;
-  if (batch_alloc_range(bt, n, &start, &cap) != HJ_OK)
+  PendingAdd p;
+  if (batch_alloc_range(bt, n, &p.start, &p.cap) != HJ_OK)
     return set_err(ctx, HJ_ERR_FULL, "no free pool range of %lld particles", (long long)n);
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  double* dz = bt->pool_z + start;
-  double* de = bt->pool_dE + start;
+  p.slot = bt->free_slots.back();
+  bt->free_slots.pop_back();
+  p.turns = turns;
+  double* dz = bt->pool_z + p.start;
+  double* de = bt->pool_dE + p.start;
   cudaError_t e;
   if (z) {
     e = cudaMemcpyAsync(dz, z, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
@@ -1672,39 +1758,74 @@ static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE,
     e = launch_gaussian_bunch(init_seed, n, 0.0, sigma_z, 0.0, sigma_E, dz, de, bt->stream);
   }
   if (e != cudaSuccess) {
-    batch_free_range(bt, start, cap);
+    batch_add_abort(bt, p);
     return set_err(ctx, HJ_ERR_CUDA, "copying the bunch into the pool failed: %s",
                    cudaGetErrorString(e));
   }
-  hj_bunch* b = new hj_bunch();
-  hj_status s = bunch_create_impl(ctx, dz, de, n, params, wake, nbins, nullptr, seed,
-                                  (void*)bt->stream, b, bt->chunk, bt->cfg);
-  if (s == HJ_OK && b->nblk > bt->max_chunks) s = set_err(ctx, HJ_ERR_FULL, "chunk table full");
+  p.b = new hj_bunch();
+  hj_status s = bunch_create_begin(ctx, dz, de, n, params, wake, nbins, nullptr, seed,
+                                   (void*)bt->stream, p.b, bt->chunk, bt->cfg);
+  if (s == HJ_OK && p.b->nblk > bt->max_chunks) s = set_err(ctx, HJ_ERR_FULL, "chunk table full");
   if (s != HJ_OK) {
-    hj_bunch_destroy(b);
-    batch_free_range(bt, start, cap);
+    batch_add_abort(bt, p);
+    return s;
+  }
+  bt->wake = wake_on;
+  bt->qe = qe;
+  *out = p;
+  return HJ_OK;
+}
+
+static hj_status batch_add_end(hj_batch* bt, PendingAdd& p, int64_t* id_out) {
+  hj_ctx* ctx = bt->ctx;
+  hj_status s = bunch_create_end(ctx, p.b, nullptr);
+  if (s != HJ_OK) {
+    batch_add_abort(bt, p);
     return s;
   }
   // move the turn state into the batch's array, with this bunch's turn budget
-  const int slot = bt->free_slots.back();
-  bt->free_slots.pop_back();
-  b->h_ts->turns_left = turns;
-  b->ts = bt->d_ts + slot;           // the arena's own TurnState stays unused
-  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
-                               bt->stream));   // ordered before the next turn's kernels
+  hj_bunch* b = p.b;
+  b->h_ts->turns_left = p.turns;
+  b->ts = bt->d_ts + p.slot;         // the arena's own TurnState stays unused
+  cudaError_t e = cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
+                                  bt->stream);   // ordered before the next turn's kernels
+  if (e != cudaSuccess) {
+    batch_add_abort(bt, p);
+    return set_err(ctx, HJ_ERR_CUDA, "turn state upload failed: %s", cudaGetErrorString(e));
+  }
   BatchMember m;
   m.id = bt->next_id++;
   m.b = b;
-  m.start = start;
-  m.cap = cap;
-  m.slot = slot;
-  m.turns = turns;
+  m.start = p.start;
+  m.cap = p.cap;
+  m.slot = p.slot;
+  m.turns = p.turns;
   bt->members.push_back(m);
-  bt->wake = wake_on;
-  bt->qe = qe;
   bt->dirty = true;
   *id_out = m.id;
+  p = PendingAdd{};
   return HJ_OK;
+}
+
+static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE, int64_t n,
+                                const hj_params* params, const hj_wake* wake, int64_t nbins,
+                                uint64_t seed, int64_t turns, int64_t* id_out, double sigma_z,
+                                double sigma_E, uint64_t init_seed) {
+  if (!bt) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (!id_out) return set_err(ctx, HJ_ERR_ARG, "id_out is NULL");
+  *id_out = 0;
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  PendingAdd p;
+  HJ_TRY(batch_add_begin(bt, z, dE, n, params, wake, nbins, seed, turns, sigma_z, sigma_E,
+                         init_seed, &p));
+  cudaError_t e = cudaStreamSynchronize(bt->stream);
+  if (e != cudaSuccess) {
+    batch_add_abort(bt, p);
+    return set_err(ctx, HJ_ERR_CUDA, "%s", cudaGetErrorString(e));
+  }
+  return batch_add_end(bt, p, id_out);
 }
 
 extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* dE, int64_t n,
@@ -1723,6 +1844,142 @@ extern "C" hj_status hj_batch_add_gaussian(hj_batch* bt, int64_t n, double sigma
     return set_err(bt->ctx, HJ_ERR_ARG, "spreads must be non-negative");
   return batch_add_impl(bt, nullptr, nullptr, n, params, wake, nbins, seed, turns, id_out,
                         sigma_z, sigma_E, init_seed);
+}
+
+extern "C" hj_status hj_batch_add_many(hj_batch* bt, int32_t count, const double* const* z,
+                                       const double* const* dE, const int64_t* n,
+                                       const hj_params* params, const hj_wake* wakes,
+                                       const int64_t* nbins, const uint64_t* seeds,
+                                       const int64_t* turns, int64_t* ids_out,
+                                       int32_t* n_added) {
+  if (!bt) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (!n_added) return set_err(ctx, HJ_ERR_ARG, "n_added is NULL");
+  *n_added = 0;
+  if (count < 0) return set_err(ctx, HJ_ERR_ARG, "count must be >= 0");
+  if (count > 0 && (!z || !dE || !n || !params || !nbins || !seeds || !turns || !ids_out))
+    return set_err(ctx, HJ_ERR_ARG, "an argument array is NULL");
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  std::vector<PendingAdd> pend;
+  pend.reserve(count);
+  hj_status first = HJ_OK;
+  std::string first_msg;
+  for (int k = 0; k < count; ++k) {
+    PendingAdd p;
+    hj_status s = (!z[k] || !dE[k])
+                      ? set_err(ctx, HJ_ERR_ARG, "particle arrays of bunch %d are NULL", k)
+                      : batch_add_begin(bt, z[k], dE[k], n[k], &params[k],
+                                        wakes ? &wakes[k] : nullptr, nbins[k], seeds[k],
+                                        turns[k], 0.0, 0.0, 0, &p);
+    if (s != HJ_OK) {
+      first = s;
+      first_msg = ctx->err;
+      break;
+    }
+    pend.push_back(p);
+  }
+  cudaError_t e = cudaStreamSynchronize(bt->stream);
+  if (e != cudaSuccess) {
+    for (auto& p : pend) batch_add_abort(bt, p);
+    return set_err(ctx, HJ_ERR_CUDA, "%s", cudaGetErrorString(e));
+  }
+  for (size_t k = 0; k < pend.size(); ++k) {
+    hj_status s = batch_add_end(bt, pend[k], &ids_out[k]);
+    if (s != HJ_OK) {
+      for (size_t j = k + 1; j < pend.size(); ++j) batch_add_abort(bt, pend[j]);
+      *n_added = (int32_t)k;
+      return s;
+    }
+  }
+  *n_added = (int32_t)pend.size();
+  if (first != HJ_OK) ctx->err = first_msg;
+  return first;
+}
+
+extern "C" hj_status hj_batch_take_many(hj_batch* bt, int32_t count, const int64_t* ids,
+                                        double* const* z_out, double* const* dE_out,
+                                        hj_result* res, double* corr_out) {
+  if (!bt) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (count < 0 || (count > 0 && !ids)) return set_err(ctx, HJ_ERR_ARG, "bad id list");
+  std::vector<hj_bunch*> bs(count);
+  for (int k = 0; k < count; ++k) {
+    const int j = batch_find(bt, ids[k]);
+    if (j < 0) return set_err(ctx, HJ_ERR_ARG, "no bunch %lld in the batch", (long long)ids[k]);
+    for (int q = 0; q < k; ++q)
+      if (ids[q] == ids[k]) return set_err(ctx, HJ_ERR_ARG, "bunch %lld listed twice", (long long)ids[k]);
+    bs[k] = bt->members[j].b;
+  }
+  // one round trip for all: pending kick and re-centring in place, moments,
+  // turn state, copies out, and every slot's state set to "no turns left"
+  TurnState dead{};
+  dead.turns_left = 0;
+  for (int k = 0; k < count; ++k) {
+    hj_bunch* b = bs[k];
+    HJ_TRY(launch_moments(b, 1, b->z, b->dE));
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 4 * b->nblk_m,
+                                 cudaMemcpyDeviceToHost, bt->stream));
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->h_ts, b->ts, sizeof(TurnState), cudaMemcpyDeviceToHost,
+                                 bt->stream));
+    if (z_out && z_out[k])
+      HJ_CUDA(ctx, cudaMemcpyAsync(z_out[k], b->z, sizeof(double) * b->n, cudaMemcpyDefault,
+                                   bt->stream));
+    if (dE_out && dE_out[k])
+      HJ_CUDA(ctx, cudaMemcpyAsync(dE_out[k], b->dE, sizeof(double) * b->n, cudaMemcpyDefault,
+                                   bt->stream));
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, &dead, sizeof(TurnState), cudaMemcpyHostToDevice,
+                                 bt->stream));
+  }
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  hj_status st = HJ_OK;
+  std::vector<double> mean_z(count), mean_e(count);
+  for (int k = 0; k < count; ++k) {
+    hj_bunch* b = bs[k];
+    double m[4];
+    sum_moments(b, m);
+    hj_status s = state_status(b);
+    if (st == HJ_OK) st = s;
+    if (res) fill_result(b, m, &res[k]);
+    mean_z[k] = m[0] / (double)b->n;
+    mean_e[k] = m[2] / (double)b->n;
+  }
+  if (corr_out) {
+    // cor(z, ΔE) of the final particles (the second pass of hj_correlation,
+    // about the means above), partial sums in the moments' buffers
+    for (int k = 0; k < count; ++k) {
+      hj_bunch* b = bs[k];
+      HJ_CUDA(ctx, launch_cor_parts(b->z, b->dE, b->n, mean_z[k], mean_e[k], 1, b->part_mom,
+                                    b->nblk_m, bt->stream));
+      HJ_CUDA(ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 3 * b->nblk_m,
+                                   cudaMemcpyDeviceToHost, bt->stream));
+    }
+    HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+    for (int k = 0; k < count; ++k) {
+      hj_bunch* b = bs[k];
+      double sxx = 0.0, syy = 0.0, sxy = 0.0;
+      for (int q = 0; q < b->nblk_m; ++q) {
+        sxx += b->h_mom[3 * q];
+        syy += b->h_mom[3 * q + 1];
+        sxy += b->h_mom[3 * q + 2];
+      }
+      const double r = sxy / (std::sqrt(sxx) * std::sqrt(syy));
+      corr_out[k] = r != r ? r : std::min(1.0, std::max(-1.0, r));
+    }
+  }
+  for (int k = 0; k < count; ++k) {
+    const int j = batch_find(bt, ids[k]);
+    BatchMember m = bt->members[j];
+    m.b->ts = nullptr;
+    hj_bunch_destroy(m.b);
+    batch_free_range(bt, m.start, m.cap);
+    bt->free_slots.push_back(m.slot);
+    bt->members[j] = bt->members.back();
+    bt->members.pop_back();
+  }
+  bt->dirty = true;
+  return st;
 }
 
 extern "C" hj_status hj_gaussian_bunch(hj_ctx* ctx, uint64_t init_seed, int64_t n,

@@ -347,17 +347,19 @@ def _finish_fom(ctx, fom, r: Run, res: EvolveResult, final) -> None:
 
 def run_batched(ctx: Context, runs: List[Run], fom: FigureOfMerit, init: _Initial, nbins: int,
                 *, chunk: int = 65536, layout: int = -1, graph_turns: int = 16,
-                block_turns: int = 16, max_resident: Optional[int] = None) -> None:
+                block_turns: int = 16, max_resident: Optional[int] = None,
+                admit_group: int = 256) -> None:
     """Every run through Batches (one per wakefield/excitation combination):
-    admit while there is room, advance in blocks, take finished runs."""
-    import torch
+    admit while there is room (groups of runs with one synchronisation each),
+    advance in blocks, take the finished runs together (the emittance's
+    correlation reduced on the device as they are taken)."""
     n = init.n
-    final = (torch.empty(n, dtype=torch.float64, device="cuda"),
-             torch.empty(n, dtype=torch.float64, device="cuda"))
+    emittance = isinstance(fom, EmittanceFoM)
     groups: Dict[tuple, List[Run]] = {}
     for r in runs:
         groups.setdefault((bool(r.params.use_wakefield), bool(r.params.use_excitation)),
                           []).append(r)
+    zp, ep = init.z.data_ptr(), init.dE.data_ptr()
     t0 = time.perf_counter()
     for todo in groups.values():
         slots = min(len(todo), max_resident or len(todo))
@@ -368,27 +370,37 @@ def run_batched(ctx: Context, runs: List[Run], fom: FigureOfMerit, init: _Initia
             live: Dict[int, Run] = {}
             while pending or live:
                 while pending:
-                    r = pending[0]
-                    try:
-                        bid = bt.add_device(init.z.data_ptr(), init.dE.data_ptr(), n, r.params,
-                                            nbins, seed=r.seed, turns=r.params.n_turns)
-                    except HaissinskiError as e:
-                        if e.status == _lib.HJ_ERR_FULL and live:
-                            break
-                        r.error = str(e)
-                        pending.pop(0)
+                    grp = pending[:admit_group]
+                    k = len(grp)
+                    ids, err = bt.add_many([zp] * k, [ep] * k, [n] * k, [r.params for r in grp],
+                                           [nbins] * k, [r.seed for r in grp],
+                                           [r.params.n_turns for r in grp])
+                    now = time.perf_counter() - t0
+                    for r, bid in zip(grp, ids):
+                        r.admitted = now
+                        live[bid] = r
+                    del pending[:len(ids)]
+                    if err is None:
                         continue
-                    r.admitted = time.perf_counter() - t0
-                    live[bid] = r
+                    if err.status == _lib.HJ_ERR_FULL:
+                        if live:
+                            break
+                        raise err
+                    pending[0].error = str(err)          # this run cannot be made
                     pending.pop(0)
                 if not live:
                     continue
                 bt.advance(block_turns)
-                for bid in bt.poll():
-                    r = live.pop(bid)
-                    res = bt.take_device(bid, final[0].data_ptr(), final[1].data_ptr())
-                    _finish_fom(ctx, fom, r, res, final)
-                    r.finished = time.perf_counter() - t0
+                done = bt.poll()
+                if done:
+                    results, corr = bt.take_many(done, correlation=emittance)
+                    now = time.perf_counter() - t0
+                    for i, bid in enumerate(done):
+                        r = live.pop(bid)
+                        r.result = results[i]
+                        r.fom = compute_fom(fom, None, results[i],
+                                            correlation=corr[i] if emittance else None)
+                        r.finished = now
         finally:
             bt.close()
 

@@ -142,8 +142,9 @@ const char* hj_last_error(const hj_ctx* ctx);
  * pinned) and the last 8 bin grids with their wake tables built from an
  * initial sigma_z (bunches of a scan start from the same particles), so that
  * admitting bunches of recurring sizes allocates and recomputes nothing.
- * hj_trim frees them now (hj_destroy frees them too).  No reference
- * counterpart. */
+ * Blocks up to 16 MB are carved from 256 MB slabs, which the context keeps
+ * until hj_destroy.  hj_trim frees the other kept blocks now (hj_destroy
+ * frees everything).  No reference counterpart. */
 hj_status hj_trim(hj_ctx* ctx);
 /* Thread layout of the fused particle pass for bunches created afterwards on
  * this context: -1 = chosen by the library (default), 0 = 4 particles per
@@ -331,6 +332,16 @@ hj_status hj_batch_add_gaussian(hj_batch* bt, int64_t n, double sigma_z, double 
                                 uint64_t init_seed, const hj_params* params,
                                 const hj_wake* wake, int64_t nbins, uint64_t seed,
                                 int64_t turns, int64_t* id_out);
+/* Admit up to `count` bunches in order with one synchronisation: bunch k has
+ * particles z[k], dE[k] (host or device, copied), n[k], params[k], wakes[k]
+ * (wakes NULL: the reference wake of each params), nbins[k], seeds[k] and
+ * turns[k]; ids_out[k] receives its id.  Stops at the first bunch that cannot
+ * be admitted and returns that bunch's status (HJ_ERR_FULL when the batch has
+ * no room); *n_added bunches, the first ones, were admitted either way. */
+hj_status hj_batch_add_many(hj_batch* bt, int32_t count, const double* const* z,
+                            const double* const* dE, const int64_t* n, const hj_params* params,
+                            const hj_wake* wakes, const int64_t* nbins, const uint64_t* seeds,
+                            const int64_t* turns, int64_t* ids_out, int32_t* n_added);
 /* Enqueue `turns` turns of every live bunch (a bunch stops at its own count). */
 hj_status hj_batch_advance(hj_batch* bt, int64_t turns);
 /* Wait for the enqueued turns; ids[0..*n_done-1] = bunches that have run all
@@ -341,6 +352,14 @@ hj_status hj_batch_poll(hj_batch* bt, int64_t* ids, int32_t cap, int32_t* n_done
  * its slot and pool range. */
 hj_status hj_batch_take(hj_batch* bt, int64_t id, double* z_out, double* dE_out,
                         hj_result* res);
+/* hj_batch_take for `count` bunches with one synchronisation (two with
+ * corr_out): z_out/dE_out (NULL, or arrays of per-bunch destinations, entries
+ * may be NULL), res[count] (or NULL), and corr_out[count] (or NULL): the
+ * correlation cor(z, ΔE) of each bunch's final particles, as hj_correlation
+ * computes it (for EmittanceFoM, src/parameter_sensitivity/figures_of_merit.jl:42). */
+hj_status hj_batch_take_many(hj_batch* bt, int32_t count, const int64_t* ids,
+                             double* const* z_out, double* const* dE_out, hj_result* res,
+                             double* corr_out);
 /* out[0] live bunches, out[1] free pool particles (largest free range),
  * out[2] free slots, out[3] turns enqueued so far. */
 hj_status hj_batch_stats(hj_batch* bt, int64_t* out4);

@@ -117,3 +117,47 @@ def test_admission_is_refused_when_the_batch_is_full(gpu_ctx):
     bt.take(bid, copy_out=False)
     bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=3)      # room again
     bt.close()
+
+
+def test_admitting_and_taking_many_at_once(gpu_ctx):
+    """hj_batch_add_many / hj_batch_take_many give the bunches that one-by-one
+    admission and retirement give, bit for bit, stop at the first bunch that
+    does not fit, and take the correlation of each final bunch."""
+    from haissinskijulia_b200.api import correlation_device
+    specs = [_spec(i) for i in range(5)]
+    turns = [12, 9, 15, 12, 10]
+
+    one = Batch(gpu_ctx, 300_000, 8, 2048, chunk=16384)
+    ids1 = [one.add(z, dE, c.params, nb, wake=c.wake, seed=s, turns=t)
+            for (c, z, dE, nb, s), t in zip(specs, turns)]
+    one.advance(16)
+    assert sorted(one.poll()) == sorted(ids1)
+    outs1 = {}
+    for i, bid in enumerate(ids1):
+        dz = torch.empty(specs[i][1].size, dtype=torch.float64, device="cuda")
+        de = torch.empty_like(dz)
+        r = one.take_device(bid, dz.data_ptr(), de.data_ptr())
+        outs1[i] = (r, correlation_device(gpu_ctx, dz.data_ptr(), de.data_ptr(), dz.numel()))
+    one.close()
+
+    many = Batch(gpu_ctx, 300_000, 8, 2048, chunk=16384)
+    keep = [(z, dE) for (_, z, dE, _, _) in specs]          # host arrays alive for the call
+    ids, err = many.add_many([k[0] for k in keep], [k[1] for k in keep],
+                             [z.size for (_, z, _, _, _) in specs], [c.params for c, *_ in specs],
+                             [nb for (_, _, _, nb, _) in specs], [s for *_, s in specs], turns,
+                             wakes=[c.wake for c, *_ in specs])
+    assert err is None and len(ids) == 5
+    many.advance(16)
+    assert sorted(many.poll()) == sorted(ids)
+    res, corr = many.take_many(ids, correlation=True)
+    assert many.stats()["live"] == 0
+    for i in range(5):
+        r1, c1 = outs1[i]
+        assert (res[i].E0, res[i].sigma_E, res[i].sigma_z) == (r1.E0, r1.sigma_E, r1.sigma_z)
+        assert abs(corr[i] - c1) <= 1e-13
+    # admission stops at the first bunch with no room and says so
+    c, z, dE, nb, s = specs[2]                                # 123457 particles
+    ids, err = many.add_many([z] * 3, [dE] * 3, [z.size] * 3, [c.params] * 3, [nb] * 3,
+                             [s] * 3, [5] * 3)
+    assert len(ids) == 2 and err is not None and err.status == _lib.HJ_ERR_FULL
+    many.close()
