@@ -51,6 +51,7 @@ struct hj_ctx {
     void* dev = nullptr;            // W[B] | λ[B] | FFT(W)[M+1], a block of the cache
     size_t cap = 0;
     uint64_t used = 0;
+    int refs = 0;                   // bunches reading the tables (read-only)
   };
   std::map<std::array<uint64_t, 8>, WakeSet> wake_sets;
   uint64_t wake_clock = 0;
@@ -99,8 +100,6 @@ struct hj_bunch {
   double* W = nullptr;
   double2* Wf = nullptr;
   double2* twP = nullptr;
-  double2* Xg = nullptr;
-  double2* zE = nullptr;
   uint32_t* part_cnt = nullptr;
   unsigned long long* part_cic = nullptr;
   unsigned long long* ngp_ovf = nullptr;   // [B] overflow of the pass's 16-bit counters
@@ -112,7 +111,15 @@ struct hj_bunch {
   TurnState* h_ts = nullptr;  // pinned
   double* h_rf = nullptr;     // pinned staging of the RF table
   // the buffers above are carved from one device block and one pinned block
-  // of the context's cache; twP is the context's shared table
+  // of the context's cache; twP is the context's shared table; W, lam and Wf
+  // point into a wake set shared with other bunches (wset) or a private block
+  // (tables); pot, potd, hist and ngp_ovf are the first zero_bytes of the
+  // arena's histogram part
+  hj_ctx::WakeSet* wset = nullptr;
+  bool batch_member = false;
+  void* tables = nullptr;
+  size_t tables_cap = 0;
+  size_t zero_bytes = 0;
   void* arena = nullptr;
   size_t arena_cap = 0;
   void* harena = nullptr;
@@ -293,8 +300,14 @@ void cache_give(hj_ctx* ctx, bool host, void* p, size_t cap) {
 // Frees the kept blocks (carved ones stay for reuse unless `slabs` is set,
 // which also frees the slabs: only when no bunch or batch holds a block).
 void cache_clear(hj_ctx* ctx, bool slabs = false) {
-  for (auto& kv : ctx->wake_sets) cache_give(ctx, false, kv.second.dev, kv.second.cap);
-  ctx->wake_sets.clear();
+  for (auto it = ctx->wake_sets.begin(); it != ctx->wake_sets.end();) {
+    if (it->second.refs > 0 && !slabs) {
+      ++it;
+      continue;
+    }
+    cache_give(ctx, false, it->second.dev, it->second.cap);
+    it = ctx->wake_sets.erase(it);
+  }
   std::multimap<size_t, void*> keep;
   for (auto& kv : ctx->dev_free) {
     if (ctx->carved.count(kv.second)) keep.insert(kv);
@@ -535,6 +548,8 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   cudaStreamSynchronize(b->stream);       // nothing queued still uses the blocks
   cache_give(b->ctx, false, b->arena, b->arena_cap);
   cache_give(b->ctx, true, b->harena, b->harena_cap);
+  if (b->wset) b->wset->refs -= 1;
+  cache_give(b->ctx, false, b->tables, b->tables_cap);
   if (b->d_sums) cudaFree(b->d_sums);
   if (b->d_log) cudaFree(b->d_log);
   for (cudaEvent_t e : b->events) cudaEventDestroy(e);
@@ -592,6 +607,7 @@ static hj_status bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int6
   }
   b->cfg = cfg >= 0 ? cfg : (ctx->pass_layout >= 0 ? ctx->pass_layout : default_pass_layout(b->B, n));
   if (chunk > 0) {
+    b->batch_member = true;
     b->nblk = (int)std::max<int64_t>((n + chunk - 1) / chunk, 1);
   } else {
     const int bps = track_blocks_per_sm(b->B, b->qe_mode, b->use_wake, b->cfg);
@@ -604,19 +620,16 @@ static hj_status bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int6
     const size_t o_ts = c.add<TurnState>(1);
     const size_t o_sum = c.add<double>((size_t)kNumSums * nb);
     const size_t o_rf = c.add<double2>(kRfTableSize);
-    size_t o[11] = {};
+    size_t o[6] = {};
     if (b->use_wake) {
-      o[0] = c.add<double>(B);                                   // W
-      o[1] = c.add<double>(B);                                   // lam
-      o[2] = c.add<double2>((size_t)b->M + 1);                   // Wf
-      o[3] = c.add<double2>((size_t)b->M);                       // Xg
-      o[4] = c.add<double2>((size_t)std::max(b->H, 1));          // zE
-      o[5] = c.add<double>(B);                                   // pot
-      o[6] = c.add<double2>(B + 1);                              // potd
-      o[7] = c.add<unsigned long long>(3 * B + 2);               // hist
-      o[8] = c.add<uint32_t>(nb * B);                            // part_cnt
-      o[9] = c.add<unsigned long long>(nb * (B + 1));            // part_cic
-      o[10] = c.add<unsigned long long>(B);                      // ngp_ovf
+      // pot, potd, hist and ngp_ovf are adjacent: one memset zeroes them
+      o[0] = c.add<double>(B);                                   // pot
+      o[1] = c.add<double2>(B + 1);                              // potd
+      o[2] = c.add<unsigned long long>(3 * B + 2);               // hist
+      o[3] = c.add<unsigned long long>(B);                       // ngp_ovf
+      b->zero_bytes = c.off - o[0];
+      o[4] = c.add<uint32_t>(nb * B);                            // part_cnt
+      o[5] = c.add<unsigned long long>(nb * (B + 1));            // part_cic
     }
     HJ_TRY(cache_take(ctx, false, c.off, &b->arena, &b->arena_cap));
     char* a = (char*)b->arena;
@@ -625,17 +638,12 @@ static hj_status bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int6
     b->part_sum = (double*)(a + o_sum);
     b->rf_table = (double2*)(a + o_rf);
     if (b->use_wake) {
-      b->W = (double*)(a + o[0]);
-      b->lam = (double*)(a + o[1]);
-      b->Wf = (double2*)(a + o[2]);
-      b->Xg = (double2*)(a + o[3]);
-      b->zE = (double2*)(a + o[4]);
-      b->pot = (double*)(a + o[5]);
-      b->potd = (double2*)(a + o[6]);
-      b->hist = (unsigned long long*)(a + o[7]);
-      b->part_cnt = (uint32_t*)(a + o[8]);
-      b->part_cic = (unsigned long long*)(a + o[9]);
-      b->ngp_ovf = (unsigned long long*)(a + o[10]);
+      b->pot = (double*)(a + o[0]);
+      b->potd = (double2*)(a + o[1]);
+      b->hist = (unsigned long long*)(a + o[2]);
+      b->ngp_ovf = (unsigned long long*)(a + o[3]);
+      b->part_cnt = (uint32_t*)(a + o[4]);
+      b->part_cic = (unsigned long long*)(a + o[5]);
     }
     Carve hc;
     const size_t h_mom = hc.add<double>(4 * (size_t)b->nblk_m);
@@ -708,59 +716,75 @@ static hj_status bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid)
     }
     HJ_TRY(shared_twiddles(ctx, b->P, &b->twP));
     const size_t wbytes = sizeof(double) * B, fbytes = sizeof(double2) * ((size_t)b->M + 1);
-    std::vector<double> W, lam;
+    void* blk = nullptr;
     if (cached) {
-      const char* src = (const char*)cached->dev;
-      HJ_CUDA(ctx, cudaMemcpyAsync(b->W, src, wbytes, cudaMemcpyDeviceToDevice, b->stream));
-      HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, src + wbytes, wbytes, cudaMemcpyDeviceToDevice,
-                                   b->stream));
-      HJ_CUDA(ctx, cudaMemcpyAsync(b->Wf, src + 2 * wbytes, fbytes, cudaMemcpyDeviceToDevice,
-                                   b->stream));
+      blk = cached->dev;
     } else {
-      W.resize(B);
-      lam.resize(B);
-      host_wake_tables(b->centers.data(), B, b->w, W.data(), lam.data());
-      HJ_CUDA(ctx, cudaMemcpyAsync(b->W, W.data(), wbytes, cudaMemcpyHostToDevice, b->stream));
-      HJ_CUDA(ctx, cudaMemcpyAsync(b->lam, lam.data(), wbytes, cudaMemcpyHostToDevice, b->stream));
-      if (b->H >= 4)
-        HJ_CUDA(ctx, launch_wake_spectrum(b->W, B, b->P, b->M, b->H, b->logH, b->twP, b->Xg,
-                                          b->Wf, b->stream));
+      // W, λ and FFT(W) of this grid in one block of the cache, read-only for
+      // every bunch; kept in wake_sets for the next bunch when the grid was
+      // built here, else private to this bunch
+      size_t cap = 0;
+      HJ_TRY(cache_take(ctx, false, 2 * wbytes + fbytes, &blk, &cap));
+      double* W = (double*)blk;
+      std::vector<double> hW(B), hl(B);
+      host_wake_tables(b->centers.data(), B, b->w, hW.data(), hl.data());
+      cudaError_t e = cudaMemcpyAsync(W, hW.data(), wbytes, cudaMemcpyHostToDevice, b->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(W + B, hl.data(), wbytes, cudaMemcpyHostToDevice, b->stream);
+      void* xg = nullptr;
+      hj_status s = HJ_OK;
+      if (e == cudaSuccess && b->H >= 4) {
+        s = scratch(ctx, sizeof(double2) * (size_t)b->M, &xg);
+        if (s == HJ_OK)
+          e = launch_wake_spectrum(W, B, b->P, b->M, b->H, b->logH, b->twP, (double2*)xg,
+                                   (double2*)((char*)blk + 2 * wbytes), b->stream);
+      }
+      cudaError_t e2 = cudaStreamSynchronize(b->stream);   // host vectors, scratch
+      if (s == HJ_OK && (e != cudaSuccess || e2 != cudaSuccess))
+        s = set_err(ctx, HJ_ERR_CUDA, "wake tables: %s",
+                    cudaGetErrorString(e != cudaSuccess ? e : e2));
+      if (s != HJ_OK) {
+        cache_give(ctx, false, blk, cap);
+        return s;
+      }
       if (!grid) {
-        // keep this grid and its tables for the next bunch with the same key
-        // (at most 8 sets; the least recently used goes)
-        if (ctx->wake_sets.size() >= 8) {
-          auto lru = ctx->wake_sets.begin();
+        constexpr size_t kWakeSets = 8;
+        if (ctx->wake_sets.size() >= kWakeSets) {   // the least recently used free set goes
+          auto lru = ctx->wake_sets.end();
           for (auto it = ctx->wake_sets.begin(); it != ctx->wake_sets.end(); ++it)
-            if (it->second.used < lru->second.used) lru = it;
-          HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
-          cache_give(ctx, false, lru->second.dev, lru->second.cap);
-          ctx->wake_sets.erase(lru);
+            if (it->second.refs == 0 && (lru == ctx->wake_sets.end() || it->second.used < lru->second.used))
+              lru = it;
+          if (lru != ctx->wake_sets.end()) {
+            cache_give(ctx, false, lru->second.dev, lru->second.cap);
+            ctx->wake_sets.erase(lru);
+          }
         }
-        hj_ctx::WakeSet ws;
-        ws.centers = b->centers;
-        ws.e0 = g.edge_first;
-        ws.eN = g.edge_last;
-        ws.estep = g.edge_step;
-        ws.used = ++ctx->wake_clock;
-        HJ_TRY(cache_take(ctx, false, 2 * wbytes + fbytes, &ws.dev, &ws.cap));
-        char* dst = (char*)ws.dev;
-        HJ_CUDA(ctx, cudaMemcpyAsync(dst, b->W, wbytes, cudaMemcpyDeviceToDevice, b->stream));
-        HJ_CUDA(ctx, cudaMemcpyAsync(dst + wbytes, b->lam, wbytes, cudaMemcpyDeviceToDevice,
-                                     b->stream));
-        HJ_CUDA(ctx, cudaMemcpyAsync(dst + 2 * wbytes, b->Wf, fbytes, cudaMemcpyDeviceToDevice,
-                                     b->stream));
-        ctx->wake_sets.insert({key, std::move(ws)});
+        if (ctx->wake_sets.size() < kWakeSets) {
+          hj_ctx::WakeSet ws;
+          ws.centers = b->centers;
+          ws.e0 = g.edge_first;
+          ws.eN = g.edge_last;
+          ws.estep = g.edge_step;
+          ws.used = ++ctx->wake_clock;
+          ws.dev = blk;
+          ws.cap = cap;
+          cached = &ctx->wake_sets.insert({key, std::move(ws)}).first->second;
+        }
+      }
+      if (!cached) {
+        b->tables = blk;
+        b->tables_cap = cap;
       }
     }
-    HJ_CUDA(ctx, cudaMemsetAsync(b->pot, 0, sizeof(double) * B, b->stream));
-    HJ_CUDA(ctx, cudaMemsetAsync(b->potd, 0, sizeof(double2) * ((size_t)B + 1), b->stream));
-    HJ_CUDA(ctx, cudaMemsetAsync(b->hist, 0, sizeof(unsigned long long) * (3 * (size_t)B + 2),
-                                 b->stream));
-    if (!cached) HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));   // host vectors W, lam
+    if (cached) {
+      cached->refs += 1;
+      b->wset = cached;
+    }
+    b->W = (double*)blk;
+    b->lam = b->W + B;
+    b->Wf = (double2*)((char*)blk + 2 * wbytes);
+    HJ_CUDA(ctx, cudaMemsetAsync(b->pot, 0, b->zero_bytes, b->stream));   // pot potd hist ovf
   }
-
-  if (b->use_wake)
-    HJ_CUDA(ctx, cudaMemsetAsync(b->ngp_ovf, 0, sizeof(unsigned long long) * b->B, b->stream));
 
   // RF table, staged in the bunch's pinned block
   host_rf_table(params->voltage, params->phi_s, kRfTableSize, b->h_rf);
@@ -778,7 +802,10 @@ static hj_status bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid)
   *b->h_ts = t;
   // staged in pinned memory that lives as long as the bunch; later work on
   // the stream is ordered after the copy, host reads of h_ts synchronise first
-  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice, b->stream));
+  // (a batch member's state goes to the batch's array instead)
+  if (!b->batch_member)
+    HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
+                                 b->stream));
   return HJ_OK;
 }
 
@@ -895,8 +922,6 @@ static void fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
   g.lam = b->lam;
   g.Wf = b->Wf;
   g.twP = b->twP;
-  g.Xg = b->Xg;
-  g.zE = b->zE;
   g.pot = b->pot;
   g.potd = b->potd;
   g.hi_idx = b->hi_idx;
