@@ -1702,8 +1702,9 @@ extern "C" hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_
     return set_err(ctx, HJ_ERR_TOO_LARGE, "max_nbins = %d exceeds the supported %lld",
                    max_nbins, (long long)kMaxBins);
   if (chunk_particles == 0) chunk_particles = 65536;
-  if (chunk_particles < 4 || chunk_particles % 4)
-    return set_err(ctx, HJ_ERR_ARG, "chunk_particles must be a positive multiple of 4");
+  if (chunk_particles < 4 || chunk_particles % 4 || chunk_particles > kMaxBlockParticles)
+    return set_err(ctx, HJ_ERR_ARG, "chunk_particles must be a positive multiple of 4, at most %lld",
+                   (long long)kMaxBlockParticles);
   if (layout != -1 && !pass_cfg_valid(layout))
     return set_err(ctx, HJ_ERR_ARG, "pass layout must be -1 (automatic), 0..%d or 8..%d",
                    kNumPassCfgs - 1, kPassN32 + kNumPassCfgs - 1);

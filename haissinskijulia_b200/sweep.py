@@ -189,7 +189,7 @@ def wave_chunks(points: List[Point], num_sms: int, waves=(1, 2, 4)) -> List[int]
     out = []
     for w in waves:
         c = -(-total // (num_sms * w))
-        c = min(max((c + 3) // 4 * 4, 4096), 1 << 22)
+        c = min(max((c + 3) // 4 * 4, 4096), (1 << 20) - 8)   # a block counts < 2^20
         out.append(int(c))
     return out
 

@@ -311,9 +311,10 @@ hj_status hj_bunch_bins(hj_bunch* b);
 
 /* A batch on ctx's device with its own stream: a particle pool of
  * pool_particles (16 B each), up to max_bunches bunches of up to max_nbins
- * bins, chunk_particles particles per block of the pass (a multiple of 4;
- * 0 = 65536) and pass layout `layout` (-1 = the default for max_nbins; values
- * as for hj_set_pass_layout). */
+ * bins, chunk_particles particles per block of the pass (a multiple of 4, at
+ * most 2^20 - 8, what a block's packed cell counters can count; 0 = 65536)
+ * and pass layout `layout` (-1 = the default for max_nbins; values as for
+ * hj_set_pass_layout). */
 hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
                           int32_t max_nbins, int64_t chunk_particles, int32_t layout,
                           hj_batch** out);
