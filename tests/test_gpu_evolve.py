@@ -278,3 +278,16 @@ def test_single_particle_with_wake(gpu_ctx, oracle):
     p = Particles(np.array([0.0]), np.array([0.0]))
     with pytest.raises(HaissinskiError, match="HJ_ERR_NONFINITE"):
         longitudinal_evolve(p, quiet, buf, wake=cfg.wake)
+
+
+def test_invalid_pass_layouts_are_refused(gpu_ctx):
+    from haissinskijulia_b200 import Context, HaissinskiError
+    from haissinskijulia_b200 import _lib
+    ctx = Context(0)
+    for bad in (-2, 5, 7, 13, 16, 24):
+        with pytest.raises(HaissinskiError) as e:
+            ctx.set_pass_layout(bad)
+        assert e.value.status == _lib.HJ_ERR_ARG
+    for good in (-1, 0, 4, 8, 12):
+        ctx.set_pass_layout(good)
+    ctx.close()
