@@ -47,8 +47,10 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--layout", type=int, default=-1,
                     help="thread layout of the fused pass (-1 = library default)")
-    ap.add_argument("--e2e-calls", type=int, default=2)
-    ap.add_argument("--e2e-turns", type=int, default=1000)
+    ap.add_argument("--e2e-calls", type=int, default=1,
+                    help="timed longitudinal_evolve calls (after one warm-up call)")
+    ap.add_argument("--e2e-turns", type=int, default=10000,
+                    help="turns per call: the at-scale configuration's 10,000")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="bounded CPU work of the cpu_baseline leg")
     ap.add_argument("--reference-seconds", type=float, default=90.0,
