@@ -5,136 +5,13 @@
 // (particle pass, histogram reduction, bins step) whose turn-to-turn state
 // (E0, pending kick, turn counter) lives in device memory, so turns never
 // wait for the host.
-#include <algorithm>
-#include <array>
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <map>
-#include <string>
-#include <unordered_set>
-#include <vector>
-
-#include "hj_host.h"
-#include "hj_internal.h"
-
-using namespace hj;
-
-struct hj_ctx {
-  int device = 0;
-  int num_sms = 148;
-  int max_smem_optin = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  void* scratch = nullptr;
-  size_t scratch_bytes = 0;
-  int pass_layout = -1;   // -1: chosen per bunch
-  // released blocks kept for reuse, by size class (device / pinned host)
-  std::multimap<size_t, void*> dev_free, host_free;
-  size_t dev_free_bytes = 0, host_free_bytes = 0;
-  // device blocks up to kSlabBlockMax are carved from large slabs (a
-  // cudaMalloc of a megabyte costs ~0.6 ms); carved blocks are reused through
-  // dev_free and released with their slabs by hj_destroy
-  std::vector<void*> dev_slabs;
-  char* slab_cur = nullptr;
-  size_t slab_left = 0;
-  std::unordered_set<void*> carved;
-  // twiddle tables of the bins step by FFT length P, shared by all bunches
-  std::map<int, double2*> twiddles;
-  // grids and wake tables built from an initial σ_z, by the bit patterns of
-  // (nbins, σ_z0, half width, F, s, cτ, sin coefficient, δ width): bunches
-  // of a scan start from the same particles and share them
-  struct WakeSet {
-    std::vector<double> centers;
-    double e0 = 0, eN = 0, estep = 0;
-    void* dev = nullptr;            // W[B] | λ[B] | FFT(W)[M+1], a block of the cache
-    size_t cap = 0;
-    uint64_t used = 0;
-    int refs = 0;                   // bunches reading the tables (read-only)
-  };
-  std::map<std::array<uint64_t, 8>, WakeSet> wake_sets;
-  uint64_t wake_clock = 0;
-};
-
-struct hj_bunch {
-  hj_ctx* ctx = nullptr;
-  cudaStream_t stream = nullptr;
-  double* z = nullptr;
-  double* dE = nullptr;
-  int64_t n = 0;
-  hj_params p{};
-  hj_wake w{};
-  int use_wake = 0;
-  int B = 0, P = 0, M = 0, H = 0, logH = 0;
-  double e0 = 0, eN = 0, estep = 0, inv_e = 0, c1 = 0, cB = 0, inv_c = 0;
-  // interpolation the reference applies to every z >= cB (src/wakefield.jl:80-102):
-  // u = (cB - c1)/Δc, cell clamp(floor(u), 0, B-2), weight u - floor(u)
-  int hi_idx = 0;
-  double hi_w = 0;
-  std::vector<double> centers;
-  double sigma_E0_initial = 0, sigma_z0_initial = 0;
-  uint64_t seed = 0;
-  int qe_mode = QE_OFF;
-  const double* draws = nullptr;
-  int64_t draws_first = 0, draws_turns = 0;
-  int nblk = 1, nblk_m = 1;
-  // a shard of a bunch split over processes: its particles are
-  // [first_particle, first_particle + n) of n_global; the bins step reads the
-  // exchanged totals (d_sums, hist) instead of this shard's partials
-  bool shard = false;
-  int64_t n_global = 0, first_particle = 0;
-  double* d_sums = nullptr;
-  // turn log: a record every log_every turns into a ring of log_capacity
-  int64_t log_every = 0, log_capacity = 0, log_count = 0;
-  int log_density = 0;
-  double* d_log = nullptr;
-  int64_t turns_done = 0;
-  // device buffers
-  TurnState* ts = nullptr;
-  double* pot = nullptr;
-  double2* potd = nullptr;              // [B+1] kick table (cell j: pot[j-1], step)
-  int cfg = 0;                          // thread layout of the fused pass
-  unsigned long long* hist = nullptr;   // counts[B] | cell counts[B+1] | cell Σw·2^24 [B+1]
-  double* lam = nullptr;
-  double* W = nullptr;
-  double2* Wf = nullptr;
-  double2* twP = nullptr;
-  uint32_t* part_cnt = nullptr;
-  unsigned long long* part_cic = nullptr;
-  unsigned long long* ngp_ovf = nullptr;   // [B] overflow of the pass's 16-bit counters
-  double2* rf_table = nullptr;             // [kRfTableSize] RF kick table of the pass
-  double rf_Vs = 0;                        // its entry 0: V sin ϕs
-  double* part_sum = nullptr;
-  double* part_mom = nullptr;
-  double* h_mom = nullptr;    // pinned
-  TurnState* h_ts = nullptr;  // pinned
-  double* h_rf = nullptr;     // pinned staging of the RF table
-  // the buffers above are carved from one device block and one pinned block
-  // of the context's cache; twP is the context's shared table; W, lam and Wf
-  // point into a wake set shared with other bunches (wset) or a private block
-  // (tables); pot, potd, hist and ngp_ovf are the first zero_bytes of the
-  // arena's histogram part
-  hj_ctx::WakeSet* wset = nullptr;
-  bool batch_member = false;
-  void* tables = nullptr;
-  size_t tables_cap = 0;
-  size_t zero_bytes = 0;
-  void* arena = nullptr;
-  size_t arena_cap = 0;
-  void* harena = nullptr;
-  size_t harena_cap = 0;
-  // profiling: three events per profiled turn (before pass, after pass, after bins)
-  bool profiling = false;
-  std::vector<cudaEvent_t> events;
-  size_t events_used = 0;
-  int64_t profiled_turns = 0;
-  int64_t profiled_launches = 0;
-};
+#include "hj_state.h"
 
 namespace {
-
 const char* kVersion = "haissinski-b200 0.1.0 (sm_100a)";
+}  // namespace
+
+namespace hj_impl {
 
 hj_status set_err(hj_ctx* ctx, hj_status code, const char* fmt, ...) {
   if (ctx) {
@@ -148,32 +25,8 @@ hj_status set_err(hj_ctx* ctx, hj_status code, const char* fmt, ...) {
   return code;
 }
 
-#define HJ_CUDA(ctx, call)                                                            \
-  do {                                                                                \
-    cudaError_t e_ = (call);                                                          \
-    if (e_ != cudaSuccess)                                                            \
-      return set_err((ctx), e_ == cudaErrorMemoryAllocation ? HJ_ERR_NOMEM : HJ_ERR_CUDA, \
-                     "%s failed: %s", #call, cudaGetErrorString(e_));                 \
-  } while (0)
 
-#define HJ_TRY(expr)             \
-  do {                           \
-    hj_status s_ = (expr);       \
-    if (s_ != HJ_OK) return s_;  \
-  } while (0)
 
-template <typename T>
-hj_status dalloc(hj_ctx* ctx, T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) count = 1;
-  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return set_err(ctx, HJ_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T),
-                   cudaGetErrorString(e));
-  }
-  return HJ_OK;
-}
 
 int64_t next_pow2(int64_t n) {
   if (n <= 0) return 1;
@@ -223,7 +76,6 @@ hj_status scratch(hj_ctx* ctx, size_t bytes, void** out) {
   return HJ_OK;
 }
 
-size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
 
 // ---- block cache.  A bunch's buffers come from one device block and one
 // pinned block; released blocks are kept (up to a cap) for the next request
@@ -299,7 +151,7 @@ void cache_give(hj_ctx* ctx, bool host, void* p, size_t cap) {
 
 // Frees the kept blocks (carved ones stay for reuse unless `slabs` is set,
 // which also frees the slabs: only when no bunch or batch holds a block).
-void cache_clear(hj_ctx* ctx, bool slabs = false) {
+void cache_clear(hj_ctx* ctx, bool slabs) {
   for (auto it = ctx->wake_sets.begin(); it != ctx->wake_sets.end();) {
     if (it->second.refs > 0 && !slabs) {
       ++it;
@@ -347,16 +199,6 @@ hj_status shared_twiddles(hj_ctx* ctx, int P, double2** out) {
   return HJ_OK;
 }
 
-// Offsets of the buffers carved from one block (each 256-byte aligned).
-struct Carve {
-  size_t off = 0;
-  template <class T>
-  size_t add(size_t count) {
-    const size_t o = off;
-    off = align_up(off + sizeof(T) * (count ? count : 1));
-    return o;
-  }
-};
 
 hj_status check_params(hj_ctx* ctx, const hj_params* p) {
   if (!p) return set_err(ctx, HJ_ERR_ARG, "params is NULL");
@@ -462,7 +304,7 @@ cudaError_t set_kernel_attributes(hj_ctx* ctx) {
   return e;
 }
 
-}  // namespace
+}  // namespace hj_impl
 
 // ====================================================================== context
 
@@ -564,11 +406,10 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
 // chunk > 0: a batch member, whose partial slots are its chunks of `chunk`
 // particles (the batch's chunk table) instead of one per block of the grid;
 // cfg >= 0 pins the pass layout.
-static hj_status bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
-                                    const hj_params* params, const hj_wake* wake,
-                                    int64_t nbins, const hj_grid* grid, uint64_t seed,
-                                    void* stream, hj_bunch* b, int64_t chunk = 0,
-                                    int cfg = -1) {
+hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                      const hj_params* params, const hj_wake* wake,
+                                      int64_t nbins, const hj_grid* grid, uint64_t seed,
+                                      void* stream, hj_bunch* b, int64_t chunk, int cfg) {
   b->ctx = ctx;
   b->stream = (cudaStream_t)stream;
   b->z = d_z;
@@ -663,7 +504,7 @@ static hj_status bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int6
   return HJ_OK;
 }
 
-static hj_status bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid) {
+hj_status hj_impl::bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid) {
   const int64_t n = b->n;
   const hj_params* params = &b->p;
   double m[4];
@@ -809,11 +650,10 @@ static hj_status bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid)
   return HJ_OK;
 }
 
-static hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
-                                   const hj_params* params, const hj_wake* wake,
-                                   int64_t nbins, const hj_grid* grid, uint64_t seed,
-                                   void* stream, hj_bunch* b, int64_t chunk = 0,
-                                   int cfg = -1) {
+hj_status hj_impl::bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                     const hj_params* params, const hj_wake* wake,
+                                     int64_t nbins, const hj_grid* grid, uint64_t seed,
+                                     void* stream, hj_bunch* b, int64_t chunk, int cfg) {
   HJ_TRY(bunch_create_begin(ctx, d_z, d_dE, n, params, wake, nbins, grid, seed, stream, b,
                             chunk, cfg));
   HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
@@ -857,7 +697,7 @@ extern "C" hj_status hj_bunch_set_draws(hj_bunch* b, const double* d_draws, int6
 }
 
 // Arguments of the fused pass and of the bins step of bunch b.
-static void fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
+void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
   a = PassArgs{};
   a.z = b->z;
   a.dE = b->dE;
@@ -1413,961 +1253,4 @@ extern "C" hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE
     HJ_CUDA(ctx, launch_interp_kick(ex[0], ex[1], n, cb.pot, B, c1, cB, inv_c, ctx->stream));
   }
   return unstage(ctx, n, dE, ex[1]);
-}
-
-// ====================================================================== batches
-//
-// A batch holds hj_bunch objects whose particles live in one pool and whose
-// turn state lives in one device array (slot per bunch), so a poll is one
-// copy.  Per turn: k_batch_pass over the chunk table, k_batch_reduce, and
-// k_batch_bins (one 2-CTA cluster per bunch); the kernels read the bunch
-// tables and the live counts from device memory and are launched over the
-// batch's capacity, so a captured graph stays valid as bunches come and go.
-// A bunch's chunking depends only on its own size and the batch's chunk size,
-// so its sums -- and its results -- do not depend on the other bunches.
-
-struct BatchMember {
-  int64_t id = 0;
-  hj_bunch* b = nullptr;
-  int64_t start = 0, cap = 0;   // pool range [start, start + cap)
-  int slot = 0;                 // index into the turn-state array
-  int64_t turns = 0;
-};
-
-struct hj_batch {
-  hj_ctx* ctx = nullptr;
-  cudaStream_t stream = nullptr;
-  int cfg = 0;
-  int64_t chunk = 65536;
-  int max_bunches = 0, max_B = 0, max_H = 0, max_chunks = 0;
-  // launch widths: the live counts rounded up to a power of two (a captured
-  // graph is re-captured only when the live counts outgrow them)
-  int grid_chunks = 0, grid_bunches = 0, grid_items = 0;
-  int wake = -1, qe = -1;                      // fixed by the first bunch
-  int64_t pool_n = 0;
-  double* pool_z = nullptr;
-  double* pool_dE = nullptr;
-  std::vector<std::pair<int64_t, int64_t>> free_ranges;   // (start, length), sorted
-  std::vector<BatchMember> members;            // dense: index = device table slot
-  std::vector<int> free_slots;
-  int64_t next_id = 1;
-  TurnState* d_ts = nullptr;                   // [max_bunches]
-  TurnState* h_ts = nullptr;                   // pinned copy for polls
-  PassArgs* d_pass = nullptr;
-  BinsArgs* d_bins = nullptr;
-  BatchChunk* d_chunks = nullptr;
-  BatchChunk* d_items = nullptr;               // merge table: groups of a bunch's partial slots
-  int32_t* d_counts = nullptr;                 // [0] chunks, [1] bunches, [2] merge items
-  PassArgs* h_pass = nullptr;                  // pinned staging
-  BinsArgs* h_bins = nullptr;
-  BatchChunk* h_chunks = nullptr;
-  BatchChunk* h_items = nullptr;
-  int32_t* h_counts = nullptr;
-  // the buffers above are carved from one device and one pinned cached block
-  void* arena = nullptr;
-  size_t arena_cap = 0;
-  void* harena = nullptr;
-  size_t harena_cap = 0;
-  bool dirty = true;
-  int bins_ctas = 2;                           // CTAs per bunch in the bins step
-  int graph_turns = 16;
-  cudaGraphExec_t graph = nullptr;
-  int64_t turns_enqueued = 0;
-};
-
-namespace {
-
-hj_status batch_alloc_range(hj_batch* bt, int64_t n, int64_t* start, int64_t* cap) {
-  const int64_t need = std::max<int64_t>((n + 3) / 4 * 4, 4);
-  for (size_t i = 0; i < bt->free_ranges.size(); ++i) {
-    auto& r = bt->free_ranges[i];
-    if (r.second >= need) {
-      *start = r.first;
-      *cap = need;
-      r.first += need;
-      r.second -= need;
-      if (r.second == 0) bt->free_ranges.erase(bt->free_ranges.begin() + i);
-      return HJ_OK;
-    }
-  }
-  return HJ_ERR_FULL;
-}
-
-void batch_free_range(hj_batch* bt, int64_t start, int64_t cap) {
-  auto& fr = bt->free_ranges;
-  auto it = std::lower_bound(fr.begin(), fr.end(), std::make_pair(start, (int64_t)0));
-  it = fr.insert(it, {start, cap});
-  // merge with the neighbours
-  size_t i = it - fr.begin();
-  if (i + 1 < fr.size() && fr[i].first + fr[i].second == fr[i + 1].first) {
-    fr[i].second += fr[i + 1].second;
-    fr.erase(fr.begin() + i + 1);
-  }
-  if (i > 0 && fr[i - 1].first + fr[i - 1].second == fr[i].first) {
-    fr[i - 1].second += fr[i].second;
-    fr.erase(fr.begin() + i);
-  }
-}
-
-int64_t batch_largest_free(const hj_batch* bt) {
-  int64_t m = 0;
-  for (auto& r : bt->free_ranges) m = std::max(m, r.second);
-  return m;
-}
-
-// Rebuild and upload the device tables (bunch arguments, chunk table, counts).
-hj_status batch_upload(hj_batch* bt) {
-  hj_ctx* ctx = bt->ctx;
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));   // staging buffers are free again
-  int nch = 0;
-  const int nb = (int)bt->members.size();
-  for (int k = 0; k < nb; ++k) {
-    hj_bunch* b = bt->members[k].b;
-    fill_turn_args(b, bt->h_pass[k], bt->h_bins[k]);
-    for (int c = 0; c < b->nblk; ++c) {
-      BatchChunk ch;
-      ch.first = (int64_t)c * bt->chunk;
-      ch.count = std::min<int64_t>(bt->chunk, b->n - ch.first);
-      ch.bunch = k;
-      ch.part = c;
-      if (nch >= bt->max_chunks) return set_err(ctx, HJ_ERR_STATE, "batch chunk table overflow");
-      bt->h_chunks[nch++] = ch;
-    }
-  }
-  // full chunks first, then the partial ones largest first: the last wave of
-  // blocks is made of the shortest chunks
-  std::stable_sort(bt->h_chunks, bt->h_chunks + nch,
-                   [](const BatchChunk& x, const BatchChunk& y) { return x.count > y.count; });
-  // merge table: each bunch's partial slots in groups of kMergeGroup
-  constexpr int kMergeGroup = 4;
-  int nit = 0;
-  for (int k = 0; k < nb; ++k) {
-    const int np = bt->members[k].b->nblk;
-    for (int p0 = 0; p0 < np; p0 += kMergeGroup) {
-      if (nit >= bt->max_chunks) return set_err(ctx, HJ_ERR_STATE, "batch merge table overflow");
-      BatchChunk it;
-      it.first = p0;
-      it.count = std::min(kMergeGroup, np - p0);
-      it.bunch = k;
-      it.part = 0;
-      bt->h_items[nit++] = it;
-    }
-  }
-  bt->h_counts[0] = nch;
-  bt->h_counts[1] = nb;
-  bt->h_counts[2] = nit;
-  if (nch > bt->grid_chunks || nb > bt->grid_bunches || nit > bt->grid_items) {
-    bt->grid_chunks = std::max(bt->grid_chunks, (int)std::min<int64_t>(next_pow2(nch), bt->max_chunks));
-    bt->grid_bunches = std::max(bt->grid_bunches, (int)std::min<int64_t>(next_pow2(nb), bt->max_bunches));
-    bt->grid_items = std::max(bt->grid_items, (int)std::min<int64_t>(next_pow2(nit), bt->max_chunks));
-    if (bt->graph) {
-      cudaGraphExecDestroy(bt->graph);
-      bt->graph = nullptr;
-    }
-  }
-  if (nb > 0) {
-    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_pass, bt->h_pass, sizeof(PassArgs) * nb,
-                                 cudaMemcpyHostToDevice, bt->stream));
-    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_bins, bt->h_bins, sizeof(BinsArgs) * nb,
-                                 cudaMemcpyHostToDevice, bt->stream));
-  }
-  if (nch > 0)
-    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_chunks, bt->h_chunks, sizeof(BatchChunk) * nch,
-                                 cudaMemcpyHostToDevice, bt->stream));
-  if (nit > 0)
-    HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_items, bt->h_items, sizeof(BatchChunk) * nit,
-                                 cudaMemcpyHostToDevice, bt->stream));
-  HJ_CUDA(ctx, cudaMemcpyAsync(bt->d_counts, bt->h_counts, sizeof(int32_t) * 3,
-                               cudaMemcpyHostToDevice, bt->stream));
-  bt->dirty = false;
-  return HJ_OK;
-}
-
-hj_status batch_launch_turn(hj_batch* bt) {
-  hj_ctx* ctx = bt->ctx;
-  HJ_CUDA(ctx, launch_batch_pass(bt->d_pass, bt->d_chunks, bt->d_counts, bt->grid_chunks,
-                                 bt->max_B, bt->wake, bt->qe, bt->cfg, bt->stream));
-  if (bt->wake)
-    HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_items, bt->d_counts + 2, bt->grid_items,
-                                     bt->max_B, bt->stream));
-  HJ_CUDA(ctx, launch_batch_bins(bt->d_bins, bt->d_counts + 1, bt->grid_bunches, bt->max_H,
-                                 bt->bins_ctas, bt->stream));
-  return HJ_OK;
-}
-
-hj_status batch_capture(hj_batch* bt) {
-  hj_ctx* ctx = bt->ctx;
-  cudaGraph_t g = nullptr;
-  HJ_CUDA(ctx, cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
-  hj_status s = HJ_OK;
-  for (int t = 0; t < bt->graph_turns && s == HJ_OK; ++t) s = batch_launch_turn(bt);
-  cudaError_t e = cudaStreamEndCapture(bt->stream, &g);
-  if (s != HJ_OK) {
-    if (g) cudaGraphDestroy(g);
-    return s;
-  }
-  if (e != cudaSuccess)
-    return set_err(ctx, HJ_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&bt->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess)
-    return set_err(ctx, HJ_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
-  return HJ_OK;
-}
-
-int batch_find(const hj_batch* bt, int64_t id) {
-  for (size_t k = 0; k < bt->members.size(); ++k)
-    if (bt->members[k].id == id) return (int)k;
-  return -1;
-}
-
-}  // namespace
-
-extern "C" void hj_batch_destroy(hj_batch* bt) {
-  if (!bt) return;
-  cudaSetDevice(bt->ctx->device);
-  if (bt->stream) cudaStreamSynchronize(bt->stream);
-  for (auto& m : bt->members) {
-    m.b->ts = nullptr;   // lives in the batch's array
-    hj_bunch_destroy(m.b);
-  }
-  if (bt->graph) cudaGraphExecDestroy(bt->graph);
-  cache_give(bt->ctx, false, bt->arena, bt->arena_cap);
-  cache_give(bt->ctx, true, bt->harena, bt->harena_cap);
-  if (bt->stream) cudaStreamDestroy(bt->stream);
-  delete bt;
-}
-
-static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
-                                   int32_t max_nbins, int64_t chunk, int32_t layout,
-                                   hj_batch* bt) {
-  bt->ctx = ctx;
-  bt->chunk = chunk;
-  bt->max_bunches = max_bunches;
-  bt->max_B = max_nbins;
-  const int64_t P = next_pow2(2 * (int64_t)max_nbins);
-  bt->max_H = (int)std::max<int64_t>(P / 4, 4);
-  bt->bins_ctas = batch_bins_ctas(bt->max_H, max_bunches, ctx->num_sms);
-  bt->cfg = layout >= 0 ? layout : default_pass_layout(max_nbins, pool_particles);
-  bt->pool_n = (pool_particles + 3) / 4 * 4;
-  bt->max_chunks = (int)std::min<int64_t>(bt->pool_n / chunk + max_bunches + 1, INT32_MAX);
-  HJ_CUDA(ctx, cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking));
-  // the pool and the tables: one device and one pinned block of the context's cache
-  const size_t nb = (size_t)max_bunches, nc = (size_t)bt->max_chunks;
-  Carve c;
-  const size_t o_z = c.add<double>((size_t)bt->pool_n), o_e = c.add<double>((size_t)bt->pool_n);
-  const size_t o_ts = c.add<TurnState>(nb), o_pass = c.add<PassArgs>(nb);
-  const size_t o_bins = c.add<BinsArgs>(nb), o_ch = c.add<BatchChunk>(nc);
-  const size_t o_it = c.add<BatchChunk>(nc), o_cnt = c.add<int32_t>(3);
-  HJ_TRY(cache_take(ctx, false, c.off, &bt->arena, &bt->arena_cap));
-  char* a = (char*)bt->arena;
-  bt->pool_z = (double*)(a + o_z);
-  bt->pool_dE = (double*)(a + o_e);
-  bt->d_ts = (TurnState*)(a + o_ts);
-  bt->d_pass = (PassArgs*)(a + o_pass);
-  bt->d_bins = (BinsArgs*)(a + o_bins);
-  bt->d_chunks = (BatchChunk*)(a + o_ch);
-  bt->d_items = (BatchChunk*)(a + o_it);
-  bt->d_counts = (int32_t*)(a + o_cnt);
-  Carve h;
-  const size_t p_ts = h.add<TurnState>(nb), p_pass = h.add<PassArgs>(nb);
-  const size_t p_bins = h.add<BinsArgs>(nb), p_ch = h.add<BatchChunk>(nc);
-  const size_t p_it = h.add<BatchChunk>(nc), p_cnt = h.add<int32_t>(3);
-  HJ_TRY(cache_take(ctx, true, h.off, &bt->harena, &bt->harena_cap));
-  char* q = (char*)bt->harena;
-  bt->h_ts = (TurnState*)(q + p_ts);
-  bt->h_pass = (PassArgs*)(q + p_pass);
-  bt->h_bins = (BinsArgs*)(q + p_bins);
-  bt->h_chunks = (BatchChunk*)(q + p_ch);
-  bt->h_items = (BatchChunk*)(q + p_it);
-  bt->h_counts = (int32_t*)(q + p_cnt);
-  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_counts, 0, sizeof(int32_t) * 3, bt->stream));
-  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_ts, 0, sizeof(TurnState) * max_bunches, bt->stream));
-  bt->free_ranges.push_back({0, bt->pool_n});
-  for (int s = max_bunches - 1; s >= 0; --s) bt->free_slots.push_back(s);
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
-                                     int32_t max_nbins, int64_t chunk_particles,
-                                     int32_t layout, hj_batch** out) {
-  HJ_TRY(ctx_ok(ctx));
-  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
-  *out = nullptr;
-  if (pool_particles <= 0 || max_bunches <= 0)
-    return set_err(ctx, HJ_ERR_ARG, "pool_particles and max_bunches must be positive");
-  if (max_nbins <= 0) return set_err(ctx, HJ_ERR_NBINS, "Buffer nbins invalid (must be > 0).");
-  if (max_nbins > kMaxBins)
-    return set_err(ctx, HJ_ERR_TOO_LARGE, "max_nbins = %d exceeds the supported %lld",
-                   max_nbins, (long long)kMaxBins);
-  if (chunk_particles == 0) chunk_particles = 65536;
-  if (chunk_particles < 4 || chunk_particles % 4 || chunk_particles > kMaxBlockParticles)
-    return set_err(ctx, HJ_ERR_ARG, "chunk_particles must be a positive multiple of 4, at most %lld",
-                   (long long)kMaxBlockParticles);
-  if (layout != -1 && !pass_cfg_valid(layout))
-    return set_err(ctx, HJ_ERR_ARG, "pass layout must be -1 (automatic), 0..%d or 8..%d",
-                   kNumPassCfgs - 1, kPassN32 + kNumPassCfgs - 1);
-  hj_batch* bt = new hj_batch();
-  hj_status s = batch_create_impl(ctx, pool_particles, max_bunches, max_nbins, chunk_particles,
-                                  layout, bt);
-  if (s != HJ_OK) {
-    hj_batch_destroy(bt);
-    return s;
-  }
-  *out = bt;
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns) {
-  if (!bt) return HJ_ERR_ARG;
-  if (turns < 0) return set_err(bt->ctx, HJ_ERR_ARG, "graph turns must be >= 0");
-  if (bt->graph) {
-    HJ_CUDA(bt->ctx, cudaStreamSynchronize(bt->stream));
-    cudaGraphExecDestroy(bt->graph);
-    bt->graph = nullptr;
-  }
-  bt->graph_turns = turns;
-  return HJ_OK;
-}
-
-// z, dE != NULL: copy them into the pool; else generate independent
-// Gaussians (σ_z, σ_E) from init_seed in place.
-// Admission in two halves (see bunch_create_begin): the first checks the
-// bunch, reserves its slot and pool range, fills its particles and enqueues
-// its initial moments; the second, after the stream has reached them,
-// completes the bunch and makes it a member.
-struct PendingAdd {
-  hj_bunch* b = nullptr;
-  int64_t start = 0, cap = 0, turns = 0;
-  int slot = -1;
-};
-
-static void batch_add_abort(hj_batch* bt, PendingAdd& p) {
-  if (p.b) hj_bunch_destroy(p.b);
-  if (p.cap) batch_free_range(bt, p.start, p.cap);
-  if (p.slot >= 0) bt->free_slots.push_back(p.slot);
-  p = PendingAdd{};
-}
-
-static hj_status batch_add_begin(hj_batch* bt, const double* z, const double* dE, int64_t n,
-                                 const hj_params* params, const hj_wake* wake, int64_t nbins,
-                                 uint64_t seed, int64_t turns, double sigma_z, double sigma_E,
-                                 uint64_t init_seed, PendingAdd* out) {
-  hj_ctx* ctx = bt->ctx;
-  HJ_TRY(check_params(ctx, params));
-  if (n <= 0) return set_err(ctx, HJ_ERR_ARG, "a batch bunch needs at least one particle");
-  if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
-  const int wake_on = params->use_wakefield ? 1 : 0;
-  const int qe = params->use_excitation ? QE_PHILOX : QE_OFF;
-  if ((bt->wake >= 0 && bt->wake != wake_on) || (bt->qe >= 0 && bt->qe != qe))
-    return set_err(ctx, HJ_ERR_ARG,
-                   "all bunches of a batch share the wakefield and quantum-excitation switches");
-  if (wake_on && nbins > bt->max_B)
-    return set_err(ctx, HJ_ERR_FULL, "nbins = %lld exceeds the batch's %d",
-                   (long long)nbins, bt->max_B);
-  if (bt->free_slots.empty()) return set_err(ctx, HJ_ERR_FULL, "the batch's bunch slots are full");
-  PendingAdd p;
-  if (batch_alloc_range(bt, n, &p.start, &p.cap) != HJ_OK)
-    return set_err(ctx, HJ_ERR_FULL, "no free pool range of %lld particles", (long long)n);
-  p.slot = bt->free_slots.back();
-  bt->free_slots.pop_back();
-  p.turns = turns;
-  double* dz = bt->pool_z + p.start;
-  double* de = bt->pool_dE + p.start;
-  cudaError_t e;
-  if (z) {
-    e = cudaMemcpyAsync(dz, z, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(de, dE, sizeof(double) * n, cudaMemcpyDefault, bt->stream);
-  } else {
-    e = launch_gaussian_bunch(init_seed, n, 0.0, sigma_z, 0.0, sigma_E, dz, de, bt->stream);
-  }
-  if (e != cudaSuccess) {
-    batch_add_abort(bt, p);
-    return set_err(ctx, HJ_ERR_CUDA, "copying the bunch into the pool failed: %s",
-                   cudaGetErrorString(e));
-  }
-  p.b = new hj_bunch();
-  hj_status s = bunch_create_begin(ctx, dz, de, n, params, wake, nbins, nullptr, seed,
-                                   (void*)bt->stream, p.b, bt->chunk, bt->cfg);
-  if (s == HJ_OK && p.b->nblk > bt->max_chunks) s = set_err(ctx, HJ_ERR_FULL, "chunk table full");
-  if (s != HJ_OK) {
-    batch_add_abort(bt, p);
-    return s;
-  }
-  bt->wake = wake_on;
-  bt->qe = qe;
-  *out = p;
-  return HJ_OK;
-}
-
-static hj_status batch_add_end(hj_batch* bt, PendingAdd& p, int64_t* id_out) {
-  hj_ctx* ctx = bt->ctx;
-  hj_status s = bunch_create_end(ctx, p.b, nullptr);
-  if (s != HJ_OK) {
-    batch_add_abort(bt, p);
-    return s;
-  }
-  // move the turn state into the batch's array, with this bunch's turn budget
-  hj_bunch* b = p.b;
-  b->h_ts->turns_left = p.turns;
-  b->ts = bt->d_ts + p.slot;         // the arena's own TurnState stays unused
-  cudaError_t e = cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
-                                  bt->stream);   // ordered before the next turn's kernels
-  if (e != cudaSuccess) {
-    batch_add_abort(bt, p);
-    return set_err(ctx, HJ_ERR_CUDA, "turn state upload failed: %s", cudaGetErrorString(e));
-  }
-  BatchMember m;
-  m.id = bt->next_id++;
-  m.b = b;
-  m.start = p.start;
-  m.cap = p.cap;
-  m.slot = p.slot;
-  m.turns = p.turns;
-  bt->members.push_back(m);
-  bt->dirty = true;
-  *id_out = m.id;
-  p = PendingAdd{};
-  return HJ_OK;
-}
-
-static hj_status batch_add_impl(hj_batch* bt, const double* z, const double* dE, int64_t n,
-                                const hj_params* params, const hj_wake* wake, int64_t nbins,
-                                uint64_t seed, int64_t turns, int64_t* id_out, double sigma_z,
-                                double sigma_E, uint64_t init_seed) {
-  if (!bt) return HJ_ERR_ARG;
-  hj_ctx* ctx = bt->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (!id_out) return set_err(ctx, HJ_ERR_ARG, "id_out is NULL");
-  *id_out = 0;
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  PendingAdd p;
-  HJ_TRY(batch_add_begin(bt, z, dE, n, params, wake, nbins, seed, turns, sigma_z, sigma_E,
-                         init_seed, &p));
-  cudaError_t e = cudaStreamSynchronize(bt->stream);
-  if (e != cudaSuccess) {
-    batch_add_abort(bt, p);
-    return set_err(ctx, HJ_ERR_CUDA, "%s", cudaGetErrorString(e));
-  }
-  return batch_add_end(bt, p, id_out);
-}
-
-extern "C" hj_status hj_batch_add(hj_batch* bt, const double* z, const double* dE, int64_t n,
-                                  const hj_params* params, const hj_wake* wake, int64_t nbins,
-                                  uint64_t seed, int64_t turns, int64_t* id_out) {
-  if (bt && (!z || !dE)) return set_err(bt->ctx, HJ_ERR_ARG, "particle arrays are NULL");
-  return batch_add_impl(bt, z, dE, n, params, wake, nbins, seed, turns, id_out, 0.0, 0.0, 0);
-}
-
-extern "C" hj_status hj_batch_add_gaussian(hj_batch* bt, int64_t n, double sigma_z,
-                                           double sigma_E, uint64_t init_seed,
-                                           const hj_params* params, const hj_wake* wake,
-                                           int64_t nbins, uint64_t seed, int64_t turns,
-                                           int64_t* id_out) {
-  if (bt && !(sigma_z >= 0.0 && sigma_E >= 0.0))
-    return set_err(bt->ctx, HJ_ERR_ARG, "spreads must be non-negative");
-  return batch_add_impl(bt, nullptr, nullptr, n, params, wake, nbins, seed, turns, id_out,
-                        sigma_z, sigma_E, init_seed);
-}
-
-extern "C" hj_status hj_batch_add_many(hj_batch* bt, int32_t count, const double* const* z,
-                                       const double* const* dE, const int64_t* n,
-                                       const hj_params* params, const hj_wake* wakes,
-                                       const int64_t* nbins, const uint64_t* seeds,
-                                       const int64_t* turns, int64_t* ids_out,
-                                       int32_t* n_added) {
-  if (!bt) return HJ_ERR_ARG;
-  hj_ctx* ctx = bt->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (!n_added) return set_err(ctx, HJ_ERR_ARG, "n_added is NULL");
-  *n_added = 0;
-  if (count < 0) return set_err(ctx, HJ_ERR_ARG, "count must be >= 0");
-  if (count > 0 && (!z || !dE || !n || !params || !nbins || !seeds || !turns || !ids_out))
-    return set_err(ctx, HJ_ERR_ARG, "an argument array is NULL");
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  std::vector<PendingAdd> pend;
-  pend.reserve(count);
-  hj_status first = HJ_OK;
-  std::string first_msg;
-  for (int k = 0; k < count; ++k) {
-    PendingAdd p;
-    hj_status s = (!z[k] || !dE[k])
-                      ? set_err(ctx, HJ_ERR_ARG, "particle arrays of bunch %d are NULL", k)
-                      : batch_add_begin(bt, z[k], dE[k], n[k], &params[k],
-                                        wakes ? &wakes[k] : nullptr, nbins[k], seeds[k],
-                                        turns[k], 0.0, 0.0, 0, &p);
-    if (s != HJ_OK) {
-      first = s;
-      first_msg = ctx->err;
-      break;
-    }
-    pend.push_back(p);
-  }
-  cudaError_t e = cudaStreamSynchronize(bt->stream);
-  if (e != cudaSuccess) {
-    for (auto& p : pend) batch_add_abort(bt, p);
-    return set_err(ctx, HJ_ERR_CUDA, "%s", cudaGetErrorString(e));
-  }
-  for (size_t k = 0; k < pend.size(); ++k) {
-    hj_status s = batch_add_end(bt, pend[k], &ids_out[k]);
-    if (s != HJ_OK) {
-      for (size_t j = k + 1; j < pend.size(); ++j) batch_add_abort(bt, pend[j]);
-      *n_added = (int32_t)k;
-      return s;
-    }
-  }
-  *n_added = (int32_t)pend.size();
-  if (first != HJ_OK) ctx->err = first_msg;
-  return first;
-}
-
-extern "C" hj_status hj_batch_take_many(hj_batch* bt, int32_t count, const int64_t* ids,
-                                        double* const* z_out, double* const* dE_out,
-                                        hj_result* res, double* corr_out) {
-  if (!bt) return HJ_ERR_ARG;
-  hj_ctx* ctx = bt->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (count < 0 || (count > 0 && !ids)) return set_err(ctx, HJ_ERR_ARG, "bad id list");
-  std::vector<hj_bunch*> bs(count);
-  for (int k = 0; k < count; ++k) {
-    const int j = batch_find(bt, ids[k]);
-    if (j < 0) return set_err(ctx, HJ_ERR_ARG, "no bunch %lld in the batch", (long long)ids[k]);
-    for (int q = 0; q < k; ++q)
-      if (ids[q] == ids[k]) return set_err(ctx, HJ_ERR_ARG, "bunch %lld listed twice", (long long)ids[k]);
-    bs[k] = bt->members[j].b;
-  }
-  // one round trip for all: pending kick and re-centring in place, moments,
-  // turn state, copies out, and every slot's state set to "no turns left"
-  TurnState dead{};
-  dead.turns_left = 0;
-  for (int k = 0; k < count; ++k) {
-    hj_bunch* b = bs[k];
-    HJ_TRY(launch_moments(b, 1, b->z, b->dE));
-    HJ_CUDA(ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 4 * b->nblk_m,
-                                 cudaMemcpyDeviceToHost, bt->stream));
-    HJ_CUDA(ctx, cudaMemcpyAsync(b->h_ts, b->ts, sizeof(TurnState), cudaMemcpyDeviceToHost,
-                                 bt->stream));
-    if (z_out && z_out[k])
-      HJ_CUDA(ctx, cudaMemcpyAsync(z_out[k], b->z, sizeof(double) * b->n, cudaMemcpyDefault,
-                                   bt->stream));
-    if (dE_out && dE_out[k])
-      HJ_CUDA(ctx, cudaMemcpyAsync(dE_out[k], b->dE, sizeof(double) * b->n, cudaMemcpyDefault,
-                                   bt->stream));
-    HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, &dead, sizeof(TurnState), cudaMemcpyHostToDevice,
-                                 bt->stream));
-  }
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  hj_status st = HJ_OK;
-  std::vector<double> mean_z(count), mean_e(count);
-  for (int k = 0; k < count; ++k) {
-    hj_bunch* b = bs[k];
-    double m[4];
-    sum_moments(b, m);
-    hj_status s = state_status(b);
-    if (st == HJ_OK) st = s;
-    if (res) fill_result(b, m, &res[k]);
-    mean_z[k] = m[0] / (double)b->n;
-    mean_e[k] = m[2] / (double)b->n;
-  }
-  if (corr_out) {
-    // cor(z, ΔE) of the final particles (the second pass of hj_correlation,
-    // about the means above), partial sums in the moments' buffers
-    for (int k = 0; k < count; ++k) {
-      hj_bunch* b = bs[k];
-      HJ_CUDA(ctx, launch_cor_parts(b->z, b->dE, b->n, mean_z[k], mean_e[k], 1, b->part_mom,
-                                    b->nblk_m, bt->stream));
-      HJ_CUDA(ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 3 * b->nblk_m,
-                                   cudaMemcpyDeviceToHost, bt->stream));
-    }
-    HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-    for (int k = 0; k < count; ++k) {
-      hj_bunch* b = bs[k];
-      double sxx = 0.0, syy = 0.0, sxy = 0.0;
-      for (int q = 0; q < b->nblk_m; ++q) {
-        sxx += b->h_mom[3 * q];
-        syy += b->h_mom[3 * q + 1];
-        sxy += b->h_mom[3 * q + 2];
-      }
-      const double r = sxy / (std::sqrt(sxx) * std::sqrt(syy));
-      corr_out[k] = r != r ? r : std::min(1.0, std::max(-1.0, r));
-    }
-  }
-  for (int k = 0; k < count; ++k) {
-    const int j = batch_find(bt, ids[k]);
-    BatchMember m = bt->members[j];
-    m.b->ts = nullptr;
-    hj_bunch_destroy(m.b);
-    batch_free_range(bt, m.start, m.cap);
-    bt->free_slots.push_back(m.slot);
-    bt->members[j] = bt->members.back();
-    bt->members.pop_back();
-  }
-  bt->dirty = true;
-  return st;
-}
-
-extern "C" hj_status hj_gaussian_bunch(hj_ctx* ctx, uint64_t init_seed, int64_t n,
-                                       double sigma_z, double sigma_E, double* d_z,
-                                       double* d_dE, void* stream) {
-  HJ_TRY(ctx_ok(ctx));
-  if (n < 0 || (n > 0 && (!d_z || !d_dE))) return set_err(ctx, HJ_ERR_ARG, "bad particle arrays");
-  if (!(sigma_z >= 0.0 && sigma_E >= 0.0)) return set_err(ctx, HJ_ERR_ARG, "spreads must be non-negative");
-  if (n == 0) return HJ_OK;
-  HJ_CUDA(ctx, launch_gaussian_bunch(init_seed, n, 0.0, sigma_z, 0.0, sigma_E, d_z, d_dE,
-                                     (cudaStream_t)stream));
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_batch_advance(hj_batch* bt, int64_t turns) {
-  if (!bt) return HJ_ERR_ARG;
-  hj_ctx* ctx = bt->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (turns < 0) return set_err(ctx, HJ_ERR_ARG, "turns must be >= 0");
-  if (bt->members.empty() || turns == 0) return HJ_OK;
-  if (bt->dirty) HJ_TRY(batch_upload(bt));
-  int64_t t = 0;
-  if (bt->graph_turns > 0 && turns >= bt->graph_turns) {
-    if (!bt->graph) HJ_TRY(batch_capture(bt));
-    for (; t + bt->graph_turns <= turns; t += bt->graph_turns)
-      HJ_CUDA(ctx, cudaGraphLaunch(bt->graph, bt->stream));
-  }
-  for (; t < turns; ++t) HJ_TRY(batch_launch_turn(bt));
-  bt->turns_enqueued += turns;
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_batch_poll(hj_batch* bt, int64_t* ids, int32_t cap, int32_t* n_done) {
-  if (!bt || !n_done || (cap > 0 && !ids)) return HJ_ERR_ARG;
-  hj_ctx* ctx = bt->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  *n_done = 0;
-  HJ_CUDA(ctx, cudaMemcpyAsync(bt->h_ts, bt->d_ts, sizeof(TurnState) * bt->max_bunches,
-                               cudaMemcpyDeviceToHost, bt->stream));
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  for (auto& m : bt->members) {
-    if (bt->h_ts[m.slot].turns_left <= 0 && *n_done < cap) ids[(*n_done)++] = m.id;
-  }
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_batch_take(hj_batch* bt, int64_t id, double* z_out, double* dE_out,
-                                   hj_result* res) {
-  if (!bt) return HJ_ERR_ARG;
-  hj_ctx* ctx = bt->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  const int k = batch_find(bt, id);
-  if (k < 0) return set_err(ctx, HJ_ERR_ARG, "no bunch %lld in the batch", (long long)id);
-  BatchMember m = bt->members[k];
-  hj_bunch* b = m.b;
-  // one round trip: pending kick and re-centring applied in place, moments
-  // and turn state read, particles copied out, and the slot's state set to
-  // "no turns left" for the kernels
-  HJ_TRY(launch_moments(b, 1, b->z, b->dE));
-  HJ_CUDA(ctx, cudaMemcpyAsync(b->h_mom, b->part_mom, sizeof(double) * 4 * b->nblk_m,
-                               cudaMemcpyDeviceToHost, bt->stream));
-  HJ_CUDA(ctx, cudaMemcpyAsync(b->h_ts, b->ts, sizeof(TurnState), cudaMemcpyDeviceToHost,
-                               bt->stream));
-  if (z_out)
-    HJ_CUDA(ctx, cudaMemcpyAsync(z_out, b->z, sizeof(double) * b->n, cudaMemcpyDefault, bt->stream));
-  if (dE_out)
-    HJ_CUDA(ctx, cudaMemcpyAsync(dE_out, b->dE, sizeof(double) * b->n, cudaMemcpyDefault,
-                                 bt->stream));
-  TurnState dead{};
-  dead.turns_left = 0;
-  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, &dead, sizeof(TurnState), cudaMemcpyHostToDevice,
-                               bt->stream));
-  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
-  double mom[4];
-  sum_moments(b, mom);
-  hj_status st = state_status(b);
-  fill_result(b, mom, res);
-  b->ts = nullptr;
-  hj_bunch_destroy(b);
-  batch_free_range(bt, m.start, m.cap);
-  bt->free_slots.push_back(m.slot);
-  bt->members[k] = bt->members.back();
-  bt->members.pop_back();
-  bt->dirty = true;
-  return st;
-}
-
-extern "C" hj_status hj_batch_stats(hj_batch* bt, int64_t* out4) {
-  if (!bt || !out4) return HJ_ERR_ARG;
-  out4[0] = (int64_t)bt->members.size();
-  out4[1] = batch_largest_free(bt);
-  out4[2] = (int64_t)bt->free_slots.size();
-  out4[3] = bt->turns_enqueued;
-  return HJ_OK;
-}
-
-// ====================================================================== shards
-//
-// A bunch split over processes (one GPU each), the reference's MPI mode
-// (src/evolution.jl:206-212 with use_mpi): every rank tracks its particles;
-// once per turn the ranks sum the merged histograms and the pass's sums
-// (exchange buffers, B*3+2 u64 and kNumSums doubles) -- one all-reduce -- and
-// every rank runs the bins step on the totals, so all ranks keep the same
-// potential and E0.  The Philox draws of particle i of a shard are those of
-// particle first_particle + i of the whole bunch.
-
-extern "C" hj_status hj_bunch_create_shard(hj_ctx* ctx, double* d_z, double* d_dE,
-                                           int64_t n_local, int64_t first_particle,
-                                           int64_t n_global, const hj_params* params,
-                                           const hj_wake* wake, const hj_grid* grid,
-                                           uint64_t seed, void* stream, hj_bunch** out) {
-  HJ_TRY(ctx_ok(ctx));
-  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
-  *out = nullptr;
-  HJ_TRY(check_params(ctx, params));
-  if (!params->use_wakefield || !grid)
-    return set_err(ctx, HJ_ERR_ARG, "a shard needs the wakefield on and the shared bin grid");
-  if (n_local <= 0 || first_particle < 0 || (first_particle & 1) ||
-      first_particle + n_local > n_global)
-    return set_err(ctx, HJ_ERR_ARG,
-                   "shard [%lld, %lld) of %lld particles: non-empty, inside, even start",
-                   (long long)first_particle, (long long)(first_particle + n_local),
-                   (long long)n_global);
-  if (!d_z || !d_dE || ((((uintptr_t)d_z) | ((uintptr_t)d_dE)) & 31))
-    return set_err(ctx, HJ_ERR_ARG, "device particle arrays must be non-NULL and 32-byte aligned");
-  hj_bunch* b = new hj_bunch();
-  hj_status s = bunch_create_impl(ctx, d_z, d_dE, n_local, params, wake, grid->nbins, grid,
-                                  seed, stream, b);
-  if (s == HJ_OK) s = dalloc(ctx, &b->d_sums, kNumSums);
-  if (s != HJ_OK) {
-    hj_bunch_destroy(b);
-    return s;
-  }
-  b->shard = true;
-  b->n_global = n_global;
-  b->first_particle = first_particle;
-  *out = b;
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_bunch_local_moments(hj_bunch* b, double* out4) {
-  if (!b || !out4) return HJ_ERR_ARG;
-  HJ_TRY(ctx_ok(b->ctx));
-  HJ_TRY(launch_moments(b, 1, nullptr, nullptr));
-  return read_moments(b, out4);
-}
-
-extern "C" hj_status hj_bunch_set_global_moments(hj_bunch* b, const double* sums4) {
-  if (!b || !sums4) return HJ_ERR_ARG;
-  hj_ctx* ctx = b->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (b->turns_done != 0) return set_err(ctx, HJ_ERR_STATE, "global moments are set before the first turn");
-  const int64_t n = b->shard ? b->n_global : b->n;
-  b->sigma_z0_initial = global_std(sums4[0], sums4[1], n);
-  b->sigma_E0_initial = global_std(sums4[2], sums4[3], n);
-  HJ_TRY(read_state(b));
-  b->h_ts->cur = make_turn_scalars(b->p.E0, b->p, b->sigma_E0_initial);
-  HJ_CUDA(ctx, cudaMemcpyAsync(b->ts, b->h_ts, sizeof(TurnState), cudaMemcpyHostToDevice,
-                               b->stream));
-  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_bunch_pass(hj_bunch* b) {
-  if (!b) return HJ_ERR_ARG;
-  hj_ctx* ctx = b->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (!b->shard) return set_err(ctx, HJ_ERR_STATE, "hj_bunch_pass is for shards (use hj_bunch_advance)");
-  PassArgs a;
-  BinsArgs g;
-  fill_turn_args(b, a, g);
-  HJ_CUDA(ctx, launch_track_pass(a, b->nblk, b->stream));
-  HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->hist, false,
-                                  b->stream, b->ngp_ovf));
-  HJ_CUDA(ctx, launch_sum_parts(b->part_sum, b->nblk, b->d_sums, b->stream));
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_bunch_exchange_buffers(hj_bunch* b, uint64_t** d_counts,
-                                               int64_t* n_counts, double** d_sums,
-                                               int64_t* n_sums) {
-  if (!b || !d_counts || !n_counts || !d_sums || !n_sums) return HJ_ERR_ARG;
-  if (!b->shard) return set_err(b->ctx, HJ_ERR_STATE, "not a shard");
-  *d_counts = (uint64_t*)b->hist;
-  *n_counts = 3 * (int64_t)b->B + 2;
-  *d_sums = b->d_sums;
-  *n_sums = kNumSums;
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_bunch_bins(hj_bunch* b) {
-  if (!b) return HJ_ERR_ARG;
-  hj_ctx* ctx = b->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (!b->shard) return set_err(ctx, HJ_ERR_STATE, "hj_bunch_bins is for shards (use hj_bunch_advance)");
-  PassArgs a;
-  BinsArgs g;
-  fill_turn_args(b, a, g);
-  HJ_CUDA(ctx, launch_bins(g, b->stream));
-  b->turns_done += 1;
-  return HJ_OK;
-}
-
-// ====================================================================== turn log
-
-extern "C" hj_status hj_bunch_set_log(hj_bunch* b, int64_t every, int64_t capacity,
-                                      int32_t density) {
-  if (!b) return HJ_ERR_ARG;
-  hj_ctx* ctx = b->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  if (every < 0 || (every > 0 && capacity <= 0))
-    return set_err(ctx, HJ_ERR_ARG, "log every >= 0 turns into capacity > 0 records");
-  if (density && !b->use_wake) return set_err(ctx, HJ_ERR_STATE, "no line density without the wakefield");
-  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
-  if (b->d_log) cudaFree(b->d_log);
-  b->d_log = nullptr;
-  b->log_every = every;
-  b->log_capacity = capacity;
-  b->log_density = density ? 1 : 0;
-  b->log_count = 0;
-  if (every > 0)
-    HJ_TRY(dalloc(ctx, &b->d_log, (size_t)capacity * (kLogHeader + (b->log_density ? b->B : 0))));
-  return HJ_OK;
-}
-
-extern "C" hj_status hj_bunch_read_log(hj_bunch* b, double* out, int64_t max_records,
-                                       int64_t* n_records) {
-  if (!b || !n_records || (max_records > 0 && !out)) return HJ_ERR_ARG;
-  hj_ctx* ctx = b->ctx;
-  HJ_TRY(ctx_ok(ctx));
-  *n_records = 0;
-  if (!b->d_log) return HJ_OK;
-  const int64_t rec = kLogHeader + (b->log_density ? b->B : 0);
-  const int64_t held = std::min(b->log_count, b->log_capacity);
-  const int64_t n = std::min(held, max_records);
-  // the n most recent records, oldest first
-  for (int64_t k = 0; k < n; ++k) {
-    const int64_t idx = (b->log_count - n + k) % b->log_capacity;
-    HJ_CUDA(ctx, cudaMemcpyAsync(out + k * rec, b->d_log + idx * rec, sizeof(double) * rec,
-                                 cudaMemcpyDeviceToHost, b->stream));
-  }
-  HJ_CUDA(ctx, cudaStreamSynchronize(b->stream));
-  *n_records = n;
-  return HJ_OK;
-}
-
-// ====================================================================== generate_particles
-
-namespace {
-// compute_std (src/utils.jl:531-544) of a device array: two passes, per-block
-// sums added on the host in block order.
-hj_status device_compute_std(hj_ctx* ctx, const double* x, int64_t n, double* part, int grid,
-                             cudaStream_t st, double* out) {
-  std::vector<double> h(grid);
-  HJ_CUDA(ctx, launch_std_parts(x, n, 0.0, 0, part, grid, st));
-  HJ_CUDA(ctx, cudaMemcpyAsync(h.data(), part, sizeof(double) * grid, cudaMemcpyDeviceToHost, st));
-  HJ_CUDA(ctx, cudaStreamSynchronize(st));
-  double s = 0.0;
-  for (double v : h) s += v;
-  const double mu = s / (double)n;
-  HJ_CUDA(ctx, launch_std_parts(x, n, mu, 1, part, grid, st));
-  HJ_CUDA(ctx, cudaMemcpyAsync(h.data(), part, sizeof(double) * grid, cudaMemcpyDeviceToHost, st));
-  HJ_CUDA(ctx, cudaStreamSynchronize(st));
-  double s2 = 0.0;
-  for (double v : h) s2 += v;
-  const double var = s2 / (double)(n - 1);
-  *out = std::sqrt(std::max(0.0, var));
-  return HJ_OK;
-}
-}  // namespace
-
-extern "C" hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E, double sigma_z,
-                                           double sigma_E, int64_t n, uint64_t seed,
-                                           double* d_z, double* d_dE, void* stream,
-                                           double* actual_sigma_E, double* actual_sigma_z) {
-  HJ_TRY(ctx_ok(ctx));
-  if (!actual_sigma_E || !actual_sigma_z) return set_err(ctx, HJ_ERR_ARG, "output spreads are NULL");
-  if (!(sigma_z >= 0.0 && sigma_E >= 0.0)) return set_err(ctx, HJ_ERR_ARG, "spreads must be non-negative");
-  cudaStream_t st = (cudaStream_t)stream;
-  if (n <= 0) {                                   // src/evolution.jl:47-53
-    *actual_sigma_E = 0.0;
-    *actual_sigma_z = 0.0;
-    return HJ_OK;
-  }
-  if (!d_z || !d_dE) return set_err(ctx, HJ_ERR_ARG, "particle arrays are NULL");
-  *actual_sigma_E = sigma_E;
-  *actual_sigma_z = sigma_z;
-  if (n < 2) {                                    // :62-67, independent draws, input spreads
-    HJ_CUDA(ctx, launch_gaussian_bunch(seed, n, mu_z, sigma_z, mu_E, sigma_E, d_z, d_dE, st));
-    HJ_CUDA(ctx, cudaStreamSynchronize(st));
-    return HJ_OK;
-  }
-  const int grid = (int)std::min<int64_t>((n + 1023) / 1024, 4 * (int64_t)ctx->num_sms);
-  double* dev = nullptr;
-  HJ_TRY(dalloc(ctx, &dev, (size_t)grid + 3));
-  hj_status s = HJ_OK;
-  do {
-    // covariance of a sample of min(n, 10000) independent draws (:69-81)
-    const int64_t S = std::min<int64_t>(n, 10000);
-    double c[3];
-    cudaError_t e = launch_gen_sample_cov(seed, S, mu_z, sigma_z, mu_E, sigma_E, dev + grid, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(c, dev + grid, sizeof(c), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-      s = set_err(ctx, HJ_ERR_CUDA, "covariance sample failed: %s", cudaGetErrorString(e));
-      break;
-    }
-    double a = std::max(1e-18, c[0]), b = c[2], d = std::max(1e-18, c[1]);
-    // positive semi-definite guard (:88-93): eigmin of [[a, b], [b, d]]
-    const double min_eig = 0.5 * (a + d) - std::sqrt(0.25 * (a - d) * (a - d) + b * b);
-    if (min_eig < 1e-12) {
-      const double add = std::max(0.0, 1e-12 - min_eig);
-      a += add;
-      d += add;
-    }
-    // MvNormal draw (:95-116): mu + L eps, L the lower Cholesky factor of the covariance
-    const double l00 = std::sqrt(a), l10 = b / l00, l11 = std::sqrt(std::max(0.0, d - l10 * l10));
-    e = launch_gen_correlated(seed, n, mu_z, mu_E, l00, l10, l11, d_z, d_dE, st);
-    if (e != cudaSuccess) {
-      s = set_err(ctx, HJ_ERR_CUDA, "bunch draw failed: %s", cudaGetErrorString(e));
-      break;
-    }
-    // actual spreads, compute_std (:119-121)
-    s = device_compute_std(ctx, d_z, n, dev, grid, st, actual_sigma_z);
-    if (s == HJ_OK) s = device_compute_std(ctx, d_dE, n, dev, grid, st, actual_sigma_E);
-  } while (false);
-  cudaFree(dev);
-  return s;
-}
-
-// ====================================================================== correlation
-
-// cor(particles.coordinates.z, particles.coordinates.ΔE) of EmittanceFoM
-// (src/parameter_sensitivity/figures_of_merit.jl:42, Julia's Statistics.cor):
-// two passes over the device arrays (means, then centred sums Sxx, Syy, Sxy),
-// per-block sums added on the host in block order, r = Sxy/(√Sxx √Syy)
-// clamped to [-1, 1].
-extern "C" hj_status hj_correlation(hj_ctx* ctx, const double* d_x, const double* d_y, int64_t n,
-                                    void* stream, double* out) {
-  HJ_TRY(ctx_ok(ctx));
-  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
-  if (n <= 0) return set_err(ctx, HJ_ERR_ARG, "correlation only defined for non-empty vectors");
-  if (!d_x || !d_y) return set_err(ctx, HJ_ERR_ARG, "arrays are NULL");
-  cudaStream_t st = (cudaStream_t)stream;
-  const int grid = (int)std::min<int64_t>((n + 4095) / 4096, 4 * (int64_t)ctx->num_sms);
-  void* base = nullptr;
-  HJ_TRY(scratch(ctx, sizeof(double) * 3 * (size_t)grid, &base));
-  double* part = (double*)base;
-  std::vector<double> h(3 * (size_t)grid);
-  double s[2][3] = {};
-  double mx = 0.0, my = 0.0;
-  for (int pass = 0; pass < 2; ++pass) {
-    HJ_CUDA(ctx, launch_cor_parts(d_x, d_y, n, mx, my, pass, part, grid, st));
-    HJ_CUDA(ctx, cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(),
-                                 cudaMemcpyDeviceToHost, st));
-    HJ_CUDA(ctx, cudaStreamSynchronize(st));
-    for (int b = 0; b < grid; ++b)
-      for (int k = 0; k < 3; ++k) s[pass][k] += h[3 * (size_t)b + k];
-    mx = s[0][0] / (double)n;
-    my = s[0][1] / (double)n;
-  }
-  const double r = s[1][2] / (std::sqrt(s[1][0]) * std::sqrt(s[1][1]));
-  *out = r != r ? r : std::min(1.0, std::max(-1.0, r));
-  return HJ_OK;
 }
