@@ -295,7 +295,8 @@ void fill_result(hj_bunch* b, const double m[4], hj_result* res) {
   res->sigma_z0_initial = b->sigma_z0_initial;
   res->mean_z = b->n > 0 ? m[0] / (double)b->n : 0.0;
   res->mean_dE = b->n > 0 ? m[2] / (double)b->n : 0.0;
-  res->turns = b->turns_done;
+  // a batch member's turns are counted on the device (its turn state was read)
+  res->turns = b->batch_member ? b->h_ts->turn - 1 : b->turns_done;
 }
 
 cudaError_t set_kernel_attributes(hj_ctx* ctx) {

@@ -161,3 +161,41 @@ def test_admitting_and_taking_many_at_once(gpu_ctx):
                              [s] * 3, [5] * 3)
     assert len(ids) == 2 and err is not None and err.status == _lib.HJ_ERR_FULL
     many.close()
+
+
+@pytest.mark.parametrize("n", [2, 3, 5, 9])
+def test_tiny_bunches_match_the_plain_path(gpu_ctx, n):
+    """Bunches of a few particles (the scalar tail of the pass, one partial
+    chunk) give in a batch what they give alone on the plain path."""
+    cfg = benchmark_ring(n_turns=1, nbins=256)
+    z, dE = _bunch(n, 7 + n, cfg)
+    bt = Batch(gpu_ctx, 1024, 2, 256, chunk=16384)
+    bid = bt.add(z, dE, cfg.params, 256, wake=cfg.wake, seed=3, turns=6)
+    bt.advance(6)
+    assert bt.poll() == [bid]
+    got = bt.take(bid)
+    bt.close()
+    _check(got, _plain(gpu_ctx, cfg, z, dE, 256, 3, 6), cfg, f"{n} particles")
+
+
+def test_a_bunch_with_no_turns_is_done_at_once(gpu_ctx):
+    cfg, z, dE, nbins, seed = _spec(0)
+    bt = Batch(gpu_ctx, 20_000, 2, 1024)
+    bid = bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=0)
+    bt.advance(1)
+    assert bt.poll() == [bid]
+    zz, ee, r = bt.take(bid)
+    bt.close()
+    assert r.turns == 0 and r.E0 == cfg.params.E0
+    assert np.array_equal(zz, z) and np.array_equal(ee, dE)
+
+
+def test_results_count_the_turns_run(gpu_ctx):
+    cfg, z, dE, nbins, seed = _spec(1)
+    bt = Batch(gpu_ctx, 100_000, 2, 1024)
+    bid = bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=11)
+    bt.advance(16)
+    assert bt.poll() == [bid]
+    _, _, r = bt.take(bid, copy_out=False)
+    bt.close()
+    assert r.turns == 11
