@@ -733,10 +733,16 @@ class Batch:
         admitted bunches -- the first ones --, the HaissinskiError that stopped
         admission, or None)."""
         k = len(n)
+        keep = []                         # host arrays converted for the call
+
         def ptrs(a):
             arr = (ctypes.c_void_p * max(k, 1))()
             for i, x in enumerate(a):
-                arr[i] = x if isinstance(x, int) else x.ctypes.data
+                if not isinstance(x, int):
+                    x = np.ascontiguousarray(x, dtype=np.float64)
+                    keep.append(x)
+                    x = x.ctypes.data
+                arr[i] = x
             return arr
         zp, ep = ptrs(z), ptrs(dE)
         nn = np.ascontiguousarray(n, dtype=np.int64)
