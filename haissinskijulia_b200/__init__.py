@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     SPEED_LIGHT,
     Batch,
     BinGrid,
+    Checkpoint,
     Context,
     EvolveResult,
     HaissinskiError,

@@ -85,6 +85,15 @@ class HjResult(ctypes.Structure):
     ]
 
 
+class HjCheckpoint(ctypes.Structure):
+    _fields_ = [
+        ("turn", c_int64),
+        ("E0", c_double),
+        ("sigma_E0_initial", c_double),
+        ("sigma_z0_initial", c_double),
+    ]
+
+
 _DP = POINTER(c_double)
 _IP = POINTER(c_int64)
 _CTX = c_void_p
@@ -118,6 +127,10 @@ SIGNATURES = {
     "hj_bunch_set_profiling": (c_int32, [_BUNCH, c_int32]),
     "hj_bunch_read_profile": (c_int32, [_BUNCH, _DP]),
     "hj_bunch_histogram": (c_int32, [_BUNCH, _IP]),
+    "hj_bunch_checkpoint": (c_int32, [_BUNCH, c_void_p, c_void_p, POINTER(HjCheckpoint)]),
+    "hj_bunch_resume": (c_int32, [_CTX, c_void_p, c_void_p, c_int64, POINTER(HjParams),
+                                  POINTER(HjWake), c_int64, POINTER(HjGrid), c_uint64,
+                                  POINTER(HjCheckpoint), c_void_p, POINTER(_BUNCH)]),
     "hj_bunch_potential": (c_int32, [_BUNCH, _DP]),
     "hj_bunch_set_log": (c_int32, [_BUNCH, c_int64, c_int64, c_int32]),
     "hj_bunch_read_log": (c_int32, [_BUNCH, _DP, c_int64, _IP]),

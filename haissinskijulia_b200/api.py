@@ -27,7 +27,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import HjGrid, HjParams, HjResult, HjWake
+from ._lib import HjCheckpoint, HjGrid, HjParams, HjResult, HjWake
 
 # src/constants.jl:5-8
 SPEED_LIGHT = 299792458.0
@@ -522,6 +522,16 @@ def gaussian_draws(seed: int, turn: int, n: int, buffers: SimulationBuffers) -> 
 # ----------------------------------------------------------------------------- resident bunch
 
 
+@dataclass
+class Checkpoint:
+    """hj_checkpoint: the next turn's number, E0 and the initial spreads."""
+
+    turn: int
+    E0: float
+    sigma_E0_initial: float
+    sigma_z0_initial: float
+
+
 class ResidentBunch:
     """A bunch whose (z, ΔE) stay in device memory between calls.
 
@@ -548,6 +558,43 @@ class ResidentBunch:
                                       ctypes.byref(h))
         _check(ctx, rc)
         self.handle = h
+
+    def checkpoint(self, d_z_out: int, d_dE_out: int) -> "Checkpoint":
+        """The particles at the turn boundary into device arrays (ints:
+        pointers) and the checkpoint that continues the run
+        (hj_bunch_checkpoint); the bunch runs on unchanged."""
+        c = HjCheckpoint()
+        _check(self.ctx, self.ctx._lib.hj_bunch_checkpoint(
+            self.handle, ctypes.c_void_p(d_z_out), ctypes.c_void_p(d_dE_out), ctypes.byref(c)))
+        return Checkpoint(int(c.turn), float(c.E0), float(c.sigma_E0_initial),
+                          float(c.sigma_z0_initial))
+
+    @classmethod
+    def resume(cls, ctx: Context, d_z: int, d_dE: int, n: int, params: SimulationParameters,
+               nbins: int, checkpoint: "Checkpoint", *, wake: Optional[WakeModel] = None,
+               grid: Optional[BinGrid] = None, seed: int = 0,
+               stream: int = 0) -> "ResidentBunch":
+        """A bunch continuing from `checkpoint` (hj_bunch_resume): d_z, d_dE
+        hold the checkpointed particles; turn counter, E0 and initial spreads
+        come from the checkpoint; the same seed continues the same draws."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.n = int(n)
+        self.nbins = int(nbins)
+        self._p = params.to_c()
+        self._w = (wake or WakeModel.reference(params)).to_c()
+        self._grid = grid
+        g = grid.to_c() if grid is not None else None
+        c = HjCheckpoint(int(checkpoint.turn), float(checkpoint.E0),
+                         float(checkpoint.sigma_E0_initial), float(checkpoint.sigma_z0_initial))
+        h = ctypes.c_void_p()
+        _check(ctx, ctx._lib.hj_bunch_resume(ctx.handle, ctypes.c_void_p(d_z), ctypes.c_void_p(d_dE),
+                                             self.n, ctypes.byref(self._p), ctypes.byref(self._w),
+                                             self.nbins, ctypes.byref(g) if g is not None else None,
+                                             int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(c),
+                                             ctypes.c_void_p(stream), ctypes.byref(h)))
+        self.handle = h
+        return self
 
     def set_draws(self, d_draws: int, first_turn: int, turns: int) -> None:
         _check(self.ctx, self.ctx._lib.hj_bunch_set_draws(self.handle, ctypes.c_void_p(d_draws),

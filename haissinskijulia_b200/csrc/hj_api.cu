@@ -505,13 +505,14 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
   return HJ_OK;
 }
 
-hj_status hj_impl::bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid) {
+hj_status hj_impl::bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid,
+                                    const hj_checkpoint* cp) {
   const int64_t n = b->n;
   const hj_params* params = &b->p;
   double m[4];
   sum_moments(b, m);
-  b->sigma_z0_initial = global_std(m[0], m[1], n);
-  b->sigma_E0_initial = global_std(m[2], m[3], n);
+  b->sigma_z0_initial = cp ? cp->sigma_z0_initial : global_std(m[0], m[1], n);
+  b->sigma_E0_initial = cp ? cp->sigma_E0_initial : global_std(m[2], m[3], n);
 
   if (b->use_wake) {
     const int B = b->B;
@@ -635,10 +636,11 @@ hj_status hj_impl::bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* gri
                                cudaMemcpyHostToDevice, b->stream));
 
   TurnState t{};
-  t.cur = make_turn_scalars(params->E0, *params, b->sigma_E0_initial);
+  t.cur = make_turn_scalars(cp ? cp->E0 : params->E0, *params, b->sigma_E0_initial);
   t.pending = 0;
   t.pending_mean = 0.0;
-  t.turn = 1;
+  t.turn = cp ? cp->turn : 1;
+  b->turns_done = cp ? cp->turn - 1 : 0;
   t.turns_left = INT64_MAX;   // a plain bunch runs until it is finished
   t.status = 0;
   *b->h_ts = t;

@@ -110,6 +110,58 @@ extern "C" hj_status hj_bunch_bins(hj_bunch* b) {
   return HJ_OK;
 }
 
+// ====================================================================== checkpoint / resume
+//
+// A host snapshot of (z, ΔE, E0, turn, initial spreads) is enough to continue
+// a run: the Philox draws are keyed by (seed, particle, turn), the grid and
+// the excitation amplitude by the initial spreads.
+
+extern "C" hj_status hj_bunch_checkpoint(hj_bunch* b, double* d_z_out, double* d_dE_out,
+                                         hj_checkpoint* out) {
+  if (!b) return HJ_ERR_ARG;
+  hj_ctx* ctx = b->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  if (!out || !d_z_out || !d_dE_out) return set_err(ctx, HJ_ERR_ARG, "output pointers are NULL");
+  if (b->shard || b->batch_member)
+    return set_err(ctx, HJ_ERR_STATE, "checkpoints are taken of whole resident bunches");
+  HJ_TRY(launch_moments(b, 1, d_z_out, d_dE_out));
+  double m[4];
+  HJ_TRY(read_moments(b, m));
+  HJ_TRY(read_state(b));
+  out->turn = b->h_ts->turn;
+  out->E0 = b->h_ts->cur.E0;
+  out->sigma_E0_initial = b->sigma_E0_initial;
+  out->sigma_z0_initial = b->sigma_z0_initial;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_bunch_resume(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                                     const hj_params* params, const hj_wake* wake,
+                                     int64_t nbins, const hj_grid* grid, uint64_t seed,
+                                     const hj_checkpoint* cp, void* stream, hj_bunch** out) {
+  HJ_TRY(ctx_ok(ctx));
+  if (!out) return set_err(ctx, HJ_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!cp || cp->turn < 1) return set_err(ctx, HJ_ERR_ARG, "a checkpoint with turn >= 1 is needed");
+  HJ_TRY(check_params(ctx, params));
+  if (n <= 0 || !d_z || !d_dE) return set_err(ctx, HJ_ERR_ARG, "particle arrays are empty or NULL");
+  if ((((uintptr_t)d_z) | ((uintptr_t)d_dE)) & 31)
+    return set_err(ctx, HJ_ERR_ARG, "device particle arrays must be 32-byte aligned");
+  hj_bunch* b = new hj_bunch();
+  hj_status s = bunch_create_begin(ctx, d_z, d_dE, n, params, wake, nbins, grid, seed, stream, b);
+  if (s == HJ_OK) {
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    s = e == cudaSuccess ? bunch_create_end(ctx, b, grid, cp)
+                         : set_err(ctx, HJ_ERR_CUDA, "%s", cudaGetErrorString(e));
+  }
+  if (s != HJ_OK) {
+    hj_bunch_destroy(b);
+    return s;
+  }
+  *out = b;
+  return HJ_OK;
+}
+
 // ====================================================================== turn log
 
 extern "C" hj_status hj_bunch_set_log(hj_bunch* b, int64_t every, int64_t capacity,

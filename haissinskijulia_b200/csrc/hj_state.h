@@ -212,7 +212,9 @@ hj_status bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
                              const hj_params* params, const hj_wake* wake, int64_t nbins,
                              const hj_grid* grid, uint64_t seed, void* stream, hj_bunch* b,
                              int64_t chunk = 0, int cfg = -1);
-hj_status bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid);
+// cp: continue from a checkpoint (its turn, E0 and initial spreads)
+hj_status bunch_create_end(hj_ctx* ctx, hj_bunch* b, const hj_grid* grid,
+                           const hj_checkpoint* cp = nullptr);
 hj_status bunch_create_impl(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
                             const hj_params* params, const hj_wake* wake, int64_t nbins,
                             const hj_grid* grid, uint64_t seed, void* stream, hj_bunch* b,

@@ -262,6 +262,29 @@ hj_status hj_bunch_set_log(hj_bunch* b, int64_t every, int64_t capacity, int32_t
 /* Copies the most recent min(held, max_records) records, oldest first, into
  * out (8 [+ nbins] doubles each); *n_records = how many. */
 hj_status hj_bunch_read_log(hj_bunch* b, double* out, int64_t max_records, int64_t* n_records);
+/* Checkpoint of a resident bunch at a turn boundary: what, with its
+ * particles, lets another bunch (another process, a later job) continue the
+ * run -- the next turn's number, E0, and the initial spreads that fix the
+ * quantum-excitation amplitude and the bin grid; with the same seed the
+ * Philox draws continue unchanged, since they are keyed by (seed, particle,
+ * turn).  No reference counterpart (the reference keeps no checkpoint). */
+typedef struct hj_checkpoint {
+  int64_t turn;              /* number of the next turn (turns done + 1) */
+  double E0;
+  double sigma_E0_initial;
+  double sigma_z0_initial;
+} hj_checkpoint;
+/* The particles at the turn boundary (the pending kick and re-centring
+ * applied, as hj_bunch_observe gives them) into device arrays d_z_out,
+ * d_dE_out, and the checkpoint.  The bunch itself runs on unchanged. */
+hj_status hj_bunch_checkpoint(hj_bunch* b, double* d_z_out, double* d_dE_out, hj_checkpoint* out);
+/* A resident bunch continuing from a checkpoint: as hj_bunch_create, with
+ * d_z, d_dE the checkpointed particles and the turn counter, E0 and initial
+ * spreads (hence the grid, when grid is NULL) taken from *cp. */
+hj_status hj_bunch_resume(hj_ctx* ctx, double* d_z, double* d_dE, int64_t n,
+                          const hj_params* params, const hj_wake* wake, int64_t nbins,
+                          const hj_grid* grid, uint64_t seed, const hj_checkpoint* cp,
+                          void* stream, hj_bunch** out);
 /* Line density of the last completed turn: integer bin counts (nbins). */
 hj_status hj_bunch_histogram(hj_bunch* b, int64_t* counts_host);
 /* Potential at the bin centers from the last completed turn (nbins). */
