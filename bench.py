@@ -229,7 +229,8 @@ def measure_sweeps(ctx, args) -> dict:
     around each (admission, turns, retirement and result read-back included)."""
     import numpy as np
     from haissinskijulia_b200.sweep import (autotune, intensity_scan, request_stream,
-                                            run_batched, run_plain, serve, sweep_points)
+                                            run_batched, run_plain, serve, serve_plain,
+                                            sweep_points)
     T = args.sweep_turns
     pts = sweep_points(256, turns=T)
     t0 = time.perf_counter()
@@ -288,6 +289,12 @@ def measure_sweeps(ctx, args) -> dict:
                         "U[1000,20000], bins in {2048,4096,8192}; admission by footprint "
                         "(8 GB budget), 200-turn blocks")
         sm["particle_turns_per_s"] = sm["particle_turns"] / sm["wall_s"]
+        pl = serve_plain(ctx, reqs).summary()
+        sm["plain"] = {"solves_per_s": pl["solves_per_s"], "p50_latency_s": pl["p50_latency_s"],
+                       "p99_latency_s": pl["p99_latency_s"], "wall_s": pl["wall_s"],
+                       "how": "the same requests one at a time on the plain resident path, "
+                              "first come first served (measured service times)"}
+        sm["speedup_vs_plain"] = sm["solves_per_s"] / pl["solves_per_s"]
         out["serving"] = sm
     if args.scan_points > 0:
         out["parameter_scan"] = measure_scan(ctx, args)

@@ -16,6 +16,8 @@ batched bins step per turn, turn blocks replayed from a CUDA graph.
 * `autotune`: times candidate (particles per block, pass layout with the
   width of the shared-memory bin counters -- the histogram privatisation --,
   K) on a sample of the workload and keeps the fastest.
+* `serve_plain`: the same stream one request at a time on the plain path
+  (first come first served), the baseline of `serve`.
 * `serve`: a request stream with arrival times; requests are admitted by
   device-memory footprint (16 B per particle plus bin tables) while others
   run, and per-request latency percentiles are reported with solves/s.
@@ -304,6 +306,24 @@ def serve(ctx: Context, requests: List[Point], *, memory_budget: int = 8 << 30,
     finally:
         bt.close()
     rep.solves = [done[i] for i in sorted(done)]
+    return rep
+
+
+def serve_plain(ctx: Context, requests: List[Point]) -> ServeReport:
+    """The same request stream served one request at a time on the plain
+    resident path, first come first served: each request's service time is
+    measured, and a request starts when it has arrived and the previous one
+    has finished (latency = finish - arrival on that timeline; no idle time
+    is spent waiting for arrivals)."""
+    rep = ServeReport()
+    clock = 0.0
+    for p in sorted(requests, key=lambda q: q.arrival):
+        start = max(clock, p.arrival)
+        s = run_plain(ctx, [p])[0]
+        service = s.finished                         # run_plain's clock starts at the request
+        clock = start + service
+        rep.solves.append(Solve(p, s.result, admitted=start, finished=clock))
+    rep.wall = clock
     return rep
 
 

@@ -4,13 +4,16 @@
   path): every point's E0, σ_E and σ_z within 1e-12;
 * serve(): requests that arrive while others run are admitted into the same
   batch, and each request's result is bit-identical to the same request
-  solved alone.
+  solved alone;
+* serve_plain(): the same stream one request at a time on the plain path
+  gives every request's result within 1e-12 of serve()'s, on a first come
+  first served timeline.
 """
 import numpy as np
 import pytest
 
 from haissinskijulia_b200.sweep import (Point, Tuning, request_stream, run_batched, run_plain,
-                                        serve, sweep_points)
+                                        serve, serve_plain, sweep_points)
 
 pytestmark = pytest.mark.gpu
 
@@ -48,3 +51,21 @@ def test_served_requests_match_their_solo_runs(gpu_ctx):
         alone = run_batched(gpu_ctx, [sv.point], tuning=Tuning(16384, -1, 8), block_turns=40)[0]
         assert (alone.result.E0, alone.result.sigma_E, alone.result.sigma_z) == \
             (sv.result.E0, sv.result.sigma_E, sv.result.sigma_z)
+
+
+def test_plain_serving_matches_batched_serving(gpu_ctx):
+    reqs = request_stream(6, rate=400.0, seed=9, n_hi=3e4)
+    for r in reqs:
+        r.turns = 120 + (r.seed % 5) * 20
+        r.nbins = [512, 1024][r.seed % 2]
+    rep = serve(gpu_ctx, reqs, memory_budget=64 << 20, max_bunches=4,
+                tuning=Tuning(16384, -1, 8), block_turns=40, max_nbins=1024)
+    plain = serve_plain(gpu_ctx, reqs)
+    s = plain.summary()
+    assert s["requests"] == len(reqs) and s["p99_latency_s"] >= s["p50_latency_s"] > 0
+    by_point = {id(sv.point): sv for sv in rep.solves}
+    prev = 0.0
+    for pv in plain.solves:             # first come first served: finishes in arrival order
+        assert pv.admitted >= pv.point.arrival and pv.finished > pv.admitted >= prev
+        prev = pv.finished
+        _same(by_point[id(pv.point)].result, pv.result, 1e-12)
