@@ -1009,8 +1009,14 @@ int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg) {
   int64_t g = (n + per_block - 1) / per_block;
   int64_t cap = (int64_t)num_sms * blocks_per_sm;
   if (g > cap) g = cap;
-  // the packed CIC counter holds at most kMaxBlockParticles per block and turn
-  const int64_t need = (n + kMaxBlockParticles - 1) / kMaxBlockParticles;
+  // The packed CIC counter holds at most kMaxBlockParticles per block and
+  // turn.  Block b takes the groups of PPT particles b·T + t + k·g·T: at most
+  // ceil((n / PPT) / (g·T)) steps of T·PPT particles, and block 0 also the
+  // n mod PPT tail.  So g is raised until no block takes more steps than fit.
+  const int64_t threads = pass_cfg_threads(cfg);
+  const int64_t steps = kMaxBlockParticles / ((int64_t)pass_cfg_ppt(cfg) * threads);
+  const int64_t groups = n / pass_cfg_ppt(cfg);
+  const int64_t need = (groups + steps * threads - 1) / (steps * threads);
   if (g < need) g = need;
   if (g < 1) g = 1;
   return (int)g;

@@ -20,9 +20,10 @@ def philox2x32_10(c0, c1, k):
     return c0, c1
 
 
-def philox_normals_reference(seed: int, turn: int, n: int) -> np.ndarray:
+def philox_normals_reference(seed: int, turn: int, n: int, first_pair: int = 0) -> np.ndarray:
+    """n normals of the pairs first_pair, first_pair + 1, ... (two per pair)."""
     npairs = (n + 1) // 2
-    p = np.arange(npairs, dtype=np.uint64)
+    p = np.arange(first_pair, first_pair + npairs, dtype=np.uint64)
     key = (seed ^ (seed >> 32)) & 0xFFFFFFFF
     c1 = (np.uint64(turn & 0xFFFFFF) | ((p >> np.uint64(32)) << np.uint64(24))) & _M
     x0, x1 = philox2x32_10(p & _M, c1, key)

@@ -15,7 +15,7 @@ import torch
 from haissinskijulia_b200 import (BinGrid, HaissinskiError, Particles, ResidentBunch, WakeModel,
                                   benchmark_ring, create_simulation_buffers, longitudinal_evolve,
                                   reference_ring, synthetic_bunch)
-from gpu_util import RTOL, assert_close, device_pair, rel_err
+from gpu_util import RTOL, assert_close, device_pair
 
 pytestmark = pytest.mark.gpu
 

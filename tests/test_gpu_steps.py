@@ -5,7 +5,6 @@ rtol = 1e-12 against the serial loop) including its synthetic inputs
 (z in [-5, 5), ΔE in [0, 0.1), tests/loop_benchmark.jl:84-122), plus the
 benchmark ring's physical inputs and edge cases.  Histograms are bit-exact.
 """
-import ctypes
 import math
 
 import numpy as np

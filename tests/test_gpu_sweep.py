@@ -9,11 +9,10 @@
   gives every request's result within 1e-12 of serve()'s, on a first come
   first served timeline.
 """
-import numpy as np
 import pytest
 
-from haissinskijulia_b200.sweep import (Point, Tuning, request_stream, run_batched, run_plain,
-                                        serve, serve_plain, sweep_points)
+from haissinskijulia_b200.sweep import (Tuning, request_stream, run_batched, run_plain, serve,
+                                        serve_plain, sweep_points)
 
 pytestmark = pytest.mark.gpu
 

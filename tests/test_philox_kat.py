@@ -25,3 +25,12 @@ def test_philox_pi_digits():
 def test_normals_moments():
     x = philox_normals_reference(7, 3, 400_000)
     assert abs(x.mean()) < 0.01 and abs(x.std() - 1) < 0.01
+
+
+def test_normals_from_a_pair_offset():
+    whole = philox_normals_reference(11, 5, 1000)
+    assert np.array_equal(philox_normals_reference(11, 5, 600, first_pair=200), whole[400:])
+    # beyond 2^32 pairs the counter's high word carries p >> 32
+    hi = philox_normals_reference(11, 5, 4, first_pair=(1 << 32) - 1)
+    lo = philox_normals_reference(11, 5, 2, first_pair=0)
+    assert not np.array_equal(hi[2:], lo)
