@@ -78,7 +78,10 @@ def workload(n: int, B: int) -> dict:
         "particles": n,
         "nbins": B,
         "turns_per_step": 1,
-        "l2": "state (16 B/particle) exceeds the 126 MB L2; no flush between turns",
+        "l2": (f"state ({16 * n / 1e6:.0f} MB, 16 B/particle) exceeds the 126 MB L2; "
+               "no flush between turns") if 16 * n > 126e6 else
+              (f"state ({16 * n / 1e6:.1f} MB) fits the 126 MB L2: a small case, "
+               "not the measured workload"),
     }
 
 

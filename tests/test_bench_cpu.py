@@ -1,0 +1,35 @@
+"""bench.py's reference arm on the CPU, launched the way multi-GPU runs are
+launched (torchrun, two ranks, rendezvous on 127.0.0.1): rank 0 alone prints
+one JSON line of the contract and both ranks exit 0."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_reference_arm_under_torchrun():
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py",
+           "--impl", "reference", "--gpus", "2", "--steps", "2", "--warmup", "1",
+           "--particles", "2e5", "--nbins", "1024", "--reference-seconds", "1"]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-3000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["steps"] == 2
+    assert d["value"] > 0 and d["higher_is_better"] is True
+    assert d["metric"] == "particle-turns/s (plain)" and d["unit"] == "particle-turns/s"
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    assert d["config"]["particles"] == 200_000 and d["config"]["nbins"] == 1024
