@@ -158,7 +158,7 @@ def test_crowded_bin_overflows_the_16bit_counters(gpu_ctx, oracle):
     b.close()
 
 
-@pytest.mark.parametrize("n", [2, 3, 5, 33, 1001])
+@pytest.mark.parametrize("n", [2, 3, 5, 31, 33, 1001])
 def test_tiny_bunches(gpu_ctx, oracle, n):
     cfg = benchmark_ring(n_turns=6, nbins=64)
     run_turn_by_turn(gpu_ctx, oracle, cfg, n, 6, seed=n)
