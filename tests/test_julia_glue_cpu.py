@@ -3,8 +3,8 @@
 Julia is not installed here, so the glue cannot run; these checks keep it
 in step with the header: its struct mirrors have the fields, order and widths
 of the ctypes mirrors (which the ABI tests compare with the C layouts), and
-every ccall names an exported entry point with the argument count and kinds
-of its declaration."""
+every ccall, in the glue and in the integration guide's examples, names an
+exported entry point with the argument count and kinds of its declaration."""
 import ctypes
 import os
 import re
@@ -91,13 +91,21 @@ def _split_types(s: str) -> list:
     return [t.strip() for t in out if t.strip()]
 
 
-def test_every_ccall_matches_its_declaration():
-    src = _glue()
-    calls = re.findall(r"ccall\(\(:(\w+), libhj\),\s*(\w+),\s*\(((?:[^()]|\([^()]*\))*)\)",
-                       src, re.S)
-    assert {c[0] for c in calls} >= {"hj_create", "hj_destroy", "hj_evolve",
-                                     "hj_wake_reference", "hj_last_error",
-                                     "hj_status_string"}
+_CCALL = r"ccall\(\(:(\w+), libhj\),\s*(\w+),\s*\(((?:[^()]|\([^()]*\))*)\)"
+
+
+@pytest.mark.parametrize("where", ["glue", "integration"])
+def test_every_ccall_matches_its_declaration(where):
+    if where == "glue":
+        src = _glue()
+        need = {"hj_create", "hj_destroy", "hj_evolve", "hj_wake_reference", "hj_last_error",
+                "hj_status_string"}
+    else:                               # the bindings shown to maintainers
+        with open(os.path.join(ROOT, "INTEGRATION.md"), encoding="utf-8") as f:
+            src = f.read()
+        need = {"hj_evolve", "hj_batch_create", "hj_batch_add_gaussian"}
+    calls = re.findall(_CCALL, src, re.S)
+    assert {c[0] for c in calls} >= need
     lib = _lib.SIGNATURES
     for name, ret, args in calls:
         assert name in lib, name
