@@ -237,6 +237,9 @@ class Context:
         _check(self, self._lib.hj_trim(self.handle))
 
     def close(self) -> None:
+        """Release the context (hj_destroy).  Bunches and batches created on it
+        keep working; the library frees the context when the last of them is
+        closed, whatever the order."""
         if getattr(self, "handle", None):
             self._lib.hj_destroy(self.handle)
             self.handle = None

@@ -356,13 +356,27 @@ extern "C" hj_status hj_create(int32_t device, hj_ctx** out) {
   return HJ_OK;
 }
 
-extern "C" void hj_destroy(hj_ctx* ctx) {
-  if (!ctx) return;
+static void ctx_free(hj_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->scratch) cudaFree(ctx->scratch);
   cache_clear(ctx, true);
   for (auto& kv : ctx->twiddles) cudaFree(kv.second);
   delete ctx;
+}
+
+extern "C" void hj_destroy(hj_ctx* ctx) {
+  if (!ctx || ctx->closing) return;
+  if (ctx->live_objects > 0) {   // freed by the last bunch or batch destroyed
+    ctx->closing = true;
+    return;
+  }
+  ctx_free(ctx);
+}
+
+void hj_impl::ctx_retain(hj_ctx* ctx) { ctx->live_objects += 1; }
+
+void hj_impl::ctx_release(hj_ctx* ctx) {
+  if (--ctx->live_objects == 0 && ctx->closing) ctx_free(ctx);
 }
 
 extern "C" const char* hj_last_error(const hj_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
@@ -387,6 +401,10 @@ extern "C" hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout) {
 
 extern "C" void hj_bunch_destroy(hj_bunch* b) {
   if (!b) return;
+  if (!b->ctx) {                          // failed before it was tied to a context
+    delete b;
+    return;
+  }
   cudaSetDevice(b->ctx->device);
   cudaStreamSynchronize(b->stream);       // nothing queued still uses the blocks
   cache_give(b->ctx, false, b->arena, b->arena_cap);
@@ -396,7 +414,10 @@ extern "C" void hj_bunch_destroy(hj_bunch* b) {
   if (b->d_sums) cudaFree(b->d_sums);
   if (b->d_log) cudaFree(b->d_log);
   for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+  hj_ctx* ctx = b->ctx;
+  const bool held = b->holds_ctx;
   delete b;
+  if (held) ctx_release(ctx);
 }
 
 // Creation of a bunch in two halves, so that a batch can admit many bunches
@@ -412,6 +433,10 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
                                       int64_t nbins, const hj_grid* grid, uint64_t seed,
                                       void* stream, hj_bunch* b, int64_t chunk, int cfg) {
   b->ctx = ctx;
+  if (!b->holds_ctx) {
+    ctx_retain(ctx);
+    b->holds_ctx = true;
+  }
   b->stream = (cudaStream_t)stream;
   b->z = d_z;
   b->dE = d_dE;

@@ -25,6 +25,7 @@ struct BatchMember {
 
 struct hj_batch {
   hj_ctx* ctx = nullptr;
+  bool holds_ctx = false;                      // counted in ctx->live_objects
   cudaStream_t stream = nullptr;
   int cfg = 0;
   int64_t chunk = 65536;
@@ -214,6 +215,10 @@ int batch_find(const hj_batch* bt, int64_t id) {
 
 extern "C" void hj_batch_destroy(hj_batch* bt) {
   if (!bt) return;
+  if (!bt->ctx) {
+    delete bt;
+    return;
+  }
   cudaSetDevice(bt->ctx->device);
   if (bt->stream) cudaStreamSynchronize(bt->stream);
   for (auto& m : bt->members) {
@@ -224,13 +229,18 @@ extern "C" void hj_batch_destroy(hj_batch* bt) {
   cache_give(bt->ctx, false, bt->arena, bt->arena_cap);
   cache_give(bt->ctx, true, bt->harena, bt->harena_cap);
   if (bt->stream) cudaStreamDestroy(bt->stream);
+  hj_ctx* ctx = bt->ctx;
+  const bool held = bt->holds_ctx;
   delete bt;
+  if (held) ctx_release(ctx);
 }
 
 static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunches,
                                    int32_t max_nbins, int64_t chunk, int32_t layout,
                                    hj_batch* bt) {
   bt->ctx = ctx;
+  ctx_retain(ctx);
+  bt->holds_ctx = true;
   bt->chunk = chunk;
   bt->max_bunches = max_bunches;
   bt->max_B = max_nbins;

@@ -54,10 +54,16 @@ struct hj_ctx {
   };
   std::map<std::array<uint64_t, 8>, WakeSet> wake_sets;
   uint64_t wake_clock = 0;
+  // Bunches and batches alive on this context.  hj_destroy with some alive
+  // only marks the context closing; the last of them to be destroyed frees it,
+  // so objects may be destroyed in any order (e.g. by a garbage collector).
+  int64_t live_objects = 0;
+  bool closing = false;
 };
 
 struct hj_bunch {
   hj_ctx* ctx = nullptr;
+  bool holds_ctx = false;   // counted in ctx->live_objects
   cudaStream_t stream = nullptr;
   double* z = nullptr;
   double* dE = nullptr;
@@ -162,6 +168,10 @@ struct Carve {
 
 hj_status set_err(hj_ctx* ctx, hj_status code, const char* fmt, ...);
 hj_status ctx_ok(hj_ctx* ctx);
+// Count an object in ctx->live_objects / drop it (the last drop of a closing
+// context frees the context).
+void ctx_retain(hj_ctx* ctx);
+void ctx_release(hj_ctx* ctx);
 
 template <typename T>
 hj_status dalloc(hj_ctx* ctx, T** p, size_t count) {

@@ -134,6 +134,11 @@ const char* hj_status_string(hj_status s);
 /* Create a context on CUDA device `device`.  No reference counterpart (the
  * reference allocates per call in create_simulation_buffers, src/utils.jl:147). */
 hj_status hj_create(int32_t device, hj_ctx** out);
+/* Free the context.  After this call the handle must not be passed to any
+ * entry point.  Bunches and batches keep their context alive: with some still
+ * alive, hj_destroy only marks the context closing, they keep working (a
+ * batch still admits bunches), and the last of them to be destroyed frees it,
+ * so objects may be destroyed in any order, as a garbage collector does. */
 void hj_destroy(hj_ctx* ctx);
 /* Message of the last failure on this context ("" if none). */
 const char* hj_last_error(const hj_ctx* ctx);

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 import torch
 
-from haissinskijulia_b200 import Batch, HaissinskiError, ResidentBunch, benchmark_ring
+from haissinskijulia_b200 import Batch, Context, HaissinskiError, ResidentBunch, benchmark_ring
 from haissinskijulia_b200 import _lib
 
 from gpu_util import assert_close, device_pair
@@ -201,3 +201,29 @@ def test_results_count_the_turns_run(gpu_ctx):
     _, _, r = bt.take(bid, copy_out=False)
     bt.close()
     assert r.turns == 11
+
+
+def test_closing_the_context_first_leaves_its_bunches_working(gpu_ctx):
+    """hj_destroy before the bunch and the batch: both keep working (the batch
+    still admits) and the last one destroyed frees the context."""
+    cfg = benchmark_ring(n_turns=1, nbins=512)
+    z, dE = _bunch(20_000, 7, cfg)
+    want = _plain(gpu_ctx, cfg, z, dE, 512, 11, 12)
+    ctx = Context(0)
+    dz, de = device_pair(z, dE)
+    b = ResidentBunch(ctx, dz.data_ptr(), de.data_ptr(), z.size, cfg.params, 512,
+                      wake=cfg.wake, seed=11)
+    bt = Batch(ctx, pool_particles=50_000, max_bunches=2, max_nbins=512, chunk=16384)
+    ctx.close()
+    bid = bt.add(z, dE, cfg.params, 512, wake=cfg.wake, seed=11, turns=12)
+    b.advance(12)
+    r = b.finish()
+    b.close()
+    _check((dz.cpu().numpy(), de.cpu().numpy(), r), want, cfg, "bunch after close")
+    for _ in range(4):
+        bt.advance(4)
+        if bid in bt.poll():
+            break
+    got = bt.take(bid)
+    bt.close()                          # the last object: frees the context
+    _check(got, want, cfg, "batch after close")
