@@ -89,9 +89,13 @@ mutable struct GPUBackend
     end
 end
 
-to_c(p::SimulationParameters) = HjParams(p.E0, p.mass, p.voltage, p.harmonic, p.radius,
-    p.pipe_radius, p.α_c, p.ϕs, p.freq_rf, p.n_turns, p.use_wakefield, p.update_η,
-    p.update_E0, p.SR_damping, p.use_excitation, 0, 0, 0)
+# The C mirror of a SimulationParameters, optionally with another RF voltage
+# (one point of a voltage sweep).
+HjParams(p::SimulationParameters; voltage::Real = p.voltage) =
+    HjParams(p.E0, p.mass, Float64(voltage), p.harmonic, p.radius, p.pipe_radius, p.α_c,
+             p.ϕs, p.freq_rf, p.n_turns, p.use_wakefield, p.update_η, p.update_E0,
+             p.SR_damping, p.use_excitation, 0, 0, 0)
+to_c(p::SimulationParameters) = HjParams(p)
 
 function reference_wake(p::HjParams)
     w = Ref{HjWake}()
