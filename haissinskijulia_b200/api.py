@@ -756,7 +756,7 @@ class Batch:
     def take(self, bid: int, copy_out: bool = True):
         """Finishes bunch `bid` and frees its slot; returns (z, dE, EvolveResult)
         (z and dE are None without copy_out)."""
-        n = self.sizes.pop(bid)
+        n = self._size(bid)
         z = np.empty(n) if copy_out else None
         dE = np.empty(n) if copy_out else None
         r = HjResult()
@@ -764,14 +764,21 @@ class Batch:
             self.handle, int(bid), z.ctypes.data_as(ctypes.c_void_p) if copy_out else None,
             dE.ctypes.data_as(ctypes.c_void_p) if copy_out else None, ctypes.byref(r))
         _check(self.ctx, rc)
+        del self.sizes[bid]               # only once the library has retired it
         return z, dE, EvolveResult.from_c(r)
+
+    def _size(self, bid: int) -> int:
+        if bid not in self.sizes:
+            raise HaissinskiError(_lib.HJ_ERR_ARG, f"no bunch {bid} in this batch")
+        return self.sizes[bid]
 
     def take_device(self, bid: int, d_z: int, d_dE: int) -> EvolveResult:
         """As take(), with (z, dE) copied to device arrays (ints: pointers)."""
-        self.sizes.pop(bid)
+        self._size(bid)
         r = HjResult()
         _check(self.ctx, self.ctx._lib.hj_batch_take(self.handle, int(bid), ctypes.c_void_p(d_z),
                                                      ctypes.c_void_p(d_dE), ctypes.byref(r)))
+        del self.sizes[bid]
         return EvolveResult.from_c(r)
 
     def add_many(self, z, dE, n, params, nbins, seeds, turns, wakes=None):
