@@ -2,6 +2,7 @@
 // pool, one turn-state array, per turn one batched pass over a chunk table,
 // one merge of the chunk partials and one batched bins step; turn blocks
 // replayed from a CUDA graph.
+#include "hj_ranges.h"
 #include "hj_state.h"
 
 // ====================================================================== batches
@@ -37,7 +38,7 @@ struct hj_batch {
   int64_t pool_n = 0;
   double* pool_z = nullptr;
   double* pool_dE = nullptr;
-  std::vector<std::pair<int64_t, int64_t>> free_ranges;   // (start, length), sorted
+  hj_ranges::Ranges free_ranges;               // free pool ranges (first fit)
   std::vector<BatchMember> members;            // dense: index = device table slot
   std::vector<int> free_slots;
   int64_t next_id = 1;
@@ -68,42 +69,14 @@ struct hj_batch {
 namespace {
 
 hj_status batch_alloc_range(hj_batch* bt, int64_t n, int64_t* start, int64_t* cap) {
-  const int64_t need = std::max<int64_t>((n + 3) / 4 * 4, 4);
-  for (size_t i = 0; i < bt->free_ranges.size(); ++i) {
-    auto& r = bt->free_ranges[i];
-    if (r.second >= need) {
-      *start = r.first;
-      *cap = need;
-      r.first += need;
-      r.second -= need;
-      if (r.second == 0) bt->free_ranges.erase(bt->free_ranges.begin() + i);
-      return HJ_OK;
-    }
-  }
-  return HJ_ERR_FULL;
+  return hj_ranges::take(bt->free_ranges, n, start, cap) ? HJ_OK : HJ_ERR_FULL;
 }
 
 void batch_free_range(hj_batch* bt, int64_t start, int64_t cap) {
-  auto& fr = bt->free_ranges;
-  auto it = std::lower_bound(fr.begin(), fr.end(), std::make_pair(start, (int64_t)0));
-  it = fr.insert(it, {start, cap});
-  // merge with the neighbours
-  size_t i = it - fr.begin();
-  if (i + 1 < fr.size() && fr[i].first + fr[i].second == fr[i + 1].first) {
-    fr[i].second += fr[i + 1].second;
-    fr.erase(fr.begin() + i + 1);
-  }
-  if (i > 0 && fr[i - 1].first + fr[i - 1].second == fr[i].first) {
-    fr[i - 1].second += fr[i].second;
-    fr.erase(fr.begin() + i);
-  }
+  hj_ranges::give(bt->free_ranges, start, cap);
 }
 
-int64_t batch_largest_free(const hj_batch* bt) {
-  int64_t m = 0;
-  for (auto& r : bt->free_ranges) m = std::max(m, r.second);
-  return m;
-}
+int64_t batch_largest_free(const hj_batch* bt) { return hj_ranges::largest(bt->free_ranges); }
 
 // Rebuild and upload the device tables (bunch arguments, chunk table, counts).
 hj_status batch_upload(hj_batch* bt) {
