@@ -25,7 +25,7 @@ LIB = PKG / "libhaissinski_gpu.so"
 CU_SOURCES = ["hj_track.cu", "hj_wake.cu", "hj_api.cu", "hj_batch.cu", "hj_extra.cu",
               "hj_noalloc.cu"]
 CPP_SOURCES = ["hj_host.cpp"]
-HEADERS = ["hj_device.cuh", "hj_internal.h", "hj_host.h", "hj_ranges.h", "hj_state.h"]
+HEADERS = ["hj_device.cuh", "hj_internal.h", "hj_host.h", "hj_launch.h", "hj_ranges.h", "hj_state.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "hj_device.cuh"
+#include "hj_launch.h"
 
 namespace hj {
 
@@ -36,22 +37,9 @@ constexpr int kNumSums = 4;         // per-block partial sums of the particle pa
 constexpr int kTrackThreads = 512;  // threads per block of the particle kernels
 constexpr int kBinsThreads = 1024;  // threads of the single-CTA bins kernel
 constexpr int64_t kMaxBins = 16384; // largest grid the shared-memory FFT holds (P = 32768)
-// Particles one block of the fused pass may deposit per turn (the packed CIC
-// counter keeps a 20-bit count per cell).
-constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
-
-// Thread layouts of the fused pass (particles/thread x threads/block; the next
-// group prefetched into registers except in 3): 0 = 4 x 512, 1 = 2 x 1024,
-// 2 = 2 x 768, 3 = 2 x 512 without prefetch, 4 = 2 x 512 at 64 registers (two
-// blocks per SM where shared memory allows).
-constexpr int kNumPassCfgs = 5;       // thread layouts of the fused pass
-constexpr int kPassLayoutMask = 7;    // layout bits of a pass configuration
-constexpr int kPassN32 = 8;           // + one 32-bit NGP counter per bin (else 16-bit pairs)
+// kMaxBlockParticles, the thread layouts and the pass grid rule: hj_launch.h
 constexpr int kRfTableSize = 128;    // entries of the fused pass's RF kick table
 constexpr int kLogHeader = 8;       // doubles before the bin counts in a turn-log record
-int pass_cfg_threads(int cfg);
-bool pass_cfg_valid(int cfg);
-int pass_cfg_ppt(int cfg);
 
 // Quantum-excitation source of the particle pass.
 enum QeMode { QE_OFF = 0, QE_PHILOX = 1, QE_DRAWS = 2 };
@@ -151,7 +139,6 @@ struct FlushArgs {
 // ---- launchers (hj_track.cu) ----
 cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin);
 cudaError_t prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
-int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg);
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
 size_t track_smem_bytes(int B, int use_wake, int cfg);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);

@@ -958,16 +958,6 @@ const void* batch_fn(int wake, int qe, int cfg) {
 }
 }  // namespace
 
-int pass_cfg_threads(int cfg) {
-  const int l = cfg & kPassLayoutMask;
-  return l == 1 ? 1024 : (l == 2 ? 768 : 512);
-}
-int pass_cfg_ppt(int cfg) { return (cfg & kPassLayoutMask) == 0 ? 4 : 2; }
-bool pass_cfg_valid(int cfg) {
-  return cfg >= 0 && (cfg & ~(kPassLayoutMask | kPassN32)) == 0 &&
-         (cfg & kPassLayoutMask) < kNumPassCfgs;
-}
-
 cudaError_t prepare_track_kernels(int max_smem) {
   for (int w = 0; w < 2; ++w)
     for (int q = 0; q < 3; ++q)
@@ -997,29 +987,6 @@ int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
                                                     pass_cfg_threads(cfg), smem) != cudaSuccess)
     bps = 1;
   return bps < 1 ? 1 : bps;
-}
-
-// Blocks of the particle pass: enough to fill the GPU, but each block should
-// move at least B/2 particles, since it writes a B-bin partial histogram
-// that the merge reads back (B/2 measured best for 1e5-1e7 particles at 4096
-// and 16384 bins).
-int track_grid_size(int64_t n, int B, int num_sms, int blocks_per_sm, int cfg) {
-  int64_t per_block = (int64_t)pass_cfg_ppt(cfg) * pass_cfg_threads(cfg);
-  if (per_block < (int64_t)B / 2) per_block = (int64_t)B / 2;
-  int64_t g = (n + per_block - 1) / per_block;
-  int64_t cap = (int64_t)num_sms * blocks_per_sm;
-  if (g > cap) g = cap;
-  // The packed CIC counter holds at most kMaxBlockParticles per block and
-  // turn.  Block b takes the groups of PPT particles b·T + t + k·g·T: at most
-  // ceil((n / PPT) / (g·T)) steps of T·PPT particles, and block 0 also the
-  // n mod PPT tail.  So g is raised until no block takes more steps than fit.
-  const int64_t threads = pass_cfg_threads(cfg);
-  const int64_t steps = kMaxBlockParticles / ((int64_t)pass_cfg_ppt(cfg) * threads);
-  const int64_t groups = n / pass_cfg_ppt(cfg);
-  const int64_t need = (groups + steps * threads - 1) / (steps * threads);
-  if (g < need) g = need;
-  if (g < 1) g = 1;
-  return (int)g;
 }
 
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
