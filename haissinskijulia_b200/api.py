@@ -386,7 +386,8 @@ def longitudinal_evolve(particles: Particles, params: SimulationParameters,
 
     The wake follows the reference's MPI branch, the one that runs with the
     wakefield on.  `comm`/`use_mpi` are accepted for signature parity; a
-    multi-rank run partitions particles with haissinskijulia_b200.parallel.
+    multi-rank run shards one bunch's particles over the ranks with
+    ShardedBunch (one all-reduce of the bin exchange per turn).
     qe_draws: optional (n_turns, n) standard normals replacing randn!.
     """
     if use_mpi and comm is None:
@@ -760,12 +761,30 @@ class Batch:
         z = np.empty(n) if copy_out else None
         dE = np.empty(n) if copy_out else None
         r = HjResult()
+        live = self._live()
         rc = self.ctx._lib.hj_batch_take(
             self.handle, int(bid), z.ctypes.data_as(ctypes.c_void_p) if copy_out else None,
             dE.ctypes.data_as(ctypes.c_void_p) if copy_out else None, ctypes.byref(r))
-        _check(self.ctx, rc)
-        del self.sizes[bid]               # only once the library has retired it
+        self._forget([bid], rc, live)
         return z, dE, EvolveResult.from_c(r)
+
+    def _live(self) -> int:
+        """Bunches the library holds in this batch (hj_batch_stats, host only)."""
+        out = np.zeros(4, dtype=np.int64)
+        _check(self.ctx, self.ctx._lib.hj_batch_stats(self.handle, _ip(out)))
+        return int(out[0])
+
+    def _forget(self, ids, rc: int, live_before: int) -> None:
+        """Drop `ids` from the host bookkeeping once the library has retired
+        them, then raise if the call failed.  hj_batch_take(_many) retires its
+        bunches as soon as their results are read back and reports a bunch's
+        own failure (a non-finite result, short host-fed draws) only after
+        that, so a failed take may or may not have retired them: the live
+        count says which."""
+        if rc == _lib.HJ_OK or self._live() < live_before:
+            for b in ids:
+                self.sizes.pop(int(b), None)
+        _check(self.ctx, rc)
 
     def _size(self, bid: int) -> int:
         if bid not in self.sizes:
@@ -776,9 +795,10 @@ class Batch:
         """As take(), with (z, dE) copied to device arrays (ints: pointers)."""
         self._size(bid)
         r = HjResult()
-        _check(self.ctx, self.ctx._lib.hj_batch_take(self.handle, int(bid), ctypes.c_void_p(d_z),
-                                                     ctypes.c_void_p(d_dE), ctypes.byref(r)))
-        del self.sizes[bid]
+        live = self._live()
+        rc = self.ctx._lib.hj_batch_take(self.handle, int(bid), ctypes.c_void_p(d_z),
+                                         ctypes.c_void_p(d_dE), ctypes.byref(r))
+        self._forget([bid], rc, live)
         return EvolveResult.from_c(r)
 
     def add_many(self, z, dE, n, params, nbins, seeds, turns, wakes=None):
@@ -827,10 +847,10 @@ class Batch:
         idv = np.ascontiguousarray(ids, dtype=np.int64)
         res = (HjResult * max(k, 1))()
         corr = np.zeros(max(k, 1)) if correlation else None
-        _check(self.ctx, self.ctx._lib.hj_batch_take_many(
-            self.handle, k, _ip(idv), None, None, res, _dp(corr) if correlation else None))
-        for b in ids:
-            self.sizes.pop(int(b), None)
+        live = self._live()
+        rc = self.ctx._lib.hj_batch_take_many(
+            self.handle, k, _ip(idv), None, None, res, _dp(corr) if correlation else None)
+        self._forget(ids, rc, live)          # all of them retire, or none
         results = [EvolveResult.from_c(res[i]) for i in range(k)]
         return results, ([float(c) for c in corr[:k]] if correlation else None)
 
