@@ -5,19 +5,21 @@ its broadband-resonator wake, every physics switch on).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one turn of the whole bunch.  `value` is device-timed (CUDA events on
-the bunch's stream, max over ranks) with the state resident in HBM; `e2e` is the
-public longitudinal_evolve call with pinned host buffers, host<->device copies
-inside the timed region.  `--impl reference` times the CPU oracle (the plain-C
-restatement of the reference's turn loop, OpenMP over all host cores) on the
-same workload, rank 0 only.  Prints one JSON line on rank 0.
+A step is 100 turns of the whole bunch, ending with the turn-log record
+(moments and line density) the at-scale configuration asks for every 100
+turns.  `value` is device-timed (CUDA events on the bunch's stream, max over
+ranks) with the state resident in HBM; `e2e` is the public longitudinal_evolve
+call with pinned host buffers, host<->device copies inside the timed region.
+`--impl reference` times the CPU oracle (the plain-C restatement of the
+reference's turn loop, OpenMP over all host cores) on the same workload, rank
+0 only, without loading the GPU library.  Prints one JSON line on rank 0.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
-import re
+import math
 import statistics
 import subprocess
 import sys
@@ -33,6 +35,10 @@ METRIC = "particle-turns/s (plain)"
 UNIT = "particle-turns/s"
 BYTES_PER_PARTICLE_TURN = 32   # read + write z and ΔE, Float64
 FALLBACK_HBM_GBS = 6650.0
+LOG_EVERY = 100                # turns between turn-log records (one per step)
+# DRAM bytes (read + write) per particle-turn of k_track_pass from one ncu
+# capture, by bin count: (bytes, the profile summary that holds the capture).
+PASS_DRAM_BYTES = {16384: (30.53, "profiles/k_track_pass_full_2e7_b16384.md")}
 
 
 def parse_args():
@@ -44,6 +50,8 @@ def parse_args():
     ap.add_argument("--particles", type=float, default=1e8)
     ap.add_argument("--nbins", type=int, default=16384)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--turns-per-step", type=int, default=LOG_EVERY,
+                    help="turns of one step (the last one writes the turn-log record)")
     ap.add_argument("--layout", type=int, default=-1,
                     help="thread layout of the fused pass (-1 = library default)")
     ap.add_argument("--e2e-calls", type=int, default=1,
@@ -69,7 +77,7 @@ def parse_args():
     return ap.parse_args()
 
 
-def workload(n: int, B: int) -> dict:
+def workload(n: int, B: int, turns_per_step: int = LOG_EVERY) -> dict:
     return {
         "workload": f"plain single bunch at scale: {n:.0e} Float64 macroparticles, {B} bins, "
                     "4 GeV benchmark ring, resonator wake (Rs=10kOhm, Q=1, fr=20GHz, 1e10 e-), "
@@ -77,7 +85,7 @@ def workload(n: int, B: int) -> dict:
                     "logged on the device every 100 turns",
         "particles": n,
         "nbins": B,
-        "turns_per_step": 1,
+        "turns_per_step": turns_per_step,
         "l2": (f"state ({16 * n / 1e6:.0f} MB, 16 B/particle) exceeds the 126 MB L2; "
                "no flush between turns") if 16 * n > 126e6 else
               (f"state ({16 * n / 1e6:.1f} MB) fits the 126 MB L2: a small case, "
@@ -94,18 +102,9 @@ def measured_hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic_per_particle_turn():
-    """DRAM bytes per particle-turn of the particle pass from the committed ncu
-    summary (profiles/), or None."""
-    for f in sorted((ROOT / "profiles").glob("*.md")):
-        m = re.search(r"dram_bytes_per_particle_turn:\s*([0-9.eE+-]+)", f.read_text())
-        if m:
-            return float(m.group(1)), f.name
-    return None, None
-
-
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """nvidia-smi clock/throttle samples every 100 ms; mark() brackets the
+    timed region so that only its samples are summarised."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -114,29 +113,47 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.marks = []
         self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"hj_clocks_{os.getpid()}.csv"
 
     def start(self):
+        """Starts the sampler and waits (up to 5 s) for its first sample."""
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device)], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "100", "-i", str(self.device)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self._lines() == 0 and self.proc.poll() is None:
+            time.sleep(0.05)
+
+    def _lines(self) -> int:
+        try:
+            return len(self.path.read_text().splitlines())
+        except Exception:
+            return 0
+
+    def mark(self):
+        self.marks.append(self._lines())
 
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)              # the sample that closes the timed region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.f.close()
+        lines = self.path.read_text().splitlines()
+        lo, hi = (self.marks[0], self.marks[1] + 1) if len(self.marks) >= 2 else (0, len(lines))
         sm, smax, reasons, power = [], [], set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
+        for line in lines[lo:hi]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -153,7 +170,8 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
                 "power_w_median": statistics.median(power) if power else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "reasons": sorted(reasons),
+                "window": "samples every 100 ms between the start and the end of the timed region"}
 
 
 def cpu_cores() -> int:
@@ -163,21 +181,44 @@ def cpu_cores() -> int:
         return os.cpu_count() or 1
 
 
-def cpu_oracle_rate(n: int, B: int, seconds: float, seed: int, threads: int):
+def ring_structs(B: int):
+    """The benchmark ring's (hj_params, hj_wake) in plain Python, so that the
+    CPU legs never load the GPU library: the values of rings.benchmark_ring
+    (E0 = 4 GeV, h = 360 at 500 MHz, V = 5 MV, α_c = 3e-4, U0 = 0.5 MeV,
+    5000-turn damping) and the resonator mapping of hj_wake_resonator
+    (Rs = 10 kΩ, Q = 1, f_r = 20 GHz, 1e10 electrons, bins over ±6σ_z)."""
+    from haissinskijulia_b200._lib import HjParams, HjWake
+    E0, U0, V, c = 4e9, 0.5e6, 5e6, 299792458.0
+    p = HjParams()
+    p.E0, p.mass, p.voltage, p.harmonic = E0, 0.51099895069e6, V, 360
+    p.radius = 4 * 8.85e-5 * (E0 / 1e9) ** 3 * 5000.0
+    p.pipe_radius, p.alpha_c, p.phi_s, p.freq_rf = 2.5e-4, 3e-4, math.pi - math.asin(U0 / V), 500e6
+    p.n_turns = 1
+    p.use_wakefield = p.update_eta = p.update_E0 = p.SR_damping = p.use_excitation = 1
+    wr = 6.283185307179586 * 20e9
+    alpha = wr / 2.0
+    wbar = math.sqrt(wr * wr - alpha * alpha)
+    w = HjWake()
+    w.wake_factor, w.wake_sqrt, w.ctau, w.sin_coef = 2.0 * alpha * 1e4, wbar / c, c / alpha, alpha / wbar
+    w.population, w.half_width_sigmas, w.delta_std = 1e10, 6.0, 0.15
+    return p, w, 4e-3, 1e-3 * E0
+
+
+def cpu_oracle_rate(n: int, B: int, seconds: float, seed: int, threads: int, tps: int = 1):
     """Particle-turns/s of the CPU oracle on an n-particle bunch of the benchmark
-    workload: whole turns until `seconds` of CPU work (at least one turn)."""
-    from haissinskijulia_b200 import benchmark_ring, synthetic_bunch
+    workload: whole blocks of `tps` turns until `seconds` of CPU work (at least one)."""
     from oracle import Oracle
-    cfg = benchmark_ring(n_turns=1, nbins=B)
+    params, wake, sigma_z, sigma_E = ring_structs(B)
     orc = Oracle(threads=threads)
-    p = synthetic_bunch(n, cfg.sigma_z, cfg.sigma_E, seed)
-    z, dE = p.coordinates.z, p.coordinates.dE
-    st = orc.state(z, dE, cfg.params.to_c(), cfg.wake.to_c(), B, None, seed=seed)
+    rng = np.random.Generator(np.random.Philox(seed))
+    z, dE = rng.normal(0.0, sigma_z, n), rng.normal(0.0, sigma_E, n)
+    st = orc.state(z, dE, params, wake, B, None, seed=seed)
     turns = 0
     t0 = time.perf_counter()
     while True:
-        st.turn(None)
-        turns += 1
+        for _ in range(tps):
+            st.turn(None)
+        turns += tps
         el = time.perf_counter() - t0
         if el >= seconds:
             break
@@ -186,38 +227,39 @@ def cpu_oracle_rate(n: int, B: int, seconds: float, seed: int, threads: int):
 
 
 def run_reference(args) -> None:
-    """--impl reference: the CPU oracle of the reference's loop, rank 0 only."""
+    """--impl reference: the CPU oracle of the reference's loop, rank 0 only,
+    on the same ring, wake and step (100 turns) as the GPU arm, over a bounded
+    sample of the bunch's particles."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n_full, B = int(args.particles), args.nbins
-    cores = cpu_cores()
-    from haissinskijulia_b200 import benchmark_ring, synthetic_bunch
     from oracle import Oracle
+    n_full, B, tps = int(args.particles), args.nbins, args.turns_per_step
+    cores = cpu_cores()
     orc = Oracle(threads=cores)
     # size the per-step sample so warmup + steps fit the CPU budget
     probe, _, _ = cpu_oracle_rate(min(n_full, 1_000_000), B, 0.5, args.seed, cores)
-    total_steps = args.steps + args.warmup
-    n = int(min(n_full, max(100_000, args.reference_seconds * probe / max(total_steps, 1))))
-    cfg = benchmark_ring(n_turns=1, nbins=B)
-    p = synthetic_bunch(n, cfg.sigma_z, cfg.sigma_E, args.seed)
-    st = orc.state(p.coordinates.z, p.coordinates.dE, cfg.params.to_c(), cfg.wake.to_c(), B,
-                   None, seed=args.seed)
-    for _ in range(args.warmup):
+    total_turns = (args.steps + args.warmup) * tps
+    n = int(min(n_full, max(20_000, args.reference_seconds * probe / max(total_turns, 1))))
+    params, wake, sigma_z, sigma_E = ring_structs(B)
+    rng = np.random.Generator(np.random.Philox(args.seed))
+    z, dE = rng.normal(0.0, sigma_z, n), rng.normal(0.0, sigma_E, n)
+    st = orc.state(z, dE, params, wake, B, None, seed=args.seed)
+    for _ in range(args.warmup * tps):
         st.turn(None)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(args.steps * tps):
         st.turn(None)
     el = time.perf_counter() - t0
-    value = n * args.steps / el
-    sample = (f"{n} of the {n_full:.0e} particles per step (one turn each, {B} bins), "
-              f"oracle/oracle.c (plain-C restatement of longitudinal_evolve!, OpenMP)")
+    value = n * args.steps * tps / el
+    sample = (f"{n} of the {n_full:.0e} particles, {tps} turns per step, {B} bins: "
+              "oracle/oracle.c (plain-C restatement of longitudinal_evolve!, OpenMP)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload(n_full, B),
+        "config": workload(n_full, B, tps),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -368,7 +410,8 @@ def run_ours(args) -> None:
     hjbuild.build()
 
     n, B, K, W = int(args.particles), args.nbins, args.steps, args.warmup
-    cfg = benchmark_ring(n_turns=K, nbins=B)
+    tps = args.turns_per_step
+    cfg = benchmark_ring(n_turns=K * tps, nbins=B)
     ctx = Context(local)
     ctx.set_pass_layout(args.layout)
     stream = torch.cuda.current_stream()
@@ -377,26 +420,30 @@ def run_ours(args) -> None:
     dE = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_E
     bunch = ResidentBunch(ctx, z.data_ptr(), dE.data_ptr(), n, cfg.params, B, wake=cfg.wake,
                           seed=args.seed + rank, stream=stream.cuda_stream)
-    # moments and line density logged on the device every 100 turns
-    bunch.set_log(100, capacity=(K + W) // 100 + 1, density=True)
+    # moments and line density logged on the device every 100 turns: each
+    # step ends with one record
+    bunch.set_log(LOG_EVERY, capacity=(K + W) * tps // LOG_EVERY + 1, density=True)
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
 
-    bunch.advance(W)
-    barrier()
-    bunch.set_profiling(True)
     clocks = ClockSampler(local)
     clocks.start()
+    bunch.advance(W * tps)
+    barrier()
+    bunch.set_profiling(True)
+    clocks.mark()
     t_wall0 = time.perf_counter()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    bunch.advance(K)
+    for _ in range(K):
+        bunch.advance(tps)
     ev1.record(stream)
     torch.cuda.synchronize()
     t_wall = time.perf_counter() - t_wall0
+    clocks.mark()
     clock_info = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     prof = bunch.read_profile()
@@ -407,14 +454,14 @@ def run_ours(args) -> None:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = n * K * world / (ms / 1e3)
+    value = n * K * tps * world / (ms / 1e3)
 
     # roofline of the dominant kernel (the fused particle pass)
     pass_ms = prof["pass_ms"] / max(prof["turns"], 1)
     bins_ms = prof["bins_ms"] / max(prof["turns"], 1)
     achieved = BYTES_PER_PARTICLE_TURN * n / (pass_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm_peak()
-    tr, tr_src = profiled_traffic_per_particle_turn()
+    tr, tr_src = PASS_DRAM_BYTES.get(B, (None, None))
     roofline = {"bound": "hbm", "kernel": "k_track_pass", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
@@ -473,11 +520,12 @@ def run_ours(args) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload(n, B), parallelism="replicas" if world > 1 else "single GPU"),
+            "config": dict(workload(n, B, tps),
+                           parallelism="replicas" if world > 1 else "single GPU"),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "sweep": sweep,
             "gpu_launches": prof["launches"], "clocks": clock_info,
             "wall_seconds_timed": t_wall,
-            "turn_log": {"every": 100, "records": int(log.shape[0]),
+            "turn_log": {"every": LOG_EVERY, "records": int(log.shape[0]),
                          "content": "turn, E0, sigma_z, sigma_E, mean z, mean dE, wake current, "
                                     f"particles in bins + {B} bin counts, written on the device",
                          "last": {"turn": float(log[-1, 0]), "E0": float(log[-1, 1]),

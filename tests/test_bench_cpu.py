@@ -33,3 +33,38 @@ def test_reference_arm_under_torchrun():
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert d["config"]["particles"] == 200_000 and d["config"]["nbins"] == 1024
+
+
+def test_reference_arm_never_loads_the_gpu_library(monkeypatch, capsys):
+    """The CPU arm builds its ring in plain Python and runs the oracle only."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from haissinskijulia_b200 import _lib
+
+    def refuse():
+        raise AssertionError("the reference arm loaded the GPU library")
+    monkeypatch.setattr(_lib, "load", refuse)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference", "--steps", "1",
+                                      "--warmup", "0", "--particles", "5e4", "--nbins", "512",
+                                      "--turns-per-step", "3", "--reference-seconds", "0.2"])
+    bench.main()
+    d = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert d["config"]["turns_per_step"] == 3
+
+
+def test_plain_python_ring_equals_the_library_ring():
+    """bench.ring_structs restates rings.benchmark_ring and hj_wake_resonator
+    field for field."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from haissinskijulia_b200 import benchmark_ring
+    p, w, sz, sE = bench.ring_structs(16384)
+    cfg = benchmark_ring(n_turns=1, nbins=16384)
+    pc, wc = cfg.params.to_c(), cfg.wake.to_c()
+    for f, _ in pc._fields_:
+        if f != "_pad":
+            assert getattr(p, f) == getattr(pc, f), f
+    for f, _ in wc._fields_:
+        assert getattr(w, f) == getattr(wc, f), f
+    assert (sz, sE) == (cfg.sigma_z, cfg.sigma_E)
