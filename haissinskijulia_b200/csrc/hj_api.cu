@@ -732,6 +732,7 @@ void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
   a.n = b->n;
   a.ts = b->ts;
   a.potd = b->potd;
+  a.win = b->use_wake ? track_window_entries(b->B, b->cfg) : 0;
   a.B = b->B;
   a.use_wake = b->use_wake;
   a.e0 = b->e0;

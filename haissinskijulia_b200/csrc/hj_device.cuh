@@ -55,6 +55,8 @@ struct TurnState {
   double last_sum_kick;  // Σ_i lerp(pot, z_i) of the last turn
   double last_n_in;      // particles inside the bin range, last turn
   int64_t turns_left;    // turns still to run (batches); a plain bunch never runs out
+  double last_mean_z;    // mean z after the last turn's drift (centres the pass's
+                         // shared-memory window of the kick table)
 };
 
 __host__ __device__ inline TurnScalars make_turn_scalars(double E0, const hj_params& p,

@@ -51,6 +51,7 @@ struct PassArgs {
   int64_t n;
   TurnState* ts;
   const double2* potd;     // [B+1] kick table of the previous turn (cell j: pot[j-1], step)
+  int32_t win;             // entries of the kick table's left values held in shared memory
   // bin grid
   int32_t B;
   int32_t use_wake;
@@ -141,6 +142,9 @@ cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin);
 cudaError_t prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
 size_t track_smem_bytes(int B, int use_wake, int cfg);
+// Kick-table entries the fused pass keeps in shared memory for B bins
+// (what the shared-memory budget leaves beside the histograms, at most B).
+int track_window_entries(int B, int cfg);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
 // Batched pass over a chunk table (*d_n_chunks entries live, grid max_chunks)
 // and the per-bunch merge of its partials.

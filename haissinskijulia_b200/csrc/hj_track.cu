@@ -44,6 +44,8 @@
 //   * switches that are off act through neutral values (a zero kick table
 //     and mean before the first turn, damping 1 without SR, r = 0 without
 //     QE), all exact, so the pass has no per-particle branches on them.
+#include <algorithm>
+
 #include "hj_internal.h"
 
 namespace hj {
@@ -154,18 +156,42 @@ __device__ __forceinline__ double2 ld_table(const double2* p) {
   return v;
 }
 
+// The pass's shared-memory window of the kick table: s_win[i] = pot_left[w0 + i]
+// (the left value, .x, of table cell w0 + i) for i < lim + 1, where the cells
+// j with w0 <= j < w0 + lim are "hot": their left value and their right
+// neighbour's left value are both in the window.  For cells 1..B-2 the step
+// of the global table is pot[j] - pot[j-1] = pot_left[j+1] - pot_left[j], and
+// for cell 0 it is pot[0] - pot[0] = 0, so a hot cell's (left value, step)
+// from the window is bit-identical to its global entry.  Cells B-1 and B
+// (whose step or value the bins step sets differently) are never hot.
+struct KickWindow {
+  const double* s_win;
+  int w0;
+  unsigned lim;
+};
+
 // Table entry and weight of the kick of z (issued early: the gather's latency
-// overlaps the RF and QE arithmetic of the pass).
+// overlaps the RF and QE arithmetic of the pass).  Hot cells read the
+// shared-memory window, the others the kick table in global memory.
 struct KickFetch {
-  double2 pd;
-  double w;
+  double p0, d, w;
 };
 __device__ __forceinline__ KickFetch kick_fetch(double z, const GridConst& g,
+                                                const KickWindow& kw,
                                                 const double2* __restrict__ potd) {
   int j;
   KickFetch f;
   kick_cell(z, g, j, f.w);
-  f.pd = ld_table(potd + j);
+  const unsigned r = (unsigned)(j - kw.w0);
+  if (r < kw.lim) {
+    const double lo = kw.s_win[r], hi = kw.s_win[r + 1];
+    f.p0 = lo;
+    f.d = __dsub_rn(hi, lo);
+  } else {
+    const double2 t = ld_table(potd + j);
+    f.p0 = t.x;
+    f.d = t.y;
+  }
   return f;
 }
 
@@ -237,16 +263,13 @@ __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
 // potential; 0 without the wake) and its RF kick increment rf_term(z), both
 // formed from the z this pass starts from: previous turn's kick and E0
 // re-centring (zero table / zero mean when nothing is pending), RF kick, QE,
-// SR, drift, moments and the deposits.  Without update_η the drift
-// coefficient is the constant-η one (zero when apply_phase_advance! would
-// skip the advance).
-template <bool WAKE, bool N32>
-__device__ __forceinline__ void pass_particle(double& z, double& e, double r, double kick,
-                                              double rf, const FusedConst& c,
-                                              const GridConst& g, double pmean, double& acc_z,
-                                              double& acc_z2, double& acc_d, uint32_t& n_in,
-                                              uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
-                                              unsigned long long* __restrict__ ngp_ovf) {
+// SR, drift.  Without update_η the drift coefficient is the constant-η one
+// (zero when apply_phase_advance! would skip the advance).  The moments and
+// deposits of the new z follow in deposit_group.
+template <bool WAKE>
+__device__ __forceinline__ void particle_turn(double& z, double& e, double r, double kick,
+                                              double rf, const FusedConst& c, double pmean,
+                                              double& acc_d) {
   if (WAKE) e = e - kick;
   e = e - pmean;
   const double e_start = e;
@@ -260,36 +283,62 @@ __device__ __forceinline__ void pass_particle(double& z, double& e, double r, do
   const double coeff = c.update_eta ? c.Kz * (c.alpha_c - ri) : c.coeff0z;
   z = fma(-coeff, e, z);
   acc_d += e - e_start;
-  if (WAKE) {
-    acc_z += z;
-    acc_z2 = fma(z, z, acc_z2);
-    bool in;
-    const int j = ngp_bin(z, g, in);
-    if (in) {
-      if (N32) {
-        atomicAdd(&s_ngp[j], 1u);   // one 32-bit counter per bin, no return value used
-      } else {
-        // 16-bit counters, two bins per word; the increment that takes a counter
-        // to 2^15 moves 2^15 counts to the global overflow array (at most 1024
-        // more increments can land before the move, so the counter never wraps)
-        const int sh = (j & 1) << 4;
-        const uint32_t old = atomicAdd(&s_ngp[j >> 1], 1u << sh);
-        if (((old >> sh) & 0xFFFFu) == 0x7FFFu) {
-          atomicSub(&s_ngp[j >> 1], 0x8000u << sh);
-          atomicAdd(ngp_ovf + j, 0x8000ull);
-        }
-      }
-      ++n_in;
-    }
-    // deposit in the kick-table cell the next pass will read for this z
-    int j2;
+}
+
+// Moments and deposits of K particles' new z: Σz, Σz², the NGP count and, in
+// the kick-table cell the next pass reads for this z, the cell count and
+// Σ w·2^24.  The shared atomics of all K particles are issued before any of
+// their returned values is used, so their latencies overlap.
+template <int K, bool N32>
+__device__ __forceinline__ void deposit_group(const double (&z)[K], const GridConst& g,
+                                              double& acc_z, double& acc_z2, uint32_t& n_in,
+                                              uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
+                                              unsigned long long* __restrict__ ngp_ovf) {
+  int nb[K], cj[K];
+  bool nin[K];
+  uint32_t cq[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    acc_z += z[k];
+    acc_z2 = fma(z[k], z[k], acc_z2);
+    nb[k] = ngp_bin(z[k], g, nin[k]);
+    n_in += nin[k] ? 1u : 0u;
     double w;
-    kick_cell(z, g, j2, w);
+    kick_cell(z[k], g, cj[k], w);
     // w·2^24 rounded to nearest (at most 2^24; a NaN z lands in cell B with
     // any q and is flagged by the moments)
-    const uint32_t q = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
-    const uint32_t old = atomicAdd(&s_lo[j2], q);
-    atomicAdd(&s_hi[j2], (1u << (kCicSumBits - 32)) + (old + q < old ? 1u : 0u));
+    cq[k] = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
+  }
+  uint32_t ong[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    ong[k] = 0u;
+    if (nin[k]) {
+      if (N32) {
+        atomicAdd(&s_ngp[nb[k]], 1u);   // one 32-bit counter per bin, no return value used
+      } else {
+        ong[k] = atomicAdd(&s_ngp[nb[k] >> 1], 1u << ((nb[k] & 1) << 4));
+      }
+    }
+  }
+  uint32_t olo[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) olo[k] = atomicAdd(&s_lo[cj[k]], cq[k]);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    atomicAdd(&s_hi[cj[k]], (1u << (kCicSumBits - 32)) + (olo[k] + cq[k] < olo[k] ? 1u : 0u));
+  if (!N32) {
+    // 16-bit counters, two bins per word: the increment that takes a counter
+    // to 2^15 moves 2^15 counts to the global overflow array (the counter has
+    // another 2^15 - 1 increments of room before the move lands)
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int sh = (nb[k] & 1) << 4;
+      if (nin[k] && ((ong[k] >> sh) & 0xFFFFu) == 0x7FFFu) {
+        atomicSub(&s_ngp[nb[k] >> 1], 0x8000u << sh);
+        atomicAdd(ngp_ovf + nb[k], 0x8000ull);
+      }
+    }
   }
 }
 
@@ -369,12 +418,15 @@ struct PassRange {
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = false>
 __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
                                           unsigned char* smem_raw) {
-  // dynamic shared memory: RF table [128] | NGP counters | cell words lo, hi [B+1];
-  // NGP counters: (B+1)/2 words of two 16-bit counters, or B 32-bit ones (N32)
+  // dynamic shared memory: RF table [128] | kick-table window [win] | NGP
+  // counters | cell words lo, hi [B+1]; NGP counters: (B+1)/2 words of two
+  // 16-bit counters, or B 32-bit ones (N32)
   const int nc = a.B + 1;                 // kick-table cells
   const int nw = N32 ? a.B : (a.B + 1) / 2;
+  const int win = WAKE ? a.win : 0;
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
-  uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_rf + kRfTableSize);
+  double* s_win = reinterpret_cast<double*>(s_rf + kRfTableSize);
+  uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_win + win);
   uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
   uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
   for (int i = threadIdx.x; i < kRfTableSize; i += THREADS) s_rf[i] = __ldg(a.rf_table + i);
@@ -412,11 +464,24 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     }
   }
 
+  // window of the kick table centred on the cell of the last turn's mean z:
+  // entries w0 .. w0 + wv - 1 (wv <= win, never beyond cell B - 1)
+  KickWindow kw{s_win, 0, 0u};
   if (WAKE) {
     for (int i = threadIdx.x; i < nc; i += THREADS) {
       if (i < nw) s_ngp[i] = 0u;
       s_lo[i] = 0u;
       s_hi[i] = 0u;
+    }
+    if (win > 0) {
+      int jm;
+      double wm;
+      kick_cell(ts->last_mean_z, g, jm, wm);
+      const int w0 = max(0, min(jm - win / 2, a.B - win));
+      const int wv = min(win, a.B - w0);
+      for (int i = threadIdx.x; i < wv; i += THREADS) s_win[i] = a.potd[w0 + i].x;
+      kw.w0 = w0;
+      kw.lim = (unsigned)max(wv - 1, 0);
     }
   }
   __syncthreads();
@@ -453,7 +518,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     KickFetch kf[PPT];
     if (WAKE) {
 #pragma unroll
-      for (int j = 0; j < PPT; ++j) kf[j] = kick_fetch(zz[j], g, potd);
+      for (int j = 0; j < PPT; ++j) kf[j] = kick_fetch(zz[j], g, kw, potd);
     }
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
@@ -470,9 +535,9 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rf);
 #pragma unroll
     for (int j = 0; j < PPT; ++j)
-      pass_particle<WAKE, N32>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].pd.y, kf[j].pd.x) : 0.0,
-                          rf[j], c, g, pmean, acc_z, acc_z2, acc_d, n_in, s_ngp, s_lo, s_hi,
-                          a.ngp_ovf);
+      particle_turn<WAKE>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].d, kf[j].p0) : 0.0,
+                          rf[j], c, pmean, acc_d);
+    if (WAKE) deposit_group<PPT, N32>(zz, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
     stp<PPT>(a.z + PPT * q, zz);
     stp<PPT>(a.dE + PPT * q, ee);
   }
@@ -483,11 +548,12 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     if (QE == QE_PHILOX) philox_normals2_rk(a.philox_rk, turn, (i >> 1) + a.pair_offset, r2);
     double r = r2[i & 1];
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
-    double z = a.z[i], e = a.dE[i];
-    const double kick = WAKE ? wake_kick(z, g, potd) : 0.0;
-    pass_particle<WAKE, N32>(z, e, r, kick, rf_term(z, c, s_rf), c, g, pmean, acc_z, acc_z2, acc_d,
-                        n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
-    a.z[i] = z;
+    double z1[1] = {a.z[i]};
+    double e = a.dE[i];
+    const double kick = WAKE ? wake_kick(z1[0], g, potd) : 0.0;
+    particle_turn<WAKE>(z1[0], e, r, kick, rf_term(z1[0], c, s_rf), c, pmean, acc_d);
+    if (WAKE) deposit_group<1, N32>(z1, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
+    a.z[i] = z1[0];
     a.dE[i] = e;
   }
 
@@ -958,7 +1024,28 @@ const void* batch_fn(int wake, int qe, int cfg) {
 }
 }  // namespace
 
+namespace {
+// Dynamic shared memory one block of the pass may take: the device's opt-in
+// limit (set when the kernels are prepared), or per block of the layout that
+// keeps two blocks on an SM (228 KB per SM, 1 KB reserved per block).
+int g_pass_smem_limit = 227 * 1024;
+
+size_t pass_smem_budget(int cfg) {
+  const size_t lim = (size_t)g_pass_smem_limit;
+  return (cfg & kPassLayoutMask) == 4 ? std::min(lim, (size_t)(113 * 1024)) : lim;
+}
+
+// RF table + NGP counts [B] (16-bit, two per word, or 32-bit with kPassN32)
+// + two 32-bit words per kick-table cell [B+1].
+size_t track_hist_bytes(int B, int cfg) {
+  const size_t rf = kRfTableSize * sizeof(double2);
+  const size_t nw = (cfg & kPassN32) ? (size_t)B : (size_t)((B + 1) / 2);
+  return rf + nw * sizeof(uint32_t) + (size_t)(B + 1) * sizeof(unsigned long long);
+}
+}  // namespace
+
 cudaError_t prepare_track_kernels(int max_smem) {
+  g_pass_smem_limit = max_smem;
   for (int w = 0; w < 2; ++w)
     for (int q = 0; q < 3; ++q)
       for (int n = 0; n < 2; ++n)
@@ -971,13 +1058,18 @@ cudaError_t prepare_track_kernels(int max_smem) {
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
 }
 
-// RF table + NGP counts [B] (16-bit, two per word, or 32-bit with kPassN32)
-// + two 32-bit words per kick-table cell [B+1].
+
+int track_window_entries(int B, int cfg) {
+  const size_t used = track_hist_bytes(B, cfg), budget = pass_smem_budget(cfg);
+  if (used >= budget) return 0;
+  const size_t w = (budget - used) / sizeof(double);
+  return (int)std::min<size_t>(w, (size_t)B);
+}
+
+// Histograms plus the kick-table window (wake on); the RF table alone otherwise.
 size_t track_smem_bytes(int B, int use_wake, int cfg) {
-  const size_t rf = kRfTableSize * sizeof(double2);
-  const size_t nw = (cfg & kPassN32) ? (size_t)B : (size_t)((B + 1) / 2);
-  return use_wake ? rf + nw * sizeof(uint32_t) + (size_t)(B + 1) * sizeof(unsigned long long)
-                  : rf;
+  if (!use_wake) return kRfTableSize * sizeof(double2);
+  return track_hist_bytes(B, cfg) + (size_t)track_window_entries(B, cfg) * sizeof(double);
 }
 
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {

@@ -600,6 +600,7 @@ __device__ __forceinline__ void bins_body(const BinsArgs& a) {
     ts->last_mean = mean;
     ts->last_sum_kick = sum_kick;
     ts->last_n_in = sh[3];
+    ts->last_mean_z = sh[0] / (double)a.n;
     ts->turn = ts->turn + 1;
     ts->turns_left = ts->turns_left - 1;
     ts->cur = make_turn_scalars(E0n, a.params, a.sigma_E0_initial);
