@@ -22,10 +22,14 @@
 //     serialise them (same stream, or events);
 //   * each call overwrites every scratch element it later reads (tables,
 //     spectra, FFT work space), so nothing has to start at zero and the
-//     previous call's leftovers are never read.
+//     previous call's leftovers are never read;
+//   * the array's device address is looked up once per device and kept for
+//     the life of the process, so the library does not survive a
+//     cudaDeviceReset of that device (nor does any of its other state);
+//   * the caller's current device is restored before the call returns.
 #include <mutex>
 
-#include "hj_internal.h"
+#include "hj_state.h"
 
 namespace hj {
 namespace {
@@ -98,6 +102,17 @@ int ilog2i(int v) {
   return l;
 }
 
+// Puts the caller's current device back when the entry point returns.
+struct DeviceRestore {
+  int device = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&device) != cudaSuccess) device = -1;
+  }
+  ~DeviceRestore() {
+    if (device >= 0) cudaSetDevice(device);
+  }
+};
+
 }  // namespace
 }  // namespace hj
 
@@ -107,17 +122,17 @@ extern "C" hj_status hj_wake_potential_noalloc(hj_ctx* ctx, const int64_t* d_cou
                                                const hj_grid* grid, const hj_wake* wake,
                                                double current, double* d_pot, void* stream) {
   if (!ctx) return HJ_ERR_ARG;
-  if (!d_counts || !d_pot || !grid || !wake || !grid->centers)
-    return ctx_set_error(ctx, HJ_ERR_ARG, "NULL counts, potential, grid, centers or wake");
-  if (grid->nbins <= 0) return ctx_set_error(ctx, HJ_ERR_NBINS, "nbins must be > 0");
+  DeviceRestore restore;
+  HJ_TRY(ctx_ok(ctx));                 // the context's device; clears the last error
+  HJ_TRY(check_grid(ctx, grid));
+  if (!d_counts || !d_pot || !wake)
+    return ctx_set_error(ctx, HJ_ERR_ARG, "NULL counts, potential or wake");
   if (grid->nbins > kNoAllocMaxBins)
     return ctx_set_error(ctx, HJ_ERR_TOO_LARGE,
                          "hj_wake_potential_noalloc holds at most 16384 bins in its static "
                          "scratch; use hj_wake_potential for larger grids");
   if (!(wake->ctau > 0)) return ctx_set_error(ctx, HJ_ERR_WAKE_PARAM, "Wake parameter cτ must be positive.");
   const int device = ctx_device(ctx);
-  if (cudaSetDevice(device) != cudaSuccess)
-    return ctx_set_error(ctx, HJ_ERR_CUDA, "cudaSetDevice failed");
   double* base = nullptr;
   cudaError_t se = scratch_address(device, &base);
   if (se != cudaSuccess)

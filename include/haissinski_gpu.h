@@ -392,6 +392,10 @@ hj_status hj_batch_take_many(hj_batch* bt, int32_t count, const int64_t* ids,
 /* out[0] live bunches, out[1] free pool particles (largest free range),
  * out[2] free slots, out[3] turns enqueued so far. */
 hj_status hj_batch_stats(hj_batch* bt, int64_t* out4);
+/* The bin counts of bunch `id`'s last completed turn (the histogram of z
+ * after that turn's drift, calculate_local_histogram! src/utils.jl:351-401)
+ * into counts_host[nbins], after the enqueued turns complete. */
+hj_status hj_batch_histogram(hj_batch* bt, int64_t id, int64_t* counts_host);
 
 /* ---------------------------------------------------------------- single steps (host buffers) */
 
@@ -442,9 +446,12 @@ hj_status hj_wake_potential(hj_ctx* ctx, const int64_t* counts, const hj_grid* g
  *   d_pot     device array of nbins doubles, written on `stream`.
  * The work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
  * stream) and is complete when that stream is.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls share the array: calls
- * whose work overlaps on the GPU race, so serialise them. */
+ * looks up the array's device address (cudaGetSymbolAddress) and keeps it
+ * for the life of the process; make that first call before any stream
+ * capture, and do not reset the device (cudaDeviceReset) while the library
+ * is in use.  All calls share the array: calls whose work overlaps on the GPU
+ * race, so serialise them.  The caller's current device is restored on
+ * return. */
 hj_status hj_wake_potential_noalloc(hj_ctx* ctx, const int64_t* d_counts, const hj_grid* grid,
                                     const hj_wake* wake, double current, double* d_pot,
                                     void* stream);
