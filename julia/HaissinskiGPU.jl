@@ -16,7 +16,7 @@ using StructArrays
 using StochasticHaissinski
 using StochasticHaissinski: Particle, SimulationParameters, SimulationBuffers
 
-export GPUBackend
+export GPUBackend, scan_voltages
 
 const libhj = get(ENV, "HAISSINSKI_GPU_LIB",
                   joinpath(@__DIR__, "..", "haissinskijulia_b200", "libhaissinski_gpu.so"))
@@ -151,6 +151,69 @@ function StochasticHaissinski.longitudinal_evolve!(
     end
     r = res[]
     return r.sigma_E, r.sigma_z, r.E0
+end
+
+"""
+    scan_voltages(backend, params, voltages, n, σ_z, σ_E, nbins; wake, block_turns = 64)
+
+The voltage scan of scan_parameter (src/parameter_sensitivity/scan.jl:182-184)
+with every point a bunch of one batch on the GPU: n independent Gaussian
+particles per point generated on the device (seed = the point's index),
+params.n_turns turns each, all points advancing together.  Returns, per
+voltage, (σ_E, σ_z, E0, cor(z, ΔE)) of the final particles -- the inputs of
+compute_fom (src/parameter_sensitivity/figures_of_merit.jl:16-48).
+"""
+function scan_voltages(backend::GPUBackend, params::SimulationParameters,
+                       voltages::AbstractVector{<:Real}, n::Integer, σ_z::Real, σ_E::Real,
+                       nbins::Integer; wake::Union{HjWake,Nothing} = nothing,
+                       block_turns::Integer = 64)
+    k = length(voltages)
+    bt = Ref{Ptr{Cvoid}}(C_NULL)
+    check(backend, ccall((:hj_batch_create, libhj), Int32,
+                         (Ptr{Cvoid}, Int64, Int32, Int32, Int64, Int32, Ref{Ptr{Cvoid}}),
+                         backend.ctx, Int64(k) * (n + 4), k, nbins, 65536, -1, bt))
+    ids = zeros(Int64, k)
+    out = Vector{NTuple{4,Float64}}(undef, k)
+    try
+        for (i, V) in enumerate(voltages)
+            p = HjParams(params; voltage = V)
+            w = wake === nothing ? reference_wake(p) : wake
+            id = Ref{Int64}(0)
+            check(backend, ccall((:hj_batch_add_gaussian, libhj), Int32,
+                                 (Ptr{Cvoid}, Int64, Float64, Float64, UInt64, Ref{HjParams},
+                                  Ref{HjWake}, Int64, UInt64, Int64, Ref{Int64}),
+                                 bt[], n, σ_z, σ_E, UInt64(i), p, w, nbins, UInt64(i),
+                                 params.n_turns, id))
+            ids[i] = id[]
+        end
+        done = Int64[]
+        finished = zeros(Int64, k)
+        while length(done) < k
+            check(backend, ccall((:hj_batch_advance, libhj), Int32, (Ptr{Cvoid}, Int64),
+                                 bt[], block_turns))
+            nd = Ref{Int32}(0)
+            check(backend, ccall((:hj_batch_poll, libhj), Int32,
+                                 (Ptr{Cvoid}, Ptr{Int64}, Int32, Ref{Int32}),
+                                 bt[], finished, k, nd))
+            append!(done, finished[1:nd[]])
+            nd[] == 0 && continue
+            # retire the finished points at once; they leave the batch here
+            res = Vector{HjResult}(undef, nd[])
+            corr = zeros(Float64, nd[])
+            check(backend, ccall((:hj_batch_take_many, libhj), Int32,
+                                 (Ptr{Cvoid}, Int32, Ptr{Int64}, Ptr{Ptr{Float64}},
+                                  Ptr{Ptr{Float64}}, Ptr{HjResult}, Ptr{Float64}),
+                                 bt[], nd[], finished, C_NULL, C_NULL, res, corr))
+            for (j, id) in enumerate(finished[1:nd[]])
+                i = findfirst(==(id), ids)
+                ids[i] = -1                           # taken
+                out[i] = (res[j].sigma_E, res[j].sigma_z, res[j].E0, corr[j])
+            end
+        end
+    finally
+        ccall((:hj_batch_destroy, libhj), Cvoid, (Ptr{Cvoid},), bt[])
+    end
+    return out
 end
 
 end # module
