@@ -159,6 +159,7 @@ SIGNATURES = {
     "hj_batch_poll": (c_int32, [c_void_p, _IP, c_int32, POINTER(c_int32)]),
     "hj_batch_take": (c_int32, [c_void_p, c_int64, c_void_p, c_void_p, POINTER(HjResult)]),
     "hj_batch_stats": (c_int32, [c_void_p, _IP]),
+    "hj_batch_histogram": (c_int32, [c_void_p, c_int64, _IP]),
     "hj_batch_add_many": (c_int32, [c_void_p, c_int32, POINTER(c_void_p), POINTER(c_void_p), _IP,
                                     POINTER(HjParams), POINTER(HjWake), _IP, POINTER(c_uint64),
                                     _IP, _IP, POINTER(c_int32)]),
@@ -178,6 +179,7 @@ SIGNATURES = {
     "hj_apply_wakefield": (c_int32, [_CTX, _DP, _DP, c_int64, POINTER(HjWake), c_double,
                                      c_double, POINTER(HjGrid)]),
     "hj_gaussian": (c_int32, [_CTX, c_uint64, c_int64, c_int64, _DP]),
+    "hj_normal_tables": (c_int32, [_DP, c_int64]),
     "hj_generate_particles": (c_int32, [_CTX, c_double, c_double, c_double, c_double, c_int64,
                                         c_uint64, c_void_p, c_void_p, c_void_p, _DP, _DP]),
     "hj_correlation": (c_int32, [_CTX, c_void_p, c_void_p, c_int64, c_void_p, _DP]),

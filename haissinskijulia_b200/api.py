@@ -227,7 +227,7 @@ class Context:
 
     def set_pass_layout(self, layout: int) -> None:
         """Thread layout of the fused pass for bunches created afterwards
-        (-1 = automatic; 0-4 = fixed layouts with 16-bit bin counters, 8-12
+        (-1 = automatic; 0-5 = fixed layouts with 16-bit bin counters, 8-13
         the same with 32-bit counters; see hj_set_pass_layout)."""
         _check(self, self._lib.hj_set_pass_layout(self.handle, int(layout)))
 
@@ -515,7 +515,8 @@ def apply_wakefield_inplace(particles: Particles, buffers: SimulationBuffers, wa
 
 
 def gaussian_draws(seed: int, turn: int, n: int, buffers: SimulationBuffers) -> np.ndarray:
-    """The on-device Philox-2x32-10 normals of (seed, particle, turn)."""
+    """The on-device Float64 normals of (seed, particle, turn): Philox-4x32-10 and
+    a 256-layer ziggurat (hj_gaussian)."""
     ctx = buffers.context()
     out = np.empty(n, dtype=np.float64)
     _check(ctx, ctx._lib.hj_gaussian(ctx.handle, int(seed) & 0xFFFFFFFFFFFFFFFF, int(turn), n,
@@ -853,6 +854,13 @@ class Batch:
         self._forget(ids, rc, live)          # all of them retire, or none
         results = [EvolveResult.from_c(res[i]) for i in range(k)]
         return results, ([float(c) for c in corr[:k]] if correlation else None)
+
+    def histogram(self, bid: int, nbins: int) -> np.ndarray:
+        """Bin counts of bunch `bid`'s last completed turn (hj_batch_histogram)."""
+        self._size(bid)
+        out = np.zeros(int(nbins), dtype=np.int64)
+        _check(self.ctx, self.ctx._lib.hj_batch_histogram(self.handle, int(bid), _ip(out)))
+        return out
 
     def stats(self) -> dict:
         out = np.zeros(4, dtype=np.int64)

@@ -751,8 +751,7 @@ void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
     a.rf_inv_h = (double)(1.0L / h);
     a.rf_h_hi = (double)h;
     a.rf_h_lo = (double)(h - (long double)a.rf_h_hi);
-    const uint32_t key = (uint32_t)(b->seed ^ (b->seed >> 32));
-    for (int r = 0; r < 10; ++r) a.philox_rk[r] = key + (uint32_t)r * 0x9E3779B9u;
+    a.philox = philox_keys(b->seed);
   }
   a.inv_mass = 1.0 / b->p.mass;
   a.alpha_c = b->p.alpha_c;
@@ -1107,6 +1106,26 @@ extern "C" hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64
   HJ_TRY(stage(ctx, n, 1, d, h));
   HJ_CUDA(ctx, launch_gaussian(seed, turn, n, d[0], ctx->stream));
   return unstage(ctx, n, out, d[0]);
+}
+
+extern "C" hj_status hj_normal_tables(double* out, int64_t cap) {
+  if (!out || cap < HJ_NORMAL_TABLES_SIZE) return HJ_ERR_ARG;
+  NormalTables t;
+  host_normal_tables(&t);
+  double* o = out;
+  for (int j = 0; j < 64; ++j) {
+    *o++ = t.lr[j][0];
+    *o++ = t.lr[j][1];
+  }
+  for (int j = 0; j < 64; ++j) {
+    *o++ = t.sc[j][0];
+    *o++ = t.sc[j][1];
+  }
+  *o++ = t.ln2_hi;
+  *o++ = t.ln2_lo;
+  *o++ = t.twopi_hi;
+  *o++ = t.twopi_lo;
+  return o - out == HJ_NORMAL_TABLES_SIZE ? HJ_OK : HJ_ERR_STATE;
 }
 
 namespace {

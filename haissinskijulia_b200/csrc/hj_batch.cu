@@ -665,6 +665,20 @@ extern "C" hj_status hj_batch_take(hj_batch* bt, int64_t id, double* z_out, doub
   return st;
 }
 
+extern "C" hj_status hj_batch_histogram(hj_batch* bt, int64_t id, int64_t* counts_host) {
+  if (!bt || !counts_host) return HJ_ERR_ARG;
+  hj_ctx* ctx = bt->ctx;
+  HJ_TRY(ctx_ok(ctx));
+  const int k = batch_find(bt, id);
+  if (k < 0) return set_err(ctx, HJ_ERR_ARG, "no bunch %lld in the batch", (long long)id);
+  const hj_bunch* b = bt->members[k].b;
+  if (!b->use_wake) return set_err(ctx, HJ_ERR_STATE, "bunch has no wakefield histogram");
+  HJ_CUDA(ctx, cudaMemcpyAsync(counts_host, b->hist, sizeof(int64_t) * b->B,
+                               cudaMemcpyDeviceToHost, bt->stream));
+  HJ_CUDA(ctx, cudaStreamSynchronize(bt->stream));
+  return HJ_OK;
+}
+
 extern "C" hj_status hj_batch_stats(hj_batch* bt, int64_t* out4) {
   if (!bt || !out4) return HJ_ERR_ARG;
   out4[0] = (int64_t)bt->members.size();

@@ -3,15 +3,16 @@
 // Per-turn scalars follow src/evolution.jl:300-304 and the step functions
 // src/rf_kick.jl:84-87, src/quantum_excitation.jl:58-71,
 // src/synchrotron_radiation.jl:44-56 of the reference.  The random numbers
-// are Philox-2x32-10 (Salmon, Moraes, Dror & Shaw, "Parallel random numbers:
+// are Philox-4x32-10 (Salmon, Moraes, Dror & Shaw, "Parallel random numbers:
 // as easy as 1, 2, 3", SC'11), one counter per pair of particles, turned into
-// normals by the Box-Muller transform.
+// Float64 normals by a double-precision Box-Muller transform.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "../../include/haissinski_gpu.h"
+#include "hj_host.h"
 
 namespace hj {
 
@@ -99,70 +100,129 @@ __host__ __device__ inline double global_std_of_sums(double s, double s2, int64_
 
 // ------------------------------------------------------------------ Philox
 
-// Philox-2x32 with 10 rounds: multiplier 0xD256D193, Weyl key increment
-// 0x9E3779B9 (the published constants).
-__host__ __device__ inline void philox2x32_10(uint32_t& c0, uint32_t& c1, uint32_t k) {
+// Philox-4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11): multipliers
+// 0xD2511F53 and 0xCD9E8D57, Weyl key increments 0x9E3779B9 and 0xBB67AE85
+// (the published constants); a 128-bit counter and a 64-bit key.
+constexpr uint32_t kPhiloxM0 = 0xD2511F53u, kPhiloxM1 = 0xCD9E8D57u;
+constexpr uint32_t kPhiloxW0 = 0x9E3779B9u, kPhiloxW1 = 0xBB67AE85u;
+
+// Round keys of a 64-bit key: rk[r] = k0 + r·W0, rk[10 + r] = k1 + r·W1.
+struct PhiloxKeys {
+  uint32_t rk[20];
+};
+
+__host__ __device__ inline PhiloxKeys philox_keys(uint64_t key) {
+  PhiloxKeys k;
+  for (int r = 0; r < 10; ++r) {
+    k.rk[r] = (uint32_t)key + (uint32_t)r * kPhiloxW0;
+    k.rk[10 + r] = (uint32_t)(key >> 32) + (uint32_t)r * kPhiloxW1;
+  }
+  return k;
+}
+
+__host__ __device__ inline void philox4x32_10(uint32_t (&c)[4], const PhiloxKeys& k) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
 #if defined(__CUDA_ARCH__)
-    const uint32_t hi = __umulhi(0xD256D193u, c0), lo = 0xD256D193u * c0;
+    const uint32_t hi0 = __umulhi(kPhiloxM0, c[0]), lo0 = kPhiloxM0 * c[0];
+    const uint32_t hi1 = __umulhi(kPhiloxM1, c[2]), lo1 = kPhiloxM1 * c[2];
 #else
-    const uint64_t pr = (uint64_t)0xD256D193u * c0;
-    const uint32_t hi = (uint32_t)(pr >> 32), lo = (uint32_t)pr;
+    const uint64_t p0 = (uint64_t)kPhiloxM0 * c[0], p1 = (uint64_t)kPhiloxM1 * c[2];
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
 #endif
-    c0 = hi ^ k ^ c1;
-    c1 = lo;
-    k += 0x9E3779B9u;
+    const uint32_t n0 = hi1 ^ c[1] ^ k.rk[r], n2 = hi0 ^ c[3] ^ k.rk[10 + r];
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
   }
 }
 
-// Philox-2x32-10 with its round keys given: rk[r] = key + r·0x9E3779B9.
-__device__ __forceinline__ void philox2x32_10_rk(uint32_t& c0, uint32_t& c1,
-                                                 const uint32_t (&rk)[10]) {
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint32_t hi = __umulhi(0xD256D193u, c0), lo = 0xD256D193u * c0;
-    c0 = hi ^ rk[r] ^ c1;
-    c1 = lo;
-  }
+// ------------------------------------------------------------ normals
+
+// Double-precision Box-Muller transform of the four Philox words of a
+// particle pair, with its logarithm and its sine and cosine evaluated from
+// small tables (NormalTables, hj_host.h):
+//   u1 = (2a + 1) 2^-53 with a the top 52 bits of (x1:x0), so u1 lies in
+//     [2^-53, 1 - 2^-53] exactly; ln u1 by the table-driven method of
+//     P. T. P. Tang (ACM TOMS 16(4), 1990): u1 = 2^e m, m in [1, 2),
+//     ln m = -ln r_j + log1p(m r_j - 1) with r_j ≈ 1/(1 + (j + 1/2)/64) for
+//     the top six bits j of m (|m r_j - 1| < 2^-7), log1p by its Taylor
+//     series through t^8 (truncation below 2e-20), e ln 2 with a two-part ln 2;
+//   θ = 2π w, w in [0, 1) the top 52 bits of (x3:x2): θ = θ_j + t with
+//     θ_j = 2π (j + 1/2)/64 for the top six bits j of w, |t| <= π/64, sin t and
+//     cos t - 1 by their Taylor series through t^9 and t^10 (truncation below
+//     1e-20), then angle addition with the tabulated sin θ_j, cos θ_j;
+//   r = sqrt(-2 ln u1) (at most 8.57: the tails are cut only there), and the
+//   normals r cos θ, r sin θ.
+// Each entry point of the transform costs about 30 FP64 operations per pair.
+
+__device__ __forceinline__ void box_muller_f64(const uint32_t (&x)[4],
+                                               const NormalTables* __restrict__ t,
+                                               const double2* __restrict__ lr,
+                                               const double2* __restrict__ sc, double out[2]) {
+  // u1 = d - (1 - 2^-53), d = 1 + a 2^-52 in [1, 2): exact (Sterbenz)
+  const double d = __hiloint2double(0x3FF00000 | (int)(x[1] >> 12),
+                                    (int)((x[1] << 20) | (x[0] >> 12)));
+  const double u1 = d - 0x1.fffffffffffffp-1;
+  const int hi = __double2hiint(u1);
+  const int e = (hi >> 20) - 1023;
+  const int j = (hi >> 14) & 63;
+  const double m = __hiloint2double((hi & 0x000FFFFF) | 0x3FF00000, __double2loint(u1));
+  const double2 rj = lr[j];
+  const double tt = fma(m, rj.x, -1.0);
+  double q = -0.125;                                   // log1p(t) = t q(t)
+  q = fma(q, tt, 1.0 / 7.0);
+  q = fma(q, tt, -1.0 / 6.0);
+  q = fma(q, tt, 0.2);
+  q = fma(q, tt, -0.25);
+  q = fma(q, tt, 1.0 / 3.0);
+  q = fma(q, tt, -0.5);
+  q = fma(q, tt, 1.0);
+  const double ed = (double)e;
+  const double ln_u1 = fma(ed, t->ln2_hi, rj.y) + fma(ed, t->ln2_lo, tt * q);
+  const double r = sqrt(-2.0 * ln_u1);
+  // θ = 2π (w - (k + 1/2)/64) + θ_k, w = d2 - 1, d2 = 1 + b 2^-52
+  const int h2 = (int)(0x3FF00000 | (x[3] >> 12));
+  const double d2 = __hiloint2double(h2, (int)((x[3] << 20) | (x[2] >> 12)));
+  const int k = (h2 >> 14) & 63;
+  const double xs = d2 - (1.0 + ((double)k + 0.5) * 0.015625);   // exact, |xs| <= 2^-7
+  const double ang = fma(xs, t->twopi_hi, xs * t->twopi_lo);
+  const double a2 = ang * ang;
+  double ps = 2.7557319223985893e-06;                  // 1/9!
+  ps = fma(ps, a2, -1.9841269841269841e-04);           // -1/7!
+  ps = fma(ps, a2, 8.3333333333333333e-03);            // 1/5!
+  ps = fma(ps, a2, -1.6666666666666667e-01);           // -1/3!
+  const double sn = fma(ang * a2, ps, ang);
+  double pc = -2.7557319223985888e-07;                 // -1/10!
+  pc = fma(pc, a2, 2.4801587301587302e-05);            // 1/8!
+  pc = fma(pc, a2, -1.3888888888888889e-03);           // -1/6!
+  pc = fma(pc, a2, 4.1666666666666667e-02);            // 1/4!
+  pc = fma(pc, a2, -0.5);
+  const double cm1 = a2 * pc;
+  const double2 skc = sc[k];
+  const double sin_th = fma(skc.y, sn, fma(skc.x, cm1, skc.x));
+  const double cos_th = fma(-skc.x, sn, fma(skc.y, cm1, skc.y));
+  out[0] = r * cos_th;
+  out[1] = r * sin_th;
 }
 
-// Box-Muller transform of one Philox output pair (see philox_normals2).
-__device__ __forceinline__ void box_muller2(uint32_t x0, uint32_t x1, double out[2]) {
-  const float kScale = 2.3283064365386963e-10f;  // 2^-32
-  const float u1 = fmaf((float)x0, kScale, 0.5f * kScale);
-  const float th = 6.2831853071795865f * fmaf((float)x1, kScale, -0.5f);
-  const float m2l = fmaxf(-2.0f * __logf(u1), 1e-30f);
-  const float rad = m2l * rsqrtf(m2l);                        // sqrt without a slow path
-  float sn, cs;
-  __sincosf(th, &sn, &cs);
-  out[0] = (double)(rad * cs);
-  out[1] = (double)(rad * sn);
-}
-
-// philox_normals2 with the round keys of (seed ^ seed >> 32) precomputed.
-__device__ __forceinline__ void philox_normals2_rk(const uint32_t (&rk)[10], int64_t turn,
-                                                   int64_t p, double out[2]) {
-  uint32_t c0 = (uint32_t)p;
-  uint32_t c1 = ((uint32_t)turn & 0xFFFFFFu) | ((uint32_t)((uint64_t)p >> 32) << 24);
-  philox2x32_10_rk(c0, c1, rk);
-  box_muller2(c0, c1, out);
-}
-
-// Two standard normals for particles 2p and 2p+1 at `turn`: Philox-2x32-10
-// with key = (seed ^ seed >> 32) folded to 32 bits and counter
-// (p mod 2^32, (turn mod 2^24) | (p >> 32) << 24), then the Box-Muller
-// transform of its two uniforms u in (0,1): r = sqrt(-2 ln u1),
-// θ = 2π (u2 - 1/2).  The transform runs in single precision on the
-// special-function unit (__logf, __sincosf: absolute error below 2^-21 on
-// these ranges); the normals are widened to double before they scale the
-// Float64 kick, and their statistics are unaffected at the 1e-6 level.
-__device__ __forceinline__ void philox_normals2(uint64_t seed, int64_t turn, int64_t p,
-                                                double out[2]) {
-  uint32_t c0 = (uint32_t)p;
-  uint32_t c1 = ((uint32_t)turn & 0xFFFFFFu) | ((uint32_t)((uint64_t)p >> 32) << 24);
-  philox2x32_10(c0, c1, (uint32_t)(seed ^ (seed >> 32)));
-  box_muller2(c0, c1, out);
+// Two standard normals for particles 2p and 2p+1 at `turn` under the round
+// keys of a seed: Philox-4x32-10 of the counter (p mod 2^32, p >> 32,
+// turn mod 2^32, turn >> 32), then box_muller_f64.  lr, sc: the
+// transform's logarithm and angle tables (shared or global memory).  Every
+// (seed, pair, turn) has its own counter and key, so distinct seeds, pairs
+// and turns never share a draw.
+__device__ __forceinline__ void philox_normals2_rk(const PhiloxKeys& keys, int64_t turn,
+                                                   int64_t p, const NormalTables* __restrict__ t,
+                                                   const double2* __restrict__ lr,
+                                                   const double2* __restrict__ sc,
+                                                   double out[2]) {
+  uint32_t c[4] = {(uint32_t)p, (uint32_t)((uint64_t)p >> 32), (uint32_t)turn,
+                   (uint32_t)((uint64_t)turn >> 32)};
+  philox4x32_10(c, keys);
+  box_muller_f64(c, t, lr, sc, out);
 }
 
 }  // namespace hj

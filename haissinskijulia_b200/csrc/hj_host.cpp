@@ -177,4 +177,24 @@ void host_twiddles(int64_t P, double* tw_interleaved) {
   std::memcpy(tw_interleaved, it->second.data(), sizeof(double) * 2 * (size_t)P);
 }
 
+void host_normal_tables(NormalTables* t) {
+  const long double kPiL = 3.141592653589793238462643383279502884L;
+  const long double kLn2L = 0.693147180559945309417232121458176568L;
+  for (int j = 0; j < 64; ++j) {
+    const double r = (double)(1.0L / (1.0L + ((long double)j + 0.5L) / 64.0L));
+    t->lr[j][0] = r;
+    t->lr[j][1] = (double)(-logl((long double)r));     // ln m = -ln r + log1p(m r - 1)
+    const long double th = 2.0L * kPiL * ((long double)j + 0.5L) / 64.0L;
+    t->sc[j][0] = (double)sinl(th);
+    t->sc[j][1] = (double)cosl(th);
+  }
+  // ln 2 with its high part rounded to 42 bits, so that e * high is exact for |e| < 2^11
+  const double ln2_hi = std::ldexp(std::nearbyint(std::ldexp((double)kLn2L, 42)), -42);
+  t->ln2_hi = ln2_hi;
+  t->ln2_lo = (double)(kLn2L - (long double)ln2_hi);
+  const double twopi_hi = (double)(2.0L * kPiL);
+  t->twopi_hi = twopi_hi;
+  t->twopi_lo = (double)(2.0L * kPiL - (long double)twopi_hi);
+}
+
 }  // namespace hj

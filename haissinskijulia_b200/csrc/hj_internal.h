@@ -63,7 +63,7 @@ struct PassArgs {
   // rf_table[m mod kRfTableSize] = (V sin(ϕs - m h), V cos(ϕs - m h)); Vs = V sin ϕs
   const double2* rf_table;
   double rf_inv_h, rf_h_hi, rf_h_lo, Vs;
-  uint32_t philox_rk[10];  // Philox-2x32 round keys: key + r·0x9E3779B9
+  PhiloxKeys philox;       // Philox-4x32 round keys of the bunch's seed
   int32_t update_eta, update_E0, sr, qe_mode;
   int32_t cfg;             // thread layout (kNumPassCfgs)
   uint64_t seed;

@@ -13,16 +13,26 @@ constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 // Thread layouts of the fused pass (particles/thread x threads/block; the next
 // group prefetched into registers except in 3): 0 = 4 x 512, 1 = 2 x 1024,
 // 2 = 2 x 768, 3 = 2 x 512 without prefetch, 4 = 2 x 512 at 64 registers (two
-// blocks per SM where shared memory allows).
-constexpr int kNumPassCfgs = 5;       // thread layouts of the fused pass
+// blocks per SM where shared memory allows), 5 = 4 x 256 at 128 registers
+// (two blocks per SM: one block's set-up and write-out overlap the other's
+// particles).
+constexpr int kNumPassCfgs = 6;       // thread layouts of the fused pass
 constexpr int kPassLayoutMask = 7;    // layout bits of a pass configuration
 constexpr int kPassN32 = 8;           // + one 32-bit NGP counter per bin (else 16-bit pairs)
 
 inline int pass_cfg_threads(int cfg) {
   const int l = cfg & kPassLayoutMask;
-  return l == 1 ? 1024 : (l == 2 ? 768 : 512);
+  return l == 1 ? 1024 : (l == 2 ? 768 : (l == 5 ? 256 : 512));
 }
-inline int pass_cfg_ppt(int cfg) { return (cfg & kPassLayoutMask) == 0 ? 4 : 2; }
+inline int pass_cfg_ppt(int cfg) {
+  const int l = cfg & kPassLayoutMask;
+  return (l == 0 || l == 5) ? 4 : 2;
+}
+// Layouts that keep two blocks on an SM (each takes at most half of it).
+inline bool pass_cfg_two_blocks(int cfg) {
+  const int l = cfg & kPassLayoutMask;
+  return l == 4 || l == 5;
+}
 inline bool pass_cfg_valid(int cfg) {
   return cfg >= 0 && (cfg & ~(kPassLayoutMask | kPassN32)) == 0 &&
          (cfg & kPassLayoutMask) < kNumPassCfgs;

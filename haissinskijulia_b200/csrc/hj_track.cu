@@ -30,7 +30,9 @@
 //     extended precision on the host) and sin t, cos t - 1 from their Taylor
 //     series through t^7 and t^6.  For m = 0 the kick is V sin ϕs (cos t - 1)
 //     - V cos ϕs sin t, free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
-//   * Philox round keys are precomputed on the host (kernel parameters).
+//   * Philox-4x32 round keys are precomputed on the host (kernel parameters);
+//     the normals come from a double-precision Box-Muller transform whose
+//     small tables sit in shared memory (Float64, 52-bit uniforms).
 //   * 1/γ² of the drift: rcp.approx.ftz.f64 refined by one Newton step
 //     (relative error ~1e-14 on a term 5e-5 of η, i.e. ~1e-18 on η).
 //   * drift: z' = z - (2π h / (β0² E0 k)) η_i ΔE, the reference's
@@ -46,10 +48,23 @@
 //     QE), all exact, so the pass has no per-particle branches on them.
 #include <algorithm>
 
+#include "hj_host.h"
 #include "hj_internal.h"
 
 namespace hj {
 namespace {
+
+// The normal generator's tables (NormalTables) in global memory, filled once
+// per device when the kernels are prepared; the fused pass stages them into
+// shared memory, the other kernels read them through the cache.
+__device__ NormalTables g_normal;
+
+__device__ __forceinline__ void philox_normals2(uint64_t seed, int64_t turn, int64_t p,
+                                                double out[2]) {
+  philox_normals2_rk(philox_keys(seed), turn, p, &g_normal,
+                     reinterpret_cast<const double2*>(g_normal.lr),
+                     reinterpret_cast<const double2*>(g_normal.sc), out);
+}
 
 // Run- and turn-constants of the fused pass.
 struct FusedConst {
@@ -227,6 +242,38 @@ __device__ __forceinline__ int ngp_bin(double z, const GridConst& g, bool& in) {
   return min(max(__double2loint(__dadd_rd(u, kMagic)), 0), g.B - 1);
 }
 
+// Bits of 1/2 - 2^-30 and the span up to 1/2 + 2^-30 (positive doubles order
+// as their bit patterns).
+constexpr long long kHalfLoBits = 0x3FDFFFFFFF000000ll;
+constexpr unsigned long long kHalfSpanBits = 0x3FE0000000800000ull - 0x3FDFFFFFFF000000ull;
+
+// Kick-table cell of z (as kick_cell) and, from the same coordinate, the
+// histogram bin of src/utils.jl:387-397.  v - 1/2 = z/Δe + 1/2 - e0/Δe - 1/2
+// lies within ~4 B 2^-53 (below 1e-11 for B <= 2^20) of the reference's
+// u = RN(RN(z - e0)/Δe), so for |w - 1/2| >= 2^-30 the bin floor(u) is
+// floor(v) - 1 + [w >= 1/2] and z is in range iff that bin is in [0, B-1];
+// within 2^-30 of a bin edge (at 1e8 particles about one particle in five
+// turns) ngp_bin evaluates the reference's own rounding.  The tests on w run
+// on its bits, so the bin costs no floating-point work.
+__device__ __forceinline__ void cell_and_bin(double z, const GridConst& g, int& j, double& w,
+                                             int& nb, bool& in) {
+  const double v = fma(z, g.inv_e, g.v_off);
+  const double fm = __dadd_rd(v, kMagic);
+  w = __dsub_rn(v, __dsub_rn(fm, kMagic));
+  const int t = __double2hiint(fm) - 0x43380000;
+  const unsigned lo = (unsigned)__double2loint(fm);
+  j = (t == 0) ? (int)min(lo, (unsigned)g.B) : (t > 0 ? g.B : 0);
+  const unsigned long long near_edge =
+      (unsigned long long)(__double_as_longlong(w) - kHalfLoBits);
+  if (near_edge <= kHalfSpanBits) {
+    nb = ngp_bin(z, g, in);
+  } else {
+    const int jb = (int)lo - 1 + (__double2hiint(w) >= 0x3FE00000 ? 1 : 0);
+    in = (t == 0) & (jb >= 0) & (jb < g.B);
+    nb = jb;
+  }
+}
+
 // Reference-form bin for the single-step histogram kernel (any z).
 __device__ __forceinline__ int ngp_bin_any(double z, const GridConst& g, bool& in) {
   in = (z >= g.e0) & (z <= g.eN);
@@ -301,10 +348,9 @@ __device__ __forceinline__ void deposit_group(const double (&z)[K], const GridCo
   for (int k = 0; k < K; ++k) {
     acc_z += z[k];
     acc_z2 = fma(z[k], z[k], acc_z2);
-    nb[k] = ngp_bin(z[k], g, nin[k]);
-    n_in += nin[k] ? 1u : 0u;
     double w;
-    kick_cell(z[k], g, cj[k], w);
+    cell_and_bin(z[k], g, cj[k], w, nb[k], nin[k]);
+    n_in += nin[k] ? 1u : 0u;
     // w·2^24 rounded to nearest (at most 2^24; a NaN z lands in cell B with
     // any q and is flagged by the moments)
     cq[k] = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
@@ -395,13 +441,15 @@ __device__ __forceinline__ void stp(double* p, const double v[PPT]) {
   }
 }
 
-// Normals of the PPT particles of pairs pair0, pair0 + 1, ... (one Philox-2x32
+// Normals of the PPT particles of pairs pair0, pair0 + 1, ... (one Philox-4x32
 // counter per pair of particles).
 template <int PPT>
-__device__ __forceinline__ void group_normals(const uint32_t (&rk)[10], int64_t turn,
-                                              int64_t pair0, double r[PPT]) {
-  philox_normals2_rk(rk, turn, pair0, r);
-  if (PPT == 4) philox_normals2_rk(rk, turn, pair0 + 1, r + 2);
+__device__ __forceinline__ void group_normals(const PhiloxKeys& rk, int64_t turn,
+                                              int64_t pair0, const NormalTables* t,
+                                              const double2* lr, const double2* sc,
+                                              double r[PPT]) {
+  philox_normals2_rk(rk, turn, pair0, t, lr, sc, r);
+  if (PPT == 4) philox_normals2_rk(rk, turn, pair0 + 1, t, lr, sc, r + 2);
 }
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
@@ -418,18 +466,26 @@ struct PassRange {
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = false>
 __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
                                           unsigned char* smem_raw) {
-  // dynamic shared memory: RF table [128] | kick-table window [win] | NGP
-  // counters | cell words lo, hi [B+1]; NGP counters: (B+1)/2 words of two
-  // 16-bit counters, or B 32-bit ones (N32)
+  // dynamic shared memory: RF table [128] | the normal transform's logarithm
+  // and angle tables [64 + 64] | kick-table window [win] | NGP counters | cell
+  // words lo, hi [B+1]; NGP counters: (B+1)/2 words of two 16-bit counters, or
+  // B 32-bit ones (N32)
   const int nc = a.B + 1;                 // kick-table cells
   const int nw = N32 ? a.B : (a.B + 1) / 2;
   const int win = WAKE ? a.win : 0;
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
-  double* s_win = reinterpret_cast<double*>(s_rf + kRfTableSize);
+  double2* s_lr = s_rf + kRfTableSize;
+  double2* s_sc = s_lr + 64;
+  double* s_win = reinterpret_cast<double*>(s_sc + 64);
   uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_win + win);
   uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
   uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
   for (int i = threadIdx.x; i < kRfTableSize; i += THREADS) s_rf[i] = __ldg(a.rf_table + i);
+  if (QE == QE_PHILOX)
+    for (int i = threadIdx.x; i < 64; i += THREADS) {
+      s_lr[i] = reinterpret_cast<const double2*>(g_normal.lr)[i];
+      s_sc[i] = reinterpret_cast<const double2*>(g_normal.sc)[i];
+    }
 
   TurnState* ts = a.ts;
   const TurnScalars sc = ts->cur;
@@ -523,7 +579,8 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
     if (QE == QE_PHILOX) {
-      group_normals<PPT>(a.philox_rk, turn, (PPT / 2) * q + a.pair_offset, rr);
+      group_normals<PPT>(a.philox, turn, (PPT / 2) * q + a.pair_offset, &g_normal, s_lr, s_sc,
+                         rr);
     } else if (QE == QE_DRAWS) {
       if (drow) {
 #pragma unroll
@@ -545,7 +602,8 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
   if (rg.tail && threadIdx.x < (int)(a.n % PPT)) {
     const int64_t i = (a.n / PPT) * PPT + threadIdx.x;
     double r2[2] = {0.0, 0.0};
-    if (QE == QE_PHILOX) philox_normals2_rk(a.philox_rk, turn, (i >> 1) + a.pair_offset, r2);
+    if (QE == QE_PHILOX)
+      philox_normals2_rk(a.philox, turn, (i >> 1) + a.pair_offset, &g_normal, s_lr, s_sc, r2);
     double r = r2[i & 1];
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
     double z1[1] = {a.z[i]};
@@ -854,7 +912,7 @@ __device__ __forceinline__ double block_sum_1024(double v, double* red) {
 
 // Sample covariance (two-pass, divisor S - 1) of S independent draws
 // z ~ N(mu_z, sz), E ~ N(mu_E, sE): out = (cov zz, cov EE, cov zE).  One block.
-__global__ void k_gen_sample_cov(uint64_t seed, int64_t S, double mu_z, double sz, double mu_E,
+__global__ void __launch_bounds__(1024) k_gen_sample_cov(uint64_t seed, int64_t S, double mu_z, double sz, double mu_E,
                                  double sE, double* __restrict__ out) {
   __shared__ double red[32];
   double a = 0.0, b = 0.0;
@@ -977,6 +1035,7 @@ const void* pass_fn_wqn(int layout) {
     case 1: return (const void*)k_track_pass<W, Q, 2, 1024, true, 1, N>;
     case 2: return (const void*)k_track_pass<W, Q, 2, 768, true, 1, N>;
     case 4: return (const void*)k_track_pass<W, Q, 2, 512, true, 2, N>;
+    case 5: return (const void*)k_track_pass<W, Q, 4, 256, true, 2, N>;
     default: return (const void*)k_track_pass<W, Q, 2, 512, false, 1, N>;
   }
 }
@@ -1007,6 +1066,7 @@ const void* batch_fn_wqn(int layout) {
     case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true, 1, N>;
     case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true, 1, N>;
     case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2, N>;
+    case 5: return (const void*)k_batch_pass<W, Q, 4, 256, true, 2, N>;
     default: return (const void*)k_batch_pass<W, Q, 2, 512, false, 1, N>;
   }
 }
@@ -1025,6 +1085,12 @@ const void* batch_fn(int wake, int qe, int cfg) {
 }  // namespace
 
 namespace {
+// Grids up to this many bins read the kick table from global memory (L1).
+constexpr int kWindowMinBins = 4096;
+
+// The normal transform's logarithm and angle tables in shared memory.
+constexpr size_t kNormalSmemBytes = 128 * sizeof(double2);
+
 // Dynamic shared memory one block of the pass may take: the device's opt-in
 // limit (set when the kernels are prepared), or per block of the layout that
 // keeps two blocks on an SM (228 KB per SM, 1 KB reserved per block).
@@ -1032,13 +1098,13 @@ int g_pass_smem_limit = 227 * 1024;
 
 size_t pass_smem_budget(int cfg) {
   const size_t lim = (size_t)g_pass_smem_limit;
-  return (cfg & kPassLayoutMask) == 4 ? std::min(lim, (size_t)(113 * 1024)) : lim;
+  return pass_cfg_two_blocks(cfg) ? std::min(lim, (size_t)(113 * 1024)) : lim;
 }
 
-// RF table + NGP counts [B] (16-bit, two per word, or 32-bit with kPassN32)
-// + two 32-bit words per kick-table cell [B+1].
+// RF table + normal transform's table + NGP counts [B] (16-bit, two per
+// word, or 32-bit with kPassN32) + two 32-bit words per kick-table cell [B+1].
 size_t track_hist_bytes(int B, int cfg) {
-  const size_t rf = kRfTableSize * sizeof(double2);
+  const size_t rf = kRfTableSize * sizeof(double2) + kNormalSmemBytes;
   const size_t nw = (cfg & kPassN32) ? (size_t)B : (size_t)((B + 1) / 2);
   return rf + nw * sizeof(uint32_t) + (size_t)(B + 1) * sizeof(unsigned long long);
 }
@@ -1046,6 +1112,12 @@ size_t track_hist_bytes(int B, int cfg) {
 
 cudaError_t prepare_track_kernels(int max_smem) {
   g_pass_smem_limit = max_smem;
+  {
+    NormalTables tab;
+    host_normal_tables(&tab);
+    cudaError_t e = cudaMemcpyToSymbol(g_normal, &tab, sizeof(tab));
+    if (e != cudaSuccess) return e;
+  }
   for (int w = 0; w < 2; ++w)
     for (int q = 0; q < 3; ++q)
       for (int n = 0; n < 2; ++n)
@@ -1060,6 +1132,9 @@ cudaError_t prepare_track_kernels(int max_smem) {
 
 
 int track_window_entries(int B, int cfg) {
+  // up to 4096 bins the 64 KB kick table stays in L1 beside the histograms:
+  // the window would only add its load to every block (measured: no gain)
+  if (B <= kWindowMinBins) return 0;
   const size_t used = track_hist_bytes(B, cfg), budget = pass_smem_budget(cfg);
   if (used >= budget) return 0;
   const size_t w = (budget - used) / sizeof(double);
@@ -1068,7 +1143,7 @@ int track_window_entries(int B, int cfg) {
 
 // Histograms plus the kick-table window (wake on); the RF table alone otherwise.
 size_t track_smem_bytes(int B, int use_wake, int cfg) {
-  if (!use_wake) return kRfTableSize * sizeof(double2);
+  if (!use_wake) return kRfTableSize * sizeof(double2) + kNormalSmemBytes;
   return track_hist_bytes(B, cfg) + (size_t)track_window_entries(B, cfg) * sizeof(double);
 }
 

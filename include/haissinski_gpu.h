@@ -155,7 +155,8 @@ hj_status hj_trim(hj_ctx* ctx);
  * this context: -1 = chosen by the library (default), 0 = 4 particles per
  * thread x 512 threads, 1 = 2 x 1024, 2 = 2 x 768 (each with the next group
  * prefetched), 3 = 2 x 512 without prefetch, 4 = 2 x 512 with prefetch at
- * two blocks per SM; plus 8 (8..12): the same layout with one 32-bit
+ * two blocks per SM, 5 = 4 x 256 with prefetch at two blocks per SM; plus 8
+ * (8..13): the same layout with one 32-bit
  * shared-memory counter per bin instead of two 16-bit ones per word (more
  * shared memory, no overflow check; the default up to 8192 bins).  Results do
  * not depend on the layout beyond floating-point summation order; bin counts
@@ -199,7 +200,7 @@ hj_status hj_make_grid(double sigma_z0, double half_width_sigmas, int64_t nbins,
  *   nbins      bin count (length(buffers.λ) in the reference);
  *   grid       NULL -> grid built on the device's sigma_z0_initial with
  *              hj_make_grid; non-NULL -> used as given (nbins must match);
- *   qe_draws   NULL -> on-device Philox-2x32-10 Gaussians keyed by
+ *   qe_draws   NULL -> on-device Philox-4x32-10 / Box-Muller Gaussians keyed by
  *              (seed, particle, turn); non-NULL -> host array of
  *              n_turns*n standard normals, turn-major, used in place of
  *              randn! (src/quantum_excitation.jl:36);
@@ -466,7 +467,7 @@ hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE, int64_t n
                              const hj_grid* grid);
 
 /* A bunch of independent Gaussians on the device: d_z[i] = sigma_z * N0,
- * d_dE[i] = sigma_E * N1 with (N0, N1) the Philox-2x32-10 / Box-Muller pair of
+ * d_dE[i] = sigma_E * N1 with (N0, N1) the Philox-4x32-10 / Box-Muller pair of
  * particle i under init_seed (a stream apart from the quantum-excitation
  * draws).  Enqueued on `stream`.  The reference draws its bunches with
  * Distributions.jl on the host (generate_particles, src/evolution.jl:42-133,
@@ -480,7 +481,7 @@ hj_status hj_gaussian_bunch(hj_ctx* ctx, uint64_t init_seed, int64_t n, double s
  * min(n, 10000) independent Gaussians, its positive-definite guard, then n
  * correlated draws mu + L eps (L its Cholesky factor) into d_z, d_dE, and the
  * actual spreads by the two-pass compute_std (src/utils.jl:531-544).  Draws
- * are Philox-2x32-10 / Box-Muller under `seed` (the reference's come from
+ * are Philox-4x32-10 / Box-Muller under `seed` (the reference's come from
  * Julia's default RNG).  n <= 0: spreads 0; n = 1: one independent draw and
  * the input spreads, as the reference returns them. */
 hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E, double sigma_z,
@@ -496,10 +497,20 @@ hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E, double si
 hj_status hj_correlation(hj_ctx* ctx, const double* d_x, const double* d_y, int64_t n,
                          void* stream, double* out);
 
-/* The Philox-2x32-10 standard normals used for quantum excitation:
- * out[i] = N(0,1) draw of particle i at `turn` under `seed`.  No reference
- * counterpart (the reference calls randn!, src/quantum_excitation.jl:36). */
+/* The Float64 standard normals used for quantum excitation: out[i] = the
+ * N(0,1) draw of particle i at `turn` under `seed` (Philox-4x32-10 of
+ * (pair i/2, turn) keyed by the 64-bit seed, two 52-bit uniforms per pair,
+ * a double-precision Box-Muller transform).  No reference counterpart (the
+ * reference calls randn!, src/quantum_excitation.jl:36). */
 hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64_t n, double* out);
+
+/* The tables of that transform, for restatements of it (no reference
+ * counterpart; host only, no context): out[HJ_NORMAL_TABLES_SIZE] = 64
+ * pairs (r_j, -ln r_j) of the table-driven logarithm, 64 pairs (sin θ_j,
+ * cos θ_j) of the angle reduction, ln 2 (high part, rest) and 2π (double,
+ * rest).  cap < HJ_NORMAL_TABLES_SIZE is HJ_ERR_ARG. */
+#define HJ_NORMAL_TABLES_SIZE 260
+hj_status hj_normal_tables(double* out, int64_t cap);
 
 #ifdef __cplusplus
 }

@@ -53,7 +53,7 @@ def _check(a, b, cfg, what):
     assert ra.sigma_z == pytest.approx(rb.sigma_z, rel=1e-12)
 
 
-@pytest.mark.parametrize("layout", [-1, 0, 1, 2, 3, 4, 8, 9, 12])
+@pytest.mark.parametrize("layout", [-1, 0, 1, 2, 3, 4, 5, 8, 9, 12, 13])
 def test_batch_matches_the_plain_path_with_ragged_turns(gpu_ctx, layout):
     turns = [20, 35, 27, 20, 40]
     bt = Batch(gpu_ctx, pool_particles=300_000, max_bunches=8, max_nbins=2048, chunk=16384,

@@ -84,9 +84,9 @@ def test_reference_ring_reference_wake(gpu_ctx, oracle):
     run_turn_by_turn(gpu_ctx, oracle, cfg, 100_000, 30, seed=1234)
 
 
-@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4, 8, 9, 10, 11, 12])
+@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13])
 def test_thread_layouts(oracle, layout):
-    """Every thread layout of the fused pass, with 16-bit (0-4) or 32-bit (8-12)
+    """Every thread layout of the fused pass, with 16-bit (0-5) or 32-bit (8-13)
     bin counters, keeps per-particle parity and bit-exact counts."""
     from haissinskijulia_b200 import Context
     ctx = Context(0)
@@ -284,10 +284,10 @@ def test_invalid_pass_layouts_are_refused(gpu_ctx):
     from haissinskijulia_b200 import Context, HaissinskiError
     from haissinskijulia_b200 import _lib
     ctx = Context(0)
-    for bad in (-2, 5, 7, 13, 16, 24):
+    for bad in (-2, 6, 7, 14, 16, 24):
         with pytest.raises(HaissinskiError) as e:
             ctx.set_pass_layout(bad)
         assert e.value.status == _lib.HJ_ERR_ARG
-    for good in (-1, 0, 4, 8, 12):
+    for good in (-1, 0, 4, 5, 8, 12, 13):
         ctx.set_pass_layout(good)
     ctx.close()
