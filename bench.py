@@ -52,6 +52,11 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--turns-per-step", type=int, default=LOG_EVERY,
                     help="turns of one step (the last one writes the turn-log record)")
+    ap.add_argument("--multi", choices=["shard", "replicas"], default="shard",
+                    help="N > 1: one bunch sharded over the ranks with one all-reduce of the "
+                         "bin exchange per turn (default), or independent replicas")
+    ap.add_argument("--plan-only", action="store_true",
+                    help="print the ranks' shard plan (rank 0) and exit; no GPU work")
     ap.add_argument("--layout", type=int, default=-1,
                     help="thread layout of the fused pass (-1 = library default)")
     ap.add_argument("--e2e-calls", type=int, default=1,
@@ -67,9 +72,13 @@ def parse_args():
     ap.add_argument("--no-sweep", action="store_true",
                     help="skip the batched-sweep / serving measurements (single GPU only)")
     ap.add_argument("--sweep-turns", type=int, default=5000)
-    ap.add_argument("--sweep-plain-points", type=int, default=8,
-                    help="points of the sweep also run one after another on the plain path")
-    ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--sweep-plain-points", type=int, default=32,
+                    help="points of the sweep (a stratified sample) also run one after "
+                         "another on the plain path")
+    ap.add_argument("--serve-requests", type=int, default=500,
+                    help="requests per offered load of the served stream (0: no serving)")
+    ap.add_argument("--serve-rates", default="5,10,20,50",
+                    help="offered loads (requests/s) of the served stream")
     ap.add_argument("--scan-points", type=int, default=32,
                     help="parameter-scan points (0: no scan measurement)")
     ap.add_argument("--scan-samples", type=int, default=20)
@@ -267,14 +276,33 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _max_rel_diff(a_solves, b_solves) -> float:
+    rel = 0.0
+    for a, b in zip(a_solves, b_solves):
+        for key in ("E0", "sigma_E", "sigma_z"):
+            x, y = getattr(a.result, key), getattr(b.result, key)
+            rel = max(rel, abs(x - y) / abs(y))
+    return rel
+
+
+def stratified_sample(points, k: int):
+    """k points, one from each of k equal strata of the points sorted by
+    particle count (the middle one of each), so that the sample's particle
+    counts follow the whole sweep's distribution."""
+    order = sorted(range(len(points)), key=lambda i: points[i].n)
+    size = len(order) / k
+    return sorted(order[int((j + 0.5) * size)] for j in range(k))
+
+
 def measure_sweeps(ctx, args) -> dict:
-    """The ragged 256-point sweep (batched vs plain point by point), the
-    32-bunch intensity scan and a served request stream, host wall clock
-    around each (admission, turns, retirement and result read-back included)."""
-    import numpy as np
-    from haissinskijulia_b200.sweep import (autotune, intensity_scan, request_stream,
-                                            run_batched, run_plain, serve, serve_plain,
-                                            sweep_points)
+    """The ragged 256-point sweep (batched vs plain point by point on a
+    stratified sample), the 32-bunch intensity scan (batched vs all 32 bunches
+    one after another) and served request streams at several offered loads
+    (batched vs one at a time), host wall clock around each (admission,
+    turns, retirement and result read-back included)."""
+    from haissinskijulia_b200.sweep import (autotune, intensity_scan, plain_service,
+                                            plain_timeline, request_stream, run_batched,
+                                            run_plain, serve, sweep_points)
     T = args.sweep_turns
     pts = sweep_points(256, turns=T)
     t0 = time.perf_counter()
@@ -284,17 +312,14 @@ def measure_sweeps(ctx, args) -> dict:
     bat = run_batched(ctx, pts, tuning=tun, block_turns=500)
     t_bat = time.perf_counter() - t0
     k = max(1, min(args.sweep_plain_points, len(pts)))
-    idx = list(range(0, len(pts), len(pts) // k))[:k]
+    idx = stratified_sample(pts, k)
     t0 = time.perf_counter()
     pla = run_plain(ctx, [pts[i] for i in idx])
     t_pla = time.perf_counter() - t0
-    rel = 0.0
-    for j, i in enumerate(idx):
-        a, b = bat[i].result, pla[j].result
-        for key in ("E0", "sigma_E", "sigma_z"):
-            x, y = getattr(a, key), getattr(b, key)
-            rel = max(rel, abs(x - y) / abs(y))
     pt = sum(p.n * p.turns for p in pts)
+    # the sample's particle-turns scaled to the whole sweep
+    sample_pt = sum(pts[i].n * pts[i].turns for i in idx)
+    plain_est_s = t_pla * pt / sample_pt
     out = {
         "config": f"256 points: V ~ U[3,7] MV, population log-U[1e9,1e11], particles "
                   f"log-U[1e4,2e6] (total {sum(p.n for p in pts):.3e}), {T} turns, 4096 bins, "
@@ -302,10 +327,14 @@ def measure_sweeps(ctx, args) -> dict:
         "batched_solves_per_s": len(pts) / t_bat, "batched_seconds": t_bat,
         "batched_particle_turns_per_s": pt / t_bat,
         "plain_solves_per_s": k / t_pla, "plain_seconds": t_pla,
-        "plain_sample": f"{k} of the 256 points (every {len(pts) // k}th), all {T} turns each, "
-                        "one after another on the plain resident path",
+        "plain_sample": f"{k} of the 256 points, one from each of {k} strata of equal size by "
+                        f"particle count (mean {np.mean([pts[i].n for i in idx]):.3e} particles "
+                        f"against {np.mean([p.n for p in pts]):.3e} for all 256), all {T} "
+                        "turns each, one after another on the plain resident path",
+        "plain_seconds_scaled_to_256_by_particle_turns": plain_est_s,
         "speedup_vs_plain": (len(pts) / t_bat) / (k / t_pla),
-        "max_rel_diff_vs_plain": rel,
+        "speedup_vs_plain_by_particle_turns": plain_est_s / t_bat,
+        "max_rel_diff_vs_plain": _max_rel_diff([bat[i] for i in idx], pla),
         "tuning": {"particles_per_block": tun.chunk, "layout": tun.layout,
                    "graph_turns": tun.graph_turns, "autotune_seconds": t_tune},
         "timing": "host wall clock: admission, every turn, retirement",
@@ -315,31 +344,48 @@ def measure_sweeps(ctx, args) -> dict:
     tun_i = autotune(ctx, scan, trial_turns=32, sample=len(scan))
     t_tune_i = time.perf_counter() - t0
     t0 = time.perf_counter()
-    run_batched(ctx, scan, tuning=tun_i, block_turns=500)
+    sbat = run_batched(ctx, scan, tuning=tun_i, block_turns=500)
     t_scan = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    spla = run_plain(ctx, scan)
+    t_scan_plain = time.perf_counter() - t0
     out["intensity_scan"] = {
         "config": f"32 bunches x 1e6 particles, populations log-spaced 1e9-1e11, {T} turns, "
                   "8192 bins, one batch",
         "solves_per_s": len(scan) / t_scan, "seconds": t_scan,
         "particle_turns_per_s": sum(p.n * p.turns for p in scan) / t_scan,
+        "plain_solves_per_s": len(scan) / t_scan_plain, "plain_seconds": t_scan_plain,
+        "plain_how": "all 32 bunches one after another on the plain resident path",
+        "speedup_vs_plain": t_scan_plain / t_scan,
+        "max_rel_diff_vs_plain": _max_rel_diff(sbat, spla),
         "tuning": {"particles_per_block": tun_i.chunk, "layout": tun_i.layout,
                    "graph_turns": tun_i.graph_turns, "autotune_seconds": t_tune_i}}
     if args.serve_requests > 0:
-        reqs = request_stream(args.serve_requests)
-        rep = serve(ctx, reqs, tuning=tun)
-        sm = rep.summary()
-        sm["config"] = (f"{args.serve_requests} requests, Poisson arrivals at 50/s, V ~ U[3,7] "
-                        "MV, population log-U[1e9,1e11], particles log-U[1e4,4e6], turns "
-                        "U[1000,20000], bins in {2048,4096,8192}; admission by footprint "
-                        "(8 GB budget), 200-turn blocks")
-        sm["particle_turns_per_s"] = sm["particle_turns"] / sm["wall_s"]
-        pl = serve_plain(ctx, reqs).summary()
-        sm["plain"] = {"solves_per_s": pl["solves_per_s"], "p50_latency_s": pl["p50_latency_s"],
-                       "p99_latency_s": pl["p99_latency_s"], "wall_s": pl["wall_s"],
-                       "how": "the same requests one at a time on the plain resident path, "
-                              "first come first served (measured service times)"}
-        sm["speedup_vs_plain"] = sm["solves_per_s"] / pl["solves_per_s"]
-        out["serving"] = sm
+        rates = [float(r) for r in args.serve_rates.split(",") if r]
+        base = request_stream(args.serve_requests, rate=rates[0])
+        service = plain_service(ctx, base)             # the same requests at every rate
+        loads = []
+        for rate in rates:
+            reqs = request_stream(args.serve_requests, rate=rate)
+            assert [(p.n, p.turns, p.seed) for p in reqs] == [(p.n, p.turns, p.seed) for p in base]
+            sm = serve(ctx, reqs, tuning=tun).summary()
+            sm["offered_rate_per_s"] = rate
+            sm["particle_turns_per_s"] = sm["particle_turns"] / sm["wall_s"]
+            pl = plain_timeline(reqs, service).summary()
+            sm["plain"] = {"solves_per_s": pl["solves_per_s"],
+                           "p50_latency_s": pl["p50_latency_s"],
+                           "p99_latency_s": pl["p99_latency_s"], "wall_s": pl["wall_s"]}
+            sm["speedup_vs_plain"] = sm["solves_per_s"] / pl["solves_per_s"]
+            loads.append(sm)
+        out["serving"] = {
+            "config": f"{args.serve_requests} requests per offered load, Poisson arrivals, V ~ "
+                      "U[3,7] MV, population log-U[1e9,1e11], particles log-U[1e4,4e6], turns "
+                      "U[1000,20000], bins in {2048,4096,8192}; admission by footprint (8 GB "
+                      "budget), 200-turn blocks; the same requests at every rate",
+            "plain_how": "the same requests one at a time on the plain resident path, first "
+                         "come first served, each taking its measured service time",
+            "plain_service_seconds_total": float(sum(s.finished for s in service)),
+            "loads": loads}
     if args.scan_points > 0:
         out["parameter_scan"] = measure_scan(ctx, args)
     return out
@@ -389,6 +435,181 @@ def measure_scan(ctx, args) -> dict:
     }
 
 
+def shard_plan(rank: int, world: int, n_per_rank: int) -> dict:
+    """Weak scaling: every rank holds n_per_rank particles of one bunch of
+    world * n_per_rank; rank r owns particles [r n, (r + 1) n), whose Philox
+    draws are those of the same particles of the whole bunch."""
+    return {"rank": rank, "n_local": n_per_rank, "first_particle": rank * n_per_rank,
+            "n_global": world * n_per_rank}
+
+
+def run_plan(args) -> None:
+    """--plan-only: the shard plan of every rank, gathered on rank 0."""
+    import datetime
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    plan = shard_plan(rank, world, int(args.particles))
+    plans = [plan]
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        plans = [None] * world
+        dist.all_gather_object(plans, plan)
+    if rank == 0:
+        print(json.dumps({"n_gpus": world, "parallelism": args.multi if world > 1 else
+                          "single GPU", "plan": plans}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_sharded(args, ctx, cfg, stream, rank, world, local, clocks) -> None:
+    """N > 1: one bunch of N x particles sharded over the ranks.  Per turn each
+    rank runs the fused pass on its particles (hj_bunch_pass), the two
+    exchange buffers (bin counts and cell deposits, 3B + 2 u64; the four sums)
+    are summed over the ranks with NCCL all-reduces on the bunch's stream, and
+    every rank runs the same bins step (hj_bunch_bins).  Timed with CUDA events
+    on that stream, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from haissinskijulia_b200 import BinGrid, ShardedBunch
+    n, B, K, W, tps = int(args.particles), args.nbins, args.steps, args.warmup, args.turns_per_step
+    plan = shard_plan(rank, world, n)
+    grid = BinGrid.make(cfg.sigma_z, B, cfg.wake.half_width_sigmas)    # the same on every rank
+    gen = torch.Generator(device="cuda").manual_seed(args.seed + 7919 * rank)
+    z = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_z
+    dE = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_E
+    sb = ShardedBunch(ctx, z.data_ptr(), dE.data_ptr(), n, plan["first_particle"],
+                      plan["n_global"], cfg.params, grid, wake=cfg.wake, seed=args.seed,
+                      stream=stream.cuda_stream)
+    counts, sums = sb.buffers()
+    pass_events = []
+
+    def turn(profile: bool):
+        if profile:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        sb.pass_()
+        if profile:
+            b.record(stream)
+            pass_events.append((a, b))
+        dist.all_reduce(counts)
+        dist.all_reduce(sums)
+        sb.bins()
+
+    for _ in range(W * tps):
+        turn(False)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks.mark()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(K * tps):
+        turn(True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks.mark()
+    clock_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    pass_ms = sum(a.elapsed_time(b) for a, b in pass_events) / len(pass_events)
+    res = sb.global_result()
+    sb.finish()
+    sb.close()
+    del z, dE, counts, sums
+    t = torch.tensor([ms, pass_ms], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, pass_ms = float(t[0].item()), float(t[1].item())
+    value = plan["n_global"] * K * tps / (ms / 1e3)
+
+    # secondary: independent replicas (no exchange), 2 steps
+    from haissinskijulia_b200 import ResidentBunch
+    zr = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_z
+    er = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_E
+    rb = ResidentBunch(ctx, zr.data_ptr(), er.data_ptr(), n, cfg.params, B, wake=cfg.wake,
+                       seed=args.seed + rank, stream=stream.cuda_stream)
+    rb.advance(tps)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rb.advance(2 * tps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    rb.finish()
+    rb.close()
+    del zr, er
+    tr = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(tr, op=dist.ReduceOp.MAX)
+    replicas = {"value": n * world * 2 * tps / (float(tr.item()) / 1e3), "unit": UNIT,
+                "turns": 2 * tps, "how": "one independent bunch per rank, no exchange"}
+
+    # e2e: host shards in pinned memory, copied in, tracked with the exchange, copied out
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.empty_cache()
+        E = args.e2e_turns
+        zh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        eh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        g = torch.Generator().manual_seed(args.seed + rank)
+        zh.copy_(torch.randn(n, dtype=torch.float64, generator=g) * cfg.sigma_z)
+        eh.copy_(torch.randn(n, dtype=torch.float64, generator=g) * cfg.sigma_E)
+        times = []
+        for c in range(2):                               # the first call warms up
+            torch.cuda.synchronize()
+            dist.barrier()
+            t0 = time.perf_counter()
+            zd = zh.to("cuda", non_blocking=True)
+            ed = eh.to("cuda", non_blocking=True)
+            s2 = ShardedBunch(ctx, zd.data_ptr(), ed.data_ptr(), n, plan["first_particle"],
+                              plan["n_global"], cfg.params, grid, wake=cfg.wake,
+                              seed=args.seed + c, stream=stream.cuda_stream)
+            c2, m2 = s2.buffers()
+            for _ in range(E):
+                s2.pass_()
+                dist.all_reduce(c2)
+                dist.all_reduce(m2)
+                s2.bins()
+            s2.finish()
+            zh.copy_(zd)
+            eh.copy_(ed)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            s2.close()
+            del zd, ed, c2, m2
+        te = torch.tensor([times[-1]], dtype=torch.float64, device="cuda")
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        t_e2e = float(te.item())
+        e2e = {"value": plan["n_global"] * E / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n, "turns_per_step": E,
+               "seconds_per_step": t_e2e,
+               "api": "haissinskijulia_b200.ShardedBunch (hj_bunch_create_shard, hj_bunch_pass, "
+                      "NCCL all-reduce, hj_bunch_bins) per rank, host shards copied in and out"}
+    if rank == 0:
+        peak, peak_kind = measured_hbm_peak()
+        achieved = BYTES_PER_PARTICLE_TURN * n / (pass_ms / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload(plan["n_global"], B, tps), parallelism=f"shard{world}",
+                           particles_per_rank=n,
+                           exchange="per turn: NCCL SUM all-reduce of the 3B+2 u64 bin "
+                                    "exchange and of the 4 double sums (replaces the "
+                                    "reference's MPI Allreduce/Scatterv/Gatherv/Bcast)",
+                           turn_log="none in the sharded arm"),
+            "roofline": {"bound": "hbm", "kernel": "k_track_pass", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "traffic": None, "algorithmic_bytes": BYTES_PER_PARTICLE_TURN * n,
+                         "pass_ms": pass_ms, "max_over_ranks": True},
+            "cpu_baseline": None, "e2e": e2e, "replicas": replicas,
+            "gpu_launches": 4 * K * tps, "clocks": clock_info,
+            "final": {"sigma_E": res.sigma_E, "sigma_z": res.sigma_z, "E0": res.E0},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -401,6 +622,7 @@ def run_ours(args) -> None:
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
+        os.environ.setdefault("NCCL_DEBUG", "INFO")     # init lines show the rank count
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
@@ -415,6 +637,13 @@ def run_ours(args) -> None:
     ctx = Context(local)
     ctx.set_pass_layout(args.layout)
     stream = torch.cuda.current_stream()
+    if world > 1 and args.multi == "shard":
+        clocks = ClockSampler(local)
+        clocks.start()
+        run_sharded(args, ctx, cfg, stream, rank, world, local, clocks)
+        dist.barrier()
+        dist.destroy_process_group()
+        return
     gen = torch.Generator(device="cuda").manual_seed(args.seed + 7919 * rank)
     z = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_z
     dE = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) * cfg.sigma_E
@@ -540,7 +769,9 @@ def run_ours(args) -> None:
 
 def main():
     args = parse_args()
-    if args.impl == "reference":
+    if args.plan_only:
+        run_plan(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

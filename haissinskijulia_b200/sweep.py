@@ -17,7 +17,9 @@ batched bins step per turn, turn blocks replayed from a CUDA graph.
   width of the shared-memory bin counters -- the histogram privatisation --,
   K) on a sample of the workload and keeps the fastest.
 * `serve_plain`: the same stream one request at a time on the plain path
-  (first come first served), the baseline of `serve`.
+  (first come first served), the baseline of `serve`; `plain_service` and
+  `plain_timeline` split it so that one set of measured service times serves
+  every arrival rate of the same requests.
 * `serve`: a request stream with arrival times; requests are admitted by
   device-memory footprint (16 B per particle plus bin tables) while others
   run, and per-request latency percentiles are reported with solves/s.
@@ -309,22 +311,32 @@ def serve(ctx: Context, requests: List[Point], *, memory_budget: int = 8 << 30,
     return rep
 
 
-def serve_plain(ctx: Context, requests: List[Point]) -> ServeReport:
-    """The same request stream served one request at a time on the plain
-    resident path, first come first served: each request's service time is
-    measured, and a request starts when it has arrived and the previous one
-    has finished (latency = finish - arrival on that timeline; no idle time
-    is spent waiting for arrivals)."""
+def plain_service(ctx: Context, requests: List[Point]) -> List[Solve]:
+    """Each request solved alone on the plain resident path; Solve.finished
+    is its measured service time (bunch generation, turns, result)."""
+    return [run_plain(ctx, [p])[0] for p in requests]
+
+
+def plain_timeline(requests: List[Point], service: List[Solve]) -> ServeReport:
+    """First come first served on one plain solver: a request starts when it
+    has arrived and the previous one has finished, and takes its measured
+    service time (latency = finish - arrival on that timeline; no idle time is
+    spent waiting for arrivals)."""
     rep = ServeReport()
     clock = 0.0
-    for p in sorted(requests, key=lambda q: q.arrival):
+    for k in sorted(range(len(requests)), key=lambda q: requests[q].arrival):
+        p, s = requests[k], service[k]
         start = max(clock, p.arrival)
-        s = run_plain(ctx, [p])[0]
-        service = s.finished                         # run_plain's clock starts at the request
-        clock = start + service
+        clock = start + s.finished
         rep.solves.append(Solve(p, s.result, admitted=start, finished=clock))
     rep.wall = clock
     return rep
+
+
+def serve_plain(ctx: Context, requests: List[Point]) -> ServeReport:
+    """The same request stream served one request at a time on the plain
+    resident path (plain_service, then plain_timeline)."""
+    return plain_timeline(requests, plain_service(ctx, requests))
 
 
 def time_batch_turns(ctx: Context, points: List[Point], turns: int, tuning: Tuning) -> float:

@@ -68,3 +68,28 @@ def test_plain_python_ring_equals_the_library_ring():
     for f, _ in wc._fields_:
         assert getattr(w, f) == getattr(wc, f), f
     assert (sz, sE) == (cfg.sigma_z, cfg.sigma_E)
+
+
+def test_sharded_arm_plan_under_torchrun():
+    """bench.py --gpus 2 shards one bunch of 2 x particles over the ranks: rank
+    r owns [r n, (r + 1) n) of 2n (the argument handling of the multi-GPU arm,
+    launched as the driver launches it; --plan-only does no GPU work)."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py",
+           "--gpus", "2", "--steps", "2", "--warmup", "1", "--particles", "1e8", "--plan-only"]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-3000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["parallelism"] == "shard"
+    assert d["plan"] == [
+        {"rank": 0, "n_local": 100_000_000, "first_particle": 0, "n_global": 200_000_000},
+        {"rank": 1, "n_local": 100_000_000, "first_particle": 100_000_000,
+         "n_global": 200_000_000}]
+
+
+def test_gpus_must_match_the_world_size():
+    out = subprocess.run([sys.executable, "bench.py", "--gpus", "2", "--plan-only"], cwd=ROOT,
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode != 0 and "WORLD_SIZE=1" in (out.stderr + out.stdout)

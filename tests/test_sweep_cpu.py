@@ -92,3 +92,35 @@ def test_serve_plain_timeline(monkeypatch):
         assert g[1] == pytest.approx(w[1]) and g[2] == pytest.approx(w[2])
     assert rep.wall == pytest.approx(3.1)
     assert all(sv.result == ("result", sv.point.seed) for sv in rep.solves)
+
+
+def test_request_streams_at_other_rates_hold_the_same_requests():
+    """The serving curve reuses one set of plain service times for every
+    offered load: only the arrival times scale with the rate."""
+    a, b = request_stream(100, rate=5.0), request_stream(100, rate=50.0)
+    assert [(p.n, p.turns, p.nbins, p.voltage, p.seed) for p in a] == \
+        [(p.n, p.turns, p.nbins, p.voltage, p.seed) for p in b]
+    assert np.allclose([p.arrival for p in a], [10.0 * p.arrival for p in b])
+
+
+def test_plain_timeline_reuses_service_times():
+    reqs = [Point(10, 5e6, 1e10, 64, 10, s, arrival=a) for s, a in [(0, 0.0), (1, 0.1)]]
+    service = [Solve(reqs[0], "r0", finished=0.5), Solve(reqs[1], "r1", finished=0.2)]
+    rep = sweep.plain_timeline(reqs, service)
+    assert [(s.admitted, s.finished, s.result) for s in rep.solves] == \
+        [(0.0, 0.5, "r0"), (0.5, pytest.approx(0.7), "r1")]
+
+
+def test_stratified_sample_follows_the_particle_distribution():
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+    import bench
+    pts = sweep_points(256)
+    idx = bench.stratified_sample(pts, 32)
+    assert len(set(idx)) == 32 and idx == sorted(idx)
+    n_all = np.sort([p.n for p in pts])
+    n_s = np.sort([pts[i].n for i in idx])
+    # the j-th sampled count is the middle of the j-th eighth-of-a-percentile stratum
+    assert np.array_equal(n_s, n_all[[int((j + 0.5) * 8) for j in range(32)]])
+    assert abs(math.log(n_s.mean() / n_all.mean())) < 0.1
