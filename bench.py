@@ -44,8 +44,8 @@ PASS_DRAM_BYTES = {16384: (30.53, "profiles/k_track_pass_full_2e7_b16384.md")}
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--particles", type=float, default=1e8)
     ap.add_argument("--nbins", type=int, default=16384)
@@ -75,7 +75,7 @@ def parse_args():
     ap.add_argument("--sweep-plain-points", type=int, default=32,
                     help="points of the sweep (a stratified sample) also run one after "
                          "another on the plain path")
-    ap.add_argument("--serve-requests", type=int, default=500,
+    ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests per offered load of the served stream (0: no serving)")
     ap.add_argument("--serve-rates", default="5,10,20,50",
                     help="offered loads (requests/s) of the served stream")
@@ -679,6 +679,27 @@ def run_ours(args) -> None:
     log = bunch.read_log()
     res = bunch.finish()
     bunch.close()
+
+    # the same pass with the opt-in single-precision excitation normals
+    # (layout 23), for the cost of the default Float64 normals: 2 steps
+    fast = None
+    if args.layout == -1:
+        ctx.set_pass_layout(23)
+        fb = ResidentBunch(ctx, z.data_ptr(), dE.data_ptr(), n, cfg.params, B, wake=cfg.wake,
+                           seed=args.seed + rank + 1, stream=stream.cuda_stream)
+        fb.advance(tps)
+        fb.set_profiling(True)
+        fb.advance(2 * tps)
+        fp = fb.read_profile()
+        fb.finish()
+        fb.close()
+        ctx.set_pass_layout(args.layout)
+        fpass = fp["pass_ms"] / max(fp["turns"], 1)
+        fast = {"layout": 23, "pass_ms": fpass,
+                "frac": BYTES_PER_PARTICLE_TURN * n / (fpass / 1e3) / 1e9 / measured_hbm_peak()[0],
+                "turns": fp["turns"],
+                "what": "k_track_pass with single-precision Box-Muller normals (opt-in layout "
+                        "23) instead of the default Float64 ones, CUDA events, same bunch"}
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -751,7 +772,8 @@ def run_ours(args) -> None:
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload(n, B, tps),
                            parallelism="replicas" if world > 1 else "single GPU"),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "sweep": sweep,
+            "roofline": roofline, "roofline_fast_normals": fast, "cpu_baseline": cpu,
+            "e2e": e2e, "sweep": sweep,
             "gpu_launches": prof["launches"], "clocks": clock_info,
             "wall_seconds_timed": t_wall,
             "turn_log": {"every": LOG_EVERY, "records": int(log.shape[0]),

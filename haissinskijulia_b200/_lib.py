@@ -148,6 +148,7 @@ SIGNATURES = {
                                   POINTER(c_void_p)]),
     "hj_batch_destroy": (None, [c_void_p]),
     "hj_batch_set_graph_turns": (c_int32, [c_void_p, c_int32]),
+    "hj_batch_set_resident": (c_int32, [c_void_p, c_int32]),
     "hj_batch_add": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, POINTER(HjParams),
                                POINTER(HjWake), c_int64, c_uint64, c_int64, _IP]),
     "hj_batch_add_gaussian": (c_int32, [c_void_p, c_int64, c_double, c_double, c_uint64,

@@ -228,7 +228,8 @@ class Context:
     def set_pass_layout(self, layout: int) -> None:
         """Thread layout of the fused pass for bunches created afterwards
         (-1 = automatic; 0-5 = fixed layouts with 16-bit bin counters, 8-13
-        the same with 32-bit counters; see hj_set_pass_layout)."""
+        the same with 32-bit counters; + 16 for single-precision excitation
+        normals, 23 = automatic with them; see hj_set_pass_layout)."""
         _check(self, self._lib.hj_set_pass_layout(self.handle, int(layout)))
 
     def trim(self) -> None:
@@ -682,7 +683,8 @@ class Batch:
     """
 
     def __init__(self, ctx: Context, pool_particles: int, max_bunches: int, max_nbins: int,
-                 chunk: int = 65536, layout: int = -1, graph_turns: int = 16):
+                 chunk: int = 65536, layout: int = -1, graph_turns: int = 16,
+                 resident: bool = True):
         self.ctx = ctx
         h = ctypes.c_void_p()
         _check(ctx, ctx._lib.hj_batch_create(ctx.handle, int(pool_particles), int(max_bunches),
@@ -692,6 +694,13 @@ class Batch:
         self.sizes = {}
         if graph_turns != 16:
             self.set_graph_turns(graph_turns)
+        if not resident:
+            self.set_resident(False)
+
+    def set_resident(self, on: bool) -> None:
+        """Resident blocks on a device-side chunk queue (True, the default) or
+        one block per chunk (hj_batch_set_resident)."""
+        _check(self.ctx, self.ctx._lib.hj_batch_set_resident(self.handle, int(bool(on))))
 
     def set_graph_turns(self, turns: int) -> None:
         _check(self.ctx, self.ctx._lib.hj_batch_set_graph_turns(self.handle, int(turns)))

@@ -277,13 +277,13 @@ hj_status read_state(hj_bunch* b) {
 
 // Thread layout of the fused pass when the context does not pin one, from
 // timings on B200: four particles per thread x 512 threads, prefetching the
-// next group; one 32-bit counter per bin up to 8192 bins (1e8 particles at
-// 4096 bins: 0.60 ms against 0.67 with 16-bit pairs), 16-bit pairs above,
-// where the 32-bit counters would shrink L1 for the kick table to 60 KB
-// (16384 bins: 0.72 ms against 0.81).
+// next group, one 32-bit counter per bin (1e8 particles, 16384 bins: 0.81 ms
+// per pass against 0.83 with 16-bit pairs, whose larger kick-table window
+// does not make up for their overflow checks).
 int default_pass_layout(int B, int64_t n) {
+  (void)B;
   (void)n;
-  return B <= 8192 ? (0 | kPassN32) : 0;
+  return 0 | kPassN32;
 }
 
 void fill_result(hj_bunch* b, const double m[4], hj_result* res) {
@@ -390,9 +390,11 @@ extern "C" hj_status hj_trim(hj_ctx* ctx) {
 
 extern "C" hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout) {
   if (!ctx) return HJ_ERR_ARG;
-  if (layout != -1 && !pass_cfg_valid(layout))
-    return set_err(ctx, HJ_ERR_ARG, "pass layout must be -1 (automatic), 0..%d or 8..%d",
-                   kNumPassCfgs - 1, kPassN32 + kNumPassCfgs - 1);
+  if (!pass_request_valid(layout))
+    return set_err(ctx, HJ_ERR_ARG,
+                   "pass layout must be -1 (automatic), %d (automatic, single-precision normals), "
+                   "0..%d or 8..%d, plus %d for single-precision normals",
+                   kPassAutoFast, kNumPassCfgs - 1, kPassN32 + kNumPassCfgs - 1, kPassFastNormals);
   ctx->pass_layout = layout;
   return HJ_OK;
 }
@@ -472,7 +474,7 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
     b->H = b->M / 2;
     b->logH = b->H >= 1 ? ilog2(b->H) : 0;
   }
-  b->cfg = cfg >= 0 ? cfg : (ctx->pass_layout >= 0 ? ctx->pass_layout : default_pass_layout(b->B, n));
+  b->cfg = cfg >= 0 ? cfg : resolve_pass_request(ctx->pass_layout, default_pass_layout(b->B, n));
   if (chunk > 0) {
     b->batch_member = true;
     b->nblk = (int)std::max<int64_t>((n + chunk - 1) / chunk, 1);
@@ -1113,11 +1115,11 @@ extern "C" hj_status hj_normal_tables(double* out, int64_t cap) {
   NormalTables t;
   host_normal_tables(&t);
   double* o = out;
-  for (int j = 0; j < 64; ++j) {
+  for (int j = 0; j < kNormalTableRows; ++j) {
     *o++ = t.lr[j][0];
     *o++ = t.lr[j][1];
   }
-  for (int j = 0; j < 64; ++j) {
+  for (int j = 0; j < kNormalTableRows; ++j) {
     *o++ = t.sc[j][0];
     *o++ = t.sc[j][1];
   }

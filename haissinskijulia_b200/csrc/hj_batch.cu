@@ -48,7 +48,10 @@ struct hj_batch {
   BinsArgs* d_bins = nullptr;
   BatchChunk* d_chunks = nullptr;
   BatchChunk* d_items = nullptr;               // merge table: groups of a bunch's partial slots
-  int32_t* d_counts = nullptr;                 // [0] chunks, [1] bunches, [2] merge items
+  int32_t* d_counts = nullptr;                 // [0] chunks, [1] bunches, [2] merge items,
+                                               // [3] the resident pass's chunk queue
+  bool resident = true;                        // the pass: resident blocks on a chunk queue
+  int resident_blocks = 0;                     // their number (SMs x blocks per SM)
   PassArgs* h_pass = nullptr;                  // pinned staging
   BinsArgs* h_bins = nullptr;
   BatchChunk* h_chunks = nullptr;
@@ -149,7 +152,9 @@ hj_status batch_upload(hj_batch* bt) {
 hj_status batch_launch_turn(hj_batch* bt) {
   hj_ctx* ctx = bt->ctx;
   HJ_CUDA(ctx, launch_batch_pass(bt->d_pass, bt->d_chunks, bt->d_counts, bt->grid_chunks,
-                                 bt->max_B, bt->wake, bt->qe, bt->cfg, bt->stream));
+                                 bt->max_B, bt->wake, bt->qe, bt->cfg,
+                                 bt->resident ? bt->d_counts + 3 : nullptr, bt->resident_blocks,
+                                 bt->stream));
   if (bt->wake)
     HJ_CUDA(ctx, launch_batch_reduce(bt->d_pass, bt->d_items, bt->d_counts + 2, bt->grid_items,
                                      bt->max_B, bt->stream));
@@ -220,7 +225,7 @@ static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t 
   const int64_t P = next_pow2(2 * (int64_t)max_nbins);
   bt->max_H = (int)std::max<int64_t>(P / 4, 4);
   bt->bins_ctas = batch_bins_ctas(bt->max_H, max_bunches, ctx->num_sms);
-  bt->cfg = layout >= 0 ? layout : default_pass_layout(max_nbins, pool_particles);
+  bt->cfg = resolve_pass_request(layout, default_pass_layout(max_nbins, pool_particles));
   bt->pool_n = (pool_particles + 3) / 4 * 4;
   bt->max_chunks = (int)std::min<int64_t>(bt->pool_n / chunk + max_bunches + 1, INT32_MAX);
   HJ_CUDA(ctx, cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking));
@@ -230,7 +235,7 @@ static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t 
   const size_t o_z = c.add<double>((size_t)bt->pool_n), o_e = c.add<double>((size_t)bt->pool_n);
   const size_t o_ts = c.add<TurnState>(nb), o_pass = c.add<PassArgs>(nb);
   const size_t o_bins = c.add<BinsArgs>(nb), o_ch = c.add<BatchChunk>(nc);
-  const size_t o_it = c.add<BatchChunk>(nc), o_cnt = c.add<int32_t>(3);
+  const size_t o_it = c.add<BatchChunk>(nc), o_cnt = c.add<int32_t>(4);
   HJ_TRY(cache_take(ctx, false, c.off, &bt->arena, &bt->arena_cap));
   char* a = (char*)bt->arena;
   bt->pool_z = (double*)(a + o_z);
@@ -253,7 +258,7 @@ static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t 
   bt->h_chunks = (BatchChunk*)(q + p_ch);
   bt->h_items = (BatchChunk*)(q + p_it);
   bt->h_counts = (int32_t*)(q + p_cnt);
-  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_counts, 0, sizeof(int32_t) * 3, bt->stream));
+  HJ_CUDA(ctx, cudaMemsetAsync(bt->d_counts, 0, sizeof(int32_t) * 4, bt->stream));
   HJ_CUDA(ctx, cudaMemsetAsync(bt->d_ts, 0, sizeof(TurnState) * max_bunches, bt->stream));
   bt->free_ranges.push_back({0, bt->pool_n});
   for (int s = max_bunches - 1; s >= 0; --s) bt->free_slots.push_back(s);
@@ -277,9 +282,11 @@ extern "C" hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_
   if (chunk_particles < 4 || chunk_particles % 4 || chunk_particles > kMaxBlockParticles)
     return set_err(ctx, HJ_ERR_ARG, "chunk_particles must be a positive multiple of 4, at most %lld",
                    (long long)kMaxBlockParticles);
-  if (layout != -1 && !pass_cfg_valid(layout))
-    return set_err(ctx, HJ_ERR_ARG, "pass layout must be -1 (automatic), 0..%d or 8..%d",
-                   kNumPassCfgs - 1, kPassN32 + kNumPassCfgs - 1);
+  if (!pass_request_valid(layout))
+    return set_err(ctx, HJ_ERR_ARG,
+                   "pass layout must be -1 (automatic), %d (automatic, single-precision normals), "
+                   "0..%d or 8..%d, plus %d for single-precision normals",
+                   kPassAutoFast, kNumPassCfgs - 1, kPassN32 + kNumPassCfgs - 1, kPassFastNormals);
   hj_batch* bt = new hj_batch();
   hj_status s = batch_create_impl(ctx, pool_particles, max_bunches, max_nbins, chunk_particles,
                                   layout, bt);
@@ -288,6 +295,17 @@ extern "C" hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_
     return s;
   }
   *out = bt;
+  return HJ_OK;
+}
+
+extern "C" hj_status hj_batch_set_resident(hj_batch* bt, int32_t on) {
+  if (!bt) return HJ_ERR_ARG;
+  if (bt->graph) {
+    HJ_CUDA(bt->ctx, cudaStreamSynchronize(bt->stream));
+    cudaGraphExecDestroy(bt->graph);
+    bt->graph = nullptr;
+  }
+  bt->resident = on != 0;
   return HJ_OK;
 }
 
@@ -368,6 +386,8 @@ static hj_status batch_add_begin(hj_batch* bt, const double* z, const double* dE
     batch_add_abort(bt, p);
     return s;
   }
+  if (bt->resident_blocks == 0 || bt->wake != wake_on || bt->qe != qe)
+    bt->resident_blocks = ctx->num_sms * batch_blocks_per_sm(bt->max_B, qe, wake_on, bt->cfg);
   bt->wake = wake_on;
   bt->qe = qe;
   *out = p;

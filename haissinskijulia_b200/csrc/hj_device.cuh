@@ -143,21 +143,20 @@ __host__ __device__ inline void philox4x32_10(uint32_t (&c)[4], const PhiloxKeys
 
 // Double-precision Box-Muller transform of the four Philox words of a
 // particle pair, with its logarithm and its sine and cosine evaluated from
-// small tables (NormalTables, hj_host.h):
+// two 128-row tables (NormalTables, hj_host.h):
 //   u1 = (2a + 1) 2^-53 with a the top 52 bits of (x1:x0), so u1 lies in
 //     [2^-53, 1 - 2^-53] exactly; ln u1 by the table-driven method of
 //     P. T. P. Tang (ACM TOMS 16(4), 1990): u1 = 2^e m, m in [1, 2),
-//     ln m = -ln r_j + log1p(m r_j - 1) with r_j ≈ 1/(1 + (j + 1/2)/64) for
-//     the top six bits j of m (|m r_j - 1| < 2^-7), log1p by its Taylor
-//     series through t^8 (truncation below 2e-20), e ln 2 with a two-part ln 2;
-//   θ = 2π w, w in [0, 1) the top 52 bits of (x3:x2): θ = θ_j + t with
-//     θ_j = 2π (j + 1/2)/64 for the top six bits j of w, |t| <= π/64, sin t and
-//     cos t - 1 by their Taylor series through t^9 and t^10 (truncation below
-//     1e-20), then angle addition with the tabulated sin θ_j, cos θ_j;
+//     ln m = -ln r_j + log1p(m r_j - 1) with r_j ≈ 1/(1 + (j + 1/2)/128) for
+//     the top seven bits j of m (|m r_j - 1| < 2^-8), log1p by its Taylor
+//     series through t^6 (truncation below 2e-18), e ln 2 with a two-part ln 2;
+//   θ = 2π w, w in [0, 1) the top 52 bits of (x3:x2): θ = θ_k + t with
+//     θ_k = 2π (k + 1/2)/128 for the top seven bits k of w, |t| <= π/128, sin t
+//     and cos t - 1 by their Taylor series through t^7 and t^8 (truncation
+//     below 1e-20), then angle addition with the tabulated sin θ_k, cos θ_k;
 //   r = sqrt(-2 ln u1) (at most 8.57: the tails are cut only there), and the
 //   normals r cos θ, r sin θ.
-// Each entry point of the transform costs about 30 FP64 operations per pair.
-
+// About 36 FP64 operations per pair.
 __device__ __forceinline__ void box_muller_f64(const uint32_t (&x)[4],
                                                const NormalTables* __restrict__ t,
                                                const double2* __restrict__ lr,
@@ -168,13 +167,11 @@ __device__ __forceinline__ void box_muller_f64(const uint32_t (&x)[4],
   const double u1 = d - 0x1.fffffffffffffp-1;
   const int hi = __double2hiint(u1);
   const int e = (hi >> 20) - 1023;
-  const int j = (hi >> 14) & 63;
+  const int j = (hi >> 13) & 127;
   const double m = __hiloint2double((hi & 0x000FFFFF) | 0x3FF00000, __double2loint(u1));
   const double2 rj = lr[j];
   const double tt = fma(m, rj.x, -1.0);
-  double q = -0.125;                                   // log1p(t) = t q(t)
-  q = fma(q, tt, 1.0 / 7.0);
-  q = fma(q, tt, -1.0 / 6.0);
+  double q = -1.0 / 6.0;                               // log1p(t) = t q(t)
   q = fma(q, tt, 0.2);
   q = fma(q, tt, -0.25);
   q = fma(q, tt, 1.0 / 3.0);
@@ -183,20 +180,20 @@ __device__ __forceinline__ void box_muller_f64(const uint32_t (&x)[4],
   const double ed = (double)e;
   const double ln_u1 = fma(ed, t->ln2_hi, rj.y) + fma(ed, t->ln2_lo, tt * q);
   const double r = sqrt(-2.0 * ln_u1);
-  // θ = 2π (w - (k + 1/2)/64) + θ_k, w = d2 - 1, d2 = 1 + b 2^-52
+  // θ = 2π (w - (k + 1/2)/128) + θ_k, w = d2 - 1, d2 = 1 + b 2^-52; the
+  // sector's centre 1 + (2k + 1)/256 is built from its bits
   const int h2 = (int)(0x3FF00000 | (x[3] >> 12));
   const double d2 = __hiloint2double(h2, (int)((x[3] << 20) | (x[2] >> 12)));
-  const int k = (h2 >> 14) & 63;
-  const double xs = d2 - (1.0 + ((double)k + 0.5) * 0.015625);   // exact, |xs| <= 2^-7
+  const int k = (h2 >> 13) & 127;
+  const double ck = __hiloint2double(0x3FF00000 | ((2 * k + 1) << 12), 0);
+  const double xs = d2 - ck;                           // exact, |xs| <= 2^-8
   const double ang = fma(xs, t->twopi_hi, xs * t->twopi_lo);
   const double a2 = ang * ang;
-  double ps = 2.7557319223985893e-06;                  // 1/9!
-  ps = fma(ps, a2, -1.9841269841269841e-04);           // -1/7!
+  double ps = -1.9841269841269841e-04;                 // -1/7!
   ps = fma(ps, a2, 8.3333333333333333e-03);            // 1/5!
   ps = fma(ps, a2, -1.6666666666666667e-01);           // -1/3!
   const double sn = fma(ang * a2, ps, ang);
-  double pc = -2.7557319223985888e-07;                 // -1/10!
-  pc = fma(pc, a2, 2.4801587301587302e-05);            // 1/8!
+  double pc = 2.4801587301587302e-05;                  // 1/8!
   pc = fma(pc, a2, -1.3888888888888889e-03);           // -1/6!
   pc = fma(pc, a2, 4.1666666666666667e-02);            // 1/4!
   pc = fma(pc, a2, -0.5);
@@ -206,6 +203,32 @@ __device__ __forceinline__ void box_muller_f64(const uint32_t (&x)[4],
   const double cos_th = fma(-skc.x, sn, fma(skc.y, cm1, skc.y));
   out[0] = r * cos_th;
   out[1] = r * sin_th;
+}
+
+// Single-precision Box-Muller transform of words 0 and 1 (the opt-in fast
+// normals of the fused pass): u1 = (x0 + 1/2) 2^-32, θ = 2π ((x1 + 1/2)
+// 2^-32 - 1/2), on the special-function unit (__logf, __sincosf), widened to
+// double.  24-bit uniforms: |normal| <= 6.0 (the tails beyond are cut),
+// relative resolution about 1e-7.
+__device__ __forceinline__ void box_muller_f32(uint32_t x0, uint32_t x1, double out[2]) {
+  const float kScale = 2.3283064365386963e-10f;         // 2^-32
+  const float u1 = fmaf((float)x0, kScale, 0.5f * kScale);
+  const float th = 6.2831853071795865f * fmaf((float)x1, kScale, -0.5f);
+  const float m2l = fmaxf(-2.0f * __logf(u1), 1e-30f);
+  const float rad = m2l * rsqrtf(m2l);
+  float sn, cs;
+  __sincosf(th, &sn, &cs);
+  out[0] = (double)(rad * cs);
+  out[1] = (double)(rad * sn);
+}
+
+// philox_normals2_rk with the single-precision transform of words 0 and 1.
+__device__ __forceinline__ void philox_normals2_fast(const PhiloxKeys& keys, int64_t turn,
+                                                     int64_t p, double out[2]) {
+  uint32_t c[4] = {(uint32_t)p, (uint32_t)((uint64_t)p >> 32), (uint32_t)turn,
+                   (uint32_t)((uint64_t)turn >> 32)};
+  philox4x32_10(c, keys);
+  box_muller_f32(c[0], c[1], out);
 }
 
 // Two standard normals for particles 2p and 2p+1 at `turn` under the round

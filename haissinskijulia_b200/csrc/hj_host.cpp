@@ -180,11 +180,12 @@ void host_twiddles(int64_t P, double* tw_interleaved) {
 void host_normal_tables(NormalTables* t) {
   const long double kPiL = 3.141592653589793238462643383279502884L;
   const long double kLn2L = 0.693147180559945309417232121458176568L;
-  for (int j = 0; j < 64; ++j) {
-    const double r = (double)(1.0L / (1.0L + ((long double)j + 0.5L) / 64.0L));
+  const long double rows = (long double)kNormalTableRows;
+  for (int j = 0; j < kNormalTableRows; ++j) {
+    const double r = (double)(1.0L / (1.0L + ((long double)j + 0.5L) / rows));
     t->lr[j][0] = r;
     t->lr[j][1] = (double)(-logl((long double)r));     // ln m = -ln r + log1p(m r - 1)
-    const long double th = 2.0L * kPiL * ((long double)j + 0.5L) / 64.0L;
+    const long double th = 2.0L * kPiL * ((long double)j + 0.5L) / rows;
     t->sc[j][0] = (double)sinl(th);
     t->sc[j][1] = (double)cosl(th);
   }

@@ -42,7 +42,9 @@ constexpr int kRfTableSize = 128;    // entries of the fused pass's RF kick tabl
 constexpr int kLogHeader = 8;       // doubles before the bin counts in a turn-log record
 
 // Quantum-excitation source of the particle pass.
-enum QeMode { QE_OFF = 0, QE_PHILOX = 1, QE_DRAWS = 2 };
+// QE_PHILOX_FAST: the same Philox words turned into normals in single
+// precision (the kPassFastNormals layouts).
+enum QeMode { QE_OFF = 0, QE_PHILOX = 1, QE_DRAWS = 2, QE_PHILOX_FAST = 3 };
 
 // Arguments of the fused per-turn particle pass (one launch per turn).
 struct PassArgs {
@@ -150,7 +152,10 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
 // and the per-bunch merge of its partials.
 cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
                               const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
-                              int qe, int cfg, cudaStream_t st);
+                              int qe, int cfg, int32_t* d_queue, int resident_blocks,
+                              cudaStream_t st);
+// Blocks of the batched pass that fit on one SM for the batch's largest grid.
+int batch_blocks_per_sm(int max_B, int qe_mode, int use_wake, int cfg);
 cudaError_t launch_sum_parts(const double* part, int nblk, double* out, cudaStream_t st);
 cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const BatchChunk* d_items,
                                 const int32_t* d_n_items, int max_items, int max_B,

@@ -19,6 +19,7 @@ constexpr int64_t kMaxBlockParticles = (1 << 20) - 8;
 constexpr int kNumPassCfgs = 6;       // thread layouts of the fused pass
 constexpr int kPassLayoutMask = 7;    // layout bits of a pass configuration
 constexpr int kPassN32 = 8;           // + one 32-bit NGP counter per bin (else 16-bit pairs)
+constexpr int kPassFastNormals = 16;  // + single-precision quantum-excitation normals
 
 inline int pass_cfg_threads(int cfg) {
   const int l = cfg & kPassLayoutMask;
@@ -34,8 +35,20 @@ inline bool pass_cfg_two_blocks(int cfg) {
   return l == 4 || l == 5;
 }
 inline bool pass_cfg_valid(int cfg) {
-  return cfg >= 0 && (cfg & ~(kPassLayoutMask | kPassN32)) == 0 &&
+  return cfg >= 0 && (cfg & ~(kPassLayoutMask | kPassN32 | kPassFastNormals)) == 0 &&
          (cfg & kPassLayoutMask) < kNumPassCfgs;
+}
+
+// A caller's layout request: -1 = automatic; kPassAutoFast = the automatic
+// layout with single-precision normals; otherwise a valid configuration.
+constexpr int kPassAutoFast = kPassFastNormals | kPassLayoutMask;
+inline bool pass_request_valid(int r) { return r == -1 || r == kPassAutoFast || pass_cfg_valid(r); }
+// The configuration a request gives for bins B, `automatic` being the
+// library's choice for them.
+inline int resolve_pass_request(int r, int automatic) {
+  if (r == -1) return automatic;
+  if (r == kPassAutoFast) return automatic | kPassFastNormals;
+  return r;
 }
 
 // Blocks of the particle pass: enough to fill the GPU, but each block should

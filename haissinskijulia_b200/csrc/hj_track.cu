@@ -443,11 +443,16 @@ __device__ __forceinline__ void stp(double* p, const double v[PPT]) {
 
 // Normals of the PPT particles of pairs pair0, pair0 + 1, ... (one Philox-4x32
 // counter per pair of particles).
-template <int PPT>
+template <int PPT, bool FAST>
 __device__ __forceinline__ void group_normals(const PhiloxKeys& rk, int64_t turn,
                                               int64_t pair0, const NormalTables* t,
                                               const double2* lr, const double2* sc,
                                               double r[PPT]) {
+  if (FAST) {
+    philox_normals2_fast(rk, turn, pair0, r);
+    if (PPT == 4) philox_normals2_fast(rk, turn, pair0 + 1, r + 2);
+    return;
+  }
   philox_normals2_rk(rk, turn, pair0, t, lr, sc, r);
   if (PPT == 4) philox_normals2_rk(rk, turn, pair0 + 1, t, lr, sc, r + 2);
 }
@@ -467,7 +472,7 @@ template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = fal
 __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
                                           unsigned char* smem_raw) {
   // dynamic shared memory: RF table [128] | the normal transform's logarithm
-  // and angle tables [64 + 64] | kick-table window [win] | NGP counters | cell
+  // and angle tables [128 + 128] | kick-table window [win] | NGP counters | cell
   // words lo, hi [B+1]; NGP counters: (B+1)/2 words of two 16-bit counters, or
   // B 32-bit ones (N32)
   const int nc = a.B + 1;                 // kick-table cells
@@ -475,14 +480,14 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
   const int win = WAKE ? a.win : 0;
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
   double2* s_lr = s_rf + kRfTableSize;
-  double2* s_sc = s_lr + 64;
-  double* s_win = reinterpret_cast<double*>(s_sc + 64);
+  double2* s_sc = s_lr + kNormalTableRows;
+  double* s_win = reinterpret_cast<double*>(s_sc + kNormalTableRows);
   uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_win + win);
   uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
   uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
   for (int i = threadIdx.x; i < kRfTableSize; i += THREADS) s_rf[i] = __ldg(a.rf_table + i);
   if (QE == QE_PHILOX)
-    for (int i = threadIdx.x; i < 64; i += THREADS) {
+    for (int i = threadIdx.x; i < kNormalTableRows; i += THREADS) {
       s_lr[i] = reinterpret_cast<const double2*>(g_normal.lr)[i];
       s_sc[i] = reinterpret_cast<const double2*>(g_normal.sc)[i];
     }
@@ -578,9 +583,9 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     }
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
-    if (QE == QE_PHILOX) {
-      group_normals<PPT>(a.philox, turn, (PPT / 2) * q + a.pair_offset, &g_normal, s_lr, s_sc,
-                         rr);
+    if (QE == QE_PHILOX || QE == QE_PHILOX_FAST) {
+      group_normals<PPT, QE == QE_PHILOX_FAST>(a.philox, turn, (PPT / 2) * q + a.pair_offset,
+                                               &g_normal, s_lr, s_sc, rr);
     } else if (QE == QE_DRAWS) {
       if (drow) {
 #pragma unroll
@@ -604,6 +609,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     double r2[2] = {0.0, 0.0};
     if (QE == QE_PHILOX)
       philox_normals2_rk(a.philox, turn, (i >> 1) + a.pair_offset, &g_normal, s_lr, s_sc, r2);
+    if (QE == QE_PHILOX_FAST) philox_normals2_fast(a.philox, turn, (i >> 1) + a.pair_offset, r2);
     double r = r2[i & 1];
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
     double z1[1] = {a.z[i]};
@@ -649,25 +655,44 @@ __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
   pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
 }
 
-// One turn over a batch of bunches: block c takes chunk c of the chunk table
-// (a contiguous run of one bunch's particles) and writes the bunch's partial
-// slot ch.part.  Blocks past the table's length, and chunks of bunches with
-// no turns left, return at once.
+// One turn over a batch of bunches.  Chunk c of the chunk table (a
+// contiguous run of one bunch's particles) is processed by one block into the
+// bunch's partial slot ch.part; chunks of bunches with no turns left are
+// skipped.  Without a queue, block c takes chunk c (blocks past the table's
+// length return at once).  With a queue (the turn's counter, zero at launch),
+// the blocks are resident -- one per SM slot -- and each takes the next
+// chunk index from the counter until the table is exhausted.  Either way a
+// chunk's arithmetic and slot do not depend on the block that takes it.
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_batch_pass(const PassArgs* __restrict__ bunches, const BatchChunk* __restrict__ chunks,
-                 const int32_t* __restrict__ n_chunks) {
+                 const int32_t* __restrict__ n_chunks, int32_t* queue) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  if ((int)blockIdx.x >= *n_chunks) return;
-  const BatchChunk ch = chunks[blockIdx.x];
-  const PassArgs a = bunches[ch.bunch];
-  if (a.ts->turns_left <= 0) return;
-  if (WAKE && ch.part == 0) {  // zero the merged histograms k_batch_reduce adds into
-    for (int i = threadIdx.x; i < 3 * a.B + 2; i += THREADS) a.hist_out[i] = 0ull;
+  __shared__ int s_chunk;
+  const int nch = *n_chunks;
+  int c = (int)blockIdx.x;
+  if (queue) {
+    if (threadIdx.x == 0) s_chunk = atomicAdd(queue, 1);
+    __syncthreads();
+    c = s_chunk;
   }
-  const PassRange rg{ch.first / PPT, THREADS, (ch.first + ch.count) / PPT, ch.part,
-                     ch.first + ch.count == a.n};
-  pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
+  while (c < nch) {
+    const BatchChunk ch = chunks[c];
+    const PassArgs a = bunches[ch.bunch];
+    if (a.ts->turns_left > 0) {
+      if (WAKE && ch.part == 0) {  // zero the merged histograms k_batch_reduce adds into
+        for (int i = threadIdx.x; i < 3 * a.B + 2; i += THREADS) a.hist_out[i] = 0ull;
+      }
+      const PassRange rg{ch.first / PPT, THREADS, (ch.first + ch.count) / PPT, ch.part,
+                         ch.first + ch.count == a.n};
+      pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
+    }
+    if (!queue) break;
+    __syncthreads();                   // the chunk's shared memory is read no more
+    if (threadIdx.x == 0) s_chunk = atomicAdd(queue, 1);
+    __syncthreads();
+    c = s_chunk;
+  }
 }
 
 // Merge of the per-block histograms.  Grid (bins/256, G): block column g sums
@@ -1049,7 +1074,9 @@ const void* pass_fn_wq(int cfg) {
 template <bool W>
 const void* pass_fn_w(int qe, int cfg) {
   switch (qe) {
-    case QE_PHILOX: return pass_fn_wq<W, QE_PHILOX>(cfg);
+    case QE_PHILOX:
+      return (cfg & kPassFastNormals) ? pass_fn_wq<W, QE_PHILOX_FAST>(cfg)
+                                      : pass_fn_wq<W, QE_PHILOX>(cfg);
     case QE_DRAWS: return pass_fn_wq<W, QE_DRAWS>(cfg);
     default: return pass_fn_wq<W, QE_OFF>(cfg);
   }
@@ -1078,9 +1105,15 @@ const void* batch_fn_wq(int cfg) {
 }
 
 // Batches draw QE normals on the device or not at all (no host-fed draws).
+template <bool W>
+const void* batch_fn_w(int qe, int cfg) {
+  if (qe != QE_PHILOX) return batch_fn_wq<W, QE_OFF>(cfg);
+  return (cfg & kPassFastNormals) ? batch_fn_wq<W, QE_PHILOX_FAST>(cfg)
+                                  : batch_fn_wq<W, QE_PHILOX>(cfg);
+}
+
 const void* batch_fn(int wake, int qe, int cfg) {
-  if (wake) return qe == QE_PHILOX ? batch_fn_wq<true, QE_PHILOX>(cfg) : batch_fn_wq<true, QE_OFF>(cfg);
-  return qe == QE_PHILOX ? batch_fn_wq<false, QE_PHILOX>(cfg) : batch_fn_wq<false, QE_OFF>(cfg);
+  return wake ? batch_fn_w<true>(qe, cfg) : batch_fn_w<false>(qe, cfg);
 }
 }  // namespace
 
@@ -1089,15 +1122,20 @@ namespace {
 constexpr int kWindowMinBins = 4096;
 
 // The normal transform's logarithm and angle tables in shared memory.
-constexpr size_t kNormalSmemBytes = 128 * sizeof(double2);
+constexpr size_t kNormalSmemBytes = 2 * kNormalTableRows * sizeof(double2);
 
 // Dynamic shared memory one block of the pass may take: the device's opt-in
 // limit (set when the kernels are prepared), or per block of the layout that
 // keeps two blocks on an SM (228 KB per SM, 1 KB reserved per block).
 int g_pass_smem_limit = 227 * 1024;
 
+// Static shared memory the pass kernels declare beside the dynamic part (the
+// batched pass's chunk index and the reduction's alignment), kept out of the
+// dynamic budget.
+constexpr size_t kPassStaticSmem = 256;
+
 size_t pass_smem_budget(int cfg) {
-  const size_t lim = (size_t)g_pass_smem_limit;
+  const size_t lim = (size_t)g_pass_smem_limit - kPassStaticSmem;
   return pass_cfg_two_blocks(cfg) ? std::min(lim, (size_t)(113 * 1024)) : lim;
 }
 
@@ -1121,12 +1159,14 @@ cudaError_t prepare_track_kernels(int max_smem) {
   for (int w = 0; w < 2; ++w)
     for (int q = 0; q < 3; ++q)
       for (int n = 0; n < 2; ++n)
-        for (int l = 0; l < kNumPassCfgs; ++l) {
-          const int c = l | (n ? kPassN32 : 0);
-          cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
-          if (e == cudaSuccess && q != QE_DRAWS) e = allow_dynamic_smem(batch_fn(w, q, c), max_smem);
-          if (e != cudaSuccess) return e;
-        }
+        for (int f = 0; f < 2; ++f)
+          for (int l = 0; l < kNumPassCfgs; ++l) {
+            const int c = l | (n ? kPassN32 : 0) | (f ? kPassFastNormals : 0);
+            cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
+            if (e == cudaSuccess && q != QE_DRAWS)
+              e = allow_dynamic_smem(batch_fn(w, q, c), max_smem);
+            if (e != cudaSuccess) return e;
+          }
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
 }
 
@@ -1165,12 +1205,28 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
 
 cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
                               const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
-                              int qe, int cfg, cudaStream_t st) {
+                              int qe, int cfg, int32_t* d_queue, int resident_blocks,
+                              cudaStream_t st) {
   const size_t smem = track_smem_bytes(max_B, wake, cfg);
   void* args[] = {const_cast<PassArgs**>(&d_bunches), const_cast<BatchChunk**>(&d_chunks),
-                  const_cast<int32_t**>(&d_n_chunks)};
-  return cudaLaunchKernel(batch_fn(wake, qe, cfg), dim3(max_chunks > 0 ? max_chunks : 1),
-                          dim3(pass_cfg_threads(cfg)), args, smem, st);
+                  const_cast<int32_t**>(&d_n_chunks), &d_queue};
+  int grid = max_chunks > 0 ? max_chunks : 1;
+  if (d_queue) {
+    cudaError_t e = cudaMemsetAsync(d_queue, 0, sizeof(int32_t), st);
+    if (e != cudaSuccess) return e;
+    grid = std::max(1, std::min(grid, resident_blocks));
+  }
+  return cudaLaunchKernel(batch_fn(wake, qe, cfg), dim3(grid), dim3(pass_cfg_threads(cfg)), args,
+                          smem, st);
+}
+
+int batch_blocks_per_sm(int max_B, int qe_mode, int use_wake, int cfg) {
+  const size_t smem = track_smem_bytes(max_B, use_wake, cfg);
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_fn(use_wake, qe_mode, cfg),
+                                                    pass_cfg_threads(cfg), smem) != cudaSuccess)
+    bps = 1;
+  return bps < 1 ? 1 : bps;
 }
 
 // Fixed-order sum of nblk per-block sum vectors into out[kNumSums] (one block).

@@ -117,6 +117,7 @@ class Tuning:
     chunk: int = 65536
     layout: int = -1
     graph_turns: int = 16
+    resident: bool = True       # resident blocks on a chunk queue, or one block per chunk
 
 
 def run_batched(ctx: Context, points: List[Point], *, pool_particles: Optional[int] = None,
@@ -129,7 +130,7 @@ def run_batched(ctx: Context, points: List[Point], *, pool_particles: Optional[i
     pool = pool_particles or sum(p.n + 4 for p in points)
     slots = max_bunches or len(points)
     bt = Batch(ctx, pool, slots, max_b, chunk=tuning.chunk, layout=tuning.layout,
-               graph_turns=tuning.graph_turns)
+               graph_turns=tuning.graph_turns, resident=tuning.resident)
     pending = list(range(len(points)))
     live: Dict[int, int] = {}
     out: List[Optional[Solve]] = [None] * len(points)
@@ -266,7 +267,7 @@ def serve(ctx: Context, requests: List[Point], *, memory_budget: int = 8 << 30,
     between turn blocks and their slots reused.  Latency = finish - arrival."""
     pool = memory_budget // 16
     bt = Batch(ctx, pool, max_bunches, max_nbins, chunk=tuning.chunk, layout=tuning.layout,
-               graph_turns=tuning.graph_turns)
+               graph_turns=tuning.graph_turns, resident=tuning.resident)
     waiting = list(range(len(requests)))
     live: Dict[int, int] = {}
     used = 0
@@ -343,7 +344,8 @@ def time_batch_turns(ctx: Context, points: List[Point], turns: int, tuning: Tuni
     """Seconds per turn of all `points` live in one Batch (after a warm-up of
     one graph block); the points are given enough turns not to finish."""
     bt = Batch(ctx, sum(p.n + 4 for p in points), len(points), max(p.nbins for p in points),
-               chunk=tuning.chunk, layout=tuning.layout, graph_turns=tuning.graph_turns)
+               chunk=tuning.chunk, layout=tuning.layout, graph_turns=tuning.graph_turns,
+               resident=tuning.resident)
     try:
         for p in points:
             cfg = p.ring()
@@ -366,7 +368,8 @@ if __name__ == "__main__":
     ap.add_argument("--chunk", type=int, default=65536)
     ap.add_argument("--layout", type=int, default=-1)
     ap.add_argument("--graph-turns", type=int, default=8)
+    ap.add_argument("--resident", type=int, default=1)
     args = ap.parse_args()
     s = time_batch_turns(Context(0), sweep_points(256), args.turns,
-                         Tuning(args.chunk, args.layout, args.graph_turns))
+                         Tuning(args.chunk, args.layout, args.graph_turns, bool(args.resident)))
     print(f"{s * 1e3:.3f} ms per batched turn of the 256-point sweep")

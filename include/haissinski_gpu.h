@@ -156,11 +156,15 @@ hj_status hj_trim(hj_ctx* ctx);
  * thread x 512 threads, 1 = 2 x 1024, 2 = 2 x 768 (each with the next group
  * prefetched), 3 = 2 x 512 without prefetch, 4 = 2 x 512 with prefetch at
  * two blocks per SM, 5 = 4 x 256 with prefetch at two blocks per SM; plus 8
- * (8..13): the same layout with one 32-bit
- * shared-memory counter per bin instead of two 16-bit ones per word (more
- * shared memory, no overflow check; the default up to 8192 bins).  Results do
- * not depend on the layout beyond floating-point summation order; bin counts
- * are the same.  No reference counterpart. */
+ * (8..13): the same layout with one 32-bit shared-memory counter per bin
+ * instead of two 16-bit ones per word (more shared memory, no overflow
+ * check; the default).  Plus 16 (16..29, or 23 for the library's choice):
+ * the quantum-excitation normals of the fused pass are formed in single
+ * precision (Philox words 0-1, 24-bit uniforms, tails cut at 6σ, about 25 %
+ * faster per pass) instead of the default double-precision transform;
+ * hj_gaussian and the single-step kernels stay in double precision.  Results
+ * do not depend on the layout beyond floating-point summation order (and the
+ * normals' precision); bin counts are the same.  No reference counterpart. */
 hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout);
 
 /* ---------------------------------------------------------------- set-up helpers */
@@ -348,6 +352,13 @@ hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunch
                           int32_t max_nbins, int64_t chunk_particles, int32_t layout,
                           hj_batch** out);
 void hj_batch_destroy(hj_batch* bt);
+/* The batched pass's launch: on != 0 (the default) runs resident blocks, one
+ * per SM slot, that take chunks of the chunk table from a device-side queue
+ * (an atomic counter reset every turn) until the table is exhausted -- one
+ * persistent launch per turn over the ragged table; 0 launches one block per
+ * chunk.  Results are the same either way (a chunk's slot and arithmetic do
+ * not depend on its block).  No reference counterpart. */
+hj_status hj_batch_set_resident(hj_batch* bt, int32_t on);
 /* Turns per captured CUDA graph (0 = launch every turn directly; default 16). */
 hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns);
 /* Admit a bunch: z, dE (host or device, n each) are copied into the pool;
@@ -505,11 +516,11 @@ hj_status hj_correlation(hj_ctx* ctx, const double* d_x, const double* d_y, int6
 hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64_t n, double* out);
 
 /* The tables of that transform, for restatements of it (no reference
- * counterpart; host only, no context): out[HJ_NORMAL_TABLES_SIZE] = 64
- * pairs (r_j, -ln r_j) of the table-driven logarithm, 64 pairs (sin θ_j,
+ * counterpart; host only, no context): out[HJ_NORMAL_TABLES_SIZE] = 128
+ * pairs (r_j, -ln r_j) of the table-driven logarithm, 128 pairs (sin θ_j,
  * cos θ_j) of the angle reduction, ln 2 (high part, rest) and 2π (double,
  * rest).  cap < HJ_NORMAL_TABLES_SIZE is HJ_ERR_ARG. */
-#define HJ_NORMAL_TABLES_SIZE 260
+#define HJ_NORMAL_TABLES_SIZE 516
 hj_status hj_normal_tables(double* out, int64_t cap);
 
 #ifdef __cplusplus

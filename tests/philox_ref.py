@@ -37,11 +37,11 @@ def normal_tables() -> dict:
     """The transform's tables as the library builds them (hj_normal_tables,
     host only)."""
     from haissinskijulia_b200 import _lib
-    out = np.zeros(260)
-    rc = _lib.load().hj_normal_tables(out.ctypes.data_as(_lib.POINTER(_lib.c_double)), 260)
+    out = np.zeros(516)
+    rc = _lib.load().hj_normal_tables(out.ctypes.data_as(_lib.POINTER(_lib.c_double)), 516)
     assert rc == 0
-    return {"lr": out[0:128].reshape(64, 2), "sc": out[128:256].reshape(64, 2),
-            "ln2_hi": out[256], "ln2_lo": out[257], "twopi_hi": out[258], "twopi_lo": out[259]}
+    return {"lr": out[0:256].reshape(128, 2), "sc": out[256:512].reshape(128, 2),
+            "ln2_hi": out[512], "ln2_lo": out[513], "twopi_hi": out[514], "twopi_lo": out[515]}
 
 
 def uniforms(x0, x1, x2, x3):
@@ -65,4 +65,21 @@ def philox_normals_reference(seed: int, turn: int, n: int, first_pair: int = 0) 
     out = np.empty((npairs, 2))
     out[:, 0] = rad * np.cos(2.0 * np.pi * w)
     out[:, 1] = rad * np.sin(2.0 * np.pi * w)
+    return out.reshape(-1)[:n]
+
+
+def fast_normals_reference(seed: int, turn: int, n: int, first_pair: int = 0) -> np.ndarray:
+    """The opt-in single-precision normals of the fused pass (the layouts with
+    16 added): Philox words 0 and 1 of the pair, u1 = (x0 + 1/2) 2^-32,
+    θ = 2π ((x1 + 1/2) 2^-32 - 1/2), evaluated here in double precision (the
+    device evaluates the transform in single precision)."""
+    npairs = (n + 1) // 2
+    p = np.arange(first_pair, first_pair + npairs, dtype=np.uint64)
+    x0, x1, _, _ = philox_words(seed, turn, p)
+    u1 = (x0.astype(np.float32) * np.float32(2.0 ** -32) + np.float32(2.0 ** -33)).astype(np.float64)
+    th = 2.0 * np.pi * (x1.astype(np.float64) * 2.0 ** -32 - 0.5)
+    rad = np.sqrt(-2.0 * np.log(u1))
+    out = np.empty((npairs, 2))
+    out[:, 0] = rad * np.cos(th)
+    out[:, 1] = rad * np.sin(th)
     return out.reshape(-1)[:n]

@@ -227,3 +227,23 @@ def test_closing_the_context_first_leaves_its_bunches_working(gpu_ctx):
     got = bt.take(bid)
     bt.close()                          # the last object: frees the context
     _check(got, want, cfg, "batch after close")
+
+
+def test_resident_queue_and_one_block_per_chunk_agree_bit_for_bit(gpu_ctx):
+    """The resident pass (blocks taking chunks from a device-side queue) and
+    one block per chunk give the same results: a chunk's slot and arithmetic
+    do not depend on the block that takes it."""
+    out = []
+    for resident in (True, False):
+        bt = Batch(gpu_ctx, 400_000, 6, 2048, chunk=16384, graph_turns=4, resident=resident)
+        ids = []
+        for i in range(5):
+            cfg, z, dE, nbins, seed = _spec(i)
+            ids.append(bt.add(z, dE, cfg.params, nbins, wake=cfg.wake, seed=seed, turns=21))
+        bt.advance(21)
+        assert sorted(bt.poll()) == sorted(ids)
+        out.append([bt.take(b) for b in ids])
+        bt.close()
+    for (za, ea, ra), (zb, eb, rb) in zip(*out):
+        assert np.array_equal(za, zb) and np.array_equal(ea, eb)
+        assert (ra.E0, ra.sigma_E, ra.sigma_z) == (rb.E0, rb.sigma_E, rb.sigma_z)

@@ -1,7 +1,8 @@
 """Statistical parity with on-device random numbers.
 
-The fused pass draws its quantum-excitation normals from Philox-2x32-10 on
-the device; the oracle draws its own (splitmix64 counter hash + Box-Muller).
+The fused pass draws its quantum-excitation normals from Philox-4x32-10 on
+the device (double precision by default, single precision in the opt-in
+layouts); the oracle draws its own (splitmix64 counter hash + Box-Muller).
 The streams differ, so per-particle parity is impossible; instead both run the
 same 20 seeded bunches through the damping-to-equilibrium and their ensemble
 means of centroid, σ_z, σ_E and the coarse line density must agree within 3
@@ -38,8 +39,14 @@ def _observables(z, dE, edges):
     return np.concatenate([[z.mean(), z.std(), dE.std(), dE.mean()], dens])
 
 
-def test_ensemble_moments_and_line_density_match_the_oracle(gpu_ctx):
+@pytest.mark.parametrize("layout", [-1, 23])
+def test_ensemble_moments_and_line_density_match_the_oracle(layout):
+    """-1: the default double-precision normals; 23: the opt-in
+    single-precision ones."""
+    from haissinskijulia_b200 import Context
     from oracle import Oracle
+    gpu_ctx = Context(0)
+    gpu_ctx.set_pass_layout(layout)
     orc = Oracle(threads=os.cpu_count() or 1)
     cfg = _ring()
     grid = BinGrid.make(cfg.sigma_z, NBINS, cfg.wake.half_width_sigmas)

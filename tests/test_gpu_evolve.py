@@ -284,10 +284,10 @@ def test_invalid_pass_layouts_are_refused(gpu_ctx):
     from haissinskijulia_b200 import Context, HaissinskiError
     from haissinskijulia_b200 import _lib
     ctx = Context(0)
-    for bad in (-2, 6, 7, 14, 16, 24):
+    for bad in (-2, 6, 7, 14, 15, 22, 30, 32):
         with pytest.raises(HaissinskiError) as e:
             ctx.set_pass_layout(bad)
         assert e.value.status == _lib.HJ_ERR_ARG
-    for good in (-1, 0, 4, 5, 8, 12, 13):
+    for good in (-1, 0, 4, 5, 8, 12, 13, 16, 23, 24, 29):
         ctx.set_pass_layout(good)
     ctx.close()

@@ -62,7 +62,7 @@ def test_block_deposits_stay_within_the_cell_counter(driver):
     sizes = [1, 2, 3, 4, 5, 31, 33, 1000, 4096, 10**5, 10**6, 10**8, 148 * 2**20,
              2 * 10**9, 2**32 + 65_538, 2**33 + 7, 10**10]
     sizes += [rng.randrange(1, 2 * 10**10) for _ in range(300)]
-    layouts = [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13]
+    layouts = [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 16, 21, 24, 29]
     cases = [(n, B, 148, bps, c) for n in sizes for B in (64, 4096, 16384)
              for bps in (1, 2) for c in layouts]
     kmax, lines = _run(driver, cases)
@@ -76,5 +76,5 @@ def test_block_deposits_stay_within_the_cell_counter(driver):
 
 
 def test_invalid_layouts(driver):
-    _, lines = _run(driver, [(1000, 64, 148, 1, c) for c in (-2, 6, 7, 14, 15, 16, 24)])
-    assert lines == ["invalid"] * 7
+    _, lines = _run(driver, [(1000, 64, 148, 1, c) for c in (-2, 6, 7, 14, 15, 22, 23, 32)])
+    assert lines == ["invalid"] * 8
