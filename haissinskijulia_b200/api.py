@@ -684,7 +684,7 @@ class Batch:
 
     def __init__(self, ctx: Context, pool_particles: int, max_bunches: int, max_nbins: int,
                  chunk: int = 65536, layout: int = -1, graph_turns: int = 16,
-                 resident: bool = True):
+                 resident: bool = False):
         self.ctx = ctx
         h = ctypes.c_void_p()
         _check(ctx, ctx._lib.hj_batch_create(ctx.handle, int(pool_particles), int(max_bunches),
@@ -694,12 +694,12 @@ class Batch:
         self.sizes = {}
         if graph_turns != 16:
             self.set_graph_turns(graph_turns)
-        if not resident:
-            self.set_resident(False)
+        if resident:
+            self.set_resident(True)
 
     def set_resident(self, on: bool) -> None:
-        """Resident blocks on a device-side chunk queue (True, the default) or
-        one block per chunk (hj_batch_set_resident)."""
+        """Resident blocks on a device-side chunk queue (True) or one block per
+        chunk (False, the default; hj_batch_set_resident)."""
         _check(self.ctx, self.ctx._lib.hj_batch_set_resident(self.handle, int(bool(on))))
 
     def set_graph_turns(self, turns: int) -> None:

@@ -50,7 +50,7 @@ struct hj_batch {
   BatchChunk* d_items = nullptr;               // merge table: groups of a bunch's partial slots
   int32_t* d_counts = nullptr;                 // [0] chunks, [1] bunches, [2] merge items,
                                                // [3] the resident pass's chunk queue
-  bool resident = true;                        // the pass: resident blocks on a chunk queue
+  bool resident = false;                       // the pass: resident blocks on a chunk queue
   int resident_blocks = 0;                     // their number (SMs x blocks per SM)
   PassArgs* h_pass = nullptr;                  // pinned staging
   BinsArgs* h_bins = nullptr;

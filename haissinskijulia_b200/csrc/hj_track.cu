@@ -658,12 +658,16 @@ __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
 // One turn over a batch of bunches.  Chunk c of the chunk table (a
 // contiguous run of one bunch's particles) is processed by one block into the
 // bunch's partial slot ch.part; chunks of bunches with no turns left are
-// skipped.  Without a queue, block c takes chunk c (blocks past the table's
-// length return at once).  With a queue (the turn's counter, zero at launch),
+// skipped.  Without QUEUE, block c takes chunk c (blocks past the table's
+// length return at once).  With QUEUE (the turn's counter, zero at launch),
 // the blocks are resident -- one per SM slot -- and each takes the next
 // chunk index from the counter until the table is exhausted.  Either way a
-// chunk's arithmetic and slot do not depend on the block that takes it.
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false>
+// chunk's arithmetic and slot do not depend on the block that takes it.  The
+// two are separate instantiations: around the inlined pass body the loop of
+// the queued form costs about 300 bytes of register spills per thread
+// (ptxas, 4 x 512 layout), which the one-chunk form does not pay.
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false,
+          bool QUEUE = false>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_batch_pass(const PassArgs* __restrict__ bunches, const BatchChunk* __restrict__ chunks,
                  const int32_t* __restrict__ n_chunks, int32_t* queue) {
@@ -671,7 +675,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
   __shared__ int s_chunk;
   const int nch = *n_chunks;
   int c = (int)blockIdx.x;
-  if (queue) {
+  if (QUEUE) {
     if (threadIdx.x == 0) s_chunk = atomicAdd(queue, 1);
     __syncthreads();
     c = s_chunk;
@@ -687,7 +691,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
                          ch.first + ch.count == a.n};
       pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
     }
-    if (!queue) break;
+    if (!QUEUE) break;
     __syncthreads();                   // the chunk's shared memory is read no more
     if (threadIdx.x == 0) s_chunk = atomicAdd(queue, 1);
     __syncthreads();
@@ -1086,34 +1090,37 @@ const void* pass_fn(int wake, int qe, int cfg) {
   return wake ? pass_fn_w<true>(qe, cfg) : pass_fn_w<false>(qe, cfg);
 }
 
-template <bool W, int Q, bool N>
-const void* batch_fn_wqn(int layout) {
+template <bool W, int Q, bool N, bool U>
+const void* batch_fn_wqnu(int layout) {
   switch (layout) {
-    case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true, 1, N>;
-    case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true, 1, N>;
-    case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true, 1, N>;
-    case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2, N>;
-    case 5: return (const void*)k_batch_pass<W, Q, 4, 256, true, 2, N>;
-    default: return (const void*)k_batch_pass<W, Q, 2, 512, false, 1, N>;
+    case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true, 1, N, U>;
+    case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true, 1, N, U>;
+    case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true, 1, N, U>;
+    case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2, N, U>;
+    case 5: return (const void*)k_batch_pass<W, Q, 4, 256, true, 2, N, U>;
+    default: return (const void*)k_batch_pass<W, Q, 2, 512, false, 1, N, U>;
   }
 }
 
-template <bool W, int Q>
-const void* batch_fn_wq(int cfg) {
-  if (W && (cfg & kPassN32)) return batch_fn_wqn<W, Q, true>(cfg & kPassLayoutMask);
-  return batch_fn_wqn<W, Q, false>(cfg & kPassLayoutMask);
+template <bool W, int Q, bool U>
+const void* batch_fn_wqu(int cfg) {
+  if (W && (cfg & kPassN32)) return batch_fn_wqnu<W, Q, true, U>(cfg & kPassLayoutMask);
+  return batch_fn_wqnu<W, Q, false, U>(cfg & kPassLayoutMask);
 }
 
 // Batches draw QE normals on the device or not at all (no host-fed draws).
-template <bool W>
-const void* batch_fn_w(int qe, int cfg) {
-  if (qe != QE_PHILOX) return batch_fn_wq<W, QE_OFF>(cfg);
-  return (cfg & kPassFastNormals) ? batch_fn_wq<W, QE_PHILOX_FAST>(cfg)
-                                  : batch_fn_wq<W, QE_PHILOX>(cfg);
+template <bool W, bool U>
+const void* batch_fn_wu(int qe, int cfg) {
+  if (qe != QE_PHILOX) return batch_fn_wqu<W, QE_OFF, U>(cfg);
+  return (cfg & kPassFastNormals) ? batch_fn_wqu<W, QE_PHILOX_FAST, U>(cfg)
+                                  : batch_fn_wqu<W, QE_PHILOX, U>(cfg);
 }
 
-const void* batch_fn(int wake, int qe, int cfg) {
-  return wake ? batch_fn_w<true>(qe, cfg) : batch_fn_w<false>(qe, cfg);
+// The batched pass for (wake, excitation mode, configuration), one block per
+// chunk or resident blocks on a chunk queue.
+const void* batch_fn(int wake, int qe, int cfg, bool queue) {
+  if (queue) return wake ? batch_fn_wu<true, true>(qe, cfg) : batch_fn_wu<false, true>(qe, cfg);
+  return wake ? batch_fn_wu<true, false>(qe, cfg) : batch_fn_wu<false, false>(qe, cfg);
 }
 }  // namespace
 
@@ -1163,8 +1170,8 @@ cudaError_t prepare_track_kernels(int max_smem) {
           for (int l = 0; l < kNumPassCfgs; ++l) {
             const int c = l | (n ? kPassN32 : 0) | (f ? kPassFastNormals : 0);
             cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
-            if (e == cudaSuccess && q != QE_DRAWS)
-              e = allow_dynamic_smem(batch_fn(w, q, c), max_smem);
+            for (int u = 0; u < 2 && e == cudaSuccess && q != QE_DRAWS; ++u)
+              e = allow_dynamic_smem(batch_fn(w, q, c, u != 0), max_smem);
             if (e != cudaSuccess) return e;
           }
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
@@ -1216,14 +1223,14 @@ cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chu
     if (e != cudaSuccess) return e;
     grid = std::max(1, std::min(grid, resident_blocks));
   }
-  return cudaLaunchKernel(batch_fn(wake, qe, cfg), dim3(grid), dim3(pass_cfg_threads(cfg)), args,
-                          smem, st);
+  return cudaLaunchKernel(batch_fn(wake, qe, cfg, d_queue != nullptr), dim3(grid),
+                          dim3(pass_cfg_threads(cfg)), args, smem, st);
 }
 
 int batch_blocks_per_sm(int max_B, int qe_mode, int use_wake, int cfg) {
   const size_t smem = track_smem_bytes(max_B, use_wake, cfg);
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_fn(use_wake, qe_mode, cfg),
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_fn(use_wake, qe_mode, cfg, true),
                                                     pass_cfg_threads(cfg), smem) != cudaSuccess)
     bps = 1;
   return bps < 1 ? 1 : bps;

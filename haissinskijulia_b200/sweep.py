@@ -117,7 +117,7 @@ class Tuning:
     chunk: int = 65536
     layout: int = -1
     graph_turns: int = 16
-    resident: bool = True       # resident blocks on a chunk queue, or one block per chunk
+    resident: bool = False      # resident blocks on a chunk queue, or one block per chunk
 
 
 def run_batched(ctx: Context, points: List[Point], *, pool_particles: Optional[int] = None,
@@ -368,7 +368,7 @@ if __name__ == "__main__":
     ap.add_argument("--chunk", type=int, default=65536)
     ap.add_argument("--layout", type=int, default=-1)
     ap.add_argument("--graph-turns", type=int, default=8)
-    ap.add_argument("--resident", type=int, default=1)
+    ap.add_argument("--resident", type=int, default=0)
     args = ap.parse_args()
     s = time_batch_turns(Context(0), sweep_points(256), args.turns,
                          Tuning(args.chunk, args.layout, args.graph_turns, bool(args.resident)))

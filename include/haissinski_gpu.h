@@ -352,12 +352,14 @@ hj_status hj_batch_create(hj_ctx* ctx, int64_t pool_particles, int32_t max_bunch
                           int32_t max_nbins, int64_t chunk_particles, int32_t layout,
                           hj_batch** out);
 void hj_batch_destroy(hj_batch* bt);
-/* The batched pass's launch: on != 0 (the default) runs resident blocks, one
- * per SM slot, that take chunks of the chunk table from a device-side queue
- * (an atomic counter reset every turn) until the table is exhausted -- one
- * persistent launch per turn over the ragged table; 0 launches one block per
- * chunk.  Results are the same either way (a chunk's slot and arithmetic do
- * not depend on its block).  No reference counterpart. */
+/* The batched pass's launch: on != 0 runs resident blocks, one per SM slot,
+ * that take chunks of the chunk table from a device-side queue (an atomic
+ * counter reset every turn) until the table is exhausted -- one persistent
+ * launch per turn over the ragged table; 0 (the default) launches one block
+ * per chunk, which the hardware scheduler hands out to free SMs as well and
+ * which compiles without the queue loop's register spills.  Results are the
+ * same either way (a chunk's slot and arithmetic do not depend on its
+ * block).  No reference counterpart. */
 hj_status hj_batch_set_resident(hj_batch* bt, int32_t on);
 /* Turns per captured CUDA graph (0 = launch every turn directly; default 16). */
 hj_status hj_batch_set_graph_turns(hj_batch* bt, int32_t turns);
