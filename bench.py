@@ -55,6 +55,9 @@ def parse_args():
     ap.add_argument("--multi", choices=["shard", "replicas"], default="shard",
                     help="N > 1: one bunch sharded over the ranks with one all-reduce of the "
                          "bin exchange per turn (default), or independent replicas")
+    ap.add_argument("--shard-one-rank", action="store_true",
+                    help="under torchrun with one rank: run the sharded arm (N > 1) over a "
+                         "one-rank NCCL group, so that its code path runs on one GPU")
     ap.add_argument("--plan-only", action="store_true",
                     help="print the ranks' shard plan (rank 0) and exit; no GPU work")
     ap.add_argument("--layout", type=int, default=-1,
@@ -86,12 +89,13 @@ def parse_args():
     return ap.parse_args()
 
 
-def workload(n: int, B: int, turns_per_step: int = LOG_EVERY) -> dict:
+def workload(n: int, B: int, turns_per_step: int = LOG_EVERY, logged: bool = True) -> dict:
     return {
         "workload": f"plain single bunch at scale: {n:.0e} Float64 macroparticles, {B} bins, "
                     "4 GeV benchmark ring, resonator wake (Rs=10kOhm, Q=1, fr=20GHz, 1e10 e-), "
-                    "RF+QE(Philox)+SR+drift+wake+E0 update every turn; moments and line density "
-                    "logged on the device every 100 turns",
+                    "RF+QE(Philox)+SR+drift+wake+E0 update every turn"
+                    + ("; moments and line density logged on the device every 100 turns"
+                       if logged else ""),
         "particles": n,
         "nbins": B,
         "turns_per_step": turns_per_step,
@@ -592,7 +596,8 @@ def run_sharded(args, ctx, cfg, stream, rank, world, local, clocks) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload(plan["n_global"], B, tps), parallelism=f"shard{world}",
+            "config": dict(workload(plan["n_global"], B, tps, logged=False),
+                           parallelism=f"shard{world}",
                            particles_per_rank=n,
                            exchange="per turn: NCCL SUM all-reduce of the 3B+2 u64 bin "
                                     "exchange and of the 4 double sums (replaces the "
@@ -620,7 +625,8 @@ def run_ours(args) -> None:
     if world != args.gpus:
         raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     torch.cuda.set_device(local)
-    if world > 1:
+    sharded = args.multi == "shard" and (world > 1 or args.shard_one_rank)
+    if world > 1 or sharded:
         import datetime
         os.environ.setdefault("NCCL_DEBUG", "INFO")     # init lines show the rank count
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
@@ -637,7 +643,7 @@ def run_ours(args) -> None:
     ctx = Context(local)
     ctx.set_pass_layout(args.layout)
     stream = torch.cuda.current_stream()
-    if world > 1 and args.multi == "shard":
+    if sharded:
         clocks = ClockSampler(local)
         clocks.start()
         run_sharded(args, ctx, cfg, stream, rank, world, local, clocks)
