@@ -200,7 +200,7 @@ def wave_chunks(points: List[Point], num_sms: int, waves=(1, 2, 4)) -> List[int]
 
 
 def autotune(ctx: Context, points: List[Point], *, trial_turns: int = 64,
-             chunks=None, layouts=(0, 1, 8, 9), graph_turns=(8, 32),
+             chunks=None, layouts=(8, 9, 13), graph_turns=(8, 32),
              sample: int = 64) -> Tuning:
     """Times each candidate (particles per block, pass layout, graph turns) on
     up to `sample` of the points for `trial_turns` turns after a warm-up and
