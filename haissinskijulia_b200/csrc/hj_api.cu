@@ -489,9 +489,6 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
     const size_t o_ts = c.add<TurnState>(1);
     const size_t o_sum = c.add<double>((size_t)kNumSums * nb);
     const size_t o_rf = c.add<double2>(kRfTableSize);
-    // queues of the particles whose Float64 normal takes the slow path
-    const bool defer = b->qe_mode == QE_PHILOX && !(b->cfg & kPassFastNormals);
-    const size_t o_dq = defer ? c.add<DeferEntry>(nb * (size_t)pass_defer_entries(b->cfg)) : 0;
     size_t o[6] = {};
     if (b->use_wake) {
       // pot, potd, hist and ngp_ovf are adjacent: one memset zeroes them
@@ -509,7 +506,6 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
     b->ts = (TurnState*)(a + o_ts);
     b->part_sum = (double*)(a + o_sum);
     b->rf_table = (double2*)(a + o_rf);
-    b->defer_q = defer ? (DeferEntry*)(a + o_dq) : nullptr;
     if (b->use_wake) {
       b->pot = (double*)(a + o[0]);
       b->potd = (double2*)(a + o[1]);
@@ -805,7 +801,6 @@ void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
 
   a.n_parts = b->nblk;
   a.pair_offset = b->first_particle / 2;
-  a.defer_q = b->defer_q;
 }
 
 extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
@@ -1120,13 +1115,18 @@ extern "C" hj_status hj_normal_tables(double* out, int64_t cap) {
   NormalTables t;
   host_normal_tables(&t);
   double* o = out;
-  for (int i = 0; i < kZigLayers; ++i) {
-    *o++ = t.xd[i][0];
-    *o++ = t.xd[i][1];
+  for (int j = 0; j < kNormalTableRows; ++j) {
+    *o++ = t.lr[j][0];
+    *o++ = t.lr[j][1];
   }
-  for (int i = 0; i <= kZigLayers; ++i) *o++ = t.f[i];
-  *o++ = t.r;
-  *o++ = t.v;
+  for (int j = 0; j < kNormalTableRows; ++j) {
+    *o++ = t.sc[j][0];
+    *o++ = t.sc[j][1];
+  }
+  *o++ = t.ln2_hi;
+  *o++ = t.ln2_lo;
+  *o++ = t.twopi_hi;
+  *o++ = t.twopi_lo;
   return o - out == HJ_NORMAL_TABLES_SIZE ? HJ_OK : HJ_ERR_STATE;
 }
 

@@ -47,14 +47,6 @@ constexpr int kLogHeader = 8;       // doubles before the bin counts in a turn-l
 enum QeMode { QE_OFF = 0, QE_PHILOX = 1, QE_DRAWS = 2, QE_PHILOX_FAST = 3 };
 
 // Arguments of the fused per-turn particle pass (one launch per turn).
-// A particle of the fused pass whose Float64 normal takes the ziggurat's slow
-// path: its index and its (z, ΔE) after the previous turn's kick and
-// re-centring.
-struct DeferEntry {
-  int64_t i;
-  double z, e;
-};
-
 struct PassArgs {
   double* z;
   double* dE;
@@ -88,8 +80,6 @@ struct PassArgs {
   unsigned long long* ngp_ovf;     // [B] counts beyond the 16-bit per-block counters
   int32_t n_parts;                 // partial slots written per turn (batches)
   int64_t pair_offset;             // Philox pair index of particle 0 (shards of a bunch)
-  DeferEntry* defer_q;             // [partial slots][warps][pass_defer_cap]: the particles
-                                   // whose Float64 normal takes the slow path
 };
 
 // One entry of a batch's chunk table: particles [first, first + count) of

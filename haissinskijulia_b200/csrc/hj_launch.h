@@ -34,14 +34,6 @@ inline bool pass_cfg_two_blocks(int cfg) {
   const int l = cfg & kPassLayoutMask;
   return l == 4 || l == 5;
 }
-// Entries of one warp's queue of particles whose Float64 normal takes the
-// ziggurat's slow path: up to 31 left from the last drain plus PPT per lane
-// of one iteration.
-inline int pass_defer_cap(int ppt) { return 32 * ppt + 32; }
-// Entries of one block's queues (one per warp).
-inline int64_t pass_defer_entries(int cfg) {
-  return (int64_t)(pass_cfg_threads(cfg) / 32) * pass_defer_cap(pass_cfg_ppt(cfg));
-}
 inline bool pass_cfg_valid(int cfg) {
   return cfg >= 0 && (cfg & ~(kPassLayoutMask | kPassN32 | kPassFastNormals)) == 0 &&
          (cfg & kPassLayoutMask) < kNumPassCfgs;

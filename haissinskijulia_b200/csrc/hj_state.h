@@ -106,7 +106,6 @@ struct hj_bunch {
   double2* Wf = nullptr;
   double2* twP = nullptr;
   uint32_t* part_cnt = nullptr;
-  DeferEntry* defer_q = nullptr;          // [nblk][pass_defer_entries(cfg)] (Float64 normals)
   unsigned long long* part_cic = nullptr;
   unsigned long long* ngp_ovf = nullptr;   // [B] overflow of the pass's 16-bit counters
   double2* rf_table = nullptr;             // [kRfTableSize] RF kick table of the pass

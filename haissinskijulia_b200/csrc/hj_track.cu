@@ -31,9 +31,8 @@
 //     series through t^7 and t^6.  For m = 0 the kick is V sin ϕs (cos t - 1)
 //     - V cos ϕs sin t, free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
 //   * Philox-4x32 round keys are precomputed on the host (kernel parameters);
-//     the Float64 normals come from a 256-layer ziggurat whose (X_i, D_i)
-//     rows sit in shared memory; the ~1.5 % of particles whose draw needs the
-//     slow path are taken back and finished 32 at a time (drain_deferred).
+//     the normals come from a double-precision Box-Muller transform whose
+//     small tables sit in shared memory (Float64, 52-bit uniforms).
 //   * 1/γ² of the drift: rcp.approx.ftz.f64 refined by one Newton step
 //     (relative error ~1e-14 on a term 5e-5 of η, i.e. ~1e-18 on η).
 //   * drift: z' = z - (2π h / (β0² E0 k)) η_i ΔE, the reference's
@@ -62,8 +61,9 @@ __device__ NormalTables g_normal;
 
 __device__ __forceinline__ void philox_normals2(uint64_t seed, int64_t turn, int64_t p,
                                                 double out[2]) {
-  philox_normals2_rk(seed, philox_keys(seed), turn, p, &g_normal,
-                     reinterpret_cast<const double2*>(g_normal.xd), out);
+  philox_normals2_rk(philox_keys(seed), turn, p, &g_normal,
+                     reinterpret_cast<const double2*>(g_normal.lr),
+                     reinterpret_cast<const double2*>(g_normal.sc), out);
 }
 
 // Run- and turn-constants of the fused pass.
@@ -290,20 +290,20 @@ __device__ __forceinline__ int ngp_bin_any(double z, const GridConst& g, bool& i
 // free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
 __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
                                           const double2* __restrict__ s_rf) {
-  const double x = __dmul_rn(z, c.k);
+  const double x = z * c.k;
   const double y = fma(x, c.rf_inv_h, kMagic);
-  const double md = __dsub_rn(y, kMagic);
+  const double md = y - kMagic;
   double t = fma(-md, c.rf_h_hi, x);
   t = fma(-md, c.rf_h_lo, t);
   const double2 rot = s_rf[__double2loint(y) & (kRfTableSize - 1)];
-  const double t2 = __dmul_rn(t, t);
+  const double t2 = t * t;
   double p = fma(t2, -1.984126984126984e-04, 8.333333333333333e-03);   // -1/7!, 1/5!
   p = fma(t2, p, -1.6666666666666666e-01);                               // -1/3!
-  const double sn = fma(__dmul_rn(t, t2), p, t);
+  const double sn = fma(t * t2, p, t);
   double q = fma(t2, -1.388888888888889e-03, 4.1666666666666664e-02);  // -1/6!, 1/4!
   q = fma(t2, q, -0.5);
-  const double cm1 = __dmul_rn(t2, q);
-  return __dadd_rn(fma(rot.x, cm1, __dmul_rn(-rot.y, sn)), __dsub_rn(rot.x, c.Vs));
+  const double cm1 = t2 * q;
+  return fma(rot.x, cm1, -rot.y * sn) + (rot.x - c.Vs);
 }
 
 // One particle for one turn, given its wake kick (lerp of the previous turn's
@@ -314,36 +314,22 @@ __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
 // (zero when apply_phase_advance! would skip the advance).  The moments and
 // deposits of the new z follow in deposit_group.
 template <bool WAKE>
-__device__ __forceinline__ void previous_kick(double& e, double kick, double pmean) {
-  if (WAKE) e = __dsub_rn(e, kick);
-  e = __dsub_rn(e, pmean);
-}
-
-// The turn itself from e_start = ΔE after the previous turn's kick and
-// re-centring: RF, QE, SR, drift; returns ΔE - e_start.  Every operation
-// rounds where it is written (no contraction), so that evaluating it again
-// anywhere reproduces it bit for bit.
-__device__ __forceinline__ double particle_advance(double& z, double& e, double r, double rf,
-                                                   const FusedConst& c) {
-  const double e_start = e;
-  e = __dadd_rn(e, rf);
-  e = fma(c.excitation, r, e);                         // r = 0 without QE
-  e = __dmul_rn(e, c.damping);                         // damping = 1 without SR
-  const double gp = fma(e, c.inv_mass, c.gamma0);     // γ0 + ΔE/m
-  const double g2 = __dmul_rn(gp, gp);
-  double ri = rcp_approx(g2);
-  ri = fma(ri, fma(-g2, ri, 1.0), ri);
-  const double coeff = c.update_eta ? __dmul_rn(c.Kz, __dsub_rn(c.alpha_c, ri)) : c.coeff0z;
-  z = fma(-coeff, e, z);
-  return __dsub_rn(e, e_start);
-}
-
-template <bool WAKE>
 __device__ __forceinline__ void particle_turn(double& z, double& e, double r, double kick,
                                               double rf, const FusedConst& c, double pmean,
                                               double& acc_d) {
-  previous_kick<WAKE>(e, kick, pmean);
-  acc_d += particle_advance(z, e, r, rf, c);
+  if (WAKE) e = e - kick;
+  e = e - pmean;
+  const double e_start = e;
+  e = e + rf;
+  e = fma(c.excitation, r, e);                         // r = 0 without QE
+  e = e * c.damping;                                   // damping = 1 without SR
+  const double gp = fma(e, c.inv_mass, c.gamma0);     // γ0 + ΔE/m
+  const double g2 = gp * gp;
+  double ri = rcp_approx(g2);
+  ri = fma(ri, fma(-g2, ri, 1.0), ri);
+  const double coeff = c.update_eta ? c.Kz * (c.alpha_c - ri) : c.coeff0z;
+  z = fma(-coeff, e, z);
+  acc_d += e - e_start;
 }
 
 // Moments and deposits of K particles' new z: Σz, Σz², the NGP count and, in
@@ -352,7 +338,7 @@ __device__ __forceinline__ void particle_turn(double& z, double& e, double r, do
 // their returned values is used, so their latencies overlap.
 template <int K, bool N32>
 __device__ __forceinline__ void deposit_group(const double (&z)[K], const GridConst& g,
-                                              double& acc_z, double& acc_z2, int32_t& n_in,
+                                              double& acc_z, double& acc_z2, uint32_t& n_in,
                                               uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
                                               unsigned long long* __restrict__ ngp_ovf) {
   int nb[K], cj[K];
@@ -364,7 +350,7 @@ __device__ __forceinline__ void deposit_group(const double (&z)[K], const GridCo
     acc_z2 = fma(z[k], z[k], acc_z2);
     double w;
     cell_and_bin(z[k], g, cj[k], w, nb[k], nin[k]);
-    n_in += nin[k] ? 1 : 0;
+    n_in += nin[k] ? 1u : 0u;
     // w·2^24 rounded to nearest (at most 2^24; a NaN z lands in cell B with
     // any q and is flagged by the moments)
     cq[k] = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
@@ -455,71 +441,20 @@ __device__ __forceinline__ void stp(double* p, const double v[PPT]) {
   }
 }
 
-// Single-precision normals of the PPT particles of pairs pair0, pair0 + 1
-// (the opt-in fast layouts).
-template <int PPT>
-__device__ __forceinline__ void group_normals_fast(const PhiloxKeys& rk, int64_t turn,
-                                                   int64_t pair0, double r[PPT]) {
-  philox_normals2_fast(rk, turn, pair0, r);
-  if (PPT == 4) philox_normals2_fast(rk, turn, pair0 + 1, r + 2);
-}
-
-// Float64 normals of the PPT particles of pairs pair0, pair0 + 1 by the
-// ziggurat's fast path: bit j of the result is set where particle j's draw
-// was accepted; r[j] holds its normal, or its rejected candidate.
-template <int PPT>
-__device__ __forceinline__ unsigned group_normals_zig(const PhiloxKeys& rk, int64_t turn,
-                                                      int64_t pair0,
-                                                      const double2* __restrict__ zt,
-                                                      double r[PPT]) {
-  unsigned ok = 0u;
-#pragma unroll
-  for (int h = 0; h < PPT / 2; ++h) {
-    const int64_t p = pair0 + h;
-    uint32_t c[4] = {(uint32_t)p, (uint32_t)((uint64_t)p >> 32), (uint32_t)turn,
-                     (uint32_t)((uint64_t)turn >> 32)};
-    philox4x32_10(c, rk);
-    ok |= (zig_fast(c[1], c[0], zt, r[2 * h]) ? 1u : 0u) << (2 * h);
-    ok |= (zig_fast(c[3], c[2], zt, r[2 * h + 1]) ? 1u : 0u) << (2 * h + 1);
+// Normals of the PPT particles of pairs pair0, pair0 + 1, ... (one Philox-4x32
+// counter per pair of particles).
+template <int PPT, bool FAST>
+__device__ __forceinline__ void group_normals(const PhiloxKeys& rk, int64_t turn,
+                                              int64_t pair0, const NormalTables* t,
+                                              const double2* lr, const double2* sc,
+                                              double r[PPT]) {
+  if (FAST) {
+    philox_normals2_fast(rk, turn, pair0, r);
+    if (PPT == 4) philox_normals2_fast(rk, turn, pair0 + 1, r + 2);
+    return;
   }
-  return ok;
-}
-
-// Float64 normals of the PPT particles of pairs pair0, pair0 + 1 with the
-// ziggurat's slow path taken in place (the last, partial iteration of a warp).
-template <int PPT>
-__device__ __forceinline__ void group_normals_inline(uint64_t seed, const PhiloxKeys& rk,
-                                                     int64_t turn, int64_t pair0,
-                                                     const double2* __restrict__ zt,
-                                                     double r[PPT]) {
-#pragma unroll
-  for (int h = 0; h < PPT / 2; ++h)
-    philox_normals2_rk(seed, rk, turn, pair0 + h, &g_normal, zt, r + 2 * h);
-}
-
-// Takes back what deposit_group added for one particle at z: the moments (to
-// rounding) and the NGP and cell deposits (exactly: the packed cell word
-// loses the 2^44 + q it gained, borrow included; with 16-bit NGP counters the
-// bunch's overflow counts take the -1, modulo 2^64).
-template <bool N32>
-__device__ __forceinline__ void undeposit(double z, const GridConst& g, double& acc_z,
-                                          double& acc_z2, int32_t& n_in, uint32_t* s_ngp,
-                                          uint32_t* s_lo, uint32_t* s_hi,
-                                          unsigned long long* __restrict__ ngp_ovf) {
-  acc_z = __dsub_rn(acc_z, z);
-  acc_z2 = fma(-z, z, acc_z2);
-  int cj, nb;
-  double w;
-  bool nin;
-  cell_and_bin(z, g, cj, w, nb, nin);
-  if (nin) {
-    n_in -= 1;
-    if (N32) atomicSub(&s_ngp[nb], 1u);
-    else atomicAdd(ngp_ovf + nb, ~0ull);
-  }
-  const uint32_t cq = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
-  const uint32_t old = atomicSub(&s_lo[cj], cq);
-  atomicSub(&s_hi[cj], (1u << (kCicSumBits - 32)) + (old < cq ? 1u : 0u));
+  philox_normals2_rk(rk, turn, pair0, t, lr, sc, r);
+  if (PPT == 4) philox_normals2_rk(rk, turn, pair0 + 1, t, lr, sc, r + 2);
 }
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
@@ -533,76 +468,29 @@ struct PassRange {
   bool tail;
 };
 
-// Shared-memory tables of the pass: RF table [kRfTableSize] | the ziggurat's
-// (X_i, D_i) rows [kZigLayers].
-constexpr size_t kPassTableBytes = (size_t)(kRfTableSize + kZigLayers) * 16u;
-
-// Finishes `count` (<= 32) deferred particles of this warp, one per lane.  The
-// pass advanced, deposited and stored each of them with its draw's rejected
-// candidate (so that its loop needs no per-particle masks) and queued it as it
-// stood before the turn.  Here that provisional turn is evaluated again, bit
-// for bit (particle_advance rounds where written), and taken back
-// (undeposit, and its share of the sums); the turn with the normal from the
-// ziggurat's slow path is then applied, deposited and stored.
-template <bool WAKE, int PPT, bool N32>
-__device__ __forceinline__ void drain_deferred(const PassArgs& a, const FusedConst& c,
-                                               const GridConst& g, int64_t turn,
-                                               const DeferEntry* entries, int count,
-                                               const double2* s_zt, const double2* s_rf,
-                                               uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
-                                               double& acc_z, double& acc_z2, double& acc_d,
-                                               int32_t& n_in) {
-  __syncwarp();                          // the warp's stores and queue entries are visible
-  const int lane = threadIdx.x & 31;
-  if (lane < count) {
-    const DeferEntry* en = entries + lane;
-    const int64_t i = __ldcg(&en->i);
-    const double zs = __ldcg(&en->z), es = __ldcg(&en->e);
-    const int64_t pr = (i >> 1) + a.pair_offset;
-    const int h = (int)(i & 1);
-    uint32_t w[4] = {(uint32_t)pr, (uint32_t)((uint64_t)pr >> 32), (uint32_t)turn,
-                     (uint32_t)((uint64_t)turn >> 32)};
-    philox4x32_10(w, a.philox);
-    const uint32_t whi = h ? w[3] : w[1], wlo = h ? w[2] : w[0];
-    double xg;
-    zig_fast(whi, wlo, s_zt, xg);
-    const double rf = rf_term(zs, c, s_rf);
-    double zg = zs, eg = es;
-    const double dg = particle_advance(zg, eg, xg, rf, c);
-    const double r = zig_slow(a.seed, turn, pr, h, whi, wlo, &g_normal);
-    double z1[1] = {zs};
-    double e1 = es;
-    const double d1 = particle_advance(z1[0], e1, r, rf, c);
-    acc_d = __dadd_rn(__dsub_rn(acc_d, dg), d1);
-    if (WAKE) {
-      undeposit<N32>(zg, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
-      deposit_group<1, N32>(z1, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
-    }
-    a.z[i] = z1[0];
-    a.dE[i] = e1;
-  }
-  __syncwarp();                          // the entries are read before they are reused
-}
-
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = false>
 __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
                                           unsigned char* smem_raw) {
-  // dynamic shared memory: RF table [128] | the ziggurat's rows [256] |
-  // kick-table window [win] | NGP counters | cell words lo, hi [B+1]; NGP
-  // counters: (B+1)/2 words of two 16-bit counters, or B 32-bit ones (N32)
+  // dynamic shared memory: RF table [128] | the normal transform's logarithm
+  // and angle tables [128 + 128] | kick-table window [win] | NGP counters | cell
+  // words lo, hi [B+1]; NGP counters: (B+1)/2 words of two 16-bit counters, or
+  // B 32-bit ones (N32)
   const int nc = a.B + 1;                 // kick-table cells
   const int nw = N32 ? a.B : (a.B + 1) / 2;
   const int win = WAKE ? a.win : 0;
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
-  double2* s_zt = s_rf + kRfTableSize;
-  double* s_win = reinterpret_cast<double*>(smem_raw + kPassTableBytes);
+  double2* s_lr = s_rf + kRfTableSize;
+  double2* s_sc = s_lr + kNormalTableRows;
+  double* s_win = reinterpret_cast<double*>(s_sc + kNormalTableRows);
   uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_win + win);
   uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
   uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
   for (int i = threadIdx.x; i < kRfTableSize; i += THREADS) s_rf[i] = __ldg(a.rf_table + i);
   if (QE == QE_PHILOX)
-    for (int i = threadIdx.x; i < kZigLayers; i += THREADS)
-      s_zt[i] = reinterpret_cast<const double2*>(g_normal.xd)[i];
+    for (int i = threadIdx.x; i < kNormalTableRows; i += THREADS) {
+      s_lr[i] = reinterpret_cast<const double2*>(g_normal.lr)[i];
+      s_sc[i] = reinterpret_cast<const double2*>(g_normal.sc)[i];
+    }
 
   TurnState* ts = a.ts;
   const TurnScalars sc = ts->cur;
@@ -660,7 +548,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
   __syncthreads();
 
   double acc_z = 0.0, acc_z2 = 0.0, acc_d = 0.0;
-  int32_t n_in = 0;
+  uint32_t n_in = 0;
   const double2* __restrict__ potd = a.potd;
   const int64_t ng = rg.q_end;
   const int64_t stride = rg.q_step;
@@ -670,84 +558,6 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
   if (kPrefetch && q < ng) {
     ldp<PPT>(a.z + PPT * q, zn);
     ldp<PPT>(a.dE + PPT * q, en);
-  }
-  // With the Float64 normals (QE_PHILOX), a particle whose draw needs the
-  // ziggurat's slow path (about 1.5 %) is advanced like the others with its
-  // draw's rejected candidate, and queued as it stands before the turn in its
-  // warp's queue (global memory: the block's row of a.defer_q); drain_deferred
-  // takes that provisional turn back and applies the right one, 32 particles at
-  // a time, so that the slow path runs on full warps and this loop carries no
-  // per-particle masks.  The queue's ballots need every lane of the warp: the
-  // loop runs while the warp's last lane has a group (q < ng_w in every lane
-  // alike); the warp's last, partial iteration, if any, runs in the loop below
-  // with the slow path in place.
-  if (QE == QE_PHILOX) {
-    constexpr unsigned kAll = (1u << PPT) - 1u;
-    constexpr int kCap = 32 * PPT + 32;    // pass_defer_cap(PPT)
-    const int lane = threadIdx.x & 31;
-    DeferEntry* s_q = a.defer_q + ((int64_t)rg.part * (THREADS / 32) + (threadIdx.x >> 5)) * kCap;
-    int queued = 0;                        // entries in the warp's queue (every lane agrees)
-    const int64_t ng_w = ng - (31 - lane);
-    for (; q < ng_w; q += stride) {
-      double zz[PPT], ee[PPT], rr[PPT];
-      if (kPrefetch) {
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) {
-          zz[j] = zn[j];
-          ee[j] = en[j];
-        }
-        const int64_t qn = q + stride;
-        if (qn < ng) {
-          ldp<PPT>(a.z + PPT * qn, zn);
-          ldp<PPT>(a.dE + PPT * qn, en);
-        }
-      } else {
-        ldp<PPT>(a.z + PPT * q, zz);
-        ldp<PPT>(a.dE + PPT * q, ee);
-      }
-      KickFetch kf[PPT];
-      if (WAKE) {
-#pragma unroll
-        for (int j = 0; j < PPT; ++j) kf[j] = kick_fetch(zz[j], g, kw, potd);
-      }
-      const unsigned ok =
-          group_normals_zig<PPT>(a.philox, turn, (PPT / 2) * q + a.pair_offset, s_zt, rr);
-      double rf[PPT];
-#pragma unroll
-      for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rf);
-#pragma unroll
-      for (int j = 0; j < PPT; ++j)
-        previous_kick<WAKE>(ee[j], WAKE ? fma(kf[j].w, kf[j].d, kf[j].p0) : 0.0, pmean);
-      // queue the deferred particles: lane l's popc(later) entries go after
-      // those of the lanes below it (a prefix over the three bits of the
-      // counts, from three ballots)
-      const unsigned later = ~ok & kAll;
-      const unsigned nl = __popc(later);
-      const unsigned b0 = __ballot_sync(0xffffffffu, nl & 1u);
-      const unsigned b1 = __ballot_sync(0xffffffffu, nl & 2u);
-      const unsigned b2 = __ballot_sync(0xffffffffu, nl & 4u);
-      if (b0 | b1 | b2) {
-        const unsigned lt = (1u << lane) - 1u;
-        int pos = queued + __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
-#pragma unroll
-        for (int j = 0; j < PPT; ++j)
-          if ((later >> j) & 1u) s_q[pos++] = DeferEntry{PPT * q + j, zz[j], ee[j]};
-        queued += __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
-      }
-#pragma unroll
-      for (int j = 0; j < PPT; ++j) acc_d += particle_advance(zz[j], ee[j], rr[j], rf[j], c);
-      if (WAKE) deposit_group<PPT, N32>(zz, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
-      stp<PPT>(a.z + PPT * q, zz);
-      stp<PPT>(a.dE + PPT * q, ee);
-      while (queued >= 32) {
-        queued -= 32;
-        drain_deferred<WAKE, PPT, N32>(a, c, g, turn, s_q + queued, 32, s_zt, s_rf, s_ngp, s_lo,
-                                       s_hi, acc_z, acc_z2, acc_d, n_in);
-      }
-    }
-    if (queued > 0)
-      drain_deferred<WAKE, PPT, N32>(a, c, g, turn, s_q, queued, s_zt, s_rf, s_ngp, s_lo, s_hi,
-                                     acc_z, acc_z2, acc_d, n_in);
   }
   for (; q < ng; q += stride) {
     double zz[PPT], ee[PPT], rr[PPT];
@@ -773,10 +583,9 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     }
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
-    if (QE == QE_PHILOX) {
-      group_normals_inline<PPT>(a.seed, a.philox, turn, (PPT / 2) * q + a.pair_offset, s_zt, rr);
-    } else if (QE == QE_PHILOX_FAST) {
-      group_normals_fast<PPT>(a.philox, turn, (PPT / 2) * q + a.pair_offset, rr);
+    if (QE == QE_PHILOX || QE == QE_PHILOX_FAST) {
+      group_normals<PPT, QE == QE_PHILOX_FAST>(a.philox, turn, (PPT / 2) * q + a.pair_offset,
+                                               &g_normal, s_lr, s_sc, rr);
     } else if (QE == QE_DRAWS) {
       if (drow) {
 #pragma unroll
@@ -799,7 +608,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     const int64_t i = (a.n / PPT) * PPT + threadIdx.x;
     double r2[2] = {0.0, 0.0};
     if (QE == QE_PHILOX)
-      philox_normals2_rk(a.seed, a.philox, turn, (i >> 1) + a.pair_offset, &g_normal, s_zt, r2);
+      philox_normals2_rk(a.philox, turn, (i >> 1) + a.pair_offset, &g_normal, s_lr, s_sc, r2);
     if (QE == QE_PHILOX_FAST) philox_normals2_fast(a.philox, turn, (i >> 1) + a.pair_offset, r2);
     double r = r2[i & 1];
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
@@ -1319,6 +1128,8 @@ namespace {
 // Grids up to this many bins read the kick table from global memory (L1).
 constexpr int kWindowMinBins = 4096;
 
+// The normal transform's logarithm and angle tables in shared memory.
+constexpr size_t kNormalSmemBytes = 2 * kNormalTableRows * sizeof(double2);
 
 // Dynamic shared memory one block of the pass may take: the device's opt-in
 // limit (set when the kernels are prepared), or per block of the layout that
@@ -1335,10 +1146,10 @@ size_t pass_smem_budget(int cfg) {
   return pass_cfg_two_blocks(cfg) ? std::min(lim, (size_t)(113 * 1024)) : lim;
 }
 
-// Tables (RF, ziggurat) + NGP counts [B] (16-bit, two per word, or 32-bit
-// with kPassN32) + two 32-bit words per kick-table cell [B+1].
+// RF table + normal transform's table + NGP counts [B] (16-bit, two per
+// word, or 32-bit with kPassN32) + two 32-bit words per kick-table cell [B+1].
 size_t track_hist_bytes(int B, int cfg) {
-  const size_t rf = kPassTableBytes;
+  const size_t rf = kRfTableSize * sizeof(double2) + kNormalSmemBytes;
   const size_t nw = (cfg & kPassN32) ? (size_t)B : (size_t)((B + 1) / 2);
   return rf + nw * sizeof(uint32_t) + (size_t)(B + 1) * sizeof(unsigned long long);
 }
@@ -1377,10 +1188,9 @@ int track_window_entries(int B, int cfg) {
   return (int)std::min<size_t>(w, (size_t)B);
 }
 
-// Tables and histograms plus the kick-table window (wake on); the tables alone
-// otherwise.
+// Histograms plus the kick-table window (wake on); the RF table alone otherwise.
 size_t track_smem_bytes(int B, int use_wake, int cfg) {
-  if (!use_wake) return kPassTableBytes;
+  if (!use_wake) return kRfTableSize * sizeof(double2) + kNormalSmemBytes;
   return track_hist_bytes(B, cfg) + (size_t)track_window_entries(B, cfg) * sizeof(double);
 }
 
