@@ -517,7 +517,7 @@ def apply_wakefield_inplace(particles: Particles, buffers: SimulationBuffers, wa
 
 def gaussian_draws(seed: int, turn: int, n: int, buffers: SimulationBuffers) -> np.ndarray:
     """The on-device Float64 normals of (seed, particle, turn): Philox-4x32-10 and
-    the table-driven double-precision Box-Muller transform (hj_gaussian)."""
+    a 2048-layer ziggurat (hj_gaussian)."""
     ctx = buffers.context()
     out = np.empty(n, dtype=np.float64)
     _check(ctx, ctx._lib.hj_gaussian(ctx.handle, int(seed) & 0xFFFFFFFFFFFFFFFF, int(turn), n,

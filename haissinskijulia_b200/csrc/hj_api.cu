@@ -5,6 +5,7 @@
 // (particle pass, histogram reduction, bins step) whose turn-to-turn state
 // (E0, pending kick, turn counter) lives in device memory, so turns never
 // wait for the host.
+#include <memory>
 #include "hj_state.h"
 
 namespace {
@@ -280,10 +281,19 @@ hj_status read_state(hj_bunch* b) {
 // next group, one 32-bit counter per bin (1e8 particles, 16384 bins: 0.81 ms
 // per pass against 0.83 with 16-bit pairs, whose larger kick-table window
 // does not make up for their overflow checks).
-int default_pass_layout(int B, int64_t n) {
-  (void)B;
+int default_pass_layout(int B, int64_t n, bool zig) {
   (void)n;
-  return 0 | kPassN32;
+  // with the Float64 normals' ziggurat table in shared memory, above 8192
+  // bins the 32-bit counters would leave almost no room for the kick-table
+  // window: 16-bit counter pairs there
+  return (zig && B > 8192) ? 0 : (0 | kPassN32);
+}
+
+// The library's layout for a request r: the automatic one for bins B, with
+// the ziggurat's table unless single-precision normals are asked for.
+int auto_pass_layout(int r, int B, int64_t n, bool philox) {
+  const bool fast = r == kPassAutoFast || (r >= 0 && (r & kPassFastNormals));
+  return resolve_pass_request(r, default_pass_layout(B, n, philox && !fast));
 }
 
 void fill_result(hj_bunch* b, const double m[4], hj_result* res) {
@@ -474,7 +484,7 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
     b->H = b->M / 2;
     b->logH = b->H >= 1 ? ilog2(b->H) : 0;
   }
-  b->cfg = cfg >= 0 ? cfg : resolve_pass_request(ctx->pass_layout, default_pass_layout(b->B, n));
+  b->cfg = cfg >= 0 ? cfg : auto_pass_layout(ctx->pass_layout, b->B, n, b->qe_mode == QE_PHILOX);
   if (chunk > 0) {
     b->batch_member = true;
     b->nblk = (int)std::max<int64_t>((n + chunk - 1) / chunk, 1);
@@ -489,6 +499,11 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
     const size_t o_ts = c.add<TurnState>(1);
     const size_t o_sum = c.add<double>((size_t)kNumSums * nb);
     const size_t o_rf = c.add<double2>(kRfTableSize);
+    // per block and warp, the staging queue of the particles whose Float64
+    // normal takes the slow path (kDeferStage indices)
+    const bool defer = b->qe_mode == QE_PHILOX && !(b->cfg & kPassFastNormals);
+    const size_t o_dq =
+        defer ? c.add<int64_t>(nb * (size_t)(pass_cfg_threads(b->cfg) / 32) * kDeferStage) : 0;
     size_t o[6] = {};
     if (b->use_wake) {
       // pot, potd, hist and ngp_ovf are adjacent: one memset zeroes them
@@ -506,6 +521,7 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
     b->ts = (TurnState*)(a + o_ts);
     b->part_sum = (double*)(a + o_sum);
     b->rf_table = (double2*)(a + o_rf);
+    b->defer_q = defer ? (int64_t*)(a + o_dq) : nullptr;
     if (b->use_wake) {
       b->pot = (double*)(a + o[0]);
       b->potd = (double2*)(a + o[1]);
@@ -734,7 +750,8 @@ void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
   a.n = b->n;
   a.ts = b->ts;
   a.potd = b->potd;
-  a.win = b->use_wake ? track_window_entries(b->B, b->cfg) : 0;
+  a.zig = (b->qe_mode == QE_PHILOX && !(b->cfg & kPassFastNormals)) ? 1 : 0;
+  a.win = b->use_wake ? track_window_entries(b->B, b->cfg, a.zig != 0) : 0;
   a.B = b->B;
   a.use_wake = b->use_wake;
   a.e0 = b->e0;
@@ -801,6 +818,7 @@ void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
 
   a.n_parts = b->nblk;
   a.pair_offset = b->first_particle / 2;
+  a.defer_q = b->defer_q;
 }
 
 extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
@@ -1112,21 +1130,17 @@ extern "C" hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64
 
 extern "C" hj_status hj_normal_tables(double* out, int64_t cap) {
   if (!out || cap < HJ_NORMAL_TABLES_SIZE) return HJ_ERR_ARG;
-  NormalTables t;
-  host_normal_tables(&t);
+  std::unique_ptr<NormalTables> tp(new NormalTables);   // 48 KB: not on the stack
+  const NormalTables& t = *tp;
+  host_normal_tables(tp.get());
   double* o = out;
-  for (int j = 0; j < kNormalTableRows; ++j) {
-    *o++ = t.lr[j][0];
-    *o++ = t.lr[j][1];
+  for (int i = 0; i < kZigLayers; ++i) {
+    *o++ = t.xd[i][0];
+    *o++ = t.xd[i][1];
   }
-  for (int j = 0; j < kNormalTableRows; ++j) {
-    *o++ = t.sc[j][0];
-    *o++ = t.sc[j][1];
-  }
-  *o++ = t.ln2_hi;
-  *o++ = t.ln2_lo;
-  *o++ = t.twopi_hi;
-  *o++ = t.twopi_lo;
+  for (int i = 0; i <= kZigLayers; ++i) *o++ = t.f[i];
+  *o++ = t.r;
+  *o++ = t.v;
   return o - out == HJ_NORMAL_TABLES_SIZE ? HJ_OK : HJ_ERR_STATE;
 }
 

@@ -5,7 +5,7 @@
 // src/synchrotron_radiation.jl:44-56 of the reference.  The random numbers
 // are Philox-4x32-10 (Salmon, Moraes, Dror & Shaw, "Parallel random numbers:
 // as easy as 1, 2, 3", SC'11), one counter per pair of particles, turned into
-// Float64 normals by a double-precision Box-Muller transform.
+// Float64 normals by a 2048-layer ziggurat (Marsaglia and Tsang, 2000).
 #pragma once
 
 #include <cstdint>
@@ -141,68 +141,88 @@ __host__ __device__ inline void philox4x32_10(uint32_t (&c)[4], const PhiloxKeys
 
 // ------------------------------------------------------------ normals
 
-// Double-precision Box-Muller transform of the four Philox words of a
-// particle pair, with its logarithm and its sine and cosine evaluated from
-// two 128-row tables (NormalTables, hj_host.h):
-//   u1 = (2a + 1) 2^-53 with a the top 52 bits of (x1:x0), so u1 lies in
-//     [2^-53, 1 - 2^-53] exactly; ln u1 by the table-driven method of
-//     P. T. P. Tang (ACM TOMS 16(4), 1990): u1 = 2^e m, m in [1, 2),
-//     ln m = -ln r_j + log1p(m r_j - 1) with r_j ≈ 1/(1 + (j + 1/2)/128) for
-//     the top seven bits j of m (|m r_j - 1| < 2^-8), log1p by its Taylor
-//     series through t^6 (truncation below 2e-18), e ln 2 with a two-part ln 2;
-//   θ = 2π w, w in [0, 1) the top 52 bits of (x3:x2): θ = θ_k + t with
-//     θ_k = 2π (k + 1/2)/128 for the top seven bits k of w, |t| <= π/128, sin t
-//     and cos t - 1 by their Taylor series through t^7 and t^8 (truncation
-//     below 1e-20), then angle addition with the tabulated sin θ_k, cos θ_k;
-//   r = sqrt(-2 ln u1) (at most 8.57: the tails are cut only there), and the
-//   normals r cos θ, r sin θ.
-// About 36 FP64 operations per pair.
-__device__ __forceinline__ void box_muller_f64(const uint32_t (&x)[4],
-                                               const NormalTables* __restrict__ t,
-                                               const double2* __restrict__ lr,
-                                               const double2* __restrict__ sc, double out[2]) {
-  // u1 = d - (1 - 2^-53), d = 1 + a 2^-52 in [1, 2): exact (Sterbenz)
-  const double d = __hiloint2double(0x3FF00000 | (int)(x[1] >> 12),
-                                    (int)((x[1] << 20) | (x[0] >> 12)));
-  const double u1 = d - 0x1.fffffffffffffp-1;
-  const int hi = __double2hiint(u1);
-  const int e = (hi >> 20) - 1023;
-  const int j = (hi >> 13) & 127;
-  const double m = __hiloint2double((hi & 0x000FFFFF) | 0x3FF00000, __double2loint(u1));
-  const double2 rj = lr[j];
-  const double tt = fma(m, rj.x, -1.0);
-  double q = -1.0 / 6.0;                               // log1p(t) = t q(t)
-  q = fma(q, tt, 0.2);
-  q = fma(q, tt, -0.25);
-  q = fma(q, tt, 1.0 / 3.0);
-  q = fma(q, tt, -0.5);
-  q = fma(q, tt, 1.0);
-  const double ed = (double)e;
-  const double ln_u1 = fma(ed, t->ln2_hi, rj.y) + fma(ed, t->ln2_lo, tt * q);
-  const double r = sqrt(-2.0 * ln_u1);
-  // θ = 2π (w - (k + 1/2)/128) + θ_k, w = d2 - 1, d2 = 1 + b 2^-52; the
-  // sector's centre 1 + (2k + 1)/256 is built from its bits
-  const int h2 = (int)(0x3FF00000 | (x[3] >> 12));
-  const double d2 = __hiloint2double(h2, (int)((x[3] << 20) | (x[2] >> 12)));
-  const int k = (h2 >> 13) & 127;
-  const double ck = __hiloint2double(0x3FF00000 | ((2 * k + 1) << 12), 0);
-  const double xs = d2 - ck;                           // exact, |xs| <= 2^-8
-  const double ang = fma(xs, t->twopi_hi, xs * t->twopi_lo);
-  const double a2 = ang * ang;
-  double ps = -1.9841269841269841e-04;                 // -1/7!
-  ps = fma(ps, a2, 8.3333333333333333e-03);            // 1/5!
-  ps = fma(ps, a2, -1.6666666666666667e-01);           // -1/3!
-  const double sn = fma(ang * a2, ps, ang);
-  double pc = 2.4801587301587302e-05;                  // 1/8!
-  pc = fma(pc, a2, -1.3888888888888889e-03);           // -1/6!
-  pc = fma(pc, a2, 4.1666666666666667e-02);            // 1/4!
-  pc = fma(pc, a2, -0.5);
-  const double cm1 = a2 * pc;
-  const double2 skc = sc[k];
-  const double sin_th = fma(skc.y, sn, fma(skc.x, cm1, skc.x));
-  const double cos_th = fma(-skc.x, sn, fma(skc.y, cm1, skc.y));
-  out[0] = r * cos_th;
-  out[1] = r * sin_th;
+// Float64 standard normals by the 2048-layer ziggurat of NormalTables
+// (hj_host.h; Marsaglia and Tsang, J. Stat. Softw. 5(8), 2000), the algorithm
+// family of Julia's randn.  One normal takes 64 random bits (hi:lo): layer
+// i = hi >> 21, sign = bit 20 of hi, and a 52-bit fraction m = (hi mod 2^20):lo,
+// U = m 2^-52.  The candidate is x = U X_i.
+//
+// Fast path (about 99.8 % of draws): 1 + m 2^-52 < D_i, i.e. x < X_{i+1},
+// where the candidate lies under the curve at any height of the layer; x is
+// returned at once: one table row and one FMA, exact to one rounding.
+//
+// Slow path (zig_slow): the tail of layer 0 beyond r, or the wedge of layer
+// i >= 1 between x = X_{i+1} and X_i, needs more random bits.  They come from
+// the retry draws of the particle: Philox-4x32-10 under the same key with the
+// counter (p mod 2^32, p >> 32, turn mod 2^32, (turn >> 32) | (2a - 1 + h) << 24)
+// for attempt a = 1, 2, ... and the particle's half h of its pair, so every
+// normal is a fixed function of (seed, particle, turn) whichever thread, and
+// in whichever order, computes it (turns below 2^56).
+//   wedge: y = f(X_i) + u (f(X_{i+1}) - f(X_i)) with u from words 0-1; accept
+//     x when y < exp(-x²/2), else take a new (layer, sign, fraction) from
+//     words 2-3 and test it again from the start;
+//   tail: u1, u2 in (0, 1) from words 0-1 and 2-3, a = -ln(u1) / r,
+//     b = -ln(u2); accept r + a when 2b > a² (Marsaglia's tail method),
+//     else the next attempt.
+// The loop stops after 127 attempts (each rejects with probability below
+// 1/2, so it never gets there) with the last candidate.
+
+// The fast path: true and x = ±U X_i when the draw (hi:lo) is accepted; x is
+// the candidate either way.  zt: the table's (X_i, D_i) rows (shared or
+// global memory).
+__device__ __forceinline__ bool zig_fast(uint32_t hi, uint32_t lo,
+                                         const double2* __restrict__ zt, double& x) {
+  const double2 t = zt[hi >> 21];
+  const double d = __hiloint2double(0x3FF00000 | (int)(hi & 0xFFFFFu), (int)lo);  // 1 + U
+  const double xs = __hiloint2double(__double2hiint(t.x) ^ (int)((hi << 11) & 0x80000000u),
+                                     __double2loint(t.x));                          // ±X_i
+  x = fma(d, xs, -xs);                                                          // ±U X_i
+  return d < t.y;
+}
+
+// The 52-bit fraction (hi mod 2^20):lo as an exact double.
+__device__ __forceinline__ double zig_fraction(uint32_t hi, uint32_t lo) {
+  return (double)(((unsigned long long)(hi & 0xFFFFFu) << 32) | lo);
+}
+
+// The slow path for the normal of particle 2p + h at `turn` under `seed`
+// whose first draw (hi:lo) failed the fast test.  Out of line, with scalar
+// arguments only: the hot loops that may call it keep their registers.
+static __device__ __noinline__ double zig_slow(uint64_t seed, int64_t turn, int64_t p, int h,
+                                               uint32_t hi, uint32_t lo,
+                                               const NormalTables* __restrict__ t) {
+  const PhiloxKeys keys = philox_keys(seed);
+  int i = (int)(hi >> 21);
+  bool neg = (hi >> 20) & 1u;
+  double d = __hiloint2double(0x3FF00000 | (int)(hi & 0xFFFFFu), (int)lo);
+  const double r = __ldg(&t->r);
+  double x = 0.0;
+  for (int a = 1; a <= 127; ++a) {
+    uint32_t c[4] = {(uint32_t)p, (uint32_t)((uint64_t)p >> 32), (uint32_t)turn,
+                     (uint32_t)((uint64_t)turn >> 32) | ((uint32_t)(2 * a - 1 + h) << 24)};
+    philox4x32_10(c, keys);
+    if (i == 0) {   // tail beyond r
+      const double u1 = __dmul_rn(__dadd_rn(zig_fraction(c[1], c[0]), 0.5), 0x1p-52);
+      const double u2 = __dmul_rn(__dadd_rn(zig_fraction(c[3], c[2]), 0.5), 0x1p-52);
+      const double ta = __ddiv_rn(-log(u1), r);
+      const double tb = -log(u2);
+      x = __dadd_rn(r, ta);
+      if (__dadd_rn(tb, tb) > __dmul_rn(ta, ta)) break;
+      continue;
+    }
+    x = __dmul_rn(__dsub_rn(d, 1.0), __ldg(&t->xd[i][0]));   // in [X_{i+1}, X_i)
+    const double fi = __ldg(&t->f[i]), fi1 = __ldg(&t->f[i + 1]);
+    const double u = __dmul_rn(zig_fraction(c[1], c[0]), 0x1p-52);
+    const double y = __dadd_rn(fi, __dmul_rn(u, __dsub_rn(fi1, fi)));
+    if (y < exp(__dmul_rn(__dmul_rn(x, x), -0.5))) break;
+    // rejected: a new draw from words 2-3, tested from the start
+    i = (int)(c[3] >> 21);
+    neg = (c[3] >> 20) & 1u;
+    d = __hiloint2double(0x3FF00000 | (int)(c[3] & 0xFFFFFu), (int)c[2]);
+    x = __dmul_rn(__dsub_rn(d, 1.0), __ldg(&t->xd[i][0]));
+    if (d < __ldg(&t->xd[i][1])) break;
+  }
+  return neg ? -x : x;
 }
 
 // Single-precision Box-Muller transform of words 0 and 1 (the opt-in fast
@@ -231,21 +251,23 @@ __device__ __forceinline__ void philox_normals2_fast(const PhiloxKeys& keys, int
   box_muller_f32(c[0], c[1], out);
 }
 
-// Two standard normals for particles 2p and 2p+1 at `turn` under the round
-// keys of a seed: Philox-4x32-10 of the counter (p mod 2^32, p >> 32,
-// turn mod 2^32, turn >> 32), then box_muller_f64.  lr, sc: the
-// transform's logarithm and angle tables (shared or global memory).  Every
-// (seed, pair, turn) has its own counter and key, so distinct seeds, pairs
-// and turns never share a draw.
-__device__ __forceinline__ void philox_normals2_rk(const PhiloxKeys& keys, int64_t turn,
-                                                   int64_t p, const NormalTables* __restrict__ t,
-                                                   const double2* __restrict__ lr,
-                                                   const double2* __restrict__ sc,
+// Two standard normals for particles 2p and 2p+1 at `turn` under `seed`
+// (keys: its round keys): Philox-4x32-10 of the counter (p mod 2^32, p >> 32,
+// turn mod 2^32, turn >> 32); words 1:0 make the first normal and 3:2 the
+// second, each by the ziggurat (fast path, else zig_slow).  zt: the table's
+// (X_i, D_i) rows (shared or global memory); t: the whole table (global).
+// Every (seed, pair, turn) has its own counter and key, so distinct seeds,
+// pairs and turns never share a draw.
+__device__ __forceinline__ void philox_normals2_rk(uint64_t seed, const PhiloxKeys& keys,
+                                                   int64_t turn, int64_t p,
+                                                   const NormalTables* __restrict__ t,
+                                                   const double2* __restrict__ zt,
                                                    double out[2]) {
   uint32_t c[4] = {(uint32_t)p, (uint32_t)((uint64_t)p >> 32), (uint32_t)turn,
                    (uint32_t)((uint64_t)turn >> 32)};
   philox4x32_10(c, keys);
-  box_muller_f64(c, t, lr, sc, out);
+  if (!zig_fast(c[1], c[0], zt, out[0])) out[0] = zig_slow(seed, turn, p, 0, c[1], c[0], t);
+  if (!zig_fast(c[3], c[2], zt, out[1])) out[1] = zig_slow(seed, turn, p, 1, c[3], c[2], t);
 }
 
 }  // namespace hj

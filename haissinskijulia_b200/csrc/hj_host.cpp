@@ -179,23 +179,46 @@ void host_twiddles(int64_t P, double* tw_interleaved) {
 
 void host_normal_tables(NormalTables* t) {
   const long double kPiL = 3.141592653589793238462643383279502884L;
-  const long double kLn2L = 0.693147180559945309417232121458176568L;
-  const long double rows = (long double)kNormalTableRows;
-  for (int j = 0; j < kNormalTableRows; ++j) {
-    const double r = (double)(1.0L / (1.0L + ((long double)j + 0.5L) / rows));
-    t->lr[j][0] = r;
-    t->lr[j][1] = (double)(-logl((long double)r));     // ln m = -ln r + log1p(m r - 1)
-    const long double th = 2.0L * kPiL * ((long double)j + 0.5L) / rows;
-    t->sc[j][0] = (double)sinl(th);
-    t->sc[j][1] = (double)cosl(th);
+  const int n = kZigLayers;
+  auto f = [](long double x) { return expl(-0.5L * x * x); };
+  // area of the base layer: the rectangle [0, r) x [0, f(r)) and the tail
+  auto area = [&](long double r) {
+    return r * f(r) + sqrtl(kPiL / 2.0L) * erfcl(r / sqrtl(2.0L));
+  };
+  // Builds X_0 .. X_{n-1} from r; returns f(X_{n-1}) + v / X_{n-1} - 1, which
+  // is 0 when layer n - 1 ends exactly at the top f = 1, positive when r is
+  // too small (the layers are too tall and reach the top early).
+  auto top = [&](long double r, long double* X) -> long double {
+    const long double v = area(r);
+    long double x = r;
+    if (X) {
+      X[0] = v / f(r);
+      X[1] = r;
+    }
+    for (int i = 1; i < n - 1; ++i) {
+      const long double y = f(x) + v / x;
+      if (y >= 1.0L) return 1.0L;
+      x = sqrtl(-2.0L * logl(y));
+      if (X) X[i + 1] = x;
+    }
+    return f(x) + v / x - 1.0L;
+  };
+  long double lo = 3.0L, hi = 6.0L;
+  for (int it = 0; it < 200; ++it) {
+    const long double mid = 0.5L * (lo + hi);
+    if (top(mid, nullptr) > 0.0L) lo = mid; else hi = mid;
   }
-  // ln 2 with its high part rounded to 42 bits, so that e * high is exact for |e| < 2^11
-  const double ln2_hi = std::ldexp(std::nearbyint(std::ldexp((double)kLn2L, 42)), -42);
-  t->ln2_hi = ln2_hi;
-  t->ln2_lo = (double)(kLn2L - (long double)ln2_hi);
-  const double twopi_hi = (double)(2.0L * kPiL);
-  t->twopi_hi = twopi_hi;
-  t->twopi_lo = (double)(2.0L * kPiL - (long double)twopi_hi);
+  std::vector<long double> X(n + 1, 0.0L);
+  top(hi, X.data());
+  X[n] = 0.0L;
+  for (int i = 0; i < n; ++i) {
+    t->xd[i][0] = (double)X[i];
+    const long double K = ceill(ldexpl(X[i + 1] / X[i], 52));   // < 2^52: X_{i+1} < X_i
+    t->xd[i][1] = (double)(1.0L + ldexpl(K, -52));              // exact in double
+  }
+  for (int i = 0; i <= n; ++i) t->f[i] = (double)f(X[i]);
+  t->r = (double)X[1];
+  t->v = (double)area(hi);
 }
 
 }  // namespace hj

@@ -80,6 +80,10 @@ struct PassArgs {
   unsigned long long* ngp_ovf;     // [B] counts beyond the 16-bit per-block counters
   int32_t n_parts;                 // partial slots written per turn (batches)
   int64_t pair_offset;             // Philox pair index of particle 0 (shards of a bunch)
+  int64_t* defer_q;                // [partial slots][warps][kDeferStage]: indices of the
+                                   // particles whose Float64 normal takes the slow path
+  int32_t zig;                     // 1: shared memory holds the ziggurat's rows (the pass
+                                   // draws the Float64 normals), 0: the RF table alone
 };
 
 // One entry of a batch's chunk table: particles [first, first + count) of
@@ -143,10 +147,12 @@ struct FlushArgs {
 cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin);
 cudaError_t prepare_track_kernels(int max_smem);   // once per device: dynamic smem limits
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
-size_t track_smem_bytes(int B, int use_wake, int cfg);
+// zig: the pass draws the Float64 normals (QE_PHILOX without the fast bit),
+// so its shared memory holds the ziggurat's rows.
+size_t track_smem_bytes(int B, int use_wake, int cfg, bool zig);
 // Kick-table entries the fused pass keeps in shared memory for B bins
 // (what the shared-memory budget leaves beside the histograms, at most B).
-int track_window_entries(int B, int cfg);
+int track_window_entries(int B, int cfg, bool zig);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
 // Batched pass over a chunk table (*d_n_chunks entries live, grid max_chunks)
 // and the per-bunch merge of its partials.

@@ -34,6 +34,9 @@ inline bool pass_cfg_two_blocks(int cfg) {
   const int l = cfg & kPassLayoutMask;
   return l == 4 || l == 5;
 }
+// Entries of a warp's staging queue of particles whose Float64 normal takes
+// the ziggurat's slow path (the fused pass finishes them 32 at a time).
+constexpr int kDeferStage = 64;
 inline bool pass_cfg_valid(int cfg) {
   return cfg >= 0 && (cfg & ~(kPassLayoutMask | kPassN32 | kPassFastNormals)) == 0 &&
          (cfg & kPassLayoutMask) < kNumPassCfgs;

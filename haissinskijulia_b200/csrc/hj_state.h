@@ -106,6 +106,7 @@ struct hj_bunch {
   double2* Wf = nullptr;
   double2* twP = nullptr;
   uint32_t* part_cnt = nullptr;
+  int64_t* defer_q = nullptr;             // [nblk][warps][kDeferStage] (Float64 normals)
   unsigned long long* part_cic = nullptr;
   unsigned long long* ngp_ovf = nullptr;   // [B] overflow of the pass's 16-bit counters
   double2* rf_table = nullptr;             // [kRfTableSize] RF kick table of the pass
@@ -211,7 +212,8 @@ hj_status read_moments(hj_bunch* b, double m[4]);
 hj_status launch_moments(hj_bunch* b, int apply, double* z_out, double* dE_out);
 hj_status state_status(hj_bunch* b);
 hj_status read_state(hj_bunch* b);
-int default_pass_layout(int B, int64_t n);
+int default_pass_layout(int B, int64_t n, bool zig);
+int auto_pass_layout(int r, int B, int64_t n, bool philox);
 void fill_result(hj_bunch* b, const double m[4], hj_result* res);
 cudaError_t set_kernel_attributes(hj_ctx* ctx);
 

@@ -31,8 +31,9 @@
 //     series through t^7 and t^6.  For m = 0 the kick is V sin ϕs (cos t - 1)
 //     - V cos ϕs sin t, free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
 //   * Philox-4x32 round keys are precomputed on the host (kernel parameters);
-//     the normals come from a double-precision Box-Muller transform whose
-//     small tables sit in shared memory (Float64, 52-bit uniforms).
+//     the Float64 normals come from a 2048-layer ziggurat whose (X_i, D_i)
+//     rows sit in shared memory; the ~0.23 % of particles whose draw needs the
+//     slow path are finished later, 32 at a time (finish_deferred).
 //   * 1/γ² of the drift: rcp.approx.ftz.f64 refined by one Newton step
 //     (relative error ~1e-14 on a term 5e-5 of η, i.e. ~1e-18 on η).
 //   * drift: z' = z - (2π h / (β0² E0 k)) η_i ΔE, the reference's
@@ -47,6 +48,7 @@
 //     and mean before the first turn, damping 1 without SR, r = 0 without
 //     QE), all exact, so the pass has no per-particle branches on them.
 #include <algorithm>
+#include <memory>
 
 #include "hj_host.h"
 #include "hj_internal.h"
@@ -61,9 +63,8 @@ __device__ NormalTables g_normal;
 
 __device__ __forceinline__ void philox_normals2(uint64_t seed, int64_t turn, int64_t p,
                                                 double out[2]) {
-  philox_normals2_rk(philox_keys(seed), turn, p, &g_normal,
-                     reinterpret_cast<const double2*>(g_normal.lr),
-                     reinterpret_cast<const double2*>(g_normal.sc), out);
+  philox_normals2_rk(seed, philox_keys(seed), turn, p, &g_normal,
+                     reinterpret_cast<const double2*>(g_normal.xd), out);
 }
 
 // Run- and turn-constants of the fused pass.
@@ -290,20 +291,20 @@ __device__ __forceinline__ int ngp_bin_any(double z, const GridConst& g, bool& i
 // free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
 __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
                                           const double2* __restrict__ s_rf) {
-  const double x = z * c.k;
+  const double x = __dmul_rn(z, c.k);
   const double y = fma(x, c.rf_inv_h, kMagic);
-  const double md = y - kMagic;
+  const double md = __dsub_rn(y, kMagic);
   double t = fma(-md, c.rf_h_hi, x);
   t = fma(-md, c.rf_h_lo, t);
   const double2 rot = s_rf[__double2loint(y) & (kRfTableSize - 1)];
-  const double t2 = t * t;
+  const double t2 = __dmul_rn(t, t);
   double p = fma(t2, -1.984126984126984e-04, 8.333333333333333e-03);   // -1/7!, 1/5!
   p = fma(t2, p, -1.6666666666666666e-01);                               // -1/3!
-  const double sn = fma(t * t2, p, t);
+  const double sn = fma(__dmul_rn(t, t2), p, t);
   double q = fma(t2, -1.388888888888889e-03, 4.1666666666666664e-02);  // -1/6!, 1/4!
   q = fma(t2, q, -0.5);
-  const double cm1 = t2 * q;
-  return fma(rot.x, cm1, -rot.y * sn) + (rot.x - c.Vs);
+  const double cm1 = __dmul_rn(t2, q);
+  return __dadd_rn(fma(rot.x, cm1, __dmul_rn(-rot.y, sn)), __dsub_rn(rot.x, c.Vs));
 }
 
 // One particle for one turn, given its wake kick (lerp of the previous turn's
@@ -317,19 +318,21 @@ template <bool WAKE>
 __device__ __forceinline__ void particle_turn(double& z, double& e, double r, double kick,
                                               double rf, const FusedConst& c, double pmean,
                                               double& acc_d) {
-  if (WAKE) e = e - kick;
-  e = e - pmean;
+  // every operation rounds where it is written (no contraction), so that a
+  // second evaluation anywhere reproduces the turn bit for bit
+  if (WAKE) e = __dsub_rn(e, kick);
+  e = __dsub_rn(e, pmean);
   const double e_start = e;
-  e = e + rf;
+  e = __dadd_rn(e, rf);
   e = fma(c.excitation, r, e);                         // r = 0 without QE
-  e = e * c.damping;                                   // damping = 1 without SR
+  e = __dmul_rn(e, c.damping);                         // damping = 1 without SR
   const double gp = fma(e, c.inv_mass, c.gamma0);     // γ0 + ΔE/m
-  const double g2 = gp * gp;
+  const double g2 = __dmul_rn(gp, gp);
   double ri = rcp_approx(g2);
   ri = fma(ri, fma(-g2, ri, 1.0), ri);
-  const double coeff = c.update_eta ? c.Kz * (c.alpha_c - ri) : c.coeff0z;
+  const double coeff = c.update_eta ? __dmul_rn(c.Kz, __dsub_rn(c.alpha_c, ri)) : c.coeff0z;
   z = fma(-coeff, e, z);
-  acc_d += e - e_start;
+  acc_d += __dsub_rn(e, e_start);
 }
 
 // Moments and deposits of K particles' new z: Σz, Σz², the NGP count and, in
@@ -338,7 +341,7 @@ __device__ __forceinline__ void particle_turn(double& z, double& e, double r, do
 // their returned values is used, so their latencies overlap.
 template <int K, bool N32>
 __device__ __forceinline__ void deposit_group(const double (&z)[K], const GridConst& g,
-                                              double& acc_z, double& acc_z2, uint32_t& n_in,
+                                              double& acc_z, double& acc_z2, int32_t& n_in,
                                               uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
                                               unsigned long long* __restrict__ ngp_ovf) {
   int nb[K], cj[K];
@@ -350,7 +353,7 @@ __device__ __forceinline__ void deposit_group(const double (&z)[K], const GridCo
     acc_z2 = fma(z[k], z[k], acc_z2);
     double w;
     cell_and_bin(z[k], g, cj[k], w, nb[k], nin[k]);
-    n_in += nin[k] ? 1u : 0u;
+    n_in += nin[k] ? 1 : 0;
     // w·2^24 rounded to nearest (at most 2^24; a NaN z lands in cell B with
     // any q and is flagged by the moments)
     cq[k] = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
@@ -441,20 +444,59 @@ __device__ __forceinline__ void stp(double* p, const double v[PPT]) {
   }
 }
 
-// Normals of the PPT particles of pairs pair0, pair0 + 1, ... (one Philox-4x32
-// counter per pair of particles).
-template <int PPT, bool FAST>
-__device__ __forceinline__ void group_normals(const PhiloxKeys& rk, int64_t turn,
-                                              int64_t pair0, const NormalTables* t,
-                                              const double2* lr, const double2* sc,
-                                              double r[PPT]) {
-  if (FAST) {
-    philox_normals2_fast(rk, turn, pair0, r);
-    if (PPT == 4) philox_normals2_fast(rk, turn, pair0 + 1, r + 2);
-    return;
+// Single-precision normals of the PPT particles of pairs pair0, pair0 + 1
+// (the opt-in fast layouts).
+template <int PPT>
+__device__ __forceinline__ void group_normals_fast(const PhiloxKeys& rk, int64_t turn,
+                                                   int64_t pair0, double r[PPT]) {
+  philox_normals2_fast(rk, turn, pair0, r);
+  if (PPT == 4) philox_normals2_fast(rk, turn, pair0 + 1, r + 2);
+}
+
+// Float64 normals of the PPT particles of pairs pair0, pair0 + 1 by the
+// ziggurat's fast path: bit j of the result is set where particle j's draw
+// was accepted; r[j] holds its normal, or its rejected candidate.
+template <int PPT>
+__device__ __forceinline__ unsigned group_normals_zig(const PhiloxKeys& rk, int64_t turn,
+                                                      int64_t pair0,
+                                                      const double2* __restrict__ zt,
+                                                      double r[PPT]) {
+  unsigned ok = 0u;
+#pragma unroll
+  for (int h = 0; h < PPT / 2; ++h) {
+    const int64_t p = pair0 + h;
+    uint32_t c[4] = {(uint32_t)p, (uint32_t)((uint64_t)p >> 32), (uint32_t)turn,
+                     (uint32_t)((uint64_t)turn >> 32)};
+    philox4x32_10(c, rk);
+    ok |= (zig_fast(c[1], c[0], zt, r[2 * h]) ? 1u : 0u) << (2 * h);
+    ok |= (zig_fast(c[3], c[2], zt, r[2 * h + 1]) ? 1u : 0u) << (2 * h + 1);
   }
-  philox_normals2_rk(rk, turn, pair0, t, lr, sc, r);
-  if (PPT == 4) philox_normals2_rk(rk, turn, pair0 + 1, t, lr, sc, r + 2);
+  return ok;
+}
+
+// Takes back what deposit_group added for one particle at z: the moments (to
+// rounding) and the NGP and cell deposits (exactly: the packed cell word
+// loses the 2^44 + q it gained, borrow included; with 16-bit NGP counters the
+// bunch's overflow counts take the -1, modulo 2^64).
+template <bool N32>
+__device__ __forceinline__ void undeposit(double z, const GridConst& g, double& acc_z,
+                                          double& acc_z2, int32_t& n_in, uint32_t* s_ngp,
+                                          uint32_t* s_lo, uint32_t* s_hi,
+                                          unsigned long long* __restrict__ ngp_ovf) {
+  acc_z = __dsub_rn(acc_z, z);
+  acc_z2 = fma(-z, z, acc_z2);
+  int cj, nb;
+  double w;
+  bool nin;
+  cell_and_bin(z, g, cj, w, nb, nin);
+  if (nin) {
+    n_in -= 1;
+    if (N32) atomicSub(&s_ngp[nb], 1u);
+    else atomicAdd(ngp_ovf + nb, ~0ull);
+  }
+  const uint32_t cq = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
+  const uint32_t old = atomicSub(&s_lo[cj], cq);
+  atomicSub(&s_hi[cj], (1u << (kCicSumBits - 32)) + (old < cq ? 1u : 0u));
 }
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
@@ -468,29 +510,122 @@ struct PassRange {
   bool tail;
 };
 
+// Shared-memory tables of the pass: RF table [kRfTableSize] | the ziggurat's
+// (X_i, D_i) rows [kZigLayers].
+constexpr size_t kPassTableBytes = (size_t)(kRfTableSize + kZigLayers) * 16u;
+
+// Finishes particle i, whose draw failed the ziggurat's fast test.  The pass
+// turned and deposited it with the rejected candidate (so that its loop needs
+// no per-particle masks) but stored it as it was loaded.  That provisional
+// turn is evaluated again, bit for bit (particle_turn rounds where written),
+// and taken back (undeposit, and its share of the sums); the turn with the
+// normal from the ziggurat's slow path is then applied, deposited and stored.
+template <bool WAKE, bool N32>
+__device__ __forceinline__ void finish_deferred(const PassArgs& a, const FusedConst& c,
+                                                const GridConst& g, const KickWindow& kw,
+                                                double pmean, int64_t turn, int64_t i,
+                                                const double2* s_zt, const double2* s_rf,
+                                                uint32_t* s_ngp, uint32_t* s_lo,
+                                                uint32_t* s_hi, double& acc_z, double& acc_z2,
+                                                double& acc_d, int32_t& n_in) {
+  const double z0 = __ldcg(a.z + i), e0 = __ldcg(a.dE + i);
+  double kick = 0.0;
+  if (WAKE) {
+    const KickFetch kf = kick_fetch(z0, g, kw, a.potd);
+    kick = fma(kf.w, kf.d, kf.p0);
+  }
+  const int64_t pr = (i >> 1) + a.pair_offset;
+  const int h = (int)(i & 1);
+  uint32_t w[4] = {(uint32_t)pr, (uint32_t)((uint64_t)pr >> 32), (uint32_t)turn,
+                   (uint32_t)((uint64_t)turn >> 32)};
+  philox4x32_10(w, a.philox);
+  const uint32_t whi = h ? w[3] : w[1], wlo = h ? w[2] : w[0];
+  double xg;
+  zig_fast(whi, wlo, s_zt, xg);
+  const double rf = rf_term(z0, c, s_rf);
+  double zg = z0, eg = e0, dg = 0.0;
+  particle_turn<WAKE>(zg, eg, xg, kick, rf, c, pmean, dg);
+  const double r = zig_slow(a.seed, turn, pr, h, whi, wlo, &g_normal);
+  double z1[1] = {z0};
+  double e1 = e0, d1 = 0.0;
+  particle_turn<WAKE>(z1[0], e1, r, kick, rf, c, pmean, d1);
+  acc_d = __dadd_rn(__dsub_rn(acc_d, dg), d1);
+  if (WAKE) {
+    undeposit<N32>(zg, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
+    deposit_group<1, N32>(z1, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
+  }
+  a.z[i] = z1[0];
+  a.dE[i] = e1;
+}
+
+// Moves the particles whose bit is set in the lanes' `pend` (bit k PPT + j:
+// particle j of the group k iterations before `qref`) into the warp's
+// staging queue wq (kDeferStage indices in global memory, `staged` of them
+// held; each lane's entries after those of the lanes below it, by a prefix
+// over the lanes' counts), and finishes them 32 at a time (finish_deferred)
+// -- all of them when `last`, else only full waves, the rest staying queued.
+// Every lane of the warp must take part.
+template <bool WAKE, int PPT, bool N32>
+__device__ __forceinline__ void drain_deferred(const PassArgs& a, const FusedConst& c,
+                                               const GridConst& g, const KickWindow& kw,
+                                               double pmean, int64_t turn, int64_t qref,
+                                               int64_t stride, unsigned long long& pend,
+                                               int64_t* wq, int& staged, bool last,
+                                               const double2* s_zt, const double2* s_rf,
+                                               uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
+                                               double& acc_z, double& acc_z2, double& acc_d,
+                                               int32_t& n_in) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const int cnt = __popcll(pend);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int space = kDeferStage - staged;
+    int slot = staged + incl - cnt;
+    while (pend && slot < kDeferStage) {
+      const int b = __ffsll(pend) - 1;
+      wq[slot++] = (int64_t)PPT * (qref - (int64_t)(b / PPT) * stride) + (b % PPT);
+      pend &= pend - 1ull;
+    }
+    staged += min(total, space);
+    __syncwarp();
+    while (staged >= 32 || (last && staged > 0)) {
+      const int n = min(staged, 32);
+      staged -= n;
+      if (lane < n)
+        finish_deferred<WAKE, N32>(a, c, g, kw, pmean, turn, __ldcg(wq + staged + lane), s_zt,
+                                   s_rf, s_ngp, s_lo, s_hi, acc_z, acc_z2, acc_d, n_in);
+      __syncwarp();
+    }
+    if (total <= space) break;
+  }
+}
+
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = false>
 __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
                                           unsigned char* smem_raw) {
-  // dynamic shared memory: RF table [128] | the normal transform's logarithm
-  // and angle tables [128 + 128] | kick-table window [win] | NGP counters | cell
-  // words lo, hi [B+1]; NGP counters: (B+1)/2 words of two 16-bit counters, or
-  // B 32-bit ones (N32)
+  // dynamic shared memory: RF table [128] | the ziggurat's rows [2048] (a.zig) |
+  // kick-table window [win] | NGP counters | cell words lo, hi [B+1]; NGP
+  // counters: (B+1)/2 words of two 16-bit counters, or B 32-bit ones (N32)
   const int nc = a.B + 1;                 // kick-table cells
   const int nw = N32 ? a.B : (a.B + 1) / 2;
   const int win = WAKE ? a.win : 0;
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
-  double2* s_lr = s_rf + kRfTableSize;
-  double2* s_sc = s_lr + kNormalTableRows;
-  double* s_win = reinterpret_cast<double*>(s_sc + kNormalTableRows);
+  double2* s_zt = s_rf + kRfTableSize;
+  double* s_win = reinterpret_cast<double*>(
+      smem_raw + (a.zig ? kPassTableBytes : kRfTableSize * sizeof(double2)));
   uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_win + win);
   uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
   uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
   for (int i = threadIdx.x; i < kRfTableSize; i += THREADS) s_rf[i] = __ldg(a.rf_table + i);
   if (QE == QE_PHILOX)
-    for (int i = threadIdx.x; i < kNormalTableRows; i += THREADS) {
-      s_lr[i] = reinterpret_cast<const double2*>(g_normal.lr)[i];
-      s_sc[i] = reinterpret_cast<const double2*>(g_normal.sc)[i];
-    }
+    for (int i = threadIdx.x; i < kZigLayers; i += THREADS)
+      s_zt[i] = reinterpret_cast<const double2*>(g_normal.xd)[i];
 
   TurnState* ts = a.ts;
   const TurnScalars sc = ts->cur;
@@ -548,7 +683,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
   __syncthreads();
 
   double acc_z = 0.0, acc_z2 = 0.0, acc_d = 0.0;
-  uint32_t n_in = 0;
+  int32_t n_in = 0;
   const double2* __restrict__ potd = a.potd;
   const int64_t ng = rg.q_end;
   const int64_t stride = rg.q_step;
@@ -559,7 +694,20 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     ldp<PPT>(a.z + PPT * q, zn);
     ldp<PPT>(a.dE + PPT * q, en);
   }
-  for (; q < ng; q += stride) {
+  // With the Float64 normals (QE_PHILOX), a particle whose draw fails the
+  // ziggurat's fast test (about 0.23 %) is turned and deposited like the
+  // others with its rejected candidate but stored as loaded, and its bit set in
+  // its lane's history `pend`; every 16 iterations (and at the end) the warp
+  // moves those particles to its staging queue and finishes them 32 at a time
+  // (drain_deferred), so that the slow path runs on full warps and this loop
+  // carries no per-particle branches.
+  constexpr bool kDefer = QE == QE_PHILOX;
+  unsigned long long pend = 0ull;
+  int it = 0, staged = 0;
+  int64_t* wq = kDefer ? a.defer_q + ((int64_t)rg.part * (THREADS / 32) + (threadIdx.x >> 5)) *
+                                         kDeferStage
+                       : nullptr;
+  for (; q < ng; q += stride, ++it) {
     double zz[PPT], ee[PPT], rr[PPT];
     if (kPrefetch) {
 #pragma unroll
@@ -583,9 +731,11 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     }
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rr[j] = 0.0;
-    if (QE == QE_PHILOX || QE == QE_PHILOX_FAST) {
-      group_normals<PPT, QE == QE_PHILOX_FAST>(a.philox, turn, (PPT / 2) * q + a.pair_offset,
-                                               &g_normal, s_lr, s_sc, rr);
+    unsigned ok = (1u << PPT) - 1u;
+    if (QE == QE_PHILOX) {
+      ok = group_normals_zig<PPT>(a.philox, turn, (PPT / 2) * q + a.pair_offset, s_zt, rr);
+    } else if (QE == QE_PHILOX_FAST) {
+      group_normals_fast<PPT>(a.philox, turn, (PPT / 2) * q + a.pair_offset, rr);
     } else if (QE == QE_DRAWS) {
       if (drow) {
 #pragma unroll
@@ -595,20 +745,40 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     double rf[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rf);
+    double zs[PPT], es[PPT];               // what is stored
 #pragma unroll
-    for (int j = 0; j < PPT; ++j)
+    for (int j = 0; j < PPT; ++j) {
+      const double z0 = zz[j], e0 = ee[j];
       particle_turn<WAKE>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].d, kf[j].p0) : 0.0,
                           rf[j], c, pmean, acc_d);
+      const bool keep = kDefer && !((ok >> j) & 1u);
+      zs[j] = keep ? z0 : zz[j];
+      es[j] = keep ? e0 : ee[j];
+    }
     if (WAKE) deposit_group<PPT, N32>(zz, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
-    stp<PPT>(a.z + PPT * q, zz);
-    stp<PPT>(a.dE + PPT * q, ee);
+    stp<PPT>(a.z + PPT * q, zs);
+    stp<PPT>(a.dE + PPT * q, es);
+    if (kDefer) {
+      pend = (pend << PPT) | (unsigned long long)(~ok & ((1u << PPT) - 1u));
+      if ((it & 15) == 15 && __activemask() == 0xffffffffu)
+        drain_deferred<WAKE, PPT, N32>(a, c, g, kw, pmean, turn, q, stride, pend, wq, staged,
+                                       false, s_zt, s_rf, s_ngp, s_lo, s_hi, acc_z, acc_z2,
+                                       acc_d, n_in);
+    }
+  }
+  if (kDefer) {
+    __syncwarp();
+    staged = __reduce_max_sync(0xffffffffu, (unsigned)staged);
+    drain_deferred<WAKE, PPT, N32>(a, c, g, kw, pmean, turn, q - stride, stride, pend, wq, staged,
+                                   true, s_zt, s_rf, s_ngp, s_lo, s_hi, acc_z, acc_z2, acc_d,
+                                   n_in);
   }
   // Tail of n % PPT particles: the first threads of the tail block, scalar.
   if (rg.tail && threadIdx.x < (int)(a.n % PPT)) {
     const int64_t i = (a.n / PPT) * PPT + threadIdx.x;
     double r2[2] = {0.0, 0.0};
     if (QE == QE_PHILOX)
-      philox_normals2_rk(a.philox, turn, (i >> 1) + a.pair_offset, &g_normal, s_lr, s_sc, r2);
+      philox_normals2_rk(a.seed, a.philox, turn, (i >> 1) + a.pair_offset, &g_normal, s_zt, r2);
     if (QE == QE_PHILOX_FAST) philox_normals2_fast(a.philox, turn, (i >> 1) + a.pair_offset, r2);
     double r = r2[i & 1];
     if (QE == QE_DRAWS) r = drow ? __ldg(drow + i) : 0.0;
@@ -1128,8 +1298,6 @@ namespace {
 // Grids up to this many bins read the kick table from global memory (L1).
 constexpr int kWindowMinBins = 4096;
 
-// The normal transform's logarithm and angle tables in shared memory.
-constexpr size_t kNormalSmemBytes = 2 * kNormalTableRows * sizeof(double2);
 
 // Dynamic shared memory one block of the pass may take: the device's opt-in
 // limit (set when the kernels are prepared), or per block of the layout that
@@ -1146,21 +1314,48 @@ size_t pass_smem_budget(int cfg) {
   return pass_cfg_two_blocks(cfg) ? std::min(lim, (size_t)(113 * 1024)) : lim;
 }
 
-// RF table + normal transform's table + NGP counts [B] (16-bit, two per
-// word, or 32-bit with kPassN32) + two 32-bit words per kick-table cell [B+1].
-size_t track_hist_bytes(int B, int cfg) {
-  const size_t rf = kRfTableSize * sizeof(double2) + kNormalSmemBytes;
+// The tables in shared memory: RF, and the ziggurat's rows when the pass draws
+// the Float64 normals.
+size_t pass_table_bytes(bool zig) {
+  return zig ? kPassTableBytes : kRfTableSize * sizeof(double2);
+}
+
+// Tables + NGP counts [B] (16-bit, two per word, or 32-bit with kPassN32) +
+// two 32-bit words per kick-table cell [B+1].
+size_t track_hist_bytes(int B, int cfg, bool zig) {
+  const size_t rf = pass_table_bytes(zig);
   const size_t nw = (cfg & kPassN32) ? (size_t)B : (size_t)((B + 1) / 2);
   return rf + nw * sizeof(uint32_t) + (size_t)(B + 1) * sizeof(unsigned long long);
 }
 }  // namespace
 
+int track_window_entries(int B, int cfg, bool zig) {
+  // up to 4096 bins the 64 KB kick table stays in L1 beside the histograms:
+  // the window would only add its load to every block (measured: no gain)
+  if (B <= kWindowMinBins) return 0;
+  const size_t used = track_hist_bytes(B, cfg, zig), budget = pass_smem_budget(cfg);
+  if (used >= budget) return 0;
+  const size_t w = (budget - used) / sizeof(double);
+  return (int)std::min<size_t>(w, (size_t)B);
+}
+
+// Tables and histograms plus the kick-table window (wake on); the tables alone
+// otherwise.
+size_t track_smem_bytes(int B, int use_wake, int cfg, bool zig) {
+  if (!use_wake) return pass_table_bytes(zig);
+  return track_hist_bytes(B, cfg, zig) + (size_t)track_window_entries(B, cfg, zig) * sizeof(double);
+}
+
+namespace {
+bool pass_zig(int qe_mode, int cfg) { return qe_mode == QE_PHILOX && !(cfg & kPassFastNormals); }
+}  // namespace
+
 cudaError_t prepare_track_kernels(int max_smem) {
   g_pass_smem_limit = max_smem;
   {
-    NormalTables tab;
-    host_normal_tables(&tab);
-    cudaError_t e = cudaMemcpyToSymbol(g_normal, &tab, sizeof(tab));
+    std::unique_ptr<NormalTables> tab(new NormalTables);   // 48 KB: not on the stack
+    host_normal_tables(tab.get());
+    cudaError_t e = cudaMemcpyToSymbol(g_normal, tab.get(), sizeof(NormalTables));
     if (e != cudaSuccess) return e;
   }
   for (int w = 0; w < 2; ++w)
@@ -1178,24 +1373,8 @@ cudaError_t prepare_track_kernels(int max_smem) {
 }
 
 
-int track_window_entries(int B, int cfg) {
-  // up to 4096 bins the 64 KB kick table stays in L1 beside the histograms:
-  // the window would only add its load to every block (measured: no gain)
-  if (B <= kWindowMinBins) return 0;
-  const size_t used = track_hist_bytes(B, cfg), budget = pass_smem_budget(cfg);
-  if (used >= budget) return 0;
-  const size_t w = (budget - used) / sizeof(double);
-  return (int)std::min<size_t>(w, (size_t)B);
-}
-
-// Histograms plus the kick-table window (wake on); the RF table alone otherwise.
-size_t track_smem_bytes(int B, int use_wake, int cfg) {
-  if (!use_wake) return kRfTableSize * sizeof(double2) + kNormalSmemBytes;
-  return track_hist_bytes(B, cfg) + (size_t)track_window_entries(B, cfg) * sizeof(double);
-}
-
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
-  const size_t smem = track_smem_bytes(B, use_wake, cfg);
+  const size_t smem = track_smem_bytes(B, use_wake, cfg, pass_zig(qe_mode, cfg));
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pass_fn(use_wake, qe_mode, cfg),
                                                     pass_cfg_threads(cfg), smem) != cudaSuccess)
@@ -1204,7 +1383,7 @@ int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
 }
 
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
-  const size_t smem = track_smem_bytes(a.B, a.use_wake, a.cfg);
+  const size_t smem = track_smem_bytes(a.B, a.use_wake, a.cfg, a.zig != 0);
   void* args[] = {const_cast<PassArgs*>(&a)};
   PdlConfig l(dim3(grid), dim3(pass_cfg_threads(a.cfg)), smem, st);
   return cudaLaunchKernelExC(&l.cfg, pass_fn(a.use_wake, a.qe_mode, a.cfg), args);
@@ -1214,7 +1393,7 @@ cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chu
                               const int32_t* d_n_chunks, int max_chunks, int max_B, int wake,
                               int qe, int cfg, int32_t* d_queue, int resident_blocks,
                               cudaStream_t st) {
-  const size_t smem = track_smem_bytes(max_B, wake, cfg);
+  const size_t smem = track_smem_bytes(max_B, wake, cfg, pass_zig(qe, cfg));
   void* args[] = {const_cast<PassArgs**>(&d_bunches), const_cast<BatchChunk**>(&d_chunks),
                   const_cast<int32_t**>(&d_n_chunks), &d_queue};
   int grid = max_chunks > 0 ? max_chunks : 1;
@@ -1228,7 +1407,7 @@ cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chu
 }
 
 int batch_blocks_per_sm(int max_B, int qe_mode, int use_wake, int cfg) {
-  const size_t smem = track_smem_bytes(max_B, use_wake, cfg);
+  const size_t smem = track_smem_bytes(max_B, use_wake, cfg, pass_zig(qe_mode, cfg));
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_fn(use_wake, qe_mode, cfg, true),
                                                     pass_cfg_threads(cfg), smem) != cudaSuccess)

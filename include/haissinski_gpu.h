@@ -204,7 +204,7 @@ hj_status hj_make_grid(double sigma_z0, double half_width_sigmas, int64_t nbins,
  *   nbins      bin count (length(buffers.λ) in the reference);
  *   grid       NULL -> grid built on the device's sigma_z0_initial with
  *              hj_make_grid; non-NULL -> used as given (nbins must match);
- *   qe_draws   NULL -> on-device Philox-4x32-10 / Box-Muller Gaussians keyed by
+ *   qe_draws   NULL -> on-device Philox-4x32-10 / ziggurat Gaussians keyed by
  *              (seed, particle, turn); non-NULL -> host array of
  *              n_turns*n standard normals, turn-major, used in place of
  *              randn! (src/quantum_excitation.jl:36);
@@ -480,7 +480,7 @@ hj_status hj_apply_wakefield(hj_ctx* ctx, const double* z, double* dE, int64_t n
                              const hj_grid* grid);
 
 /* A bunch of independent Gaussians on the device: d_z[i] = sigma_z * N0,
- * d_dE[i] = sigma_E * N1 with (N0, N1) the Philox-4x32-10 / Box-Muller pair of
+ * d_dE[i] = sigma_E * N1 with (N0, N1) the Philox-4x32-10 / ziggurat pair of
  * particle i under init_seed (a stream apart from the quantum-excitation
  * draws).  Enqueued on `stream`.  The reference draws its bunches with
  * Distributions.jl on the host (generate_particles, src/evolution.jl:42-133,
@@ -494,7 +494,7 @@ hj_status hj_gaussian_bunch(hj_ctx* ctx, uint64_t init_seed, int64_t n, double s
  * min(n, 10000) independent Gaussians, its positive-definite guard, then n
  * correlated draws mu + L eps (L its Cholesky factor) into d_z, d_dE, and the
  * actual spreads by the two-pass compute_std (src/utils.jl:531-544).  Draws
- * are Philox-4x32-10 / Box-Muller under `seed` (the reference's come from
+ * are Philox-4x32-10 / ziggurat normals under `seed` (the reference's come from
  * Julia's default RNG).  n <= 0: spreads 0; n = 1: one independent draw and
  * the input spreads, as the reference returns them. */
 hj_status hj_generate_particles(hj_ctx* ctx, double mu_z, double mu_E, double sigma_z,
@@ -512,17 +512,20 @@ hj_status hj_correlation(hj_ctx* ctx, const double* d_x, const double* d_y, int6
 
 /* The Float64 standard normals used for quantum excitation: out[i] = the
  * N(0,1) draw of particle i at `turn` under `seed` (Philox-4x32-10 of
- * (pair i/2, turn) keyed by the 64-bit seed, two 52-bit uniforms per pair,
- * a double-precision Box-Muller transform).  No reference counterpart (the
- * reference calls randn!, src/quantum_excitation.jl:36). */
+ * (pair i/2, turn) keyed by the 64-bit seed, 64 bits per normal, a 2048-layer
+ * ziggurat whose rare slow path draws further Philox words keyed by
+ * (pair, turn, attempt); turns below 2^56).  No reference counterpart (the
+ * reference calls randn!, src/quantum_excitation.jl:36, whose algorithm is
+ * also a ziggurat). */
 hj_status hj_gaussian(hj_ctx* ctx, uint64_t seed, int64_t turn, int64_t n, double* out);
 
-/* The tables of that transform, for restatements of it (no reference
- * counterpart; host only, no context): out[HJ_NORMAL_TABLES_SIZE] = 128
- * pairs (r_j, -ln r_j) of the table-driven logarithm, 128 pairs (sin θ_j,
- * cos θ_j) of the angle reduction, ln 2 (high part, rest) and 2π (double,
- * rest).  cap < HJ_NORMAL_TABLES_SIZE is HJ_ERR_ARG. */
-#define HJ_NORMAL_TABLES_SIZE 516
+/* The ziggurat's tables, for restatements of it (no reference counterpart;
+ * host only, no context): out[HJ_NORMAL_TABLES_SIZE] = 2048 pairs (X_i, D_i)
+ * (layer i's width and its fast-acceptance bound 1 + ceil(2^52 X_{i+1}/X_i)
+ * 2^-52, X_2048 = 0), the 2049 values f(X_i) = exp(-X_i^2/2), r = X_1 (the
+ * tail's start) and v (the layers' common area).  cap <
+ * HJ_NORMAL_TABLES_SIZE is HJ_ERR_ARG. */
+#define HJ_NORMAL_TABLES_SIZE 6147
 hj_status hj_normal_tables(double* out, int64_t cap);
 
 #ifdef __cplusplus

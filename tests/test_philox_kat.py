@@ -1,12 +1,14 @@
 """Philox-4x32-10 known-answer vectors (Random123 kat_vectors) for the
-restatement the GPU normals are checked against, the Box-Muller transform's
-tables against 40-digit values, its table-driven logarithm, sine and cosine
-restated against math, and the restated normals as a distribution."""
+restatement the GPU normals are checked against, the ziggurat's tables
+against their defining equations in 40-digit arithmetic, its
+fast-acceptance rate, its tail sampler against the conditional normal tail,
+and the restated normals as a distribution."""
 import math
 
 import numpy as np
 
-from philox_ref import normal_tables, philox4x32_10, philox_normals_reference, uniforms
+from philox_ref import (fraction, normal_tables, philox4x32_10, philox_normals_reference, zig_fast,
+                        zig_slow)
 
 
 def _kat(ctr, key):
@@ -28,15 +30,22 @@ def test_philox_pi_digits():
         [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
 
 
-def test_uniforms_stay_inside_the_open_interval():
-    lo = np.zeros(1, np.uint64)
-    hi = np.full(1, 0xFFFFFFFF, np.uint64)
-    u1, w = uniforms(lo, lo, lo, lo)
-    assert u1[0] == 2.0 ** -53 and w[0] == 0.0
-    u1, w = uniforms(hi, hi, hi, hi)
-    assert u1[0] == 1.0 - 2.0 ** -53 and w[0] == 1.0 - 2.0 ** -52
-    # the largest normal radius the transform can produce
-    assert math.sqrt(-2.0 * math.log(2.0 ** -53)) < 8.58
+def test_draw_decoding_and_extremes():
+    """A draw's layer is hi >> 21, its sign bit 20 of hi and its fraction the
+    52 bits (hi mod 2^20):lo; the all-zero draw is 0 (accepted) and every draw
+    of the top layer goes to the slow path."""
+    t = normal_tables()
+    zero = np.zeros(1, np.uint64)
+    x, ok = zig_fast(zero, zero, t)
+    assert x[0] == 0.0 and ok[0]
+    hi = np.array([(7 << 21) | (1 << 20) | 0xABCDE], np.uint64)
+    lo = np.array([0x12345678], np.uint64)
+    assert fraction(hi, lo)[0] == float((0xABCDE << 32) | 0x12345678)
+    x, _ = zig_fast(hi, lo, t)
+    assert x[0] == -(fraction(hi, lo)[0] * 2.0 ** -52) * t["xd"][7, 0]
+    top = np.array([0xFFEFFFFF], np.uint64)
+    _, ok = zig_fast(top, np.zeros(1, np.uint64), t)
+    assert not ok[0] and t["xd"][2047, 1] == 1.0
 
 
 def test_normals_moments():
@@ -60,59 +69,74 @@ def test_seeds_differing_only_in_the_high_word_give_different_streams():
     assert not np.array_equal(a, b) and not np.array_equal(a, c)
 
 
-def test_transform_tables_against_40_digit_values():
-    """The library's tables against 40-digit mpmath: r_j, -ln r_j, sin θ_j,
-    cos θ_j, and the two-part ln 2 and 2π."""
+def test_ziggurat_tables_against_40_digit_values():
+    """The library's tables against their defining equations in 40-digit
+    mpmath: every layer's area equal to v, the base layer (rectangle and
+    tail) too, the recursion ending at the top, f(X_i) to its rounding, and
+    each fast bound D_i = 1 + ceil(2^52 X_{i+1}/X_i) 2^-52 (to one unit of
+    K_i).  (For 256 layers the same construction gives Marsaglia and Tsang's
+    published r = 3.6541528853610088.)"""
     import mpmath as mp
     mp.mp.dps = 40
     t = normal_tables()
-    for j in range(128):
-        r = t["lr"][j][0]
-        assert abs(r - float(1 / (1 + (mp.mpf(j) + 0.5) / 128))) <= 2.0 ** -53 * r
-        # extended precision rounded once: within one ulp of the exact value
-        lnr = -mp.log(mp.mpf(r))
-        assert abs(mp.mpf(t["lr"][j][1]) - lnr) <= 2.0 ** -52 * abs(lnr)
-        th = 2 * mp.pi * (mp.mpf(j) + 0.5) / 128
-        for got, want in ((t["sc"][j][0], mp.sin(th)), (t["sc"][j][1], mp.cos(th))):
-            assert abs(mp.mpf(got) - want) <= 2.0 ** -52 * abs(want)
-    # the two parts carry the long double constants (64-bit mantissas): 1e-18 is
-    # far below what e ln 2 (|e| <= 53) and 2π w need
-    assert abs(mp.mpf(t["ln2_hi"]) + mp.mpf(t["ln2_lo"]) - mp.log(2)) < 1e-18
-    assert t["ln2_hi"] * 2.0 ** 42 == int(t["ln2_hi"] * 2.0 ** 42)   # e * hi exact, |e| < 2^11
-    assert abs(mp.mpf(t["twopi_hi"]) + mp.mpf(t["twopi_lo"]) - 2 * mp.pi) < 1e-18
+    n = len(t["xd"])
+    X = [mp.mpf(float(x)) for x in t["xd"][:, 0]] + [mp.mpf(0)]
+    r, v = X[1], mp.mpf(float(t["v"]))
+    assert n == 2048 and 4.2 < float(t["r"]) < 4.23 and X[1] == mp.mpf(float(t["r"]))
+    f = lambda x: mp.exp(-x * x / 2)
+    base = r * f(r) + mp.sqrt(mp.pi / 2) * mp.erfc(r / mp.sqrt(2))
+    assert abs(base - v) <= 1e-15 * v
+    assert abs(X[0] * f(r) - v) <= 1e-15 * v
+    for i in range(1, n):
+        area = X[i] * (f(X[i + 1]) - f(X[i]))
+        assert abs(area - v) <= 2e-12 * v, (i, float(area / v - 1))
+    assert abs(f(X[n - 1]) + v / X[n - 1] - 1) <= 1e-14
+    # f was rounded once from the extended-precision X_i, X_i once to double:
+    # both within an ulp, and |d ln f / d ln X| = X² < 16
+    for i in range(n + 1):
+        assert abs(mp.mpf(float(t["f"][i])) - f(X[i])) <= 2.0 ** -52 * (1 + X[i] ** 2) * f(X[i])
+    # K_i comes from the extended-precision X: within one unit of the value
+    # from the double X_i
+    for i in range(n):
+        k = mp.ceil(mp.ldexp(X[i + 1] / X[i], 52))
+        assert abs(mp.ldexp(mp.mpf(float(t["xd"][i, 1])) - 1, 52) - k) <= 1
 
 
-def test_table_driven_transform_restated():
-    """The device's table-driven logarithm, sine and cosine (hj_device.cuh,
-    box_muller_f64) restated in float64 with the library's tables, against
-    40-digit logarithms, sines and cosines on uniforms that span their
-    ranges."""
-    import mpmath as mp
-    mp.mp.dps = 40
+def test_fast_acceptance_rate():
+    """The fraction of draws the fast path accepts is the mean of
+    X_{i+1}/X_i over the layers (99.77 % for 2048 layers); 1e6 restated first
+    draws agree within 4 standard errors."""
+    from philox_ref import philox_words
     t = normal_tables()
-    rng = np.random.default_rng(4)
-    us = np.concatenate([rng.random(3000), 2.0 ** -rng.uniform(1, 53, 3000),
-                         [2.0 ** -53, 0.5, 1 - 2.0 ** -53]])
-    for u in us:
-        m, e = math.frexp(u)                       # u = m 2^e, m in [0.5, 1)
-        m, e = 2 * m, e - 1
-        j = int((m - 1) * 128)
-        r, nlr = t["lr"][j]
-        tt = m * r - 1.0
-        q = sum((-1) ** (k + 1) * tt ** (k - 1) / k for k in range(1, 7))
-        got = e * t["ln2_hi"] + nlr + e * t["ln2_lo"] + tt * q
-        want = float(mp.log(mp.mpf(u)))
-        assert abs(got - want) <= 6e-16 * max(1.0, abs(want))
-    for w in np.concatenate([rng.random(3000), [0.0, 0.5, 1 - 2.0 ** -52]]):
-        k = int(w * 128)
-        xs = w - (k + 0.5) / 128
-        a = xs * t["twopi_hi"] + xs * t["twopi_lo"]
-        sn = sum((-1) ** i * a ** (2 * i + 1) / math.factorial(2 * i + 1) for i in range(4))
-        cm1 = sum((-1) ** i * a ** (2 * i) / math.factorial(2 * i) for i in range(1, 5))
-        sk, ck = t["sc"][k]
-        th = 2 * mp.pi * mp.mpf(w)
-        assert abs(sk * (1 + cm1) + ck * sn - float(mp.sin(th))) <= 4e-16
-        assert abs(ck * (1 + cm1) - sk * sn - float(mp.cos(th))) <= 4e-16
+    X = np.append(t["xd"][:, 0], 0.0)
+    p = float(np.mean(X[1:] / X[:-1]))
+    assert 0.9975 < p < 0.998
+    w0, w1, w2, w3 = philox_words(99, 4, np.arange(500_000, dtype=np.uint64))
+    ok = np.concatenate([zig_fast(w1, w0, t)[1], zig_fast(w3, w2, t)[1]])
+    n = ok.size
+    assert abs(ok.sum() - n * p) <= 4 * math.sqrt(n * p * (1 - p))
+
+
+def test_tail_sampler_is_the_conditional_normal_tail():
+    """Draws of the base layer beyond r go to Marsaglia's tail method: 2e5 of
+    them (distinct pairs) follow P(|x| > s | |x| > r) = erfc(s/√2)/erfc(r/√2)
+    (KS at the 1 % level), with the draw's sign."""
+    from scipy.special import erfc
+    t = normal_tables()
+    n = 200_000
+    hi = np.full(n, 0x000FFFFF, np.uint64)          # layer 0, positive, fraction near 1
+    lo = np.full(n, 0xFFFFFFFF, np.uint64)
+    assert not np.any(zig_fast(hi, lo, t)[1])
+    x = zig_slow(17, 3, np.arange(n, dtype=np.uint64), 0, hi, lo, t)
+    assert np.all(x > t["r"])
+    xs = np.sort(x)
+    r = t["r"]
+    cdf = 1.0 - erfc(xs / math.sqrt(2.0)) / erfc(r / math.sqrt(2.0))
+    d = max(np.max(np.arange(1, n + 1) / n - cdf), np.max(cdf - np.arange(n) / n))
+    assert d < 1.63 / math.sqrt(n)
+    neg = zig_slow(17, 3, np.arange(8, dtype=np.uint64), 1, hi[:8] | np.uint64(1 << 20),
+                   lo[:8], t)
+    assert np.all(neg < -t["r"])
 
 
 def test_normal_tail_and_ks_of_the_restatement():
