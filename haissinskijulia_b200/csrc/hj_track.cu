@@ -289,22 +289,42 @@ __device__ __forceinline__ int ngp_bin_any(double z, const GridConst& g, bool& i
 // their Taylor series through t^7 and t^6 (truncation below 1e-20); the kick
 // V sin θm (cos t - 1) - V cos θm sin t + (V sin θm - V sin ϕs) is, for m = 0,
 // free of the cancellation in sin(ϕ) - sin ϕs.  No branches.
+// EXACT: every operation rounds where it is written (no contraction), so
+// that a second evaluation anywhere reproduces the result bit for bit (the
+// Float64-normals pass needs that to take a provisional turn back).
+template <bool EXACT>
 __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
                                           const double2* __restrict__ s_rf) {
-  const double x = __dmul_rn(z, c.k);
+  if (EXACT) {
+    const double x = __dmul_rn(z, c.k);
+    const double y = fma(x, c.rf_inv_h, kMagic);
+    const double md = __dsub_rn(y, kMagic);
+    double t = fma(-md, c.rf_h_hi, x);
+    t = fma(-md, c.rf_h_lo, t);
+    const double2 rot = s_rf[__double2loint(y) & (kRfTableSize - 1)];
+    const double t2 = __dmul_rn(t, t);
+    double p = fma(t2, -1.984126984126984e-04, 8.333333333333333e-03);   // -1/7!, 1/5!
+    p = fma(t2, p, -1.6666666666666666e-01);                               // -1/3!
+    const double sn = fma(__dmul_rn(t, t2), p, t);
+    double q = fma(t2, -1.388888888888889e-03, 4.1666666666666664e-02);  // -1/6!, 1/4!
+    q = fma(t2, q, -0.5);
+    const double cm1 = __dmul_rn(t2, q);
+    return __dadd_rn(fma(rot.x, cm1, __dmul_rn(-rot.y, sn)), __dsub_rn(rot.x, c.Vs));
+  }
+  const double x = z * c.k;
   const double y = fma(x, c.rf_inv_h, kMagic);
-  const double md = __dsub_rn(y, kMagic);
+  const double md = y - kMagic;
   double t = fma(-md, c.rf_h_hi, x);
   t = fma(-md, c.rf_h_lo, t);
   const double2 rot = s_rf[__double2loint(y) & (kRfTableSize - 1)];
-  const double t2 = __dmul_rn(t, t);
-  double p = fma(t2, -1.984126984126984e-04, 8.333333333333333e-03);   // -1/7!, 1/5!
-  p = fma(t2, p, -1.6666666666666666e-01);                               // -1/3!
-  const double sn = fma(__dmul_rn(t, t2), p, t);
-  double q = fma(t2, -1.388888888888889e-03, 4.1666666666666664e-02);  // -1/6!, 1/4!
+  const double t2 = t * t;
+  double p = fma(t2, -1.984126984126984e-04, 8.333333333333333e-03);
+  p = fma(t2, p, -1.6666666666666666e-01);
+  const double sn = fma(t * t2, p, t);
+  double q = fma(t2, -1.388888888888889e-03, 4.1666666666666664e-02);
   q = fma(t2, q, -0.5);
-  const double cm1 = __dmul_rn(t2, q);
-  return __dadd_rn(fma(rot.x, cm1, __dmul_rn(-rot.y, sn)), __dsub_rn(rot.x, c.Vs));
+  const double cm1 = t2 * q;
+  return fma(rot.x, cm1, -rot.y * sn) + (rot.x - c.Vs);
 }
 
 // One particle for one turn, given its wake kick (lerp of the previous turn's
@@ -314,25 +334,39 @@ __device__ __forceinline__ double rf_term(double z, const FusedConst& c,
 // SR, drift.  Without update_η the drift coefficient is the constant-η one
 // (zero when apply_phase_advance! would skip the advance).  The moments and
 // deposits of the new z follow in deposit_group.
-template <bool WAKE>
+template <bool WAKE, bool EXACT = false>
 __device__ __forceinline__ void particle_turn(double& z, double& e, double r, double kick,
                                               double rf, const FusedConst& c, double pmean,
                                               double& acc_d) {
-  // every operation rounds where it is written (no contraction), so that a
-  // second evaluation anywhere reproduces the turn bit for bit
-  if (WAKE) e = __dsub_rn(e, kick);
-  e = __dsub_rn(e, pmean);
+  if (EXACT) {   // every operation rounds where it is written (see rf_term)
+    if (WAKE) e = __dsub_rn(e, kick);
+    e = __dsub_rn(e, pmean);
+    const double e_start = e;
+    e = __dadd_rn(e, rf);
+    e = fma(c.excitation, r, e);
+    e = __dmul_rn(e, c.damping);
+    const double gp = fma(e, c.inv_mass, c.gamma0);
+    const double g2 = __dmul_rn(gp, gp);
+    double ri = rcp_approx(g2);
+    ri = fma(ri, fma(-g2, ri, 1.0), ri);
+    const double coeff = c.update_eta ? __dmul_rn(c.Kz, __dsub_rn(c.alpha_c, ri)) : c.coeff0z;
+    z = fma(-coeff, e, z);
+    acc_d += __dsub_rn(e, e_start);
+    return;
+  }
+  if (WAKE) e = e - kick;
+  e = e - pmean;
   const double e_start = e;
-  e = __dadd_rn(e, rf);
+  e = e + rf;
   e = fma(c.excitation, r, e);                         // r = 0 without QE
-  e = __dmul_rn(e, c.damping);                         // damping = 1 without SR
+  e = e * c.damping;                                   // damping = 1 without SR
   const double gp = fma(e, c.inv_mass, c.gamma0);     // γ0 + ΔE/m
-  const double g2 = __dmul_rn(gp, gp);
+  const double g2 = gp * gp;
   double ri = rcp_approx(g2);
   ri = fma(ri, fma(-g2, ri, 1.0), ri);
-  const double coeff = c.update_eta ? __dmul_rn(c.Kz, __dsub_rn(c.alpha_c, ri)) : c.coeff0z;
+  const double coeff = c.update_eta ? c.Kz * (c.alpha_c - ri) : c.coeff0z;
   z = fma(-coeff, e, z);
-  acc_d += __dsub_rn(e, e_start);
+  acc_d += e - e_start;
 }
 
 // Moments and deposits of K particles' new z: Σz, Σz², the NGP count and, in
@@ -542,13 +576,13 @@ __device__ __forceinline__ void finish_deferred(const PassArgs& a, const FusedCo
   const uint32_t whi = h ? w[3] : w[1], wlo = h ? w[2] : w[0];
   double xg;
   zig_fast(whi, wlo, s_zt, xg);
-  const double rf = rf_term(z0, c, s_rf);
+  const double rf = rf_term<true>(z0, c, s_rf);
   double zg = z0, eg = e0, dg = 0.0;
-  particle_turn<WAKE>(zg, eg, xg, kick, rf, c, pmean, dg);
+  particle_turn<WAKE, true>(zg, eg, xg, kick, rf, c, pmean, dg);
   const double r = zig_slow(a.seed, turn, pr, h, whi, wlo, &g_normal);
   double z1[1] = {z0};
   double e1 = e0, d1 = 0.0;
-  particle_turn<WAKE>(z1[0], e1, r, kick, rf, c, pmean, d1);
+  particle_turn<WAKE, true>(z1[0], e1, r, kick, rf, c, pmean, d1);
   acc_d = __dadd_rn(__dsub_rn(acc_d, dg), d1);
   if (WAKE) {
     undeposit<N32>(zg, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
@@ -744,13 +778,14 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     }
     double rf[PPT];
 #pragma unroll
-    for (int j = 0; j < PPT; ++j) rf[j] = rf_term(zz[j], c, s_rf);
+    for (int j = 0; j < PPT; ++j) rf[j] = rf_term<kDefer>(zz[j], c, s_rf);
     double zs[PPT], es[PPT];               // what is stored
 #pragma unroll
     for (int j = 0; j < PPT; ++j) {
       const double z0 = zz[j], e0 = ee[j];
-      particle_turn<WAKE>(zz[j], ee[j], rr[j], WAKE ? fma(kf[j].w, kf[j].d, kf[j].p0) : 0.0,
-                          rf[j], c, pmean, acc_d);
+      particle_turn<WAKE, kDefer>(zz[j], ee[j], rr[j],
+                                  WAKE ? fma(kf[j].w, kf[j].d, kf[j].p0) : 0.0, rf[j], c, pmean,
+                                  acc_d);
       const bool keep = kDefer && !((ok >> j) & 1u);
       zs[j] = keep ? z0 : zz[j];
       es[j] = keep ? e0 : ee[j];
@@ -785,7 +820,8 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     double z1[1] = {a.z[i]};
     double e = a.dE[i];
     const double kick = WAKE ? wake_kick(z1[0], g, potd) : 0.0;
-    particle_turn<WAKE>(z1[0], e, r, kick, rf_term(z1[0], c, s_rf), c, pmean, acc_d);
+    particle_turn<WAKE, kDefer>(z1[0], e, r, kick, rf_term<kDefer>(z1[0], c, s_rf), c, pmean,
+                               acc_d);
     if (WAKE) deposit_group<1, N32>(z1, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
     a.z[i] = z1[0];
     a.dE[i] = e;
