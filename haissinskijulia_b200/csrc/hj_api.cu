@@ -281,19 +281,15 @@ hj_status read_state(hj_bunch* b) {
 // next group, one 32-bit counter per bin (1e8 particles, 16384 bins: 0.81 ms
 // per pass against 0.83 with 16-bit pairs, whose larger kick-table window
 // does not make up for their overflow checks).
-int default_pass_layout(int B, int64_t n, bool zig) {
+int default_pass_layout(int B, int64_t n) {
+  (void)B;
   (void)n;
-  // with the Float64 normals' ziggurat table in shared memory, above 8192
-  // bins the 32-bit counters would leave almost no room for the kick-table
-  // window: 16-bit counter pairs there
-  return (zig && B > 8192) ? 0 : (0 | kPassN32);
+  return 0 | kPassN32;
 }
 
-// The library's layout for a request r: the automatic one for bins B, with
-// the ziggurat's table unless single-precision normals are asked for.
-int auto_pass_layout(int r, int B, int64_t n, bool philox) {
-  const bool fast = r == kPassAutoFast || (r >= 0 && (r & kPassFastNormals));
-  return resolve_pass_request(r, default_pass_layout(B, n, philox && !fast));
+// The library's layout for a request r (-1: the default for B bins).
+int auto_pass_layout(int r, int B, int64_t n) {
+  return resolve_pass_request(r, default_pass_layout(B, n));
 }
 
 void fill_result(hj_bunch* b, const double m[4], hj_result* res) {
@@ -484,7 +480,7 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
     b->H = b->M / 2;
     b->logH = b->H >= 1 ? ilog2(b->H) : 0;
   }
-  b->cfg = cfg >= 0 ? cfg : auto_pass_layout(ctx->pass_layout, b->B, n, b->qe_mode == QE_PHILOX);
+  b->cfg = cfg >= 0 ? cfg : auto_pass_layout(ctx->pass_layout, b->B, n);
   if (chunk > 0) {
     b->batch_member = true;
     b->nblk = (int)std::max<int64_t>((n + chunk - 1) / chunk, 1);
@@ -506,11 +502,11 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
         defer ? c.add<int64_t>(nb * (size_t)(pass_cfg_threads(b->cfg) / 32) * kDeferStage) : 0;
     size_t o[6] = {};
     if (b->use_wake) {
-      // pot, potd, hist and ngp_ovf are adjacent: one memset zeroes them
+      // pot, potd, hist and hist_spill are adjacent: one memset zeroes them
       o[0] = c.add<double>(B);                                   // pot
       o[1] = c.add<double2>(B + 1);                              // potd
       o[2] = c.add<unsigned long long>(3 * B + 2);               // hist
-      o[3] = c.add<unsigned long long>(B);                       // ngp_ovf
+      o[3] = c.add<unsigned long long>(3 * B + 2);               // hist_spill
       b->zero_bytes = c.off - o[0];
       o[4] = c.add<uint32_t>(nb * B);                            // part_cnt
       o[5] = c.add<unsigned long long>(nb * (B + 1));            // part_cic
@@ -526,7 +522,7 @@ hj_status hj_impl::bunch_create_begin(hj_ctx* ctx, double* d_z, double* d_dE, in
       b->pot = (double*)(a + o[0]);
       b->potd = (double2*)(a + o[1]);
       b->hist = (unsigned long long*)(a + o[2]);
-      b->ngp_ovf = (unsigned long long*)(a + o[3]);
+      b->hist_spill = (unsigned long long*)(a + o[3]);
       b->part_cnt = (uint32_t*)(a + o[4]);
       b->part_cic = (unsigned long long*)(a + o[5]);
     }
@@ -751,7 +747,11 @@ void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
   a.ts = b->ts;
   a.potd = b->potd;
   a.zig = (b->qe_mode == QE_PHILOX && !(b->cfg & kPassFastNormals)) ? 1 : 0;
-  a.win = b->use_wake ? track_window_entries(b->B, b->cfg, a.zig != 0) : 0;
+  if (b->use_wake) {
+    const PassWindows w = track_windows(b->B, b->cfg, a.zig != 0);
+    a.win = w.kick;
+    a.hwin = w.hot;
+  }
   a.B = b->B;
   a.use_wake = b->use_wake;
   a.e0 = b->e0;
@@ -788,7 +788,7 @@ void hj_impl::fill_turn_args(const hj_bunch* b, PassArgs& a, BinsArgs& g) {
   a.part_cic = b->part_cic;
   a.part_sum = b->part_sum;
   a.hist_out = b->hist;
-  a.ngp_ovf = b->ngp_ovf;
+  a.hist_spill = b->hist_spill;
 
   g = BinsArgs{};
   g.ts = b->ts;
@@ -846,7 +846,7 @@ extern "C" hj_status hj_bunch_advance(hj_bunch* b, int64_t turns) {
     if (b->profiling) HJ_CUDA(ctx, cudaEventRecord(ev[1], b->stream));
     if (b->use_wake)
       HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->hist, false,
-                                      b->stream, b->ngp_ovf));
+                                      b->stream, b->hist_spill));
     HJ_CUDA(ctx, launch_bins(g, b->stream));
     if (b->profiling) {
       HJ_CUDA(ctx, cudaEventRecord(ev[2], b->stream));

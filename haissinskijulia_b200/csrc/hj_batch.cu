@@ -225,7 +225,7 @@ static hj_status batch_create_impl(hj_ctx* ctx, int64_t pool_particles, int32_t 
   const int64_t P = next_pow2(2 * (int64_t)max_nbins);
   bt->max_H = (int)std::max<int64_t>(P / 4, 4);
   bt->bins_ctas = batch_bins_ctas(bt->max_H, max_bunches, ctx->num_sms);
-  bt->cfg = auto_pass_layout(layout, max_nbins, pool_particles, true);
+  bt->cfg = auto_pass_layout(layout, max_nbins, pool_particles);
   bt->pool_n = (pool_particles + 3) / 4 * 4;
   bt->max_chunks = (int)std::min<int64_t>(bt->pool_n / chunk + max_bunches + 1, INT32_MAX);
   HJ_CUDA(ctx, cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking));

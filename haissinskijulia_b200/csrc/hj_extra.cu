@@ -80,7 +80,7 @@ extern "C" hj_status hj_bunch_pass(hj_bunch* b) {
   fill_turn_args(b, a, g);
   HJ_CUDA(ctx, launch_track_pass(a, b->nblk, b->stream));
   HJ_CUDA(ctx, launch_hist_reduce(b->part_cnt, b->part_cic, b->nblk, b->B, b->hist, false,
-                                  b->stream, b->ngp_ovf));
+                                  b->stream, b->hist_spill));
   HJ_CUDA(ctx, launch_sum_parts(b->part_sum, b->nblk, b->d_sums, b->stream));
   return HJ_OK;
 }

@@ -77,13 +77,15 @@ struct PassArgs {
   unsigned long long* part_cic;    // [grid][B+1] packed cell deposit (count << 44 | Σw·2^24)
   double* part_sum;                // [grid][kNumSums]
   unsigned long long* hist_out;    // [3B+2] merged histograms, zeroed by the pass
-  unsigned long long* ngp_ovf;     // [B] counts beyond the 16-bit per-block counters
+  unsigned long long* hist_spill;  // [3B+2] deposits outside the hot window and beyond the
+                                   // 16-bit counters (the merged layout), cleared by the merge
   int32_t n_parts;                 // partial slots written per turn (batches)
   int64_t pair_offset;             // Philox pair index of particle 0 (shards of a bunch)
   int64_t* defer_q;                // [partial slots][warps][kDeferStage]: indices of the
                                    // particles whose Float64 normal takes the slow path
   int32_t zig;                     // 1: shared memory holds the ziggurat's rows (the pass
                                    // draws the Float64 normals), 0: the RF table alone
+  int32_t hwin;                    // bins and cells of the pass's hot histogram window
 };
 
 // One entry of a batch's chunk table: particles [first, first + count) of
@@ -150,9 +152,13 @@ int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg);
 // zig: the pass draws the Float64 normals (QE_PHILOX without the fast bit),
 // so its shared memory holds the ziggurat's rows.
 size_t track_smem_bytes(int B, int use_wake, int cfg, bool zig);
-// Kick-table entries the fused pass keeps in shared memory for B bins
-// (what the shared-memory budget leaves beside the histograms, at most B).
-int track_window_entries(int B, int cfg, bool zig);
+// Shared-memory windows of the fused pass for B bins (with the wake): `hot`
+// bins and cells whose per-block histograms are in shared memory (at most
+// B + 1), and `kick` kick-table entries (0 up to 4096 bins, else min(hot, B)).
+struct PassWindows {
+  int32_t hot, kick;
+};
+PassWindows track_windows(int B, int cfg, bool zig);
 cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st);
 // Batched pass over a chunk table (*d_n_chunks entries live, grid max_chunks)
 // and the per-bunch merge of its partials.
@@ -170,7 +176,7 @@ cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const BatchChunk* d_i
 // zero_first clears out before the merge (the fused pass clears it itself).
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
                                int nblk, int B, unsigned long long* out, bool zero_first,
-                               cudaStream_t st, unsigned long long* ovf = nullptr);
+                               cudaStream_t st, unsigned long long* spill = nullptr);
 cudaError_t launch_flush(const FlushArgs& a, int grid, cudaStream_t st);
 // generate_particles on the device (covariance sample, correlated bunch, two-pass std)
 cudaError_t launch_gen_sample_cov(uint64_t seed, int64_t S, double mu_z, double sz, double mu_E,

@@ -20,6 +20,9 @@ constexpr int kNumPassCfgs = 6;       // thread layouts of the fused pass
 constexpr int kPassLayoutMask = 7;    // layout bits of a pass configuration
 constexpr int kPassN32 = 8;           // + one 32-bit NGP counter per bin (else 16-bit pairs)
 constexpr int kPassFastNormals = 16;  // + single-precision quantum-excitation normals
+// Launch-only bit (never in a caller's configuration): the pass's hot window
+// holds fewer than all B + 1 cells, so its deposits are range-checked.
+constexpr int kPassWindowed = 32;
 
 inline int pass_cfg_threads(int cfg) {
   const int l = cfg & kPassLayoutMask;

@@ -108,7 +108,8 @@ struct hj_bunch {
   uint32_t* part_cnt = nullptr;
   int64_t* defer_q = nullptr;             // [nblk][warps][kDeferStage] (Float64 normals)
   unsigned long long* part_cic = nullptr;
-  unsigned long long* ngp_ovf = nullptr;   // [B] overflow of the pass's 16-bit counters
+  unsigned long long* hist_spill = nullptr;   // [3B+2] the pass's deposits outside its hot
+                                              // window and beyond its 16-bit counters
   double2* rf_table = nullptr;             // [kRfTableSize] RF kick table of the pass
   double rf_Vs = 0;                        // its entry 0: V sin ϕs
   double* part_sum = nullptr;
@@ -119,7 +120,7 @@ struct hj_bunch {
   // the buffers above are carved from one device block and one pinned block
   // of the context's cache; twP is the context's shared table; W, lam and Wf
   // point into a wake set shared with other bunches (wset) or a private block
-  // (tables); pot, potd, hist and ngp_ovf are the first zero_bytes of the
+  // (tables); pot, potd, hist and hist_spill are the first zero_bytes of the
   // arena's histogram part
   hj_ctx::WakeSet* wset = nullptr;
   bool batch_member = false;
@@ -212,8 +213,8 @@ hj_status read_moments(hj_bunch* b, double m[4]);
 hj_status launch_moments(hj_bunch* b, int apply, double* z_out, double* dE_out);
 hj_status state_status(hj_bunch* b);
 hj_status read_state(hj_bunch* b);
-int default_pass_layout(int B, int64_t n, bool zig);
-int auto_pass_layout(int r, int B, int64_t n, bool philox);
+int default_pass_layout(int B, int64_t n);
+int auto_pass_layout(int r, int B, int64_t n);
 void fill_result(hj_bunch* b, const double m[4], hj_result* res);
 cudaError_t set_kernel_attributes(hj_ctx* ctx);
 

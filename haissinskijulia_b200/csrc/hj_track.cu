@@ -172,18 +172,27 @@ __device__ __forceinline__ double2 ld_table(const double2* p) {
   return v;
 }
 
-// The pass's shared-memory window of the kick table: s_win[i] = pot_left[w0 + i]
-// (the left value, .x, of table cell w0 + i) for i < lim + 1, where the cells
-// j with w0 <= j < w0 + lim are "hot": their left value and their right
-// neighbour's left value are both in the window.  For cells 1..B-2 the step
-// of the global table is pot[j] - pot[j-1] = pot_left[j+1] - pot_left[j], and
-// for cell 0 it is pot[0] - pot[0] = 0, so a hot cell's (left value, step)
-// from the window is bit-identical to its global entry.  Cells B-1 and B
-// (whose step or value the bins step sets differently) are never hot.
-struct KickWindow {
+// The pass's shared-memory windows, both starting at cell w0 (centred on the
+// cell of the last turn's mean z).
+// * Kick table: s_win[i] = pot_left[w0 + i] (the left value, .x, of table
+//   cell w0 + i) for i < lim + 1, where the cells j with w0 <= j < w0 + lim
+//   are "hot": their left value and their right neighbour's left value are
+//   both in the window.  For cells 1..B-2 the step of the global table is
+//   pot[j] - pot[j-1] = pot_left[j+1] - pot_left[j], and for cell 0 it is
+//   pot[0] - pot[0] = 0, so a hot cell's (left value, step) from the window
+//   is bit-identical to its global entry.  Cells B-1 and B (whose step or
+//   value the bins step sets differently) are never hot.
+// * Histograms: bins and cells w0 .. w0 + h - 1 have their per-block
+//   counters in shared memory.  A deposit outside goes to the bunch's spill
+//   histograms in global memory (u64, laid out as the merged ones: counts [B]
+//   | cell counts [B+1] | cell Σw·2^24 [B+1]), which the merge folds in and
+//   clears; h = B + 1 (w0 = 0) where all cells fit.
+struct PassWindow {
   const double* s_win;
   int w0;
   unsigned lim;
+  unsigned h;
+  unsigned inner;   // max(h, 1) - 1: cells w0 + 1 .. w0 + inner have their bin inside too
 };
 
 // Table entry and weight of the kick of z (issued early: the gather's latency
@@ -193,7 +202,7 @@ struct KickFetch {
   double p0, d, w;
 };
 __device__ __forceinline__ KickFetch kick_fetch(double z, const GridConst& g,
-                                                const KickWindow& kw,
+                                                const PassWindow& kw,
                                                 const double2* __restrict__ potd) {
   int j;
   KickFetch f;
@@ -372,15 +381,24 @@ __device__ __forceinline__ void particle_turn(double& z, double& e, double r, do
 // Moments and deposits of K particles' new z: Σz, Σz², the NGP count and, in
 // the kick-table cell the next pass reads for this z, the cell count and
 // Σ w·2^24.  The shared atomics of all K particles are issued before any of
-// their returned values is used, so their latencies overlap.
-template <int K, bool N32>
+// their returned values is used, so their latencies overlap.  s_ngp, s_lo and
+// s_hi are the shared arrays offset by the window's start (w0 even, so that
+// bin b is at word b >> 1, half b & 1, of the 16-bit pairs): bin b's counter
+// is s_ngp[b] (s_ngp[b >> 1]), cell c's words s_lo[c], s_hi[c], for b and c
+// in the window.  An in-range particle's bin is its cell or the one below, so
+// a cell in (w0, w0 + h) puts both in the window: when all K are there the
+// deposits run unchecked, else each is checked and spilled when outside.
+// Without WIN the window holds every cell and nothing is checked.
+template <int K, bool N32, bool WIN>
 __device__ __forceinline__ void deposit_group(const double (&z)[K], const GridConst& g,
-                                              double& acc_z, double& acc_z2, int32_t& n_in,
-                                              uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
-                                              unsigned long long* __restrict__ ngp_ovf) {
+                                              const PassWindow& hw, double& acc_z,
+                                              double& acc_z2, int32_t& n_in, uint32_t* s_ngp,
+                                              uint32_t* s_lo, uint32_t* s_hi,
+                                              unsigned long long* __restrict__ spill) {
   int nb[K], cj[K];
   bool nin[K];
   uint32_t cq[K];
+  bool inner = true;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     acc_z += z[k];
@@ -391,35 +409,61 @@ __device__ __forceinline__ void deposit_group(const double (&z)[K], const GridCo
     // w·2^24 rounded to nearest (at most 2^24; a NaN z lands in cell B with
     // any q and is flagged by the moments)
     cq[k] = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
+    if (WIN) inner &= (uint32_t)(cj[k] - hw.w0 - 1) < hw.inner;
   }
-  uint32_t ong[K];
+  uint32_t ong[K], olo[K];
+  if (inner) {
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    ong[k] = 0u;
-    if (nin[k]) {
-      if (N32) {
-        atomicAdd(&s_ngp[nb[k]], 1u);   // one 32-bit counter per bin, no return value used
+    for (int k = 0; k < K; ++k) {
+      ong[k] = 0u;
+      if (nin[k]) {
+        if (N32) {
+          atomicAdd(&s_ngp[nb[k]], 1u);   // one 32-bit counter per bin, no return value used
+        } else {
+          ong[k] = atomicAdd(&s_ngp[nb[k] >> 1], 1u << ((nb[k] & 1) << 4));
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) olo[k] = atomicAdd(&s_lo[cj[k]], cq[k]);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      atomicAdd(&s_hi[cj[k]], (1u << (kCicSumBits - 32)) + (olo[k] + cq[k] < olo[k] ? 1u : 0u));
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      ong[k] = 0u;
+      if (nin[k]) {
+        if ((uint32_t)(nb[k] - hw.w0) < hw.h) {
+          if (N32) atomicAdd(&s_ngp[nb[k]], 1u);
+          else ong[k] = atomicAdd(&s_ngp[nb[k] >> 1], 1u << ((nb[k] & 1) << 4));
+        } else {
+          atomicAdd(spill + nb[k], 1ull);
+          nin[k] = false;                 // no 16-bit counter to check below
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if ((uint32_t)(cj[k] - hw.w0) < hw.h) {
+        olo[k] = atomicAdd(&s_lo[cj[k]], cq[k]);
+        atomicAdd(&s_hi[cj[k]], (1u << (kCicSumBits - 32)) + (olo[k] + cq[k] < olo[k] ? 1u : 0u));
       } else {
-        ong[k] = atomicAdd(&s_ngp[nb[k] >> 1], 1u << ((nb[k] & 1) << 4));
+        atomicAdd(spill + g.B + cj[k], 1ull);
+        atomicAdd(spill + 2 * g.B + 1 + cj[k], (unsigned long long)cq[k]);
       }
     }
   }
-  uint32_t olo[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) olo[k] = atomicAdd(&s_lo[cj[k]], cq[k]);
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-    atomicAdd(&s_hi[cj[k]], (1u << (kCicSumBits - 32)) + (olo[k] + cq[k] < olo[k] ? 1u : 0u));
   if (!N32) {
     // 16-bit counters, two bins per word: the increment that takes a counter
-    // to 2^15 moves 2^15 counts to the global overflow array (the counter has
-    // another 2^15 - 1 increments of room before the move lands)
+    // to 2^15 moves 2^15 counts to the spill counts (the counter has another
+    // 2^15 - 1 increments of room before the move lands)
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int sh = (nb[k] & 1) << 4;
       if (nin[k] && ((ong[k] >> sh) & 0xFFFFu) == 0x7FFFu) {
         atomicSub(&s_ngp[nb[k] >> 1], 0x8000u << sh);
-        atomicAdd(ngp_ovf + nb[k], 0x8000ull);
+        atomicAdd(spill + nb[k], 0x8000ull);
       }
     }
   }
@@ -510,13 +554,14 @@ __device__ __forceinline__ unsigned group_normals_zig(const PhiloxKeys& rk, int6
 
 // Takes back what deposit_group added for one particle at z: the moments (to
 // rounding) and the NGP and cell deposits (exactly: the packed cell word
-// loses the 2^44 + q it gained, borrow included; with 16-bit NGP counters the
-// bunch's overflow counts take the -1, modulo 2^64).
+// loses the 2^44 + q it gained, borrow included; the spill histograms, and
+// the spill counts in place of a 16-bit NGP counter, take the negative,
+// modulo 2^64).
 template <bool N32>
-__device__ __forceinline__ void undeposit(double z, const GridConst& g, double& acc_z,
-                                          double& acc_z2, int32_t& n_in, uint32_t* s_ngp,
-                                          uint32_t* s_lo, uint32_t* s_hi,
-                                          unsigned long long* __restrict__ ngp_ovf) {
+__device__ __forceinline__ void undeposit(double z, const GridConst& g, const PassWindow& hw,
+                                          double& acc_z, double& acc_z2, int32_t& n_in,
+                                          uint32_t* s_ngp, uint32_t* s_lo, uint32_t* s_hi,
+                                          unsigned long long* __restrict__ spill) {
   acc_z = __dsub_rn(acc_z, z);
   acc_z2 = fma(-z, z, acc_z2);
   int cj, nb;
@@ -525,12 +570,17 @@ __device__ __forceinline__ void undeposit(double z, const GridConst& g, double& 
   cell_and_bin(z, g, cj, w, nb, nin);
   if (nin) {
     n_in -= 1;
-    if (N32) atomicSub(&s_ngp[nb], 1u);
-    else atomicAdd(ngp_ovf + nb, ~0ull);
+    if (N32 && (uint32_t)(nb - hw.w0) < hw.h) atomicSub(&s_ngp[nb], 1u);
+    else atomicAdd(spill + nb, ~0ull);
   }
   const uint32_t cq = min((uint32_t)__double2loint(fma(w, 16777216.0, kMagic)), 16777216u);
-  const uint32_t old = atomicSub(&s_lo[cj], cq);
-  atomicSub(&s_hi[cj], (1u << (kCicSumBits - 32)) + (old < cq ? 1u : 0u));
+  if ((uint32_t)(cj - hw.w0) < hw.h) {
+    const uint32_t old = atomicSub(&s_lo[cj], cq);
+    atomicSub(&s_hi[cj], (1u << (kCicSumBits - 32)) + (old < cq ? 1u : 0u));
+  } else {
+    atomicAdd(spill + g.B + cj, ~0ull);
+    atomicAdd(spill + 2 * g.B + 1 + cj, 0ull - (unsigned long long)cq);
+  }
 }
 
 // One turn over the bunch.  PPT particles per thread per iteration (4 with the
@@ -554,9 +604,9 @@ constexpr size_t kPassTableBytes = (size_t)(kRfTableSize + kZigLayers) * 16u;
 // turn is evaluated again, bit for bit (particle_turn rounds where written),
 // and taken back (undeposit, and its share of the sums); the turn with the
 // normal from the ziggurat's slow path is then applied, deposited and stored.
-template <bool WAKE, bool N32>
+template <bool WAKE, bool N32, bool WIN>
 __device__ __forceinline__ void finish_deferred(const PassArgs& a, const FusedConst& c,
-                                                const GridConst& g, const KickWindow& kw,
+                                                const GridConst& g, const PassWindow& kw,
                                                 double pmean, int64_t turn, int64_t i,
                                                 const double2* s_zt, const double2* s_rf,
                                                 uint32_t* s_ngp, uint32_t* s_lo,
@@ -585,8 +635,9 @@ __device__ __forceinline__ void finish_deferred(const PassArgs& a, const FusedCo
   particle_turn<WAKE, true>(z1[0], e1, r, kick, rf, c, pmean, d1);
   acc_d = __dadd_rn(__dsub_rn(acc_d, dg), d1);
   if (WAKE) {
-    undeposit<N32>(zg, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
-    deposit_group<1, N32>(z1, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
+    undeposit<N32>(zg, g, kw, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.hist_spill);
+    deposit_group<1, N32, WIN>(z1, g, kw, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi,
+                               a.hist_spill);
   }
   a.z[i] = z1[0];
   a.dE[i] = e1;
@@ -599,9 +650,9 @@ __device__ __forceinline__ void finish_deferred(const PassArgs& a, const FusedCo
 // over the lanes' counts), and finishes them 32 at a time (finish_deferred)
 // -- all of them when `last`, else only full waves, the rest staying queued.
 // Every lane of the warp must take part.
-template <bool WAKE, int PPT, bool N32>
+template <bool WAKE, int PPT, bool N32, bool WIN>
 __device__ __forceinline__ void drain_deferred(const PassArgs& a, const FusedConst& c,
-                                               const GridConst& g, const KickWindow& kw,
+                                               const GridConst& g, const PassWindow& kw,
                                                double pmean, int64_t turn, int64_t qref,
                                                int64_t stride, unsigned long long& pend,
                                                int64_t* wq, int& staged, bool last,
@@ -632,7 +683,7 @@ __device__ __forceinline__ void drain_deferred(const PassArgs& a, const FusedCon
       const int n = min(staged, 32);
       staged -= n;
       if (lane < n)
-        finish_deferred<WAKE, N32>(a, c, g, kw, pmean, turn, __ldcg(wq + staged + lane), s_zt,
+        finish_deferred<WAKE, N32, WIN>(a, c, g, kw, pmean, turn, __ldcg(wq + staged + lane), s_zt,
                                    s_rf, s_ngp, s_lo, s_hi, acc_z, acc_z2, acc_d, n_in);
       __syncwarp();
     }
@@ -640,22 +691,25 @@ __device__ __forceinline__ void drain_deferred(const PassArgs& a, const FusedCon
   }
 }
 
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = false>
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, bool N32 = false,
+          bool WIN = false>
 __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg,
                                           unsigned char* smem_raw) {
   // dynamic shared memory: RF table [128] | the ziggurat's rows [2048] (a.zig) |
-  // kick-table window [win] | NGP counters | cell words lo, hi [B+1]; NGP
-  // counters: (B+1)/2 words of two 16-bit counters, or B 32-bit ones (N32)
+  // kick-table window [win] | NGP counters | cell words lo, hi [hot] for the
+  // hot window's `hot` bins and cells; NGP counters: (hot+1)/2 words of two
+  // 16-bit counters, or hot 32-bit ones (N32)
   const int nc = a.B + 1;                 // kick-table cells
-  const int nw = N32 ? a.B : (a.B + 1) / 2;
+  const int hot = WAKE ? a.hwin : 0;
+  const int nw = N32 ? hot : (hot + 1) / 2;
   const int win = WAKE ? a.win : 0;
   double2* s_rf = reinterpret_cast<double2*>(smem_raw);
   double2* s_zt = s_rf + kRfTableSize;
   double* s_win = reinterpret_cast<double*>(
       smem_raw + (a.zig ? kPassTableBytes : kRfTableSize * sizeof(double2)));
-  uint32_t* s_ngp = reinterpret_cast<uint32_t*>(s_win + win);
-  uint32_t* s_lo = s_ngp + (WAKE ? nw : 0);
-  uint32_t* s_hi = s_lo + (WAKE ? nc : 0);
+  uint32_t* const h_ngp = reinterpret_cast<uint32_t*>(s_win + win);
+  uint32_t* const h_lo = h_ngp + nw;
+  uint32_t* const h_hi = h_lo + hot;
   for (int i = threadIdx.x; i < kRfTableSize; i += THREADS) s_rf[i] = __ldg(a.rf_table + i);
   if (QE == QE_PHILOX)
     for (int i = threadIdx.x; i < kZigLayers; i += THREADS)
@@ -694,27 +748,37 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     }
   }
 
-  // window of the kick table centred on the cell of the last turn's mean z:
-  // entries w0 .. w0 + wv - 1 (wv <= win, never beyond cell B - 1)
-  KickWindow kw{s_win, 0, 0u};
+  // windows centred on the cell of the last turn's mean z: histogram cells
+  // w0 .. w0 + hot - 1 (never beyond cell B) and kick-table entries w0 .. w0 +
+  // wv - 1 (wv <= win, never beyond cell B - 1)
+  PassWindow kw{s_win, 0, 0u, 0u, 0u};
   if (WAKE) {
-    for (int i = threadIdx.x; i < nc; i += THREADS) {
-      if (i < nw) s_ngp[i] = 0u;
-      s_lo[i] = 0u;
-      s_hi[i] = 0u;
+    for (int i = threadIdx.x; i < hot; i += THREADS) {
+      if (i < nw) h_ngp[i] = 0u;
+      h_lo[i] = 0u;
+      h_hi[i] = 0u;
     }
-    if (win > 0) {
+    int w0 = 0;
+    if (WIN && hot < nc) {   // even, so that the 16-bit pairs keep bin b at word b >> 1
       int jm;
       double wm;
       kick_cell(ts->last_mean_z, g, jm, wm);
-      const int w0 = max(0, min(jm - win / 2, a.B - win));
+      w0 = max(0, min(jm - hot / 2, nc - hot)) & ~1;
+    }
+    kw.w0 = w0;
+    kw.h = (unsigned)hot;
+    kw.inner = hot > 0 ? (unsigned)hot - 1u : 0u;
+    if (win > 0) {
       const int wv = min(win, a.B - w0);
       for (int i = threadIdx.x; i < wv; i += THREADS) s_win[i] = a.potd[w0 + i].x;
-      kw.w0 = w0;
       kw.lim = (unsigned)max(wv - 1, 0);
     }
   }
   __syncthreads();
+  // the histograms indexed by absolute bin and cell (valid inside the window)
+  uint32_t* const s_ngp = h_ngp - (N32 ? kw.w0 : kw.w0 / 2);
+  uint32_t* const s_lo = h_lo - kw.w0;
+  uint32_t* const s_hi = h_hi - kw.w0;
 
   double acc_z = 0.0, acc_z2 = 0.0, acc_d = 0.0;
   int32_t n_in = 0;
@@ -790,13 +854,14 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
       zs[j] = keep ? z0 : zz[j];
       es[j] = keep ? e0 : ee[j];
     }
-    if (WAKE) deposit_group<PPT, N32>(zz, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
+    if (WAKE)
+      deposit_group<PPT, N32, WIN>(zz, g, kw, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.hist_spill);
     stp<PPT>(a.z + PPT * q, zs);
     stp<PPT>(a.dE + PPT * q, es);
     if (kDefer) {
       pend = (pend << PPT) | (unsigned long long)(~ok & ((1u << PPT) - 1u));
       if ((it & 15) == 15 && __activemask() == 0xffffffffu)
-        drain_deferred<WAKE, PPT, N32>(a, c, g, kw, pmean, turn, q, stride, pend, wq, staged,
+        drain_deferred<WAKE, PPT, N32, WIN>(a, c, g, kw, pmean, turn, q, stride, pend, wq, staged,
                                        false, s_zt, s_rf, s_ngp, s_lo, s_hi, acc_z, acc_z2,
                                        acc_d, n_in);
     }
@@ -804,7 +869,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
   if (kDefer) {
     __syncwarp();
     staged = __reduce_max_sync(0xffffffffu, (unsigned)staged);
-    drain_deferred<WAKE, PPT, N32>(a, c, g, kw, pmean, turn, q - stride, stride, pend, wq, staged,
+    drain_deferred<WAKE, PPT, N32, WIN>(a, c, g, kw, pmean, turn, q - stride, stride, pend, wq, staged,
                                    true, s_zt, s_rf, s_ngp, s_lo, s_hi, acc_z, acc_z2, acc_d,
                                    n_in);
   }
@@ -822,7 +887,8 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     const double kick = WAKE ? wake_kick(z1[0], g, potd) : 0.0;
     particle_turn<WAKE, kDefer>(z1[0], e, r, kick, rf_term<kDefer>(z1[0], c, s_rf), c, pmean,
                                acc_d);
-    if (WAKE) deposit_group<1, N32>(z1, g, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.ngp_ovf);
+    if (WAKE)
+      deposit_group<1, N32, WIN>(z1, g, kw, acc_z, acc_z2, n_in, s_ngp, s_lo, s_hi, a.hist_spill);
     a.z[i] = z1[0];
     a.dE[i] = e;
   }
@@ -838,16 +904,21 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const PassRange& rg
     __syncthreads();
     uint32_t* pc = a.part_cnt + (size_t)rg.part * a.B;
     unsigned long long* pq = a.part_cic + (size_t)rg.part * nc;
-    for (int i = threadIdx.x; i < nc; i += THREADS) {
-      if (i < a.B) pc[i] = N32 ? s_ngp[i] : (s_ngp[i >> 1] >> ((i & 1) << 4)) & 0xFFFFu;
-      pq[i] = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
+    for (int i = threadIdx.x; i < nc; i += THREADS) {   // zeros outside the hot window
+      const unsigned r = (unsigned)(i - kw.w0);
+      const bool in = r < kw.h;
+      if (i < a.B)
+        pc[i] = !in ? 0u : N32 ? h_ngp[r] : (h_ngp[r >> 1] >> ((r & 1) << 4)) & 0xFFFFu;
+      pq[i] = in ? ((unsigned long long)h_hi[r] << 32) | h_lo[r] : 0ull;
     }
   }
 }
 
 // One turn over one bunch: block b takes groups b, b + grid, ... (THREADS
-// apart) and writes partial slot b; block 0 takes the tail.
-template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false>
+// apart) and writes partial slot b; block 0 takes the tail.  WIN: the hot
+// window holds fewer than all cells (kPassWindowed).
+template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false,
+          bool WIN = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   grid_dependency_wait();
@@ -858,7 +929,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
   }
   const PassRange rg{(int64_t)blockIdx.x * THREADS, (int64_t)gridDim.x * THREADS, a.n / PPT,
                      (int32_t)blockIdx.x, blockIdx.x == 0};
-  pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
+  pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32, WIN>(a, rg, smem_raw);
 }
 
 // One turn over a batch of bunches.  Chunk c of the chunk table (a
@@ -873,7 +944,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_track_pass(PassArgs a) {
 // the queued form costs about 300 bytes of register spills per thread
 // (ptxas, 4 x 512 layout), which the one-chunk form does not pay.
 template <bool WAKE, int QE, int PPT, int THREADS, bool PREFETCH, int MINB = 1, bool N32 = false,
-          bool QUEUE = false>
+          bool QUEUE = false, bool WIN = false>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_batch_pass(const PassArgs* __restrict__ bunches, const BatchChunk* __restrict__ chunks,
                  const int32_t* __restrict__ n_chunks, int32_t* queue) {
@@ -895,7 +966,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
       }
       const PassRange rg{ch.first / PPT, THREADS, (ch.first + ch.count) / PPT, ch.part,
                          ch.first + ch.count == a.n};
-      pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32>(a, rg, smem_raw);
+      pass_body<WAKE, QE, PPT, THREADS, PREFETCH, N32, WIN>(a, rg, smem_raw);
     }
     if (!QUEUE) break;
     __syncthreads();                   // the chunk's shared memory is read no more
@@ -909,20 +980,29 @@ __global__ void __launch_bounds__(THREADS, MINB)
 // the partials of blocks g, g+G, ... and adds them to the merged arrays with
 // integer atomics (exact, so the result does not depend on their order).
 // out layout (u64): counts[B] | cell counts[B+1] | cell Σw·2^24 [B+1].
-// ovf (optional): counts the pass moved out of its 16-bit counters; folded in
+// spill (optional): the pass's deposits outside its hot window and beyond its
+// 16-bit counters, in out's layout (counts only without part_cic); folded in
 // and cleared for the next turn.
 __global__ void k_hist_reduce(const uint32_t* __restrict__ part_cnt,
                               const unsigned long long* __restrict__ part_cic, int nblk, int B,
                               unsigned long long* __restrict__ out,
-                              unsigned long long* __restrict__ ovf) {
+                              unsigned long long* __restrict__ spill) {
   grid_dependency_wait();
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = B + 1;
   if (b >= (part_cic ? nc : B)) return;
   unsigned long long sc = 0ull, sn = 0ull, sw = 0ull;
-  if (ovf && blockIdx.y == 0 && b < B) {
-    sc = ovf[b];
-    ovf[b] = 0ull;
+  if (spill && blockIdx.y == 0) {
+    if (b < B) {
+      sc = spill[b];
+      if (sc) spill[b] = 0ull;
+    }
+    if (part_cic) {
+      sn = spill[B + b];
+      sw = spill[B + nc + b];
+      if (sn) spill[B + b] = 0ull;
+      if (sw) spill[B + nc + b] = 0ull;
+    }
   }
   for (int k = blockIdx.y; k < nblk; k += gridDim.y) {
     if (b < B) sc += __ldg(part_cnt + (size_t)k * B + b);
@@ -955,9 +1035,16 @@ __global__ void k_batch_reduce(const PassArgs* __restrict__ bunches,
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nc) return;
   unsigned long long sc = 0ull, sn = 0ull, sw = 0ull;
-  if (b < B && it.first == 0) {
-    sc = a.ngp_ovf[b];
-    a.ngp_ovf[b] = 0ull;
+  if (it.first == 0) {   // the spill histograms, once per bunch
+    unsigned long long* sp = a.hist_spill;
+    if (b < B) {
+      sc = sp[b];
+      if (sc) sp[b] = 0ull;
+    }
+    sn = sp[B + b];
+    sw = sp[B + nc + b];
+    if (sn) sp[B + b] = 0ull;
+    if (sw) sp[B + nc + b] = 0ull;
   }
   for (int64_t k = it.first; k < it.first + it.count; ++k) {
     if (b < B) sc += __ldg(a.part_cnt + (size_t)k * B + b);
@@ -1262,23 +1349,34 @@ cudaError_t allow_dynamic_smem(const void* fn, int max_smem_optin) {
 }
 
 namespace {
-// cfg: thread layout (bits 0-2) | kPassN32 (32-bit NGP counters)
-template <bool W, int Q, bool N>
-const void* pass_fn_wqn(int layout) {
+// cfg: thread layout (bits 0-2) | kPassN32 (32-bit NGP counters) |
+// kPassFastNormals | kPassWindowed (range-checked deposits; with the wake only)
+template <bool W, int Q, bool N, bool H>
+const void* pass_fn_wqnh(int layout) {
   switch (layout) {
-    case 0: return (const void*)k_track_pass<W, Q, 4, 512, true, 1, N>;
-    case 1: return (const void*)k_track_pass<W, Q, 2, 1024, true, 1, N>;
-    case 2: return (const void*)k_track_pass<W, Q, 2, 768, true, 1, N>;
-    case 4: return (const void*)k_track_pass<W, Q, 2, 512, true, 2, N>;
-    case 5: return (const void*)k_track_pass<W, Q, 4, 256, true, 2, N>;
-    default: return (const void*)k_track_pass<W, Q, 2, 512, false, 1, N>;
+    case 0: return (const void*)k_track_pass<W, Q, 4, 512, true, 1, N, H>;
+    case 1: return (const void*)k_track_pass<W, Q, 2, 1024, true, 1, N, H>;
+    case 2: return (const void*)k_track_pass<W, Q, 2, 768, true, 1, N, H>;
+    case 4: return (const void*)k_track_pass<W, Q, 2, 512, true, 2, N, H>;
+    case 5: return (const void*)k_track_pass<W, Q, 4, 256, true, 2, N, H>;
+    default: return (const void*)k_track_pass<W, Q, 2, 512, false, 1, N, H>;
   }
+}
+
+template <bool W, int Q, bool N>
+const void* pass_fn_wqn(int cfg) {
+  if constexpr (W) {   // without the wake nothing is deposited: one form
+    if (cfg & kPassWindowed) return pass_fn_wqnh<W, Q, N, true>(cfg & kPassLayoutMask);
+  }
+  return pass_fn_wqnh<W, Q, N, false>(cfg & kPassLayoutMask);
 }
 
 template <bool W, int Q>
 const void* pass_fn_wq(int cfg) {
-  if (W && (cfg & kPassN32)) return pass_fn_wqn<W, Q, true>(cfg & kPassLayoutMask);
-  return pass_fn_wqn<W, Q, false>(cfg & kPassLayoutMask);
+  if constexpr (W) {
+    if (cfg & kPassN32) return pass_fn_wqn<W, Q, true>(cfg);
+  }
+  return pass_fn_wqn<W, Q, false>(cfg);
 }
 
 template <bool W>
@@ -1296,22 +1394,32 @@ const void* pass_fn(int wake, int qe, int cfg) {
   return wake ? pass_fn_w<true>(qe, cfg) : pass_fn_w<false>(qe, cfg);
 }
 
-template <bool W, int Q, bool N, bool U>
-const void* batch_fn_wqnu(int layout) {
+template <bool W, int Q, bool N, bool U, bool H>
+const void* batch_fn_wqnuh(int layout) {
   switch (layout) {
-    case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true, 1, N, U>;
-    case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true, 1, N, U>;
-    case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true, 1, N, U>;
-    case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2, N, U>;
-    case 5: return (const void*)k_batch_pass<W, Q, 4, 256, true, 2, N, U>;
-    default: return (const void*)k_batch_pass<W, Q, 2, 512, false, 1, N, U>;
+    case 0: return (const void*)k_batch_pass<W, Q, 4, 512, true, 1, N, U, H>;
+    case 1: return (const void*)k_batch_pass<W, Q, 2, 1024, true, 1, N, U, H>;
+    case 2: return (const void*)k_batch_pass<W, Q, 2, 768, true, 1, N, U, H>;
+    case 4: return (const void*)k_batch_pass<W, Q, 2, 512, true, 2, N, U, H>;
+    case 5: return (const void*)k_batch_pass<W, Q, 4, 256, true, 2, N, U, H>;
+    default: return (const void*)k_batch_pass<W, Q, 2, 512, false, 1, N, U, H>;
   }
+}
+
+template <bool W, int Q, bool N, bool U>
+const void* batch_fn_wqnu(int cfg) {
+  if constexpr (W) {
+    if (cfg & kPassWindowed) return batch_fn_wqnuh<W, Q, N, U, true>(cfg & kPassLayoutMask);
+  }
+  return batch_fn_wqnuh<W, Q, N, U, false>(cfg & kPassLayoutMask);
 }
 
 template <bool W, int Q, bool U>
 const void* batch_fn_wqu(int cfg) {
-  if (W && (cfg & kPassN32)) return batch_fn_wqnu<W, Q, true, U>(cfg & kPassLayoutMask);
-  return batch_fn_wqnu<W, Q, false, U>(cfg & kPassLayoutMask);
+  if constexpr (W) {
+    if (cfg & kPassN32) return batch_fn_wqnu<W, Q, true, U>(cfg);
+  }
+  return batch_fn_wqnu<W, Q, false, U>(cfg);
 }
 
 // Batches draw QE normals on the device or not at all (no host-fed draws).
@@ -1356,34 +1464,46 @@ size_t pass_table_bytes(bool zig) {
   return zig ? kPassTableBytes : kRfTableSize * sizeof(double2);
 }
 
-// Tables + NGP counts [B] (16-bit, two per word, or 32-bit with kPassN32) +
-// two 32-bit words per kick-table cell [B+1].
-size_t track_hist_bytes(int B, int cfg, bool zig) {
-  const size_t rf = pass_table_bytes(zig);
-  const size_t nw = (cfg & kPassN32) ? (size_t)B : (size_t)((B + 1) / 2);
-  return rf + nw * sizeof(uint32_t) + (size_t)(B + 1) * sizeof(unsigned long long);
-}
 }  // namespace
 
-int track_window_entries(int B, int cfg, bool zig) {
-  // up to 4096 bins the 64 KB kick table stays in L1 beside the histograms:
-  // the window would only add its load to every block (measured: no gain)
-  if (B <= kWindowMinBins) return 0;
-  const size_t used = track_hist_bytes(B, cfg, zig), budget = pass_smem_budget(cfg);
-  if (used >= budget) return 0;
-  const size_t w = (budget - used) / sizeof(double);
-  return (int)std::min<size_t>(w, (size_t)B);
+// The pass's hot window for B bins: per cell a pair of cell words (8 bytes),
+// an NGP counter (4 bytes, or 2 with 16-bit pairs) and, above kWindowMinBins
+// bins, a kick-table entry (8 bytes), as many cells as the shared-memory
+// budget leaves beside the tables, at most B + 1 (up to 4096 bins the 64 KB
+// kick table stays in L1 beside the histograms: a kick window would only add
+// its load to every block, measured no gain).
+PassWindows track_windows(int B, int cfg, bool zig) {
+  const size_t tables = pass_table_bytes(zig), budget = pass_smem_budget(cfg);
+  const bool kick = B > kWindowMinBins;
+  const size_t per = 8 + ((cfg & kPassN32) ? 4 : 2) + (kick ? 8 : 0);
+  const size_t room = budget > tables + 4 ? budget - tables - 4 : 0;   // 4: an odd 16-bit word
+  const size_t hot = std::min(room / per, (size_t)B + 1);
+  PassWindows w;
+  w.hot = (int)hot;
+  w.kick = kick ? (int)std::min(hot, (size_t)B) : 0;
+  return w;
 }
 
-// Tables and histograms plus the kick-table window (wake on); the tables alone
-// otherwise.
+// Tables, and with the wake the windows: kick-table entries, NGP counters and
+// cell words of the hot window.
 size_t track_smem_bytes(int B, int use_wake, int cfg, bool zig) {
   if (!use_wake) return pass_table_bytes(zig);
-  return track_hist_bytes(B, cfg, zig) + (size_t)track_window_entries(B, cfg, zig) * sizeof(double);
+  const PassWindows w = track_windows(B, cfg, zig);
+  const size_t nw = (cfg & kPassN32) ? (size_t)w.hot : (size_t)(w.hot + 1) / 2;
+  return pass_table_bytes(zig) + (size_t)w.kick * sizeof(double) + nw * sizeof(uint32_t) +
+         (size_t)w.hot * 2 * sizeof(uint32_t);
 }
 
 namespace {
 bool pass_zig(int qe_mode, int cfg) { return qe_mode == QE_PHILOX && !(cfg & kPassFastNormals); }
+
+// The configuration a pass over B bins is launched with: cfg, plus
+// kPassWindowed where the hot window holds fewer than all B + 1 cells.
+int launch_cfg(int B, int use_wake, int qe_mode, int cfg) {
+  if (!use_wake) return cfg;
+  const PassWindows w = track_windows(B, cfg, pass_zig(qe_mode, cfg));
+  return w.hot < B + 1 ? (cfg | kPassWindowed) : cfg;
+}
 }  // namespace
 
 cudaError_t prepare_track_kernels(int max_smem) {
@@ -1398,13 +1518,15 @@ cudaError_t prepare_track_kernels(int max_smem) {
     for (int q = 0; q < 3; ++q)
       for (int n = 0; n < 2; ++n)
         for (int f = 0; f < 2; ++f)
-          for (int l = 0; l < kNumPassCfgs; ++l) {
-            const int c = l | (n ? kPassN32 : 0) | (f ? kPassFastNormals : 0);
-            cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
-            for (int u = 0; u < 2 && e == cudaSuccess && q != QE_DRAWS; ++u)
-              e = allow_dynamic_smem(batch_fn(w, q, c, u != 0), max_smem);
-            if (e != cudaSuccess) return e;
-          }
+          for (int h = 0; h < 2; ++h)
+            for (int l = 0; l < kNumPassCfgs; ++l) {
+              const int c = l | (n ? kPassN32 : 0) | (f ? kPassFastNormals : 0) |
+                            (h ? kPassWindowed : 0);
+              cudaError_t e = allow_dynamic_smem(pass_fn(w, q, c), max_smem);
+              for (int u = 0; u < 2 && e == cudaSuccess && q != QE_DRAWS; ++u)
+                e = allow_dynamic_smem(batch_fn(w, q, c, u != 0), max_smem);
+              if (e != cudaSuccess) return e;
+            }
   return allow_dynamic_smem((const void*)k_histogram, max_smem);
 }
 
@@ -1412,8 +1534,9 @@ cudaError_t prepare_track_kernels(int max_smem) {
 int track_blocks_per_sm(int B, int qe_mode, int use_wake, int cfg) {
   const size_t smem = track_smem_bytes(B, use_wake, cfg, pass_zig(qe_mode, cfg));
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pass_fn(use_wake, qe_mode, cfg),
-                                                    pass_cfg_threads(cfg), smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &bps, pass_fn(use_wake, qe_mode, launch_cfg(B, use_wake, qe_mode, cfg)),
+          pass_cfg_threads(cfg), smem) != cudaSuccess)
     bps = 1;
   return bps < 1 ? 1 : bps;
 }
@@ -1422,7 +1545,8 @@ cudaError_t launch_track_pass(const PassArgs& a, int grid, cudaStream_t st) {
   const size_t smem = track_smem_bytes(a.B, a.use_wake, a.cfg, a.zig != 0);
   void* args[] = {const_cast<PassArgs*>(&a)};
   PdlConfig l(dim3(grid), dim3(pass_cfg_threads(a.cfg)), smem, st);
-  return cudaLaunchKernelExC(&l.cfg, pass_fn(a.use_wake, a.qe_mode, a.cfg), args);
+  const int cfg = a.use_wake && a.hwin < a.B + 1 ? (a.cfg | kPassWindowed) : a.cfg;
+  return cudaLaunchKernelExC(&l.cfg, pass_fn(a.use_wake, a.qe_mode, cfg), args);
 }
 
 cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chunks,
@@ -1438,15 +1562,16 @@ cudaError_t launch_batch_pass(const PassArgs* d_bunches, const BatchChunk* d_chu
     if (e != cudaSuccess) return e;
     grid = std::max(1, std::min(grid, resident_blocks));
   }
-  return cudaLaunchKernel(batch_fn(wake, qe, cfg, d_queue != nullptr), dim3(grid),
-                          dim3(pass_cfg_threads(cfg)), args, smem, st);
+  return cudaLaunchKernel(batch_fn(wake, qe, launch_cfg(max_B, wake, qe, cfg), d_queue != nullptr),
+                          dim3(grid), dim3(pass_cfg_threads(cfg)), args, smem, st);
 }
 
 int batch_blocks_per_sm(int max_B, int qe_mode, int use_wake, int cfg) {
   const size_t smem = track_smem_bytes(max_B, use_wake, cfg, pass_zig(qe_mode, cfg));
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_fn(use_wake, qe_mode, cfg, true),
-                                                    pass_cfg_threads(cfg), smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &bps, batch_fn(use_wake, qe_mode, launch_cfg(max_B, use_wake, qe_mode, cfg), true),
+          pass_cfg_threads(cfg), smem) != cudaSuccess)
     bps = 1;
   return bps < 1 ? 1 : bps;
 }
@@ -1475,7 +1600,7 @@ cudaError_t launch_batch_reduce(const PassArgs* d_bunches, const BatchChunk* d_i
 
 cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long long* part_cic,
                                int nblk, int B, unsigned long long* out, bool zero_first,
-                               cudaStream_t st, unsigned long long* ovf) {
+                               cudaStream_t st, unsigned long long* spill) {
   if (zero_first) {
     cudaError_t e = cudaMemsetAsync(
         out, 0, sizeof(unsigned long long) * (part_cic ? 3 * (size_t)B + 2 : (size_t)B), st);
@@ -1484,7 +1609,8 @@ cudaError_t launch_hist_reduce(const uint32_t* part_cnt, const unsigned long lon
   const int G = nblk < 16 ? nblk : 16;
   dim3 grid((B + 1 + 255) / 256, G > 0 ? G : 1);
   PdlConfig l(grid, dim3(256), 0, st);
-  cudaError_t e = cudaLaunchKernelEx(&l.cfg, k_hist_reduce, part_cnt, part_cic, nblk, B, out, ovf);
+  cudaError_t e = cudaLaunchKernelEx(&l.cfg, k_hist_reduce, part_cnt, part_cic, nblk, B, out,
+                                     spill);
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
