@@ -38,7 +38,7 @@ FALLBACK_HBM_GBS = 6650.0
 LOG_EVERY = 100                # turns between turn-log records (one per step)
 # DRAM bytes (read + write) per particle-turn of k_track_pass from one ncu
 # capture, by bin count: (bytes, the profile summary that holds the capture).
-PASS_DRAM_BYTES = {16384: (30.53, "profiles/k_track_pass_full_2e7_b16384.md")}
+PASS_DRAM_BYTES = {16384: (31.45, "profiles/k_track_pass_full_2e7_b16384.md")}
 
 
 def parse_args():
