@@ -157,14 +157,18 @@ hj_status hj_trim(hj_ctx* ctx);
  * prefetched), 3 = 2 x 512 without prefetch, 4 = 2 x 512 with prefetch at
  * two blocks per SM, 5 = 4 x 256 with prefetch at two blocks per SM; plus 8
  * (8..13): the same layout with one 32-bit shared-memory counter per bin
- * instead of two 16-bit ones per word (more shared memory, no overflow
- * check; the default).  Plus 16 (16..29, or 23 for the library's choice):
- * the quantum-excitation normals of the fused pass are formed in single
- * precision (Philox words 0-1, 24-bit uniforms, tails cut at 6σ, about 25 %
- * faster per pass) instead of the default double-precision transform;
- * hj_gaussian and the single-step kernels stay in double precision.  Results
- * do not depend on the layout beyond floating-point summation order (and the
- * normals' precision); bin counts are the same.  No reference counterpart. */
+ * instead of two 16-bit ones per word (no overflow check; the default).  The
+ * pass keeps its per-block bin counters, cell words and kick-table entries in
+ * shared memory for the cells around the bunch's last mean position, as many
+ * as fit (all of them up to 8192 bins), and deposits the rest with global
+ * integer atomics.  Plus 16 (16..29, or 23 for the library's choice): the
+ * quantum-excitation normals of the fused pass are formed in single precision
+ * (a Box-Muller transform of Philox words 0-1, 24-bit uniforms, tails cut at
+ * 6σ, about 12 % faster per pass at 16384 bins) instead of the default
+ * Float64 ziggurat; hj_gaussian and the single-step kernels stay in double
+ * precision.  Results do not depend on the layout beyond floating-point
+ * summation order (and the normals' precision); bin counts are the same.  No
+ * reference counterpart. */
 hj_status hj_set_pass_layout(hj_ctx* ctx, int32_t layout);
 
 /* ---------------------------------------------------------------- set-up helpers */
