@@ -11,7 +11,9 @@ seed, turn by turn, for the Float64 normals; host draws otherwise).
 Cases: the default layout (32-bit counters) and layout 0 (16-bit counter
 pairs) with the Float64 normals, whose ziggurat table shrinks the window; host
 draws (no table, a wider window); a bunch off the grid's centre, whose window
-is clamped at the grid's edge; a batch member at 16384 bins."""
+is clamped at the grid's edge; layout 13 (4 x 256 threads, two blocks per SM:
+half the shared memory, a window of about 4000 cells); a batch member at
+16384 bins."""
 import numpy as np
 import pytest
 import torch
@@ -39,10 +41,13 @@ def halo_bunch(n, sigma_z, sigma_E, shift, seed):
     return z + shift, rng.normal(0.0, sigma_E, n)
 
 
+LAYOUTS = {"float64_layout0": 0, "float64_layout13": 13}
+
+
 @pytest.mark.parametrize("case", ["float64_default", "float64_layout0", "draws_default",
-                                  "float64_off_centre"])
+                                  "float64_off_centre", "float64_layout13"])
 def test_spilled_deposits_keep_exact_counts(gpu_buffers, oracle, case):
-    layout = 0 if case == "float64_layout0" else -1
+    layout = LAYOUTS.get(case, -1)
     philox = not case.startswith("draws")
     ctx = Context(0)
     ctx.set_pass_layout(layout)
